@@ -1,0 +1,43 @@
+// Launchers of the evaluator kernels (host side).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cstddef>
+#include <cstdint>
+
+namespace cdfmm_b200 {
+
+void launch_gather_moments(const void *user, int dtype, const int *perm, int ns, int K,
+                           double scale, float4 *mom, cudaStream_t s);
+size_t p2m_smem_bytes(int n, int p, int K, int chunk);
+void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
+                float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s);
+void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *coef, int n, int K,
+                int parent_level, cudaStream_t s);
+void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
+                int child_level, cudaStream_t s);
+void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
+                const float4 *near, int n, int p, int K, int nt, int depth, unsigned output,
+                int layout, float phi_scale, float *field, float *potential, cudaStream_t s);
+void configure_far_kernels(size_t max_smem);
+
+// M2L, FP32 SIMT, all levels 2..depth in one launch (overwrites L there).
+void launch_m2l_simt(const float *M, float *L, const float *T, const float *scale_m,
+                     const float *scale_l, const int4 *tiles, int n_tiles, int n, int ld, int K,
+                     cudaStream_t s);
+void configure_m2l_simt(size_t max_smem);
+int m2l_simt_beta_per_thread(int n);
+
+// list1 P2P near field.
+void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
+                const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
+                bool want_phi, float4 *near, cudaStream_t s);
+void configure_p2p(size_t max_smem);
+
+// FP64 direct sum (validation reference).
+void launch_direct_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,
+                        const int *self, double *phi, double *field, cudaStream_t s);
+
+} // namespace cdfmm_b200

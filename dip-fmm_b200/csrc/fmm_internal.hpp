@@ -1,0 +1,117 @@
+// Internal declarations of the B200 evaluator (not part of the public ABI).
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "cdfmm_b200.h"
+
+namespace cdfmm_b200 {
+
+constexpr int kMaxOrder = 10;
+constexpr int kMaxDepth = 8;
+constexpr int kMaxCoef = (kMaxOrder + 1) * (kMaxOrder + 2) * (kMaxOrder + 3) / 6; // 286
+
+inline int basis_size(int p) { return p < 0 ? 0 : (p + 1) * (p + 2) * (p + 3) / 6; }
+inline int level_offset(int level) {
+  long long p = 1;
+  for (int i = 0; i < level; ++i) p *= 8;
+  return static_cast<int>((p - 1) / 7);
+}
+inline int round_up(int v, int m) { return (v + m - 1) / m * m; }
+
+// Host tables of the expansion basis and of every geometry-dependent operator.
+// All values are computed in FP64 (long double for the derivative recurrence)
+// and rounded once to FP32, as the reference FP32 plan rounds its FP64 operator
+// entries once (src/uniform_fmm.cpp:719-824 upstream).
+struct HostOperators {
+  int p = 0;
+  int n = 0;       // coefficients per expansion
+  int depth = 0;
+  std::vector<int> ax, ay, az; // basis multi-indices in basis order
+
+  // M2M / L2L: for output coefficient a, pairs [off[a], off[a+1]) of
+  // (monomial index g, input coefficient index).  Coefficient value for
+  // (level, child class, g) is coef[(level * 8 + class) * n + g].
+  std::vector<int> m2m_off, l2l_off;
+  std::vector<int> m2m_pair_g, m2m_pair_in, l2l_pair_g, l2l_pair_in;
+  std::vector<float> m2m_coef, l2l_coef; // [(depth+1) * 8][n]
+
+  // Normalised M2L matrices T^(t)[beta][alpha] = D^{alpha+beta} G(t) for the
+  // 7x7x7 integer translation stencil (slot = (tx+3)*49 + (ty+3)*7 + (tz+3));
+  // slots inside the 3x3x3 near stencil are zero and never used.
+  // Stored FP32 as [slot][alpha][beta_pad] with beta_pad = m2l_ld.
+  int m2l_ld = 0;
+  std::vector<float> m2l_T;
+};
+
+HostOperators build_host_operators(int p, int depth, int m2l_ld_multiple);
+
+// D^gamma G(R) for G = 1/(4 pi |R|) and every gamma of total degree <= order,
+// in basis order (FP64).  Cartesian recurrence for the Taylor coefficients
+// of 1/|R|:  |g| r^2 a_g + (2|g|-1) sum_i R_i a_{g-e_i} + (|g|-1) sum_i a_{g-2e_i} = 0.
+std::vector<double> laplace_derivatives(int order, const double R[3]);
+
+struct Plan;
+
+} // namespace cdfmm_b200
+
+// The opaque ABI handle.
+struct cdfmm_b200_plan {
+  int device = 0;
+  int ns = 0, nt = 0, p = 0, n = 0, depth = 0, n_leaves = 0, n_nodes = 0;
+  int max_states = 1;
+  int m2l_mode = CDFMM_B200_M2L_FP32;
+  double root_centre[3] = {0, 0, 0};
+  double root_half_width = 1.0;
+  double scale = 2.0;         // root width: FP32 coordinates are (x - c) / scale
+  float inv_scale3 = 1.0F;    // moments are multiplied by 1 / scale^3
+  float phi_scale = 1.0F;     // potential is multiplied by scale
+  bool has_self = false;
+  bool timing = false;
+  std::string last_error;
+
+  cdfmm_b200::HostOperators ops;
+
+  cudaStream_t stream = nullptr;   // far-field / main stream
+  cudaStream_t near_stream = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  cudaEvent_t ev_t[16] = {};
+
+  // geometry (device)
+  float4 *src_rel = nullptr;   // [ns] (x - leaf centre) normalised, .w unused
+  float4 *tgt_rel = nullptr;   // [nt]
+  int *src_off = nullptr;      // [n_leaves + 1]
+  int *tgt_off = nullptr;      // [n_leaves + 1]
+  int *src_perm = nullptr;     // [ns] sorted -> user
+  int *tgt_perm = nullptr;     // [nt]
+  int *self_idx = nullptr;     // [nt] sorted target -> sorted source, -1 none
+
+  // operators (device)
+  int *m2m_off = nullptr, *m2m_pair = nullptr; // pair = g | (in << 16)
+  int *l2l_off = nullptr, *l2l_pair = nullptr;
+  float *m2m_coef = nullptr, *l2l_coef = nullptr;
+  float *m2l_T = nullptr;
+  float *scale_m = nullptr;    // [depth+1][n] 2^(level*|alpha|)   (exact)
+  float *scale_l = nullptr;    // [depth+1][n] 2^(level*(|beta|+1)) (exact)
+  int4 *m2l_tiles = nullptr;   // SIMT M2L work tiles (level, class, packed parent origin)
+  int n_tiles = 0;
+  int8_t *basis = nullptr;     // [n][4] ax, ay, az, degree
+  int p2m_chunk = 64;
+  int last_K = 0;
+
+  // state (device), sized for max_states
+  float4 *mom = nullptr;       // [ns][K] sorted scaled moments
+  float *M = nullptr;          // [n_nodes][n][K]
+  float *L = nullptr;          // [n_nodes][n][K]
+  float4 *near = nullptr;      // [nt][K] (phi, Hx, Hy, Hz) near field
+  void *stage_in = nullptr;    // device copy of host moments
+  size_t stage_in_bytes = 0;
+  void *stage_out = nullptr;   // device results before D2H
+  size_t stage_out_bytes = 0;
+
+  cdfmm_b200_stats stats{};
+};

@@ -1,0 +1,41 @@
+// Device helpers shared by the evaluator kernels.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <cstdint>
+
+namespace cdfmm_b200 {
+
+// 1 / (4 pi) in FP32 (the kernel constant of G(r) = 1 / (4 pi |r|)).
+constexpr float kInvFourPiF = 0.0795774715459476678844418816862571810F;
+
+__host__ __device__ inline int basis_size_d(int p) { return p < 0 ? 0 : (p + 1) * (p + 2) * (p + 3) / 6; }
+
+// Position of multi-index (a, b, c) in the total-degree basis.
+__host__ __device__ inline int rank3(int a, int b, int c) {
+  const int d = a + b + c;
+  return d * (d + 1) * (d + 2) / 6 + a * (d + 1) - a * (a - 1) / 2 + b;
+}
+
+__host__ __device__ inline int level_offset_d(int level) { return ((1 << (3 * level)) - 1) / 7; }
+
+__host__ __device__ inline uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
+  uint32_t m = 0;
+  for (int b = 0; b < 10; ++b) {
+    m |= ((x >> b) & 1u) << (3 * b);
+    m |= ((y >> b) & 1u) << (3 * b + 1);
+    m |= ((z >> b) & 1u) << (3 * b + 2);
+  }
+  return m;
+}
+
+__host__ __device__ inline void demorton3(uint32_t m, int &x, int &y, int &z) {
+  x = y = z = 0;
+  for (int b = 0; b < 10; ++b) {
+    x |= static_cast<int>((m >> (3 * b)) & 1u) << b;
+    y |= static_cast<int>((m >> (3 * b + 1)) & 1u) << b;
+    z |= static_cast<int>((m >> (3 * b + 2)) & 1u) << b;
+  }
+}
+
+} // namespace cdfmm_b200

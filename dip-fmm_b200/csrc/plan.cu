@@ -1,0 +1,675 @@
+// C ABI of the B200 evaluator: plan construction and the evaluate pipeline.
+//
+// Pipeline of one evaluate call (K states), stream-ordered:
+//   [H2D moments] -> gather (user -> Morton order, / scale^3)
+//   far stream : P2M -> M2M (levels d-1..0) -> M2L (levels 2..d) -> L2L (3..d)
+//   near stream: list1 P2P                       (runs concurrently with far)
+//   join -> L2P + near/far combine + unsort to user order -> [D2H results]
+// (upstream src/cuda_fmm.cu:3457-3655 orders the same stages with a far and a
+// near stream and an event join before the combine).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+#include "cdfmm_b200.h"
+#include "far_kernels.hpp"
+#include "fmm_internal.hpp"
+#include "kernels.cuh"
+
+namespace {
+
+using namespace cdfmm_b200;
+
+thread_local std::string g_last_error;
+
+struct AbiError : std::runtime_error {
+  int code;
+  AbiError(int c, const std::string &m) : std::runtime_error(m), code(c) {}
+};
+
+void check(cudaError_t e, const char *what) {
+  if (e != cudaSuccess) {
+    const int code = e == cudaErrorMemoryAllocation ? CDFMM_B200_ERR_OUT_OF_MEMORY : CDFMM_B200_ERR_RUNTIME;
+    throw AbiError(code, std::string(what) + ": " + cudaGetErrorString(e));
+  }
+}
+
+void require(bool ok, const std::string &what) {
+  if (!ok) throw AbiError(CDFMM_B200_ERR_INVALID_ARGUMENT, what);
+}
+
+template <typename T> T *dalloc(size_t count, uint64_t &bytes) {
+  void *p = nullptr;
+  if (count == 0) count = 1;
+  check(cudaMalloc(&p, count * sizeof(T)), "cudaMalloc");
+  bytes += count * sizeof(T);
+  return static_cast<T *>(p);
+}
+
+template <typename T> void upload(T *dst, const T *src, size_t count, uint64_t &bytes) {
+  if (count == 0) return;
+  check(cudaMemcpy(dst, src, count * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  bytes += count * sizeof(T);
+}
+
+void free_plan(cdfmm_b200_plan *p) {
+  if (p == nullptr) return;
+  void *ptrs[] = {p->src_rel, p->tgt_rel, p->src_off, p->tgt_off, p->src_perm, p->tgt_perm,
+                  p->self_idx, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
+                  p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
+                  p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles};
+  for (void *q : ptrs)
+    if (q != nullptr) cudaFree(q);
+  if (p->ev_fork) cudaEventDestroy(p->ev_fork);
+  if (p->ev_join) cudaEventDestroy(p->ev_join);
+  for (cudaEvent_t &e : p->ev_t)
+    if (e) cudaEventDestroy(e);
+  if (p->near_stream) cudaStreamDestroy(p->near_stream);
+  if (p->stream) cudaStreamDestroy(p->stream);
+  delete p;
+}
+
+// Normalised (root width = 1) coordinates relative to the centre of the leaf
+// that holds each point; the FP64 subtraction order follows the reference's
+// FP32 normalisation (src/uniform_fmm.cpp:379-417 upstream).
+std::vector<float4> relative_positions(const double *pos, const int32_t *leaf_off, int n_leaves,
+                                       int depth, const double centre[3], double hw, double scale) {
+  const int side = 1 << depth;
+  std::vector<float4> out(static_cast<size_t>(leaf_off[n_leaves]));
+  const double inv = 1.0 / scale;
+  for (int m = 0; m < n_leaves; ++m) {
+    if (leaf_off[m + 1] == leaf_off[m]) continue;
+    int ix, iy, iz;
+    demorton3(static_cast<uint32_t>(m), ix, iy, iz);
+    const int c3[3] = {ix, iy, iz};
+    double nc[3];
+    for (int a = 0; a < 3; ++a) {
+      const double offset = ((static_cast<double>(c3[a]) + 0.5) / static_cast<double>(side) - 0.5) * 2.0 * hw;
+      const double leaf_centre = centre[a] + offset;
+      nc[a] = (leaf_centre - centre[a]) * inv;
+    }
+    for (int j = leaf_off[m]; j < leaf_off[m + 1]; ++j) {
+      double np[3];
+      for (int a = 0; a < 3; ++a) np[a] = (pos[3 * static_cast<size_t>(j) + a] - centre[a]) * inv;
+      out[static_cast<size_t>(j)] = make_float4(static_cast<float>(np[0] - nc[0]), static_cast<float>(np[1] - nc[1]),
+                                                static_cast<float>(np[2] - nc[2]), 0.0F);
+    }
+  }
+  return out;
+}
+
+int fail(cdfmm_b200_plan *plan, int code, const std::string &msg) {
+  if (plan != nullptr) plan->last_error = msg;
+  g_last_error = msg;
+  return code;
+}
+
+size_t device_smem_optin(int device) {
+  int v = 0;
+  cudaDeviceGetAttribute(&v, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+  return static_cast<size_t>(v);
+}
+
+} // namespace
+
+extern "C" {
+
+int cdfmm_b200_device_count(int32_t *count) {
+  if (count == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "count is NULL");
+  int c = 0;
+  const cudaError_t e = cudaGetDeviceCount(&c);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    c = 0;
+  }
+  *count = c;
+  return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_device_info(int32_t device, char *name, size_t name_len, int32_t *cc_major,
+                           int32_t *cc_minor) {
+  cudaDeviceProp prop{};
+  const cudaError_t e = cudaGetDeviceProperties(&prop, device);
+  if (e != cudaSuccess) {
+    cudaGetLastError();
+    return fail(nullptr, CDFMM_B200_ERR_NO_DEVICE, std::string("cudaGetDeviceProperties: ") + cudaGetErrorString(e));
+  }
+  if (name != nullptr && name_len > 0) {
+    std::strncpy(name, prop.name, name_len - 1);
+    name[name_len - 1] = '\0';
+  }
+  if (cc_major) *cc_major = prop.major;
+  if (cc_minor) *cc_minor = prop.minor;
+  return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **out_plan) {
+  cdfmm_b200_plan *plan = nullptr;
+  try {
+    require(desc != nullptr && out_plan != nullptr, "desc and out_plan must not be NULL");
+    *out_plan = nullptr;
+    require(desc->struct_size == static_cast<int32_t>(sizeof(cdfmm_b200_plan_desc)), "desc.struct_size mismatch");
+    require(desc->n_sources >= 0 && desc->n_targets >= 0, "negative population size");
+    require(desc->order >= 0 && desc->order <= kMaxOrder, "order must be in [0, 10]");
+    require(desc->depth >= 0 && desc->depth <= kMaxDepth, "depth must be in [0, 8]");
+    require(desc->max_states >= 1 && desc->max_states <= 1024, "max_states must be in [1, 1024]");
+    require(desc->root_half_width > 0.0 && std::isfinite(desc->root_half_width), "root_half_width must be positive");
+    require(desc->m2l_mode >= CDFMM_B200_M2L_AUTO && desc->m2l_mode <= CDFMM_B200_M2L_BF16X3, "unknown m2l_mode");
+    const int n_leaves = 1 << (3 * desc->depth);
+    require(desc->leaf_source_offsets != nullptr && desc->leaf_target_offsets != nullptr, "leaf offsets are required");
+    require(desc->leaf_source_offsets[0] == 0 && desc->leaf_source_offsets[n_leaves] == desc->n_sources,
+            "leaf_source_offsets must span [0, n_sources]");
+    require(desc->leaf_target_offsets[0] == 0 && desc->leaf_target_offsets[n_leaves] == desc->n_targets,
+            "leaf_target_offsets must span [0, n_targets]");
+    for (int m = 0; m < n_leaves; ++m) {
+      require(desc->leaf_source_offsets[m + 1] >= desc->leaf_source_offsets[m], "leaf_source_offsets must be non-decreasing");
+      require(desc->leaf_target_offsets[m + 1] >= desc->leaf_target_offsets[m], "leaf_target_offsets must be non-decreasing");
+    }
+    require(desc->n_sources == 0 || (desc->sorted_source_positions && desc->source_permutation), "source arrays are required");
+    require(desc->n_targets == 0 || (desc->sorted_target_positions && desc->target_permutation), "target arrays are required");
+
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+      cudaGetLastError();
+      throw AbiError(CDFMM_B200_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    require(desc->device >= 0 && desc->device < devices, "device ordinal out of range");
+    check(cudaSetDevice(desc->device), "cudaSetDevice");
+
+    plan = new cdfmm_b200_plan();
+    plan->device = desc->device;
+    plan->ns = desc->n_sources;
+    plan->nt = desc->n_targets;
+    plan->p = desc->order;
+    plan->depth = desc->depth;
+    plan->n_leaves = n_leaves;
+    plan->n_nodes = level_offset(desc->depth + 1);
+    plan->max_states = desc->max_states;
+    plan->m2l_mode = CDFMM_B200_M2L_FP32; // tensor-core M2L is selected below when available
+    for (int a = 0; a < 3; ++a) plan->root_centre[a] = desc->root_centre[a];
+    plan->root_half_width = desc->root_half_width;
+    plan->scale = 2.0 * desc->root_half_width;
+    plan->inv_scale3 = static_cast<float>(1.0 / (plan->scale * plan->scale * plan->scale));
+    plan->phi_scale = static_cast<float>(plan->scale);
+
+    HostOperators &ops = plan->ops;
+    ops = build_host_operators(plan->p, plan->depth, 16);
+    plan->n = ops.n;
+    const int n = ops.n;
+    const int J = m2l_simt_beta_per_thread(n);
+    if (ops.m2l_ld < 16 * J) {
+      ops = build_host_operators(plan->p, plan->depth, 16 * J);
+    }
+    uint64_t &bytes = plan->stats.persistent_device_bytes;
+    uint64_t &h2d = plan->stats.setup_h2d_bytes;
+
+    check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&plan->near_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaEventCreateWithFlags(&plan->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&plan->ev_join, cudaEventDisableTiming), "cudaEventCreate");
+    for (cudaEvent_t &e : plan->ev_t) check(cudaEventCreate(&e), "cudaEventCreate");
+
+    // geometry
+    const std::vector<float4> srel = relative_positions(desc->sorted_source_positions, desc->leaf_source_offsets,
+                                                        n_leaves, plan->depth, plan->root_centre,
+                                                        plan->root_half_width, plan->scale);
+    const std::vector<float4> trel = relative_positions(desc->sorted_target_positions, desc->leaf_target_offsets,
+                                                        n_leaves, plan->depth, plan->root_centre,
+                                                        plan->root_half_width, plan->scale);
+    for (int j = 0; j < plan->ns; ++j)
+      require(desc->source_permutation[j] >= 0 && desc->source_permutation[j] < plan->ns, "source_permutation out of range");
+    for (int j = 0; j < plan->nt; ++j)
+      require(desc->target_permutation[j] >= 0 && desc->target_permutation[j] < plan->nt, "target_permutation out of range");
+    plan->src_rel = dalloc<float4>(plan->ns, bytes);
+    plan->tgt_rel = dalloc<float4>(plan->nt, bytes);
+    plan->src_off = dalloc<int>(n_leaves + 1, bytes);
+    plan->tgt_off = dalloc<int>(n_leaves + 1, bytes);
+    plan->src_perm = dalloc<int>(plan->ns, bytes);
+    plan->tgt_perm = dalloc<int>(plan->nt, bytes);
+    plan->self_idx = dalloc<int>(plan->nt, bytes);
+    upload(plan->src_rel, srel.data(), srel.size(), h2d);
+    upload(plan->tgt_rel, trel.data(), trel.size(), h2d);
+    upload(plan->src_off, desc->leaf_source_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
+    upload(plan->tgt_off, desc->leaf_target_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
+    upload(plan->src_perm, desc->source_permutation, static_cast<size_t>(plan->ns), h2d);
+    upload(plan->tgt_perm, desc->target_permutation, static_cast<size_t>(plan->nt), h2d);
+
+    // operators
+    std::vector<int8_t> basis(static_cast<size_t>(n) * 4);
+    for (int a = 0; a < n; ++a) {
+      basis[4 * a] = static_cast<int8_t>(ops.ax[a]);
+      basis[4 * a + 1] = static_cast<int8_t>(ops.ay[a]);
+      basis[4 * a + 2] = static_cast<int8_t>(ops.az[a]);
+      basis[4 * a + 3] = static_cast<int8_t>(ops.ax[a] + ops.ay[a] + ops.az[a]);
+    }
+    std::vector<int> m2m_pair(ops.m2m_pair_g.size()), l2l_pair(ops.l2l_pair_g.size());
+    for (size_t e = 0; e < m2m_pair.size(); ++e) m2m_pair[e] = ops.m2m_pair_g[e] | (ops.m2m_pair_in[e] << 16);
+    for (size_t e = 0; e < l2l_pair.size(); ++e) l2l_pair[e] = ops.l2l_pair_g[e] | (ops.l2l_pair_in[e] << 16);
+    plan->basis = dalloc<int8_t>(basis.size(), bytes);
+    plan->m2m_off = dalloc<int>(ops.m2m_off.size(), bytes);
+    plan->l2l_off = dalloc<int>(ops.l2l_off.size(), bytes);
+    plan->m2m_pair = dalloc<int>(m2m_pair.size(), bytes);
+    plan->l2l_pair = dalloc<int>(l2l_pair.size(), bytes);
+    plan->m2m_coef = dalloc<float>(ops.m2m_coef.size(), bytes);
+    plan->l2l_coef = dalloc<float>(ops.l2l_coef.size(), bytes);
+    upload(plan->basis, basis.data(), basis.size(), h2d);
+    upload(plan->m2m_off, ops.m2m_off.data(), ops.m2m_off.size(), h2d);
+    upload(plan->l2l_off, ops.l2l_off.data(), ops.l2l_off.size(), h2d);
+    upload(plan->m2m_pair, m2m_pair.data(), m2m_pair.size(), h2d);
+    upload(plan->l2l_pair, l2l_pair.data(), l2l_pair.size(), h2d);
+    upload(plan->m2m_coef, ops.m2m_coef.data(), ops.m2m_coef.size(), h2d);
+    upload(plan->l2l_coef, ops.l2l_coef.data(), ops.l2l_coef.size(), h2d);
+
+    // M2L: matrices, exact power-of-two level scalings, and the work tiles.
+    std::vector<float> sm(static_cast<size_t>(plan->depth + 1) * n), sl(sm.size());
+    for (int level = 0; level <= plan->depth; ++level)
+      for (int a = 0; a < n; ++a) {
+        const int deg = ops.ax[a] + ops.ay[a] + ops.az[a];
+        sm[static_cast<size_t>(level) * n + a] = std::ldexp(1.0F, level * deg);
+        sl[static_cast<size_t>(level) * n + a] = std::ldexp(1.0F, level * (deg + 1));
+      }
+    std::vector<int4> tiles;
+    for (int level = plan->depth; level >= 2; --level) {
+      const int pside = 1 << (level - 1);
+      for (int cls = 0; cls < 8; ++cls)
+        for (int pz = 0; pz < pside; pz += 4)
+          for (int py = 0; py < pside; py += 4)
+            for (int px = 0; px < pside; px += 4) tiles.push_back(make_int4(level, cls, px | (py << 10) | (pz << 20), 0));
+    }
+    plan->n_tiles = static_cast<int>(tiles.size());
+    plan->scale_m = dalloc<float>(sm.size(), bytes);
+    plan->scale_l = dalloc<float>(sl.size(), bytes);
+    plan->m2l_tiles = dalloc<int4>(tiles.size(), bytes);
+    upload(plan->scale_m, sm.data(), sm.size(), h2d);
+    upload(plan->scale_l, sl.data(), sl.size(), h2d);
+    upload(plan->m2l_tiles, tiles.data(), tiles.size(), h2d);
+    if (plan->depth >= 2) {
+      plan->m2l_T = dalloc<float>(ops.m2l_T.size(), bytes);
+      upload(plan->m2l_T, ops.m2l_T.data(), ops.m2l_T.size(), h2d);
+      plan->stats.m2l_matrix_bytes = ops.m2l_T.size() * sizeof(float);
+    }
+
+    // statistics of the implicit interaction lists (counted on the host)
+    {
+      uint64_t classes = 0, inter = 0, pairs = 0;
+      bool used[343] = {};
+      const int32_t *so = desc->leaf_source_offsets;
+      const int32_t *to = desc->leaf_target_offsets;
+      // occupancy of every level for sources and targets
+      std::vector<std::vector<int>> socc(plan->depth + 1), tocc(plan->depth + 1);
+      for (int level = 0; level <= plan->depth; ++level) {
+        socc[level].assign(static_cast<size_t>(1) << (3 * level), 0);
+        tocc[level].assign(static_cast<size_t>(1) << (3 * level), 0);
+      }
+      for (int m = 0; m < n_leaves; ++m) {
+        for (int level = 0; level <= plan->depth; ++level) {
+          const int shift = 3 * (plan->depth - level);
+          socc[level][m >> shift] += so[m + 1] - so[m];
+          tocc[level][m >> shift] += to[m + 1] - to[m];
+        }
+      }
+      for (int level = 2; level <= plan->depth; ++level) {
+        const int side = 1 << level;
+        for (int t = 0; t < side * side * side; ++t) {
+          if (tocc[level][t] == 0) continue;
+          int tx, ty, tz;
+          demorton3(static_cast<uint32_t>(t), tx, ty, tz);
+          for (int sz = 2 * (tz >> 1) - 2; sz <= 2 * (tz >> 1) + 3; ++sz)
+            for (int sy = 2 * (ty >> 1) - 2; sy <= 2 * (ty >> 1) + 3; ++sy)
+              for (int sx = 2 * (tx >> 1) - 2; sx <= 2 * (tx >> 1) + 3; ++sx) {
+                if (sx < 0 || sy < 0 || sz < 0 || sx >= side || sy >= side || sz >= side) continue;
+                if (std::abs(sx - tx) <= 1 && std::abs(sy - ty) <= 1 && std::abs(sz - tz) <= 1) continue;
+                if (socc[level][morton3(sx, sy, sz)] == 0) continue;
+                ++inter;
+                const int slot = (tx - sx + 3) * 49 + (ty - sy + 3) * 7 + (tz - sz + 3);
+                if (!used[slot]) {
+                  used[slot] = true;
+                  ++classes;
+                }
+              }
+        }
+      }
+      const int side = 1 << plan->depth;
+      for (int m = 0; m < n_leaves; ++m) {
+        const int nt_leaf = to[m + 1] - to[m];
+        if (nt_leaf == 0) continue;
+        int x, y, z;
+        demorton3(static_cast<uint32_t>(m), x, y, z);
+        for (int dz = -1; dz <= 1; ++dz)
+          for (int dy = -1; dy <= 1; ++dy)
+            for (int dx = -1; dx <= 1; ++dx) {
+              const int a = x + dx, b = y + dy, c = z + dz;
+              if (a < 0 || b < 0 || c < 0 || a >= side || b >= side || c >= side) continue;
+              const uint32_t q = morton3(a, b, c);
+              pairs += static_cast<uint64_t>(nt_leaf) * static_cast<uint64_t>(so[q + 1] - so[q]);
+            }
+      }
+      plan->stats.m2l_classes = classes;
+      plan->stats.m2l_interactions = inter;
+      plan->stats.p2p_pairs = pairs;
+    }
+
+    // state buffers sized for max_states
+    const size_t K = static_cast<size_t>(plan->max_states);
+    plan->mom = dalloc<float4>(static_cast<size_t>(plan->ns) * K, bytes);
+    plan->M = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
+    plan->L = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
+    plan->near = dalloc<float4>(static_cast<size_t>(plan->nt) * K, bytes);
+    check(cudaMemset(plan->M, 0, static_cast<size_t>(plan->n_nodes) * n * K * sizeof(float)), "cudaMemset");
+    check(cudaMemset(plan->L, 0, static_cast<size_t>(plan->n_nodes) * n * K * sizeof(float)), "cudaMemset");
+    check(cudaMemset(plan->near, 0, static_cast<size_t>(std::max(plan->nt, 1)) * K * sizeof(float4)), "cudaMemset");
+
+    const size_t smem = device_smem_optin(plan->device);
+    configure_far_kernels(smem);
+    configure_m2l_simt(smem);
+    configure_p2p(smem);
+    plan->p2m_chunk = 64;
+    while (plan->p2m_chunk > 8 && p2m_smem_bytes(n, plan->p, static_cast<int>(K), plan->p2m_chunk) > smem) plan->p2m_chunk /= 2;
+    require(p2m_smem_bytes(n, plan->p, static_cast<int>(K), plan->p2m_chunk) <= smem &&
+                sizeof(float) * static_cast<size_t>(n) * K <= smem,
+            "order and max_states exceed the shared-memory budget of one CTA");
+    check(cudaDeviceSynchronize(), "plan upload");
+    plan->stats.m2l_mode_resolved = plan->m2l_mode;
+    *out_plan = plan;
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    free_plan(plan);
+    return fail(nullptr, e.code, e.what());
+  } catch (const std::bad_alloc &) {
+    free_plan(plan);
+    return fail(nullptr, CDFMM_B200_ERR_OUT_OF_MEMORY, "host allocation failed");
+  } catch (const std::exception &e) {
+    free_plan(plan);
+    return fail(nullptr, CDFMM_B200_ERR_RUNTIME, e.what());
+  }
+}
+
+void cdfmm_b200_plan_destroy(cdfmm_b200_plan *plan) {
+  if (plan == nullptr) return;
+  cudaSetDevice(plan->device);
+  if (plan->stream) cudaStreamSynchronize(plan->stream);
+  if (plan->near_stream) cudaStreamSynchronize(plan->near_stream);
+  free_plan(plan);
+}
+
+int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_self) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  try {
+    check(cudaSetDevice(plan->device), "cudaSetDevice");
+    if (sorted_self == nullptr) {
+      plan->has_self = false;
+      return CDFMM_B200_OK;
+    }
+    for (int i = 0; i < plan->nt; ++i)
+      require(sorted_self[i] >= -1 && sorted_self[i] < plan->ns, "self index out of range");
+    check(cudaStreamSynchronize(plan->near_stream), "sync");
+    check(cudaStreamSynchronize(plan->stream), "sync");
+    if (plan->nt > 0)
+      check(cudaMemcpy(plan->self_idx, sorted_self, sizeof(int) * plan->nt, cudaMemcpyHostToDevice), "cudaMemcpy");
+    plan->has_self = true;
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(plan, e.code, e.what());
+  }
+}
+
+int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  try {
+    require(a != nullptr, "args is NULL");
+    require(a->n_states >= 1 && a->n_states <= plan->max_states, "n_states must be in [1, max_states]");
+    require(a->moments_dtype == 0 || a->moments_dtype == 1, "moments_dtype must be 0 (float32) or 1 (float64)");
+    require((a->output & 3u) != 0u && (a->output & ~3u) == 0u, "output must request potential and/or field");
+    require(a->layout == CDFMM_B200_LAYOUT_SEPARATE || a->layout == CDFMM_B200_LAYOUT_INTERLEAVED, "unknown layout");
+    require(plan->ns == 0 || a->moments != nullptr, "moments is NULL");
+    const bool want_phi = (a->output & CDFMM_B200_OUTPUT_POTENTIAL) != 0u;
+    const bool want_h = (a->output & CDFMM_B200_OUTPUT_FIELD) != 0u;
+    if (a->layout == CDFMM_B200_LAYOUT_INTERLEAVED || want_h) require(plan->nt == 0 || a->field != nullptr, "field is NULL");
+    if (a->layout == CDFMM_B200_LAYOUT_SEPARATE && want_phi) require(plan->nt == 0 || a->potential != nullptr, "potential is NULL");
+    if (a->layout == CDFMM_B200_LAYOUT_INTERLEAVED && (a->memory & CDFMM_B200_RESULTS_ON_HOST) == 0u)
+      require(reinterpret_cast<uintptr_t>(a->field) % 16 == 0, "interleaved device results need a 16-byte aligned field pointer");
+    if ((a->memory & CDFMM_B200_MOMENTS_ON_HOST) == 0u)
+      require(reinterpret_cast<uintptr_t>(a->moments) % (a->moments_dtype == 1 ? 8 : 4) == 0, "misaligned moments pointer");
+    check(cudaSetDevice(plan->device), "cudaSetDevice");
+
+    const int K = a->n_states;
+    const int n = plan->n;
+    cudaStream_t s = a->stream != nullptr ? static_cast<cudaStream_t>(a->stream) : plan->stream;
+    const bool host_in = (a->memory & CDFMM_B200_MOMENTS_ON_HOST) != 0u;
+    const bool host_out = (a->memory & CDFMM_B200_RESULTS_ON_HOST) != 0u;
+    const size_t in_bytes = static_cast<size_t>(K) * plan->ns * 3 * (a->moments_dtype == 1 ? 8 : 4);
+    const size_t out_field_bytes = static_cast<size_t>(K) * plan->nt * sizeof(float) *
+                                   (a->layout == CDFMM_B200_LAYOUT_INTERLEAVED ? 4 : 3);
+    const size_t out_phi_bytes = (a->layout == CDFMM_B200_LAYOUT_SEPARATE && want_phi)
+                                     ? static_cast<size_t>(K) * plan->nt * sizeof(float) : 0;
+    const bool timing = plan->timing;
+    int launches = 0;
+    if (timing) check(cudaEventRecord(plan->ev_t[0], s), "event");
+
+    const void *moments = a->moments;
+    if (host_in && in_bytes > 0) {
+      if (plan->stage_in_bytes < in_bytes) {
+        if (plan->stage_in) cudaFree(plan->stage_in);
+        plan->stage_in = nullptr;
+        plan->stage_in_bytes = 0;
+        check(cudaMalloc(&plan->stage_in, in_bytes), "cudaMalloc staging");
+        plan->stage_in_bytes = in_bytes;
+      }
+      check(cudaMemcpyAsync(plan->stage_in, a->moments, in_bytes, cudaMemcpyHostToDevice, s), "H2D moments");
+      plan->stats.evaluation_h2d_bytes += in_bytes;
+      plan->stats.evaluation_h2d_calls += 1;
+      moments = plan->stage_in;
+    }
+    float *field = a->field;
+    float *potential = a->potential;
+    if (host_out) {
+      const size_t need = out_field_bytes + out_phi_bytes;
+      if (plan->stage_out_bytes < need) {
+        if (plan->stage_out) cudaFree(plan->stage_out);
+        plan->stage_out = nullptr;
+        plan->stage_out_bytes = 0;
+        check(cudaMalloc(&plan->stage_out, need), "cudaMalloc staging");
+        plan->stage_out_bytes = need;
+      }
+      field = static_cast<float *>(plan->stage_out);
+      potential = out_phi_bytes > 0 ? reinterpret_cast<float *>(static_cast<char *>(plan->stage_out) + out_field_bytes) : nullptr;
+    }
+
+    launch_gather_moments(moments, a->moments_dtype, plan->src_perm, plan->ns, K, plan->scale, plan->mom, s);
+    launches += plan->ns > 0 ? 1 : 0;
+    if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
+
+    // near field on its own stream
+    check(cudaEventRecord(plan->ev_fork, s), "event");
+    check(cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0), "wait");
+    if (timing) check(cudaEventRecord(plan->ev_t[8], plan->near_stream), "event");
+    launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
+               plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi, plan->near, plan->near_stream);
+    ++launches;
+    if (timing) check(cudaEventRecord(plan->ev_t[9], plan->near_stream), "event");
+    check(cudaEventRecord(plan->ev_join, plan->near_stream), "event");
+
+    // far field
+    launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
+               plan->p2m_chunk, s);
+    ++launches;
+    if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
+    for (int level = plan->depth - 1; level >= 0; --level) {
+      launch_m2m(plan->M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level, s);
+      ++launches;
+    }
+    if (timing) check(cudaEventRecord(plan->ev_t[3], s), "event");
+    if (plan->depth >= 2) {
+      launch_m2l_simt(plan->M, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles,
+                      plan->n_tiles, n, plan->ops.m2l_ld, K, s);
+      ++launches;
+    }
+    if (timing) check(cudaEventRecord(plan->ev_t[4], s), "event");
+    for (int level = 3; level <= plan->depth; ++level) {
+      launch_l2l(plan->L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level, s);
+      ++launches;
+    }
+    if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
+    check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
+    if (timing) check(cudaEventRecord(plan->ev_t[6], s), "event");
+    launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->near, n, plan->p, K, plan->nt,
+               plan->depth, a->output, a->layout, plan->phi_scale, field, potential, s);
+    ++launches;
+    check(cudaGetLastError(), "kernel launch");
+    if (timing) check(cudaEventRecord(plan->ev_t[7], s), "event");
+
+    if (host_out) {
+      if (out_field_bytes > 0 && plan->nt > 0 && (want_h || a->layout == CDFMM_B200_LAYOUT_INTERLEAVED)) {
+        check(cudaMemcpyAsync(a->field, field, out_field_bytes, cudaMemcpyDeviceToHost, s), "D2H field");
+        plan->stats.evaluation_d2h_bytes += out_field_bytes;
+        plan->stats.evaluation_d2h_calls += 1;
+      }
+      if (out_phi_bytes > 0 && plan->nt > 0) {
+        check(cudaMemcpyAsync(a->potential, potential, out_phi_bytes, cudaMemcpyDeviceToHost, s), "D2H potential");
+        plan->stats.evaluation_d2h_bytes += out_phi_bytes;
+        plan->stats.evaluation_d2h_calls += 1;
+      }
+    }
+    if (a->synchronize || host_out || timing) check(cudaStreamSynchronize(s), "evaluate");
+    if (timing) {
+      auto ms = [&](int i, int j) {
+        float v = 0.0F;
+        cudaEventElapsedTime(&v, plan->ev_t[i], plan->ev_t[j]);
+        return static_cast<double>(v);
+      };
+      plan->stats.ms_gather = ms(0, 1);
+      plan->stats.ms_p2m = ms(1, 2);
+      plan->stats.ms_m2m = ms(2, 3);
+      plan->stats.ms_m2l = ms(3, 4);
+      plan->stats.ms_l2l = ms(4, 5);
+      plan->stats.ms_p2p = ms(8, 9);
+      plan->stats.ms_l2p = ms(6, 7);
+      plan->stats.ms_total = ms(0, 7);
+    }
+    plan->last_K = K;
+    plan->stats.evaluations += 1;
+    plan->stats.kernel_launches_last = static_cast<uint64_t>(launches);
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(plan, e.code, e.what());
+  } catch (const std::exception &e) {
+    return fail(plan, CDFMM_B200_ERR_RUNTIME, e.what());
+  }
+}
+
+int cdfmm_b200_read_expansions(const cdfmm_b200_plan *plan, int32_t which, int32_t state, float *out,
+                               size_t out_count) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  auto *mp = const_cast<cdfmm_b200_plan *>(plan);
+  try {
+    require(which == 0 || which == 1, "which must be 0 (multipoles) or 1 (locals)");
+    require(state >= 0 && state < std::max(plan->last_K, 1), "state out of range");
+    const size_t need = static_cast<size_t>(plan->n_nodes) * plan->n;
+    require(out != nullptr && out_count >= need, "output buffer too small");
+    check(cudaSetDevice(plan->device), "cudaSetDevice");
+    check(cudaStreamSynchronize(plan->stream), "sync");
+    const int K = std::max(plan->last_K, 1);
+    std::vector<float> all(need * K);
+    check(cudaMemcpy(all.data(), which == 0 ? plan->M : plan->L, all.size() * sizeof(float), cudaMemcpyDeviceToHost),
+          "D2H expansions");
+    for (size_t q = 0; q < need; ++q) out[q] = all[q * K + state];
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(mp, e.code, e.what());
+  }
+}
+
+int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  plan->timing = enabled != 0;
+  plan->stats.timing_enabled = plan->timing ? 1 : 0;
+  return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out) {
+  if (plan == nullptr || out == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan and out must not be NULL");
+  *out = plan->stats;
+  return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_direct_fp64(int32_t device, int32_t ns, const double *src, const double *mom, int32_t nt,
+                           const double *tgt, const int32_t *self, double *phi, double *field) {
+  void *buf[6] = {};
+  try {
+    require(ns >= 0 && nt >= 0, "negative population size");
+    require(ns == 0 || (src && mom), "source arrays are required");
+    require(nt == 0 || tgt, "target positions are required");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+      cudaGetLastError();
+      throw AbiError(CDFMM_B200_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    check(cudaSetDevice(device), "cudaSetDevice");
+    if (nt == 0) return CDFMM_B200_OK;
+    uint64_t bytes = 0, h2d = 0;
+    double *dsrc = dalloc<double>(3 * static_cast<size_t>(ns), bytes);
+    buf[0] = dsrc;
+    double *dmom = dalloc<double>(3 * static_cast<size_t>(ns), bytes);
+    buf[1] = dmom;
+    double *dtgt = dalloc<double>(3 * static_cast<size_t>(nt), bytes);
+    buf[2] = dtgt;
+    int *dself = nullptr;
+    if (self) {
+      dself = dalloc<int>(nt, bytes);
+      buf[3] = dself;
+      upload(dself, self, nt, h2d);
+    }
+    double *dphi = phi ? dalloc<double>(nt, bytes) : nullptr;
+    buf[4] = dphi;
+    double *dfield = field ? dalloc<double>(3 * static_cast<size_t>(nt), bytes) : nullptr;
+    buf[5] = dfield;
+    upload(dsrc, src, 3 * static_cast<size_t>(ns), h2d);
+    upload(dmom, mom, 3 * static_cast<size_t>(ns), h2d);
+    upload(dtgt, tgt, 3 * static_cast<size_t>(nt), h2d);
+    launch_direct_fp64(dsrc, dmom, ns, dtgt, nt, dself, dphi, dfield, nullptr);
+    check(cudaGetLastError(), "direct kernel");
+    check(cudaDeviceSynchronize(), "direct kernel");
+    if (phi) check(cudaMemcpy(phi, dphi, sizeof(double) * nt, cudaMemcpyDeviceToHost), "D2H");
+    if (field) check(cudaMemcpy(field, dfield, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost), "D2H");
+    for (void *b : buf)
+      if (b) cudaFree(b);
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    for (void *b : buf)
+      if (b) cudaFree(b);
+    return fail(nullptr, e.code, e.what());
+  }
+}
+
+int cdfmm_b200_m2l_matrix(int32_t order, const double *R, double *out, size_t out_count) {
+  try {
+    require(order >= 0 && order <= kMaxOrder, "order must be in [0, 10]");
+    require(R != nullptr && out != nullptr, "R and out must not be NULL");
+    require(R[0] != 0.0 || R[1] != 0.0 || R[2] != 0.0, "R must be nonzero");
+    const int n = basis_size(order);
+    require(out_count >= static_cast<size_t>(n) * n, "output buffer too small");
+    const HostOperators ops = build_host_operators(order, 0, 1);
+    const std::vector<double> d = laplace_derivatives(2 * order, R);
+    for (int a = 0; a < n; ++a)
+      for (int b = 0; b < n; ++b) {
+        const int r = rank3(ops.ax[a] + ops.ax[b], ops.ay[a] + ops.ay[b], ops.az[a] + ops.az[b]);
+        out[static_cast<size_t>(b) + static_cast<size_t>(n) * a] = d[static_cast<size_t>(r)];
+      }
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(nullptr, e.code, e.what());
+  }
+}
+
+const char *cdfmm_b200_last_error(const cdfmm_b200_plan *plan) {
+  if (plan != nullptr) return plan->last_error.c_str();
+  return g_last_error.c_str();
+}
+
+} // extern "C"

@@ -1,0 +1,284 @@
+"""ctypes binding of the B200 evaluator's C ABI (include/cdfmm_b200.h).
+
+This is the thin FFI a host program uses when it talks to the evaluator
+without the C++ layer (the pybind11 `cdfmm` module goes through
+libcdfmm.so -> libcdfmm_b200.so instead).  Arrays are numpy (host memory) or
+anything exposing `data_ptr()` (e.g. torch CUDA tensors, device memory).
+
+The library must have been built (`make -C dip-fmm_b200`); importing this
+module raises if it is missing -- there is no fallback implementation.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIBRARY_PATH = os.path.join(_HERE, "..", "lib", "libcdfmm_b200.so")
+
+OK = 0
+ERR_INVALID_ARGUMENT = 1
+ERR_RUNTIME = 2
+ERR_OUT_OF_MEMORY = 3
+ERR_LOGIC = 4
+ERR_NO_DEVICE = 5
+ERR_TIMEOUT = 6
+
+OUTPUT_POTENTIAL = 1
+OUTPUT_FIELD = 2
+M2L_AUTO, M2L_FP32, M2L_BF16X3 = 0, 1, 2
+MOMENTS_ON_HOST = 1
+RESULTS_ON_HOST = 2
+LAYOUT_SEPARATE = 0
+LAYOUT_INTERLEAVED = 1
+
+EXPORTED = (
+    "cdfmm_b200_device_count", "cdfmm_b200_device_info", "cdfmm_b200_plan_create",
+    "cdfmm_b200_plan_destroy", "cdfmm_b200_set_self_indices", "cdfmm_b200_evaluate",
+    "cdfmm_b200_read_expansions", "cdfmm_b200_set_timing", "cdfmm_b200_get_stats",
+    "cdfmm_b200_direct_fp64", "cdfmm_b200_m2l_matrix", "cdfmm_b200_last_error",
+)
+
+
+class PlanDesc(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("n_sources", ctypes.c_int32), ("n_targets", ctypes.c_int32),
+        ("order", ctypes.c_int32), ("depth", ctypes.c_int32), ("max_states", ctypes.c_int32),
+        ("m2l_mode", ctypes.c_int32), ("device", ctypes.c_int32),
+        ("root_centre", ctypes.c_double * 3), ("root_half_width", ctypes.c_double),
+        ("sorted_source_positions", ctypes.c_void_p), ("sorted_target_positions", ctypes.c_void_p),
+        ("source_permutation", ctypes.c_void_p), ("target_permutation", ctypes.c_void_p),
+        ("leaf_source_offsets", ctypes.c_void_p), ("leaf_target_offsets", ctypes.c_void_p),
+    ]
+
+
+class EvalArgs(ctypes.Structure):
+    _fields_ = [
+        ("moments", ctypes.c_void_p), ("moments_dtype", ctypes.c_int32), ("n_states", ctypes.c_int32),
+        ("output", ctypes.c_uint32), ("layout", ctypes.c_int32), ("field", ctypes.c_void_p),
+        ("potential", ctypes.c_void_p), ("memory", ctypes.c_uint32), ("stream", ctypes.c_void_p),
+        ("synchronize", ctypes.c_int32),
+    ]
+
+
+class Stats(ctypes.Structure):
+    _fields_ = [
+        ("persistent_device_bytes", ctypes.c_uint64), ("setup_h2d_bytes", ctypes.c_uint64),
+        ("evaluation_h2d_bytes", ctypes.c_uint64), ("evaluation_d2h_bytes", ctypes.c_uint64),
+        ("evaluation_h2d_calls", ctypes.c_uint64), ("evaluation_d2h_calls", ctypes.c_uint64),
+        ("evaluations", ctypes.c_uint64), ("m2l_classes", ctypes.c_uint64),
+        ("m2l_interactions", ctypes.c_uint64), ("m2l_matrix_bytes", ctypes.c_uint64),
+        ("p2p_pairs", ctypes.c_uint64), ("kernel_launches_last", ctypes.c_uint64),
+        ("m2l_mode_resolved", ctypes.c_int32), ("timing_enabled", ctypes.c_int32),
+        ("ms_gather", ctypes.c_double), ("ms_p2m", ctypes.c_double), ("ms_m2m", ctypes.c_double),
+        ("ms_m2l", ctypes.c_double), ("ms_l2l", ctypes.c_double), ("ms_l2p", ctypes.c_double),
+        ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
+    ]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class CdfmmError(RuntimeError):
+    def __init__(self, code, message):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+_lib = None
+
+
+def library() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = os.path.abspath(LIBRARY_PATH)
+    if not os.path.exists(path):
+        raise ImportError(f"{path} is missing: build it with `make -C dip-fmm_b200`")
+    lib = ctypes.CDLL(path)
+    vp, i32, u64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_size_t
+    lib.cdfmm_b200_device_count.argtypes = [ctypes.POINTER(i32)]
+    lib.cdfmm_b200_device_info.argtypes = [i32, ctypes.c_char_p, u64, ctypes.POINTER(i32), ctypes.POINTER(i32)]
+    lib.cdfmm_b200_plan_create.argtypes = [ctypes.POINTER(PlanDesc), ctypes.POINTER(vp)]
+    lib.cdfmm_b200_plan_destroy.argtypes = [vp]
+    lib.cdfmm_b200_plan_destroy.restype = None
+    lib.cdfmm_b200_set_self_indices.argtypes = [vp, vp]
+    lib.cdfmm_b200_evaluate.argtypes = [vp, ctypes.POINTER(EvalArgs)]
+    lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
+    lib.cdfmm_b200_set_timing.argtypes = [vp, i32]
+    lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
+    lib.cdfmm_b200_direct_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
+    lib.cdfmm_b200_m2l_matrix.argtypes = [i32, vp, vp, u64]
+    lib.cdfmm_b200_last_error.argtypes = [vp]
+    lib.cdfmm_b200_last_error.restype = ctypes.c_char_p
+    _lib = lib
+    return lib
+
+
+def _check(code, plan=None):
+    if code != OK:
+        msg = library().cdfmm_b200_last_error(plan).decode()
+        if code == ERR_INVALID_ARGUMENT:
+            raise ValueError(msg)
+        raise CdfmmError(code, msg)
+
+
+def _ptr(a):
+    if a is None:
+        return None
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.ctypes.data)
+
+
+def device_count() -> int:
+    c = ctypes.c_int32(0)
+    _check(library().cdfmm_b200_device_count(ctypes.byref(c)))
+    return int(c.value)
+
+
+def m2l_matrix(order: int, R) -> np.ndarray:
+    """(n, n) FP64 matrix [beta, alpha] = D^{alpha+beta} G(R), as generated by the plan."""
+    n = (order + 1) * (order + 2) * (order + 3) // 6
+    out = np.zeros(n * n)
+    Rv = np.ascontiguousarray(R, dtype=np.float64)
+    _check(library().cdfmm_b200_m2l_matrix(order, _ptr(Rv), _ptr(out), out.size))
+    return out.reshape(n, n).T.copy()
+
+
+def direct_fp64(sources, moments, targets, self_indices=None, device=0):
+    """FP64 direct sum on the device; returns (phi, H)."""
+    s = np.ascontiguousarray(sources, dtype=np.float64).reshape(-1, 3)
+    m = np.ascontiguousarray(moments, dtype=np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1, 3)
+    ids = None if self_indices is None else np.ascontiguousarray(self_indices, dtype=np.int32)
+    phi = np.zeros(len(t))
+    H = np.zeros((len(t), 3))
+    _check(library().cdfmm_b200_direct_fp64(device, len(s), _ptr(s), _ptr(m), len(t), _ptr(t), _ptr(ids),
+                                            _ptr(phi), _ptr(H)))
+    return phi, H
+
+
+class DevicePlan:
+    """One fixed geometry on the device (cdfmm_b200_plan)."""
+
+    def __init__(self, sorted_sources, sorted_targets, source_permutation, target_permutation,
+                 leaf_source_offsets, leaf_target_offsets, root_centre, root_half_width, order, depth,
+                 max_states=1, m2l_mode=M2L_AUTO, device=0):
+        lib = library()
+        self._keep = [np.ascontiguousarray(sorted_sources, dtype=np.float64).reshape(-1, 3),
+                      np.ascontiguousarray(sorted_targets, dtype=np.float64).reshape(-1, 3),
+                      np.ascontiguousarray(source_permutation, dtype=np.int32),
+                      np.ascontiguousarray(target_permutation, dtype=np.int32),
+                      np.ascontiguousarray(leaf_source_offsets, dtype=np.int32),
+                      np.ascontiguousarray(leaf_target_offsets, dtype=np.int32)]
+        d = PlanDesc()
+        d.struct_size = ctypes.sizeof(PlanDesc)
+        d.n_sources = len(self._keep[0])
+        d.n_targets = len(self._keep[1])
+        d.order = order
+        d.depth = depth
+        d.max_states = max_states
+        d.m2l_mode = m2l_mode
+        d.device = device
+        for a in range(3):
+            d.root_centre[a] = float(root_centre[a])
+        d.root_half_width = float(root_half_width)
+        (d.sorted_source_positions, d.sorted_target_positions, d.source_permutation,
+         d.target_permutation, d.leaf_source_offsets, d.leaf_target_offsets) = [a.ctypes.data for a in self._keep]
+        handle = ctypes.c_void_p()
+        _check(lib.cdfmm_b200_plan_create(ctypes.byref(d), ctypes.byref(handle)))
+        self._h = handle
+        self.n_sources, self.n_targets, self.order, self.depth = d.n_sources, d.n_targets, order, depth
+        self.n_coefficients = (order + 1) * (order + 2) * (order + 3) // 6
+        self.n_nodes = ((1 << (3 * (depth + 1))) - 1) // 7
+        self.max_states = max_states
+        self._keep = None
+
+    @classmethod
+    def from_tree(cls, tree, order, **kw):
+        """Builds the descriptor from a cdfmm.UniformTree (the host tree)."""
+        depth = tree.max_level
+        soff = np.asarray(tree.leaf_source_offsets(), dtype=np.int32)
+        toff = np.asarray(tree.leaf_target_offsets(), dtype=np.int32)
+        rc = tree.root_centre
+        return cls(tree.sorted_source_positions(), tree.sorted_target_positions(), tree.source_permutation,
+                   tree.target_permutation, soff, toff, (rc.x, rc.y, rc.z), tree.root_half_width, order, depth, **kw)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().cdfmm_b200_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_self_indices(self, sorted_self):
+        if sorted_self is None:
+            _check(library().cdfmm_b200_set_self_indices(self._h, None), self._h)
+            return
+        a = np.ascontiguousarray(sorted_self, dtype=np.int32)
+        if a.shape != (self.n_targets,):
+            raise ValueError("sorted_self must have one entry per target")
+        _check(library().cdfmm_b200_set_self_indices(self._h, _ptr(a)), self._h)
+
+    def set_timing(self, enabled=True):
+        _check(library().cdfmm_b200_set_timing(self._h, 1 if enabled else 0), self._h)
+
+    def stats(self) -> dict:
+        s = Stats()
+        _check(library().cdfmm_b200_get_stats(self._h, ctypes.byref(s)), self._h)
+        return s.as_dict()
+
+    def evaluate(self, moments, output="field", layout=LAYOUT_SEPARATE, field=None, potential=None,
+                 stream=None, synchronize=True):
+        """Evaluates K states.
+
+        moments: (K, n_sources, 3) or (n_sources, 3) host numpy (float32 or
+        float64) or a device tensor with data_ptr().  Host inputs give host
+        results (allocated here when not supplied); device inputs need device
+        `field` / `potential` buffers.
+        """
+        flags = {"field": OUTPUT_FIELD, "potential": OUTPUT_POTENTIAL, "both": OUTPUT_FIELD | OUTPUT_POTENTIAL}[output]
+        on_device = hasattr(moments, "data_ptr")
+        if on_device:
+            K = int(moments.shape[0]) if len(moments.shape) == 3 else 1
+            dtype = 1 if str(moments.dtype).endswith("float64") else 0
+            memory = 0
+        else:
+            moments = np.ascontiguousarray(moments)
+            if moments.dtype not in (np.float32, np.float64):
+                moments = moments.astype(np.float64)
+            K = moments.shape[0] if moments.ndim == 3 else 1
+            dtype = 1 if moments.dtype == np.float64 else 0
+            memory = MOMENTS_ON_HOST | RESULTS_ON_HOST
+            width = 4 if layout == LAYOUT_INTERLEAVED else 3
+            if field is None and (flags & OUTPUT_FIELD or layout == LAYOUT_INTERLEAVED):
+                field = np.zeros((K, self.n_targets, width), dtype=np.float32)
+            if potential is None and flags & OUTPUT_POTENTIAL and layout == LAYOUT_SEPARATE:
+                potential = np.zeros((K, self.n_targets), dtype=np.float32)
+        a = EvalArgs()
+        a.moments = _ptr(moments).value if moments is not None else None
+        a.moments_dtype = dtype
+        a.n_states = K
+        a.output = flags
+        a.layout = layout
+        a.field = _ptr(field).value if field is not None else None
+        a.potential = _ptr(potential).value if potential is not None else None
+        a.memory = memory
+        a.stream = stream
+        a.synchronize = 1 if synchronize else 0
+        _check(library().cdfmm_b200_evaluate(self._h, ctypes.byref(a)), self._h)
+        return {"H": field, "phi": potential}
+
+    def read_expansions(self, which="multipole", state=0) -> np.ndarray:
+        out = np.zeros(self.n_nodes * self.n_coefficients, dtype=np.float32)
+        w = 0 if which == "multipole" else 1
+        _check(library().cdfmm_b200_read_expansions(self._h, w, state, _ptr(out), out.size), self._h)
+        return out.reshape(self.n_nodes, self.n_coefficients)

@@ -1,0 +1,189 @@
+/*
+ * cdfmm_b200 -- C ABI of the B200 (sm_100a) evaluator for the static-geometry
+ * uniform-octree dipole FMM.
+ *
+ * This is the drop-in boundary for upstream dip-fmm's device executor.  In the
+ * reference, UniformFmm hands its CPU-built static plan to
+ *   CudaFullPlan::CudaFullPlan(const FloatCudaFullPlanData&)   src/cuda_fmm_plan.hpp:95-101
+ *   CudaFullPlan::evaluate(moments, fields, sorted_self_indices) src/cuda_fmm_plan.hpp:103-108
+ * (owned through UniformFmm::CudaFullPlanOwner, src/uniform_fmm_internal.hpp:27-32,
+ * dispatched from src/uniform_fmm.cpp:1102-1136 and :1307-1349).  Here the
+ * caller hands over only the Morton-sorted geometry; every operator is
+ * generated inside the plan, and one evaluate call processes K moment states.
+ *
+ * Conventions
+ *  - Plain C: pointers, sizes and status codes; no exceptions cross the ABI.
+ *  - Every function returns CDFMM_B200_OK (0) or an error status; the message
+ *    of the last failure is available from cdfmm_b200_last_error().
+ *  - Moments and results use the caller's (user) source / target order; the
+ *    plan applies the Morton permutations internally.
+ *  - Positions, moments, potential and field are in physical units.  The plan
+ *    evaluates in root-width-normalised FP32 coordinates exactly as the
+ *    reference FP32 plan does (src/uniform_fmm.cpp:379-417, :1315-1323, :1448-1451).
+ *  - A plan is not re-entrant: calls on one plan must not overlap.
+ */
+#ifndef CDFMM_B200_H
+#define CDFMM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Status codes.  The C++ wrapper maps INVALID_ARGUMENT to std::invalid_argument,
+ * LOGIC to std::logic_error and the rest to std::runtime_error, which is how
+ * the reference reports the same conditions (src/uniform_fmm.cpp:1290-1311,
+ * src/cuda_fmm.cu:32-54). */
+#define CDFMM_B200_OK 0
+#define CDFMM_B200_ERR_INVALID_ARGUMENT 1
+#define CDFMM_B200_ERR_RUNTIME 2
+#define CDFMM_B200_ERR_OUT_OF_MEMORY 3
+#define CDFMM_B200_ERR_LOGIC 4
+#define CDFMM_B200_ERR_NO_DEVICE 5
+#define CDFMM_B200_ERR_TIMEOUT 6
+
+/* Output selection: same bit values as cdfmm::OutputFlags (include/cdfmm/output_flags.hpp:12-17 upstream). */
+#define CDFMM_B200_OUTPUT_POTENTIAL 1u
+#define CDFMM_B200_OUTPUT_FIELD 2u
+
+/* M2L arithmetic. */
+#define CDFMM_B200_M2L_AUTO 0        /* split-BF16 tensor cores where supported, else FP32 */
+#define CDFMM_B200_M2L_FP32 1        /* FP32 SIMT (the plain per-state path) */
+#define CDFMM_B200_M2L_BF16X3 2      /* tcgen05, BF16 hi/lo with three products, FP32 accumulate */
+
+/* Where the caller's arrays live (cdfmm_b200_eval_args.memory). */
+#define CDFMM_B200_MOMENTS_ON_HOST 1u
+#define CDFMM_B200_RESULTS_ON_HOST 2u
+
+/* Result layout (cdfmm_b200_eval_args.layout). */
+#define CDFMM_B200_LAYOUT_SEPARATE 0    /* field[K][Nt][3] and potential[K][Nt] */
+#define CDFMM_B200_LAYOUT_INTERLEAVED 1 /* field[K][Nt][4] = {phi, Hx, Hy, Hz}: cdfmm::FloatPotentialField */
+
+typedef struct cdfmm_b200_plan cdfmm_b200_plan;
+
+/* Geometry of one problem, as produced by the host tree
+ * (include/cdfmm/uniform_tree.hpp; upstream src/uniform_tree.cpp:129-523).
+ * Replaces FloatCudaFullPlanData (src/cuda_fmm_plan.hpp:69-86 upstream). */
+typedef struct cdfmm_b200_plan_desc {
+  int32_t struct_size;             /* sizeof(cdfmm_b200_plan_desc) */
+  int32_t n_sources;               /* >= 0 */
+  int32_t n_targets;               /* >= 0 */
+  int32_t order;                   /* expansion order p, 0..10 */
+  int32_t depth;                   /* tree max_level, 0..8 */
+  int32_t max_states;              /* largest K passed to one evaluate call, >= 1 */
+  int32_t m2l_mode;                /* CDFMM_B200_M2L_* */
+  int32_t device;                  /* CUDA device ordinal */
+  double root_centre[3];           /* cubic root box (UniformTree::root_centre) */
+  double root_half_width;          /* (UniformTree::root_half_width), > 0 */
+  const double *sorted_source_positions; /* [n_sources][3], Morton-sorted (host memory) */
+  const double *sorted_target_positions; /* [n_targets][3], Morton-sorted (host memory) */
+  const int32_t *source_permutation;     /* [n_sources] sorted index -> user index */
+  const int32_t *target_permutation;     /* [n_targets] sorted index -> user index */
+  const int32_t *leaf_source_offsets;    /* [8^depth + 1], sources of Morton leaf m are [o[m], o[m+1]) */
+  const int32_t *leaf_target_offsets;    /* [8^depth + 1] */
+} cdfmm_b200_plan_desc;
+
+/* One evaluate call: K moment states on the plan's fixed geometry.
+ * Replaces CudaFullPlan::evaluate (src/cuda_fmm.cu:3457-3655 upstream), which
+ * handles one state, field only, host memory and a blocking D2H. */
+typedef struct cdfmm_b200_eval_args {
+  const void *moments;   /* [n_states][n_sources][3], user source order, physical units */
+  int32_t moments_dtype; /* 0 = float32, 1 = float64 */
+  int32_t n_states;      /* K, 1..max_states */
+  uint32_t output;       /* CDFMM_B200_OUTPUT_* bits; at least one */
+  int32_t layout;        /* CDFMM_B200_LAYOUT_* */
+  float *field;          /* see layout; required when FIELD is requested or layout is interleaved */
+  float *potential;      /* [n_states][n_targets] for LAYOUT_SEPARATE with POTENTIAL, else unused */
+  uint32_t memory;       /* CDFMM_B200_*_ON_HOST bits */
+  void *stream;          /* cudaStream_t to order the work on; NULL = the plan's own stream */
+  int32_t synchronize;   /* nonzero: return only after results are complete */
+} cdfmm_b200_eval_args;
+
+/* Per-plan counters (mirrors the reference's CudaPlanStatistics fields it has,
+ * include/cdfmm/timings.hpp:182-223 upstream) and the device time of the last
+ * evaluate per stage (milliseconds; filled only when timing is enabled). */
+typedef struct cdfmm_b200_stats {
+  uint64_t persistent_device_bytes;
+  uint64_t setup_h2d_bytes;
+  uint64_t evaluation_h2d_bytes;
+  uint64_t evaluation_d2h_bytes;
+  uint64_t evaluation_h2d_calls;
+  uint64_t evaluation_d2h_calls;
+  uint64_t evaluations;
+  uint64_t m2l_classes;          /* distinct translation vectors used (<= 316) */
+  uint64_t m2l_interactions;     /* list2 pairs summed over levels */
+  uint64_t m2l_matrix_bytes;
+  uint64_t p2p_pairs;            /* list1 (target, source) pairs, self included */
+  uint64_t kernel_launches_last; /* kernels launched by the last evaluate */
+  int32_t m2l_mode_resolved;
+  int32_t timing_enabled;
+  double ms_gather, ms_p2m, ms_m2m, ms_m2l, ms_l2l, ms_l2p, ms_p2p, ms_total;
+} cdfmm_b200_stats;
+
+/* Library / device probing.  Returns OK and *count = 0 when no device. */
+int cdfmm_b200_device_count(int32_t *count);
+
+/* Name and compute capability of a device (the reference's
+ * cuda_device_description, include/cdfmm/uniform_fmm.hpp:89-90 upstream). */
+int cdfmm_b200_device_info(int32_t device, char *name, size_t name_len, int32_t *cc_major,
+                           int32_t *cc_minor);
+
+/* Build operators and upload the geometry (the reference's CudaFullPlan ctor,
+ * src/cuda_fmm.cu:2937-3155 upstream).  Host arrays may be freed on return. */
+int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **out_plan);
+
+/* Releases every device allocation of the plan.  NULL is ignored. */
+void cdfmm_b200_plan_destroy(cdfmm_b200_plan *plan);
+
+/* Sets the target -> source self-exclusion map in SORTED numbering
+ * ([n_targets], -1 = no self source), or clears it when NULL.  The list1 P2P
+ * skips exactly that source for each target (upstream
+ * src/uniform_fmm.cpp:1028-1043 builds the same sorted map from user
+ * identities).  Coordinate equality is never used as identity. */
+int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_self_indices);
+
+/* Runs P2M -> M2M -> M2L -> L2L -> L2P plus list1 P2P for K states and writes
+ * the results in user target order (the reference's UniformFmm::evaluate_into_float32
+ * with CudaFull, src/uniform_fmm.cpp:1281-1349 upstream, generalised to K states,
+ * potential output and device-resident arrays). */
+int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args);
+
+/* Copies the FP32 multipole (which = 0) or local (which = 1) expansions of one
+ * state of the last evaluate to host memory as out[node][coefficient], node in
+ * flat level-wise Morton order and coefficients in the total-degree basis
+ * order; the values are in the normalised units of the reference FP32 plan
+ * (UniformFmm::multipole_float32 / local_float32, include/cdfmm/uniform_fmm.hpp:262-269 upstream). */
+int cdfmm_b200_read_expansions(const cdfmm_b200_plan *plan, int32_t which, int32_t state,
+                               float *out, size_t out_count);
+
+/* Enables (nonzero) or disables per-stage CUDA-event timing of evaluate. */
+int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled);
+
+int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out);
+
+/* FP64 O(N*M) direct sum on the device with explicit self exclusion: the
+ * oracle-grade reference field (upstream validation.cpp:71-111 on the CPU and
+ * dipole_field_kernel, src/cuda_fmm.cu:518-569).  Host arrays in user order;
+ * self_indices may be NULL; phi and/or H may be NULL to skip them. */
+int cdfmm_b200_direct_fp64(int32_t device, int32_t n_sources, const double *source_positions,
+                           const double *moments, int32_t n_targets,
+                           const double *target_positions, const int32_t *self_indices,
+                           double *phi, double *field);
+
+/* The FP64 M2L matrix the plan generates for translation R = target centre -
+ * source centre: out[beta + n*alpha] = D^{alpha+beta} G(R), n = (p+1)(p+2)(p+3)/6
+ * (the reference's build_static_m2l_matrix, src/static_operators.cpp:159-184,
+ * and its Python static_m2l_matrix, python/bindings.cpp:932-943).  Host only. */
+int cdfmm_b200_m2l_matrix(int32_t order, const double *R, double *out, size_t out_count);
+
+/* Message of the last failure on this plan (or of the last failure of a call
+ * without a plan, on this thread, when plan is NULL).  Never NULL. */
+const char *cdfmm_b200_last_error(const cdfmm_b200_plan *plan);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CDFMM_B200_H */

@@ -1,0 +1,248 @@
+"""GPU parity tests of the B200 path (run with -m gpu on a B200).
+
+Checked against (a) golden vectors of the upstream reference's CpuStatic
+FP32 / FP64 backends and FP64 direct sum (tests/golden/fmm.npz), (b) the CPU
+oracle (oracle/, FP64 restatement pinned to the same goldens), and (c) the
+device FP64 direct sum.  Tolerances are the reference's own FP32 bars:
+rel-L2(H) <= 3e-5 FP32 vs FP64 (upstream tests/test_precision.cpp:332-367),
+per-element rtol 2e-5 (python_tests/test_fmm_precision.py:56-74).
+"""
+
+import numpy as np
+import pytest
+
+import cdfmm
+import cdfmm_b200
+import oracle
+from conftest import group_names, load_group
+
+pytestmark = pytest.mark.gpu
+
+FP32_REL_L2 = 3e-5
+
+
+def make_fmm(g_or_src, tgt=None, order=4, depth=3, root=None, fixed=None, max_states=1, m2l=None):
+    o = cdfmm.UniformFmmOptions()
+    o.expansion_order = order
+    o.tree.max_level = depth
+    o.max_states = max_states
+    if m2l is not None:
+        o.b200_m2l = m2l
+    if root is not None:
+        o.tree.root_centre = cdfmm.Vec3(*root[:3])
+        o.tree.root_half_width = float(root[3])
+    if fixed is not None:
+        o.fixed_target_source_indices = list(map(int, fixed))
+    return cdfmm.UniformFmm(g_or_src, tgt, o)
+
+
+def golden_fmm(name):
+    g = load_group("fmm.npz", name)
+    root = g["root_in"] if bool(g["has_root"]) else None
+    f = make_fmm(g["sources"], g["targets"], int(g["order"]), int(g["depth"]), root)
+    ids = g["identities"] if g["identities"].size else None
+    return g, f, ids
+
+
+@pytest.mark.parametrize("name", group_names("fmm.npz"))
+def test_evaluate_matches_reference_cpustatic(name):
+    g, f, ids = golden_fmm(name)
+    r = f.evaluate(g["moments"], output="both", target_source_indices=None if ids is None else ids.tolist())
+    assert r["H"].dtype == np.float32 and r["phi"].dtype == np.float32
+    assert oracle.rel_l2(r["H"], g["H64"]) < FP32_REL_L2
+    assert oracle.rel_l2(r["H"], g["H32"]) < FP32_REL_L2
+    assert oracle.rel_l2(r["phi"], g["phi64"]) < FP32_REL_L2
+    assert f.static_plan_statistics["transfer_classes"] == int(g["transfer_classes"])
+    assert f.static_plan_statistics["interactions"] == int(g["interactions"])
+    if int(g["depth"]) == 0:
+        assert oracle.rel_l2(r["H"], g["H_direct"]) < 1e-6
+
+
+def test_stage_expansions_match_reference():
+    g, f, ids = golden_fmm("expansions_p4_d3")
+    f.evaluate(g["moments"], target_source_indices=ids.tolist())
+    nn = len(f.tree.nodes)
+    M = np.stack([f.multipole(i) for i in range(nn)]).astype(np.float64)
+    L = np.stack([f.local(i) for i in range(nn)]).astype(np.float64)
+    for ours, ref in ((M, g["M32"].astype(np.float64)), (L, g["L32"].astype(np.float64))):
+        scale = np.abs(ref).max(axis=1, keepdims=True)
+        err = np.abs(ours - ref).max(axis=1, keepdims=True)
+        assert np.all(err <= 2e-5 * scale + 1e-30)
+
+
+def test_field_only_and_potential_only_outputs():
+    g, f, ids = golden_fmm("small_p4_d3")
+    both = f.evaluate(g["moments"], output="both", target_source_indices=ids.tolist())
+    field = f.evaluate(g["moments"], output="field", target_source_indices=ids.tolist())
+    pot = f.evaluate(g["moments"], output="potential", target_source_indices=ids.tolist())
+    np.testing.assert_array_equal(field["H"], both["H"])
+    np.testing.assert_array_equal(field["phi"], 0.0)
+    np.testing.assert_array_equal(pot["phi"], both["phi"])
+    np.testing.assert_array_equal(pot["H"], 0.0)
+
+
+def test_repeated_state_and_zero_moments_reset():
+    g, f, ids = golden_fmm("small_p2_d2")
+    a = f.evaluate(g["moments"], target_source_indices=ids.tolist())["H"]
+    z = f.evaluate(np.zeros_like(g["moments"]), target_source_indices=ids.tolist())["H"]
+    b = f.evaluate(g["moments"], target_source_indices=ids.tolist())["H"]
+    np.testing.assert_array_equal(z, 0.0)
+    np.testing.assert_array_equal(a, b)
+    for node in f.tree.nodes:
+        assert np.all(np.isfinite(f.local(node.index)))
+
+
+def test_user_order_is_preserved_under_permutation():
+    rng = np.random.default_rng(3)
+    x = rng.uniform(-1, 1, (500, 3))
+    m = rng.normal(size=(500, 3))
+    perm = rng.permutation(500)
+    f1 = make_fmm(x, x, 4, 3)
+    f2 = make_fmm(x[perm], x[perm], 4, 3)
+    h1 = f1.evaluate(m, target_source_indices=list(range(500)))["H"]
+    h2 = f2.evaluate(m[perm], target_source_indices=list(range(500)))["H"]
+    np.testing.assert_allclose(h2, h1[perm], rtol=2e-5, atol=2e-5 * np.abs(h1).max())
+
+
+def test_identity_map_contract():
+    rng = np.random.default_rng(4)
+    x = rng.uniform(0, 1, (300, 3))
+    m = rng.normal(size=(300, 3))
+    ids = np.arange(300)
+    f = make_fmm(x, x, 4, 2, fixed=ids)
+    implicit = f.evaluate(m)["H"]
+    explicit = f.evaluate(m, target_source_indices=ids.tolist())["H"]
+    np.testing.assert_array_equal(implicit, explicit)
+    changed = ids.copy()
+    changed[0] = 5
+    with pytest.raises(ValueError, match="identity map changed"):
+        f.evaluate(m, target_source_indices=changed.tolist())
+    with pytest.raises(ValueError, match="incorrect length"):
+        make_fmm(x, x, 4, 2).evaluate(m, target_source_indices=[0, 1])
+    with pytest.raises(ValueError, match="invalid index"):
+        make_fmm(x, x, 4, 2).evaluate(m, target_source_indices=[300] * 300)
+    with pytest.raises(ValueError, match="one dipole moment per source"):
+        f.evaluate(m[:-1])
+
+
+def test_coincident_non_self_pair_is_nan_like_reference():
+    x = np.array([[0.1, 0.2, 0.3], [0.1, 0.2, 0.3], [0.7, 0.6, 0.5], [0.4, 0.9, 0.2]])
+    m = np.ones((4, 3))
+    f = make_fmm(x, x, 3, 1)
+    with_ids = f.evaluate(m, target_source_indices=[0, 1, 2, 3])["H"]
+    assert np.isnan(with_ids[0]).all() and np.isnan(with_ids[1]).all()
+    assert np.isfinite(with_ids[2:]).all()
+
+
+def test_empty_geometry_is_accepted():
+    o = cdfmm.UniformFmmOptions()
+    o.tree.max_level = 2
+    f = cdfmm.UniformFmm(np.zeros((0, 3)), np.zeros((0, 3)), o)
+    r = f.evaluate(np.zeros((0, 3)))
+    assert r["H"].shape == (0, 3)
+    f2 = cdfmm.UniformFmm(np.random.default_rng(0).uniform(0, 1, (20, 3)), np.zeros((0, 3)), o)
+    assert f2.evaluate(np.ones((20, 3)))["H"].shape == (0, 3)
+
+
+def test_upward_pass_root_matches_oracle():
+    rng = np.random.default_rng(11)
+    x = rng.uniform(-1, 1, (400, 3))
+    m = rng.normal(size=(400, 3))
+    o = cdfmm.UniformFmmOptions()
+    o.expansion_order = 5
+    o.tree.max_level = 3
+    o.tree.root_centre = cdfmm.Vec3(0, 0, 0)
+    o.tree.root_half_width = 1.0
+    f = cdfmm.UniformFmm(x, o)
+    f.upward_pass(m)
+    r = oracle.fmm(x, np.zeros((0, 3)), m, 5, 3, root_centre=[0, 0, 0], root_half_width=1.0, expansions=True)
+    deg = oracle.basis(5).sum(axis=1)
+    root_ref = r["M"][0] * 2.0 ** (-(deg + 2.0))
+    np.testing.assert_allclose(f.root_multipole, root_ref, rtol=1e-5, atol=1e-5 * np.abs(root_ref).max())
+
+
+@pytest.mark.parametrize("K", [2, 5, 16])
+def test_batched_states_match_single_state_calls(K):
+    rng = np.random.default_rng(100 + K)
+    x = rng.uniform(0, 1, (3000, 3))
+    ms = rng.normal(size=(K, 3000, 3)).astype(np.float32)
+    f = make_fmm(x, x, 5, 3, max_states=K)
+    ids = list(range(3000))
+    batch = f.evaluate_states(ms, output="both", target_source_indices=ids)
+    for k in range(K):
+        single = f.evaluate(ms[k].astype(np.float64), output="both", target_source_indices=ids)
+        assert oracle.rel_l2(batch["H"][k], single["H"]) < 2e-6
+        assert oracle.rel_l2(batch["phi"][k], single["phi"]) < 2e-6
+
+
+def test_c_abi_layouts_dtypes_and_transfer_counts():
+    rng = np.random.default_rng(12)
+    x = rng.uniform(0, 1, (2000, 3))
+    t = rng.uniform(0.2, 0.8, (1000, 3))
+    m = rng.normal(size=(3, 2000, 3))
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, t, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, 4, max_states=3)
+    sep = plan.evaluate(m, output="both")
+    inter = plan.evaluate(m.astype(np.float32), output="both", layout=cdfmm_b200.LAYOUT_INTERLEAVED)
+    np.testing.assert_allclose(inter["H"][..., 1:], sep["H"], rtol=1e-5, atol=1e-5 * np.abs(sep["H"]).max())
+    np.testing.assert_allclose(inter["H"][..., 0], sep["phi"], rtol=1e-5, atol=1e-5 * np.abs(sep["phi"]).max())
+    ref = oracle.fmm(x, t, m[1], 4, 3)
+    assert oracle.rel_l2(sep["H"][1], ref["H"]) < FP32_REL_L2
+    assert oracle.rel_l2(sep["phi"][1], ref["phi"]) < FP32_REL_L2
+    st = plan.stats()
+    assert st["evaluations"] == 2
+    assert st["evaluation_h2d_bytes"] == 3 * 2000 * 3 * 8 + 3 * 2000 * 3 * 4
+    assert st["evaluation_d2h_bytes"] == 3 * 1000 * 4 * 4 + 3 * 1000 * 4 * 4
+
+
+def test_device_resident_arrays_through_c_abi():
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(13)
+    x = rng.uniform(0, 1, (4000, 3))
+    m = rng.normal(size=(4, 4000, 3)).astype(np.float32)
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, 5, max_states=4)
+    host = plan.evaluate(m, output="both")
+    dm = torch.from_numpy(m).cuda()
+    dH = torch.zeros((4, 4000, 3), dtype=torch.float32, device="cuda")
+    dphi = torch.zeros((4, 4000), dtype=torch.float32, device="cuda")
+    plan.evaluate(dm, output="both", field=dH, potential=dphi)
+    np.testing.assert_array_equal(dH.cpu().numpy(), host["H"])
+    np.testing.assert_array_equal(dphi.cpu().numpy(), host["phi"])
+
+
+def test_device_direct_fp64_matches_oracle():
+    rng = np.random.default_rng(14)
+    x = rng.uniform(0, 1, (1500, 3))
+    m = rng.normal(size=(1500, 3))
+    ids = np.arange(1500)
+    phi_d, H_d = cdfmm_b200.direct_fp64(x, m, x, ids)
+    phi_o, H_o = oracle.direct(x, m, x, ids)
+    np.testing.assert_allclose(H_d, H_o, rtol=1e-11, atol=1e-11 * np.abs(H_o).max())
+    np.testing.assert_allclose(phi_d, phi_o, rtol=1e-11, atol=1e-11 * np.abs(phi_o).max())
+
+
+def test_large_uniform_accuracy_linearity_and_oracle():
+    """N = 131072 at p = 6, d = 4 (~32 per leaf): accuracy vs the FP64 direct
+    sum on a subsample, and linearity in the moments."""
+    rng = np.random.default_rng(15)
+    N = 131072
+    x = rng.uniform(0, 1, (N, 3))
+    d = rng.normal(size=(N, 3))
+    m1 = d / np.linalg.norm(d, axis=1, keepdims=True) * rng.uniform(0.5, 1.5, (N, 1))
+    m2 = rng.normal(size=(N, 3))
+    f = make_fmm(x, x, 6, 4, max_states=2)
+    ids = np.arange(N)
+    r1 = f.evaluate(m1, output="both", target_source_indices=ids.tolist())
+    sub = rng.choice(N, 4096, replace=False)
+    phi_ref, H_ref = cdfmm_b200.direct_fp64(x, m1, x[sub], sub)
+    assert oracle.rel_l2(r1["H"][sub], H_ref) < 5e-5
+    assert oracle.rel_l2(r1["phi"][sub], phi_ref) < 5e-5
+    both = f.evaluate_states(np.stack([m1, m2]).astype(np.float32), output="field",
+                             target_source_indices=ids.tolist())["H"]
+    comb = f.evaluate((2.0 * m1 - 0.5 * m2), output="field", target_source_indices=ids.tolist())["H"]
+    assert oracle.rel_l2(comb, 2.0 * both[0] - 0.5 * both[1]) < 1e-5
