@@ -1,0 +1,415 @@
+#!/usr/bin/env python
+"""Benchmark of the static-geometry uniform dipole FMM on B200.
+
+Workload (one GPU): N = 1,048,576 dipoles uniform in the unit cube (seeded),
+targets = sources with self exclusion, moments = random unit direction x
+U[0.5, 1.5], expansion order p = 6, depth 5 (32,768 leaves, ~32 per leaf),
+field + potential, K = 64 moment states per step evaluated in one batched
+call.  Metric: target x state evaluations per second (N * K / step time).
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Under torchrun (N > 1) every rank evaluates its own K states on the same
+geometry (replicas, no data-path collective; weak scaling); the step time is
+the max over ranks of the CUDA-event time.
+
+Reported beside `value` (device-resident inputs):
+  e2e           the same metric through the C ABI with pinned host buffers,
+                H2D of moments and D2H of results inside the timed region;
+  plain         the plain per-state FP32 path (K = 1 calls, FP32 SIMT M2L);
+  rel_l2_*      accuracy of state 0 vs the FP64 direct sum on 16,384 targets;
+  roofline      dominant kernel: algorithmic work / CUDA-event duration;
+  cpu_baseline  the reference CpuStatic (oracle/_ref, built from the upstream
+                sources) on the host cores, on a bounded sample.
+--impl reference times the reference CpuStatic path (FP32, field+potential)
+on the host cores on that same bounded sample and prints the same line.
+"""
+
+from __future__ import annotations
+
+import argparse
+import datetime
+import json
+import os
+import signal
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+for _p in (ROOT, os.path.join(ROOT, "dip-fmm_b200", "python")):
+    if _p not in sys.path:
+        sys.path.insert(0, _p)
+
+METRIC = "target·state field evals/s at rel-L2≤1e-5 vs FP64: batched B200 vs plain path"
+UNIT = "target-state evals/s"
+REF_SAMPLE = dict(n=131072, order=6, depth=4)  # ~32 dipoles per leaf, like the full workload
+FALLBACK_PEAKS = {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}
+FP32_NOMINAL_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12  # 74.4
+
+
+def parse_args():
+    ap = argparse.ArgumentParser(description=__doc__, formatter_class=argparse.RawDescriptionHelpFormatter)
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["b200", "reference"], default="b200")
+    ap.add_argument("--n", type=int, default=1048576)
+    ap.add_argument("--order", type=int, default=6)
+    ap.add_argument("--depth", type=int, default=5)
+    ap.add_argument("--states", type=int, default=64)
+    ap.add_argument("--m2l", choices=["auto", "fp32", "bf16x3"], default="auto")
+    ap.add_argument("--seed", type=int, default=314159)
+    ap.add_argument("--plain-states", type=int, default=8)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    return ap.parse_args()
+
+
+def unit_moments(rng, k, n):
+    d = rng.normal(size=(k, n, 3))
+    d /= np.linalg.norm(d, axis=2, keepdims=True)
+    return (d * rng.uniform(0.5, 1.5, size=(k, n, 1))).astype(np.float32)
+
+
+def load_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return json.load(f), "measured"
+    except OSError:
+        return dict(FALLBACK_PEAKS), "fallback"
+
+
+# ------------------------------------------------------------------ clocks
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.file = None
+
+    def start(self):
+        try:
+            self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+        except (OSError, ValueError):
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return None
+        self.proc.send_signal(signal.SIGTERM)
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.file.flush()
+        self.file.seek(0)
+        rows = [r.split(",") for r in self.file.read().strip().splitlines() if r.strip()]
+        os.unlink(self.file.name)
+        sm, smax, reasons = [], 0.0, set()
+        names = ("hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap")
+        for r in rows:
+            try:
+                sm.append(float(r[1]))
+                smax = max(smax, float(r[2]))
+                for name, v in zip(names, r[5:9]):
+                    if v.strip().lower() == "active":
+                        reasons.add(name)
+            except (ValueError, IndexError):
+                continue
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# --------------------------------------------------------------- reference
+def write_ref_input(path, x, moments, order, depth, warmup, steps):
+    n = len(x)
+    hdr = np.array([n, n, order, depth, 0, 3, len(moments), warmup, steps, 1, 0, 0], dtype=np.int32)
+    with open(path, "wb") as f:
+        f.write(b"CDFMMIN1")
+        f.write(hdr.tobytes())
+        f.write(np.zeros(4).tobytes())
+        f.write(np.ascontiguousarray(x, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(x, dtype=np.float64).tobytes())
+        f.write(np.ascontiguousarray(moments, dtype=np.float64).tobytes())
+        f.write(np.arange(n, dtype=np.int32).tobytes())
+
+
+def run_reference_cpu(seed, warmup, steps):
+    """Reference CpuStatic (FP32, field+potential) on the host cores; returns
+    (target-states/s, detail).  Falls back to the oracle port if the reference
+    build is absent."""
+    s = REF_SAMPLE
+    rng = np.random.default_rng(seed)
+    x = rng.uniform(0.0, 1.0, size=(s["n"], 3))
+    m = unit_moments(rng, 1, s["n"])
+    cores = os.cpu_count() or 1
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    sample = (f"N={s['n']} uniform dipoles, p={s['order']}, depth {s['depth']} (~32/leaf), one state per "
+              f"evaluation, field+potential, FP32 CpuStatic; {steps} timed evaluations after {warmup} warm-up")
+    if os.path.exists(exe):
+        with tempfile.TemporaryDirectory() as tmp:
+            inp, out = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+            write_ref_input(inp, x, m, s["order"], s["depth"], warmup, steps)
+            env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close", OMP_PLACES="cores")
+            r = subprocess.run([exe, inp, out], capture_output=True, text=True, env=env, timeout=1800)
+            if r.returncode != 0:
+                raise RuntimeError(f"reference run failed: {r.stderr[-400:]}")
+            info = json.loads(r.stdout.strip().splitlines()[-1])
+        per_step = info["median_step_s"]
+        return s["n"] / per_step, {"kind": "reference", "cores": info["threads"], "sample": sample,
+                                   "setup_s": info["setup_s"], "ms_per_state": per_step * 1e3}
+    import oracle
+
+    t0 = time.perf_counter()
+    oracle.fmm(x, x, m[0], s["order"], s["depth"], identities=np.arange(s["n"]))
+    per_step = time.perf_counter() - t0
+    return s["n"] / per_step, {"kind": "port", "cores": cores, "sample": sample.replace("FP32 CpuStatic",
+                                                                                         "FP64 oracle port"),
+                               "ms_per_state": per_step * 1e3}
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    value, info = run_reference_cpu(args.seed, max(1, args.warmup), max(1, args.steps))
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": info["ms_per_state"],
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+            "data": "synthetic: seeded uniform dipoles, unit-direction x U[0.5,1.5] moments",
+            "config": {"workload": "reference CpuStatic on a bounded sample of the uniform p=6 workload",
+                       "n_dipoles": REF_SAMPLE["n"], "order": REF_SAMPLE["order"], "depth": REF_SAMPLE["depth"],
+                       "states_per_step": 1, "output": "field+potential"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": info["cores"], "kind": info["kind"],
+                             "sample": info["sample"]},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------- B200
+def b200_arm(args):
+    import torch
+
+    import cdfmm
+    import cdfmm_b200
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=180),
+                                device_id=torch.device("cuda", local))
+    else:
+        torch.cuda.set_device(local)
+    if cdfmm_b200.device_count() == 0:
+        raise RuntimeError("bench.py needs a CUDA device")
+
+    N, K, p, d = args.n, args.states, args.order, args.depth
+    mode = {"auto": cdfmm_b200.M2L_AUTO, "fp32": cdfmm_b200.M2L_FP32, "bf16x3": cdfmm_b200.M2L_BF16X3}[args.m2l]
+    rng = np.random.default_rng(args.seed)
+    x = rng.uniform(0.0, 1.0, size=(N, 3))
+    opts = cdfmm.UniformTreeOptions()
+    opts.max_level = d
+    tree = cdfmm.UniformTree(x, x, opts)
+    sorted_self = np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)]
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, p, max_states=K, m2l_mode=mode, device=local)
+    plan.set_self_indices(sorted_self)
+    moments = unit_moments(np.random.default_rng(args.seed + 1000 * (rank + 1)), K, N)
+    # A dedicated stream: torch's events and our kernels are ordered on it.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
+    dm = torch.from_numpy(moments).cuda()
+    dH = torch.empty((K, N, 3), dtype=torch.float32, device="cuda")
+    dphi = torch.empty((K, N), dtype=torch.float32, device="cuda")
+
+    def step():
+        plan.evaluate(dm, output="both", field=dH, potential=dphi, stream=stream.cuda_stream, synchronize=False)
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    def max_over_ranks(v):
+        if dist is None:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    for _ in range(max(args.warmup, 0)):
+        step()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    barrier()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(args.steps):
+        step()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    barrier()
+    clock_info = clocks.stop()
+    ms_step = max_over_ranks(e0.elapsed_time(e1) / args.steps)
+    value = N * K * world / (ms_step * 1e-3)
+    launches = plan.stats()["kernel_launches_last"] * args.steps
+
+    # accuracy of state 0 (FP64 direct sum on a 16,384-target subsample)
+    sub = np.random.default_rng(args.seed + 7).choice(N, size=min(N, 16384), replace=False)
+    phi_ref, H_ref = cdfmm_b200.direct_fp64(x, moments[0].astype(np.float64), x[sub], sub, device=local)
+    H0 = dH[0].cpu().numpy()[sub]
+    phi0 = dphi[0].cpu().numpy()[sub]
+    rel_h = float(np.sqrt(np.sum((H0 - H_ref) ** 2) / np.sum(H_ref ** 2)))
+    rel_phi = float(np.sqrt(np.sum((phi0 - phi_ref) ** 2) / np.sum(phi_ref ** 2)))
+
+    # per-stage device times (separate, instrumented evaluations)
+    plan.set_timing(True)
+    stage_runs = []
+    for _ in range(3):
+        step()
+        torch.cuda.synchronize()
+        stage_runs.append(plan.stats())
+    plan.set_timing(False)
+    st = plan.stats()
+    stages = {k[3:]: statistics.median(r[k] for r in stage_runs) for k in st if k.startswith("ms_")}
+
+    # end to end through the C ABI with pinned host buffers
+    e2e = None
+    if not args.no_e2e:
+        hm = torch.from_numpy(moments).pin_memory()
+        hH = torch.empty((K, N, 3), dtype=torch.float32).pin_memory()
+        hphi = torch.empty((K, N), dtype=torch.float32).pin_memory()
+
+        def host_step():
+            plan.evaluate(hm, output="both", field=hH, potential=hphi, stream=stream.cuda_stream,
+                          synchronize=True, memory=cdfmm_b200.MOMENTS_ON_HOST | cdfmm_b200.RESULTS_ON_HOST)
+
+        host_step()
+        torch.cuda.synchronize()
+        barrier()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            host_step()
+        t_e2e = max_over_ranks((time.perf_counter() - t0) / args.steps)
+        barrier()
+        e2e = {"value": N * K * world / t_e2e, "unit": UNIT, "ms_per_step": t_e2e * 1e3,
+               "h2d_bytes_per_step": int(hm.numel() * 4), "d2h_bytes_per_step": int((hH.numel() + hphi.numel()) * 4)}
+        del hm, hH, hphi
+
+    # the plain per-state FP32 path on the same GPU (K sequential single-state calls)
+    plain_plan = cdfmm_b200.DevicePlan.from_tree(tree, p, max_states=1, m2l_mode=cdfmm_b200.M2L_FP32, device=local)
+    plain_plan.set_self_indices(sorted_self)
+    ks = max(1, min(args.plain_states, K))
+    pH = torch.empty((1, N, 3), dtype=torch.float32, device="cuda")
+    pphi = torch.empty((1, N), dtype=torch.float32, device="cuda")
+    states = [dm[k:k + 1] for k in range(ks)]
+
+    def plain_step():
+        for s in states:
+            plain_plan.evaluate(s, output="both", field=pH, potential=pphi, stream=stream.cuda_stream,
+                                synchronize=False)
+
+    plain_step()
+    torch.cuda.synchronize()
+    barrier()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(stream)
+    plain_step()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    ms_state_plain = max_over_ranks(p0.elapsed_time(p1) / ks)
+    plain_value = N * world / (ms_state_plain * 1e-3)
+    plain_plan.close()
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    peaks, peak_kind = load_peaks()
+    n = (p + 1) * (p + 2) * (p + 3) // 6
+    m2l_flop = 2.0 * n * n * st["m2l_interactions"] * K
+    p2p_flop = (st["p2p_pairs"] - N) * (13.0 + 20.0 * K)
+    cand = {"m2l": (stages.get("m2l", 0.0), m2l_flop), "p2p": (stages.get("p2p", 0.0), p2p_flop)}
+    dom = max(cand, key=lambda k: cand[k][0])
+    ms_dom, flop_dom = cand[dom]
+    if dom == "m2l":
+        peak = peaks.get("bf16_tflops_sustained", FALLBACK_PEAKS["bf16_tflops_sustained"])
+        roofline = {"kernel": "m2l", "bound": "tensor", "unit": "TFLOP/s",
+                    "algorithmic_flop": m2l_flop, "peak_source": f"{peak_kind} bf16_tflops_sustained"}
+    else:
+        peak = FP32_NOMINAL_TFLOPS
+        roofline = {"kernel": "p2p", "bound": "fp32", "unit": "TFLOP/s", "algorithmic_flop": p2p_flop,
+                    "peak_source": "nominal FP32 FMA (148 SM x 128 lanes x 2 x 1.965 GHz)"}
+    achieved = flop_dom / (ms_dom * 1e-3) / 1e12 if ms_dom > 0 else 0.0
+    roofline.update({"achieved": achieved, "peak": peak, "frac": achieved / peak if peak else None,
+                     "kernel_ms": ms_dom, "traffic": traffic_from_profiles(dom)})
+
+    cpu = None
+    if world == 1 and not args.no_cpu_baseline:
+        v, info = run_reference_cpu(args.seed, 1, 3)
+        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"]}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic: seeded uniform dipoles in the unit cube, unit-direction x U[0.5,1.5] moments",
+        "config": {"workload": f"uniform N={N} dipoles, p={p}, depth {d}, K={K} states per step, field+potential",
+                   "n_dipoles": N, "order": p, "depth": d, "states_per_step": K, "output": "field+potential",
+                   "m2l": ["auto", "fp32", "bf16x3"][st["m2l_mode_resolved"]],
+                   "l2": f"inputs larger than L2 ({dm.numel() * 4 / 2**20:.0f} MiB of moments per step)",
+                   "parallelism": "replicas (independent states per GPU)" if world > 1 else "single GPU"},
+        "rel_l2_H": rel_h, "rel_l2_phi": rel_phi,
+        "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info, "roofline": roofline,
+        "cpu_baseline": cpu, "stages_ms": stages,
+        "plain": {"value": plain_value, "unit": UNIT, "ms_per_state": ms_state_plain, "states_timed": ks,
+                  "m2l": "fp32"},
+        "batched_over_plain": value / plain_value,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def traffic_from_profiles(kernel):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "dram_traffic.json")
+    try:
+        with open(path) as f:
+            return json.load(f).get(kernel)
+    except (OSError, ValueError):
+        return None
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        reference_arm(args)
+    else:
+        b200_arm(args)
+
+
+if __name__ == "__main__":
+    main()

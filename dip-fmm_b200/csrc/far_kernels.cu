@@ -54,11 +54,11 @@ __device__ inline void monomials(float dx, float dy, float dz, int q, float *out
       float xc = xb;
       for (int c = 0; a + b + c <= q; ++c) {
         out[rank3(a, b, c)] = xc;
-        xc = xc * dz / static_cast<float>(c + 1);
+        xc = xc * dz * kInvInt[c + 1];
       }
-      xb = xb * dy / static_cast<float>(b + 1);
+      xb = xb * dy * kInvInt[b + 1];
     }
-    xa = xa * dx / static_cast<float>(a + 1);
+    xa = xa * dx * kInvInt[a + 1];
   }
 }
 
@@ -117,61 +117,82 @@ __global__ void p2m_kernel(const float4 *__restrict__ src_rel, const float4 *__r
 // ---------------------------------------------------------------------------
 // M2M for one parent level (upstream src/far_field.cpp:303-331):
 //   M_parent[alpha] = sum_children sum_{g <= alpha} A_class[g] M_child[alpha - g]
-__global__ void m2m_kernel(float *__restrict__ M, const int *__restrict__ pair_off,
-                           const int *__restrict__ pairs, const float *__restrict__ coef,
-                           int n, int K, int parent_level) {
+// Stages the pair list (offsets + packed pairs) and the 8 class coefficient
+// rows of one level in shared memory.
+__device__ inline void stage_pairs(const int *pair_off, const int *pairs, const float *cf, int n, int n_pairs,
+                                   int *soff, int *spair, float *scoef) {
+  for (int q = threadIdx.x; q <= n; q += blockDim.x) soff[q] = pair_off[q];
+  for (int q = threadIdx.x; q < n_pairs; q += blockDim.x) spair[q] = pairs[q];
+  for (int q = threadIdx.x; q < 8 * n; q += blockDim.x) scoef[q] = cf[q];
+  __syncthreads();
+}
+
+// One thread per parent output coefficient (parent, alpha, state); the loads
+// of the 8 children are independent of each other, so they overlap.
+__global__ void __launch_bounds__(256) m2m_kernel(float *__restrict__ M, const int *__restrict__ pair_off,
+                                                  const int *__restrict__ pairs, const float *__restrict__ coef,
+                                                  int n, int K, int parent_level, int n_pairs) {
+  extern __shared__ int shp[];
+  int *soff = shp;
+  int *spair = soff + n + 1;
+  float *scoef = reinterpret_cast<float *>(spair + n_pairs);
+  stage_pairs(pair_off, pairs, coef + static_cast<long long>(parent_level + 1) * 8 * n, n, n_pairs, soff, spair,
+              scoef);
   const int parent_base = level_offset_d(parent_level);
   const int child_base = level_offset_d(parent_level + 1);
-  const long long count = static_cast<long long>(1) << (3 * parent_level);
-  const long long total = count * n * K;
-  const float *cf = coef + static_cast<long long>(parent_level + 1) * 8 * n;
-  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < total;
-       q += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long parent = q / (static_cast<long long>(n) * K);
-    const int rem = static_cast<int>(q - parent * n * K);
-    const int a = rem / K;
-    const int k = rem - a * K;
-    const int e0 = pair_off[a], e1 = pair_off[a + 1];
-    float v = 0.0F;
-    for (int c = 0; c < 8; ++c) {
-      const float *child = M + (child_base + parent * 8 + c) * static_cast<long long>(n) * K + k;
-      const float *cc = cf + c * n;
-      for (int e = e0; e < e1; ++e) {
-        const int pr = pairs[e];
-        v = fmaf(cc[pr & 0xffff], child[static_cast<long long>(pr >> 16) * K], v);
-      }
+  const long long per = static_cast<long long>(n) * K;
+  const long long total = (static_cast<long long>(1) << (3 * parent_level)) * per;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q >= total) return;
+  const long long parent = q / per;
+  const int rem = static_cast<int>(q - parent * per);
+  const int a = rem / K;
+  const int k = rem - a * K;
+  const int e0 = soff[a], e1 = soff[a + 1];
+  const float *child0 = M + (child_base + parent * 8) * per + k;
+  float v = 0.0F;
+#pragma unroll 2
+  for (int c = 0; c < 8; ++c) {
+    const float *child = child0 + c * per;
+    const float *cc = scoef + c * n;
+    for (int e = e0; e < e1; ++e) {
+      const int pr = spair[e];
+      v = fmaf(cc[pr & 0xffff], __ldg(child + static_cast<long long>(pr >> 16) * K), v);
     }
-    M[(parent_base + parent) * static_cast<long long>(n) * K + rem] = v;
   }
+  M[(parent_base + parent) * per + rem] = v;
 }
 
 // ---------------------------------------------------------------------------
 // L2L for one child level (upstream src/far_field.cpp:533-581):
 //   L_child[beta] += sum_{|beta + g| <= p} B_class[g] L_parent[beta + g]
-__global__ void l2l_kernel(float *__restrict__ L, const int *__restrict__ pair_off,
-                           const int *__restrict__ pairs, const float *__restrict__ coef,
-                           int n, int K, int child_level) {
+__global__ void __launch_bounds__(256) l2l_kernel(float *__restrict__ L, const int *__restrict__ pair_off,
+                                                  const int *__restrict__ pairs, const float *__restrict__ coef,
+                                                  int n, int K, int child_level, int n_pairs) {
+  extern __shared__ int shl[];
+  int *soff = shl;
+  int *spair = soff + n + 1;
+  float *scoef = reinterpret_cast<float *>(spair + n_pairs);
+  stage_pairs(pair_off, pairs, coef + static_cast<long long>(child_level) * 8 * n, n, n_pairs, soff, spair, scoef);
   const int child_base = level_offset_d(child_level);
   const int parent_base = level_offset_d(child_level - 1);
-  const long long count = static_cast<long long>(1) << (3 * child_level);
-  const long long total = count * n * K;
-  const float *cf = coef + static_cast<long long>(child_level) * 8 * n;
-  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < total;
-       q += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long child = q / (static_cast<long long>(n) * K);
-    const int rem = static_cast<int>(q - child * n * K);
-    const int b = rem / K;
-    const int k = rem - b * K;
-    const int cls = static_cast<int>(child & 7);
-    const float *parent = L + (parent_base + (child >> 3)) * static_cast<long long>(n) * K + k;
-    const float *cc = cf + cls * n;
-    float v = 0.0F;
-    for (int e = pair_off[b]; e < pair_off[b + 1]; ++e) {
-      const int pr = pairs[e];
-      v = fmaf(cc[pr & 0xffff], parent[static_cast<long long>(pr >> 16) * K], v);
-    }
-    L[(child_base + child) * static_cast<long long>(n) * K + rem] += v;
+  const long long per = static_cast<long long>(n) * K;
+  const long long total = (static_cast<long long>(1) << (3 * child_level)) * per;
+  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
+  if (q >= total) return;
+  const long long child = q / per;
+  const int rem = static_cast<int>(q - child * per);
+  const int b = rem / K;
+  const int k = rem - b * K;
+  const int cls = static_cast<int>(child & 7);
+  const float *parent = L + (parent_base + (child >> 3)) * per + k;
+  const float *cc = scoef + cls * n;
+  float v = 0.0F;
+  for (int e = soff[b]; e < soff[b + 1]; ++e) {
+    const int pr = spair[e];
+    v = fmaf(cc[pr & 0xffff], __ldg(parent + static_cast<long long>(pr >> 16) * K), v);
   }
+  L[(child_base + child) * per + rem] += v;
 }
 
 // ---------------------------------------------------------------------------
@@ -227,11 +248,11 @@ __global__ void l2p_kernel(const float *__restrict__ L, const float4 *__restrict
               }
             }
           }
-          xc = xc * d.z / static_cast<float>(c + 1);
+          xc = xc * d.z * kInvInt[c + 1];
         }
-        xb = xb * d.y / static_cast<float>(b + 1);
+        xb = xb * d.y * kInvInt[b + 1];
       }
-      xa = xa * d.x / static_cast<float>(a + 1);
+      xa = xa * d.x * kInvInt[a + 1];
     }
     const int u = tgt_perm[i];
 #pragma unroll
@@ -291,18 +312,24 @@ void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, co
                                        level_offset_d(depth), chunk);
 }
 
+static size_t pair_smem(int n, int n_pairs) {
+  return sizeof(int) * (static_cast<size_t>(n) + 1 + n_pairs) + sizeof(float) * 8 * static_cast<size_t>(n);
+}
+
 void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *coef, int n, int K,
-                int parent_level, cudaStream_t s) {
+                int parent_level, int n_pairs, cudaStream_t s) {
   const long long total = (static_cast<long long>(1) << (3 * parent_level)) * n * K;
-  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
-  m2m_kernel<<<blocks, 256, 0, s>>>(M, pair_off, pairs, coef, n, K, parent_level);
+  const long long blocks = (total + 255) / 256;
+  m2m_kernel<<<static_cast<unsigned>(blocks), 256, pair_smem(n, n_pairs), s>>>(M, pair_off, pairs, coef, n, K,
+                                                                              parent_level, n_pairs);
 }
 
 void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
-                int child_level, cudaStream_t s) {
+                int child_level, int n_pairs, cudaStream_t s) {
   const long long total = (static_cast<long long>(1) << (3 * child_level)) * n * K;
-  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 32));
-  l2l_kernel<<<blocks, 256, 0, s>>>(L, pair_off, pairs, coef, n, K, child_level);
+  const long long blocks = (total + 255) / 256;
+  l2l_kernel<<<static_cast<unsigned>(blocks), 256, pair_smem(n, n_pairs), s>>>(L, pair_off, pairs, coef, n, K,
+                                                                              child_level, n_pairs);
 }
 
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
@@ -316,8 +343,10 @@ void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const
 }
 
 void configure_far_kernels(size_t max_smem) {
-  cudaFuncSetAttribute(p2m_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(max_smem));
-  cudaFuncSetAttribute(l2p_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(max_smem));
+  allow_dynamic_smem(p2m_kernel, max_smem);
+  allow_dynamic_smem(l2p_kernel, max_smem);
+  allow_dynamic_smem(m2m_kernel, max_smem);
+  allow_dynamic_smem(l2l_kernel, max_smem);
 }
 
 } // namespace cdfmm_b200

@@ -15,9 +15,9 @@ size_t p2m_smem_bytes(int n, int p, int K, int chunk);
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
                 float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s);
 void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *coef, int n, int K,
-                int parent_level, cudaStream_t s);
+                int parent_level, int n_pairs, cudaStream_t s);
 void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
-                int child_level, cudaStream_t s);
+                int child_level, int n_pairs, cudaStream_t s);
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
                 const float4 *near, int n, int p, int K, int nt, int depth, unsigned output,
                 int layout, float phi_scale, float *field, float *potential, cudaStream_t s);

@@ -46,6 +46,9 @@ struct HostOperators {
   // Stored FP32 as [slot][alpha][beta_pad] with beta_pad = m2l_ld.
   int m2l_ld = 0;
   std::vector<float> m2l_T;
+  // The same matrices in FP64, [slot][alpha][beta] with leading dimension n
+  // (input of the BF16 hi/lo split of the tensor-core path).
+  std::vector<double> m2l_T64;
 };
 
 HostOperators build_host_operators(int p, int depth, int m2l_ld_multiple);
@@ -102,6 +105,18 @@ struct cdfmm_b200_plan {
   int8_t *basis = nullptr;     // [n][4] ax, ay, az, degree
   int p2m_chunk = 64;
   int last_K = 0;
+
+  // tensor-core M2L (split BF16): availability, shapes, buffers, tiles
+  bool tc_supported = false;
+  int tc_Kpad = 0, tc_Npad = 0, tc_stages = 0, tc_Kp_max = 0;
+  uint32_t tc_tmem_cols = 0;
+  void *tc_a_hi = nullptr, *tc_a_lo = nullptr; // [boxes + 1][Kp_max * Kpad] BF16
+  void *tc_b = nullptr;                        // [343][2][Npad * Kpad] BF16
+  int4 *tc_tiles = nullptr;
+  size_t tc_tiles_capacity = 0;
+  int tc_tiles_Kp = 0, tc_n_tiles = 0;
+  int *error_flag = nullptr;                   // device: nonzero after an expired bounded wait
+  bool last_m2l_tc = false;
 
   // state (device), sized for max_states
   float4 *mom = nullptr;       // [ns][K] sorted scaled moments

@@ -9,6 +9,12 @@ namespace cdfmm_b200 {
 // 1 / (4 pi) in FP32 (the kernel constant of G(r) = 1 / (4 pi |r|)).
 constexpr float kInvFourPiF = 0.0795774715459476678844418816862571810F;
 
+// 1/k for k = 0..15 (entry 0 unused), correctly rounded FP32: monomial
+// recurrences d^(k+1)/(k+1)! = d^k/k! * d * (1/(k+1)) multiply instead of divide.
+__constant__ constexpr float kInvInt[16] = {
+    0.0F,         1.0F,        0.5F,         1.0F / 3.0F,  0.25F,       0.2F,        1.0F / 6.0F, 1.0F / 7.0F,
+    0.125F,       1.0F / 9.0F, 0.1F,         1.0F / 11.0F, 1.0F / 12.0F, 1.0F / 13.0F, 1.0F / 14.0F, 1.0F / 15.0F};
+
 __host__ __device__ inline int basis_size_d(int p) { return p < 0 ? 0 : (p + 1) * (p + 2) * (p + 3) / 6; }
 
 // Position of multi-index (a, b, c) in the total-degree basis.
@@ -27,6 +33,23 @@ __host__ __device__ inline uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) 
     m |= ((z >> b) & 1u) << (3 * b + 2);
   }
   return m;
+}
+
+// Lets `kernel` use all opt-in shared memory left after its static shared
+// memory.  Returns false (and clears the runtime's last error) on failure.
+template <typename Kernel> inline bool allow_dynamic_smem(Kernel *kernel, size_t optin) {
+  cudaFuncAttributes attr{};
+  if (cudaFuncGetAttributes(&attr, kernel) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  const size_t room = optin > attr.sharedSizeBytes ? optin - attr.sharedSizeBytes : 0;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(room)) !=
+      cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return true;
 }
 
 __host__ __device__ inline void demorton3(uint32_t m, int &x, int &y, int &z) {

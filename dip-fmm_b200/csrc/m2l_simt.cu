@@ -170,16 +170,15 @@ void launch_m2l_simt(const float *M, float *L, const float *T, const float *scal
 }
 
 void configure_m2l_simt(size_t max_smem) {
-  const int v = static_cast<int>(max_smem);
-  cudaFuncSetAttribute(m2l_simt_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<6>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<8>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<11>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<14>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(m2l_simt_kernel<18>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+  allow_dynamic_smem(m2l_simt_kernel<1>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<2>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<3>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<4>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<6>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<8>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<11>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<14>, max_smem);
+  allow_dynamic_smem(m2l_simt_kernel<18>, max_smem);
 }
 
 } // namespace cdfmm_b200

@@ -1,0 +1,36 @@
+// Tensor-core (tcgen05) M2L: launch interface.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstddef>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+
+namespace cdfmm_b200 {
+
+struct TcArgs {
+  const uint8_t *a_hi;     // packed BF16 hi boxes [box][Kp rows][Kpad] (core-matrix tiled)
+  const uint8_t *a_lo;     // packed BF16 lo boxes
+  const uint8_t *b_tiles;  // [343 slots][hi, lo][Npad x Kpad] (core-matrix tiled)
+  const int4 *tiles;       // per CTA: (level, class, first parent Morton index, target count)
+  const float *scale_l;    // [depth+1][n] exact powers of two
+  float *L;                // [node][n][K] FP32 locals (overwritten)
+  int *error_flag;         // set nonzero if a bounded wait expired
+  int n, K, Kp, Kpad, Npad;
+  int node_base;           // flat node index of packed box 0
+  int zero_node;           // packed index of the all-zero box
+  int stages;
+  uint32_t tmem_cols;
+  uint32_t box_bytes;      // Kp * Kpad * 2
+};
+
+size_t m2l_tc_smem_bytes(int Kpad, int Npad, int stages);
+void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,
+                     int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s);
+void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s);
+bool configure_m2l_tc(size_t max_smem);
+std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, int Npad, int Kpad);
+
+} // namespace cdfmm_b200

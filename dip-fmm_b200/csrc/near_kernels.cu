@@ -363,11 +363,10 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
 }
 
 void configure_p2p(size_t max_smem) {
-  const int v = static_cast<int>(max_smem);
-  cudaFuncSetAttribute(p2p_kn_kernel<8, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(p2p_kn_kernel<8, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(p2p_kn_kernel<4, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
-  cudaFuncSetAttribute(p2p_kn_kernel<4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, v);
+  allow_dynamic_smem(p2p_kn_kernel<8, true>, max_smem);
+  allow_dynamic_smem(p2p_kn_kernel<8, false>, max_smem);
+  allow_dynamic_smem(p2p_kn_kernel<4, true>, max_smem);
+  allow_dynamic_smem(p2p_kn_kernel<4, false>, max_smem);
 }
 
 void launch_direct_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,

@@ -141,6 +141,7 @@ HostOperators build_host_operators(int p, int depth, int m2l_ld_multiple) {
   ops.m2l_ld = round_up(n, m2l_ld_multiple);
   const int ld = ops.m2l_ld;
   ops.m2l_T.assign(static_cast<std::size_t>(343) * n * ld, 0.0F);
+  if (depth >= 2) ops.m2l_T64.assign(static_cast<std::size_t>(343) * n * n, 0.0);
   if (depth >= 2) {
     const BasisTable D(2 * p);
     for (int tx = -3; tx <= 3; ++tx)
@@ -151,10 +152,13 @@ HostOperators build_host_operators(int p, int depth, int m2l_ld_multiple) {
           const std::vector<double> deriv = laplace_derivatives(2 * p, R);
           const int slot = (tx + 3) * 49 + (ty + 3) * 7 + (tz + 3);
           float *T = ops.m2l_T.data() + static_cast<std::size_t>(slot) * n * ld;
+          double *T64 = ops.m2l_T64.data() + static_cast<std::size_t>(slot) * n * n;
           for (int a = 0; a < n; ++a)
-            for (int b = 0; b < n; ++b)
-              T[static_cast<std::size_t>(a) * ld + b] = static_cast<float>(
-                  deriv[BasisTable::rank(B.ax[a] + B.ax[b], B.ay[a] + B.ay[b], B.az[a] + B.az[b])]);
+            for (int b = 0; b < n; ++b) {
+              const double v = deriv[BasisTable::rank(B.ax[a] + B.ax[b], B.ay[a] + B.ay[b], B.az[a] + B.az[b])];
+              T[static_cast<std::size_t>(a) * ld + b] = static_cast<float>(v);
+              T64[static_cast<std::size_t>(a) * n + b] = v;
+            }
         }
   }
   return ops;

@@ -21,6 +21,7 @@
 #include "far_kernels.hpp"
 #include "fmm_internal.hpp"
 #include "kernels.cuh"
+#include "m2l_tc.hpp"
 
 namespace {
 
@@ -63,7 +64,8 @@ void free_plan(cdfmm_b200_plan *p) {
   void *ptrs[] = {p->src_rel, p->tgt_rel, p->src_off, p->tgt_off, p->src_perm, p->tgt_perm,
                   p->self_idx, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
-                  p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles};
+                  p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
+                  p->tc_b, p->tc_tiles, p->error_flag};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
@@ -375,7 +377,46 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
                 sizeof(float) * static_cast<size_t>(n) * K <= smem,
             "order and max_states exceed the shared-memory budget of one CTA");
     check(cudaDeviceSynchronize(), "plan upload");
-    plan->stats.m2l_mode_resolved = plan->m2l_mode;
+    plan->error_flag = dalloc<int>(1, bytes);
+    check(cudaMemset(plan->error_flag, 0, sizeof(int)), "cudaMemset");
+
+    // Tensor-core M2L: sm_100 devices, order <= 9 (N = 16 * ceil(n/16) <= 256
+    // accumulator columns) and at least one pipeline stage in shared memory.
+    {
+      int major = 0;
+      cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, plan->device);
+      const int Kpad = round_up(n, 16);
+      const int Npad = round_up(n, 16);
+      int stages = 0;
+      while (stages < 4 && m2l_tc_smem_bytes(Kpad, Npad, stages + 1) <= std::min<size_t>(smem, 210 * 1024)) ++stages;
+      plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 1 &&
+                           desc->m2l_mode != CDFMM_B200_M2L_FP32 && desc->max_states >= 1 &&
+                           configure_m2l_tc(smem);
+      if (plan->tc_supported) {
+        plan->tc_Kpad = Kpad;
+        plan->tc_Npad = Npad;
+        plan->tc_stages = stages;
+        uint32_t cols = 32;
+        while (cols < static_cast<uint32_t>(Npad)) cols <<= 1;
+        plan->tc_tmem_cols = cols;
+        plan->tc_Kp_max = round_up(std::min(plan->max_states, 128), 8);
+        const size_t boxes = static_cast<size_t>(plan->n_nodes - level_offset(2)) + 1;
+        const size_t box_elems = static_cast<size_t>(plan->tc_Kp_max) * Kpad;
+        plan->tc_a_hi = dalloc<uint16_t>(boxes * box_elems, bytes);
+        plan->tc_a_lo = dalloc<uint16_t>(boxes * box_elems, bytes);
+        const std::vector<uint16_t> bt = pack_m2l_b_tiles(ops.m2l_T64, n, Npad, Kpad);
+        plan->tc_b = dalloc<uint16_t>(bt.size(), bytes);
+        upload(static_cast<uint16_t *>(plan->tc_b), bt.data(), bt.size(), h2d);
+      } else if (desc->m2l_mode == CDFMM_B200_M2L_BF16X3) {
+        throw AbiError(CDFMM_B200_ERR_RUNTIME,
+                       "split-BF16 tensor-core M2L needs an sm_100 device, depth >= 2 and order <= 9");
+      }
+    }
+    ops.m2l_T64.clear();
+    ops.m2l_T64.shrink_to_fit();
+    plan->m2l_mode = desc->m2l_mode;
+    plan->stats.m2l_mode_resolved = plan->tc_supported ? (desc->m2l_mode == CDFMM_B200_M2L_FP32 ? CDFMM_B200_M2L_FP32 : CDFMM_B200_M2L_BF16X3)
+                                                       : CDFMM_B200_M2L_FP32;
     *out_plan = plan;
     return CDFMM_B200_OK;
   } catch (const AbiError &e) {
@@ -393,8 +434,7 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
 void cdfmm_b200_plan_destroy(cdfmm_b200_plan *plan) {
   if (plan == nullptr) return;
   cudaSetDevice(plan->device);
-  if (plan->stream) cudaStreamSynchronize(plan->stream);
-  if (plan->near_stream) cudaStreamSynchronize(plan->near_stream);
+  cudaDeviceSynchronize();
   free_plan(plan);
 }
 
@@ -408,8 +448,7 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
     }
     for (int i = 0; i < plan->nt; ++i)
       require(sorted_self[i] >= -1 && sorted_self[i] < plan->ns, "self index out of range");
-    check(cudaStreamSynchronize(plan->near_stream), "sync");
-    check(cudaStreamSynchronize(plan->stream), "sync");
+    check(cudaDeviceSynchronize(), "sync");
     if (plan->nt > 0)
       check(cudaMemcpy(plan->self_idx, sorted_self, sizeof(int) * plan->nt, cudaMemcpyHostToDevice), "cudaMemcpy");
     plan->has_self = true;
@@ -437,10 +476,15 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     if ((a->memory & CDFMM_B200_MOMENTS_ON_HOST) == 0u)
       require(reinterpret_cast<uintptr_t>(a->moments) % (a->moments_dtype == 1 ? 8 : 4) == 0, "misaligned moments pointer");
     check(cudaSetDevice(plan->device), "cudaSetDevice");
+    // A launch error reported below must come from these launches, not from
+    // an earlier unrelated runtime call of the host process.
+    (void)cudaGetLastError();
 
     const int K = a->n_states;
     const int n = plan->n;
-    cudaStream_t s = a->stream != nullptr ? static_cast<cudaStream_t>(a->stream) : plan->stream;
+    // NULL is the legacy default stream, as everywhere in CUDA (a torch tensor
+    // on the default stream and our kernels are then ordered).
+    cudaStream_t s = static_cast<cudaStream_t>(a->stream);
     const bool host_in = (a->memory & CDFMM_B200_MOMENTS_ON_HOST) != 0u;
     const bool host_out = (a->memory & CDFMM_B200_RESULTS_ON_HOST) != 0u;
     const size_t in_bytes = static_cast<size_t>(K) * plan->ns * 3 * (a->moments_dtype == 1 ? 8 : 4);
@@ -485,15 +529,21 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     launches += plan->ns > 0 ? 1 : 0;
     if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
 
-    // near field on its own stream
-    check(cudaEventRecord(plan->ev_fork, s), "event");
-    check(cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0), "wait");
-    if (timing) check(cudaEventRecord(plan->ev_t[8], plan->near_stream), "event");
+    // Near field on its own stream, concurrent with the far field.  With
+    // stage timing enabled it runs first on the main stream instead, so that
+    // each stage's events measure that stage alone.
+    cudaStream_t ns = timing ? s : plan->near_stream;
+    if (!timing) {
+      check(cudaEventRecord(plan->ev_fork, s), "event");
+      check(cudaStreamWaitEvent(ns, plan->ev_fork, 0), "wait");
+    }
+    if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
     launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
-               plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi, plan->near, plan->near_stream);
+               plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi, plan->near, ns);
     ++launches;
-    if (timing) check(cudaEventRecord(plan->ev_t[9], plan->near_stream), "event");
-    check(cudaEventRecord(plan->ev_join, plan->near_stream), "event");
+    if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
+    if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
+    if (!timing) check(cudaEventRecord(plan->ev_join, ns), "event");
 
     // far field
     launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
@@ -501,22 +551,75 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     ++launches;
     if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
     for (int level = plan->depth - 1; level >= 0; --level) {
-      launch_m2m(plan->M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level, s);
+      launch_m2m(plan->M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level,
+                 static_cast<int>(plan->ops.m2m_pair_g.size()), s);
       ++launches;
     }
     if (timing) check(cudaEventRecord(plan->ev_t[3], s), "event");
-    if (plan->depth >= 2) {
+    const bool use_tc = plan->depth >= 2 && plan->tc_supported && K <= 128 &&
+                        (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || (plan->m2l_mode == CDFMM_B200_M2L_AUTO && K >= 8));
+    if (use_tc) {
+      const int Kp = round_up(K, 8);
+      if (plan->tc_tiles_Kp != Kp) {
+        // Work tiles: per level (deepest first) and parity class, runs of
+        // T = 128 / Kp targets (consecutive parents in Morton order).
+        const int T = 128 / Kp;
+        std::vector<int4> tiles;
+        for (int level = plan->depth; level >= 2; --level) {
+          const int parents = 1 << (3 * (level - 1));
+          for (int cls = 0; cls < 8; ++cls)
+            for (int p0 = 0; p0 < parents; p0 += T) tiles.push_back(make_int4(level, cls, p0, std::min(T, parents - p0)));
+        }
+        check(cudaStreamSynchronize(s), "sync");
+        if (plan->tc_tiles_capacity < tiles.size()) {
+          if (plan->tc_tiles) cudaFree(plan->tc_tiles);
+          plan->tc_tiles = nullptr;
+          plan->tc_tiles_capacity = 0;
+          check(cudaMalloc(&plan->tc_tiles, tiles.size() * sizeof(int4)), "cudaMalloc tiles");
+          plan->tc_tiles_capacity = tiles.size();
+        }
+        check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
+        plan->tc_tiles_Kp = Kp;
+        plan->tc_n_tiles = static_cast<int>(tiles.size());
+      }
+      const int node_base = level_offset(2);
+      const int boxes = plan->n_nodes - node_base;
+      launch_m2l_pack(plan->M, plan->scale_m, plan->basis, plan->tc_a_hi, plan->tc_a_lo, n, K, Kp, plan->tc_Kpad,
+                      plan->depth, node_base, boxes, s);
+      TcArgs ta{};
+      ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
+      ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
+      ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b);
+      ta.tiles = plan->tc_tiles;
+      ta.scale_l = plan->scale_l;
+      ta.L = plan->L;
+      ta.error_flag = plan->error_flag;
+      ta.n = n;
+      ta.K = K;
+      ta.Kp = Kp;
+      ta.Kpad = plan->tc_Kpad;
+      ta.Npad = plan->tc_Npad;
+      ta.node_base = node_base;
+      ta.zero_node = boxes;
+      ta.stages = plan->tc_stages;
+      ta.tmem_cols = plan->tc_tmem_cols;
+      ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
+      launch_m2l_tc(ta, plan->tc_n_tiles, s);
+      launches += 2;
+    } else if (plan->depth >= 2) {
       launch_m2l_simt(plan->M, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles,
                       plan->n_tiles, n, plan->ops.m2l_ld, K, s);
       ++launches;
     }
+    plan->last_m2l_tc = use_tc;
     if (timing) check(cudaEventRecord(plan->ev_t[4], s), "event");
     for (int level = 3; level <= plan->depth; ++level) {
-      launch_l2l(plan->L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level, s);
+      launch_l2l(plan->L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level,
+                 static_cast<int>(plan->ops.l2l_pair_g.size()), s);
       ++launches;
     }
     if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
-    check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
+    if (!timing) check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
     if (timing) check(cudaEventRecord(plan->ev_t[6], s), "event");
     launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->near, n, plan->p, K, plan->nt,
                plan->depth, a->output, a->layout, plan->phi_scale, field, potential, s);
@@ -536,14 +639,26 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
         plan->stats.evaluation_d2h_calls += 1;
       }
     }
-    if (a->synchronize || host_out || timing) check(cudaStreamSynchronize(s), "evaluate");
+    if (a->synchronize || host_out || timing) {
+      check(cudaStreamSynchronize(s), "evaluate");
+      if (plan->last_m2l_tc) {
+        int flag = 0;
+        check(cudaMemcpy(&flag, plan->error_flag, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+        if (flag != 0) {
+          cudaMemset(plan->error_flag, 0, sizeof(int));
+          throw AbiError(CDFMM_B200_ERR_TIMEOUT, "tensor-core M2L: a bounded wait expired (code " +
+                                                     std::to_string(flag) + "); results are invalid");
+        }
+      }
+    }
+    plan->stats.m2l_mode_resolved = plan->last_m2l_tc ? CDFMM_B200_M2L_BF16X3 : CDFMM_B200_M2L_FP32;
     if (timing) {
       auto ms = [&](int i, int j) {
         float v = 0.0F;
         cudaEventElapsedTime(&v, plan->ev_t[i], plan->ev_t[j]);
         return static_cast<double>(v);
       };
-      plan->stats.ms_gather = ms(0, 1);
+      plan->stats.ms_gather = ms(0, 8);
       plan->stats.ms_p2m = ms(1, 2);
       plan->stats.ms_m2m = ms(2, 3);
       plan->stats.ms_m2l = ms(3, 4);
@@ -573,7 +688,7 @@ int cdfmm_b200_read_expansions(const cdfmm_b200_plan *plan, int32_t which, int32
     const size_t need = static_cast<size_t>(plan->n_nodes) * plan->n;
     require(out != nullptr && out_count >= need, "output buffer too small");
     check(cudaSetDevice(plan->device), "cudaSetDevice");
-    check(cudaStreamSynchronize(plan->stream), "sync");
+    check(cudaDeviceSynchronize(), "sync");
     const int K = std::max(plan->last_K, 1);
     std::vector<float> all(need * K);
     check(cudaMemcpy(all.data(), which == 0 ? plan->M : plan->L, all.size() * sizeof(float), cudaMemcpyDeviceToHost),

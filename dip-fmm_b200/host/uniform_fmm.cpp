@@ -435,6 +435,13 @@ void UniformFmm::refresh_expansions(int which) const {
     check_plan(cdfmm_b200_read_expansions(plan_.get(), which, 0, dst.data(), dst.size()), plan_.get());
   }
   if (which == 1 && upward_only_) std::fill(dst.begin(), dst.end(), 0.0F);
+  // The reference never forms locals of boxes without targets (nor
+  // multipoles of boxes without sources): they read as zero there.
+  const std::size_t n = static_cast<std::size_t>(basis_.size());
+  for (const TreeNode &node : tree_.nodes()) {
+    const bool empty = which == 0 ? node.source_count() == 0 : node.target_count() == 0;
+    if (empty) std::fill_n(dst.begin() + static_cast<std::ptrdiff_t>(node.index * n), n, 0.0F);
+  }
   expansion_valid_[which] = true;
 }
 

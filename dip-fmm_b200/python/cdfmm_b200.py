@@ -237,20 +237,22 @@ class DevicePlan:
         return s.as_dict()
 
     def evaluate(self, moments, output="field", layout=LAYOUT_SEPARATE, field=None, potential=None,
-                 stream=None, synchronize=True):
+                 stream=None, synchronize=True, memory=None):
         """Evaluates K states.
 
         moments: (K, n_sources, 3) or (n_sources, 3) host numpy (float32 or
-        float64) or a device tensor with data_ptr().  Host inputs give host
-        results (allocated here when not supplied); device inputs need device
-        `field` / `potential` buffers.
+        float64) or a tensor with data_ptr().  numpy inputs give numpy host
+        results (allocated here when not supplied).  For tensors the caller
+        supplies `field` / `potential` and `memory` defaults to "device" for
+        CUDA tensors and "host" (pinned, ideally) for CPU tensors.
         """
         flags = {"field": OUTPUT_FIELD, "potential": OUTPUT_POTENTIAL, "both": OUTPUT_FIELD | OUTPUT_POTENTIAL}[output]
-        on_device = hasattr(moments, "data_ptr")
-        if on_device:
+        is_tensor = hasattr(moments, "data_ptr")
+        if is_tensor:
             K = int(moments.shape[0]) if len(moments.shape) == 3 else 1
             dtype = 1 if str(moments.dtype).endswith("float64") else 0
-            memory = 0
+            if memory is None:
+                memory = 0 if getattr(moments, "is_cuda", False) else MOMENTS_ON_HOST | RESULTS_ON_HOST
         else:
             moments = np.ascontiguousarray(moments)
             if moments.dtype not in (np.float32, np.float64):

@@ -97,7 +97,7 @@ typedef struct cdfmm_b200_eval_args {
   float *field;          /* see layout; required when FIELD is requested or layout is interleaved */
   float *potential;      /* [n_states][n_targets] for LAYOUT_SEPARATE with POTENTIAL, else unused */
   uint32_t memory;       /* CDFMM_B200_*_ON_HOST bits */
-  void *stream;          /* cudaStream_t to order the work on; NULL = the plan's own stream */
+  void *stream;          /* cudaStream_t to order the work on; NULL = the legacy default stream */
   int32_t synchronize;   /* nonzero: return only after results are complete */
 } cdfmm_b200_eval_args;
 
