@@ -62,6 +62,10 @@ struct Plan;
 
 } // namespace cdfmm_b200
 
+// Records `msg` as the last error of `plan` (may be NULL) and of this thread,
+// as reported by cdfmm_b200_last_error.
+void cdfmm_b200_record_error(cdfmm_b200_plan *plan, const std::string &msg);
+
 // The opaque ABI handle.
 struct cdfmm_b200_plan {
   int device = 0;

@@ -120,6 +120,11 @@ size_t device_smem_optin(int device) {
 
 } // namespace
 
+void cdfmm_b200_record_error(cdfmm_b200_plan *plan, const std::string &msg) {
+  if (plan != nullptr) plan->last_error = msg;
+  g_last_error = msg;
+}
+
 extern "C" {
 
 int cdfmm_b200_device_count(int32_t *count) {

@@ -40,7 +40,11 @@ EXPORTED = (
     "cdfmm_b200_plan_destroy", "cdfmm_b200_set_self_indices", "cdfmm_b200_evaluate",
     "cdfmm_b200_read_expansions", "cdfmm_b200_set_timing", "cdfmm_b200_get_stats",
     "cdfmm_b200_direct_fp64", "cdfmm_b200_m2l_matrix", "cdfmm_b200_last_error",
+    "cdfmm_b200_evaluate_noalloc",
 )
+
+# Scratch capacity of cdfmm_b200_evaluate_noalloc (bytes).
+NOALLOC_SCRATCH_BYTES = 64 << 20
 
 
 class PlanDesc(ctypes.Structure):
@@ -107,6 +111,7 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_plan_destroy.restype = None
     lib.cdfmm_b200_set_self_indices.argtypes = [vp, vp]
     lib.cdfmm_b200_evaluate.argtypes = [vp, ctypes.POINTER(EvalArgs)]
+    lib.cdfmm_b200_evaluate_noalloc.argtypes = [vp, ctypes.POINTER(EvalArgs)]
     lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
     lib.cdfmm_b200_set_timing.argtypes = [vp, i32]
     lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -278,6 +283,25 @@ class DevicePlan:
         a.synchronize = 1 if synchronize else 0
         _check(library().cdfmm_b200_evaluate(self._h, ctypes.byref(a)), self._h)
         return {"H": field, "phi": potential}
+
+    def evaluate_noalloc(self, moments, field, potential=None, output="field", layout=LAYOUT_SEPARATE,
+                         stream=None, synchronize=True):
+        """Allocation-free evaluation (cdfmm_b200_evaluate_noalloc) on
+        device-resident tensors; scratch comes from the library's fixed
+        64 MiB device array instead of the plan."""
+        flags = {"field": OUTPUT_FIELD, "potential": OUTPUT_POTENTIAL, "both": OUTPUT_FIELD | OUTPUT_POTENTIAL}[output]
+        a = EvalArgs()
+        a.moments = _ptr(moments).value
+        a.moments_dtype = 1 if str(moments.dtype).endswith("float64") else 0
+        a.n_states = int(moments.shape[0]) if len(moments.shape) == 3 else 1
+        a.output = flags
+        a.layout = layout
+        a.field = _ptr(field).value if field is not None else None
+        a.potential = _ptr(potential).value if potential is not None else None
+        a.memory = 0
+        a.stream = stream
+        a.synchronize = 1 if synchronize else 0
+        _check(library().cdfmm_b200_evaluate_noalloc(self._h, ctypes.byref(a)), self._h)
 
     def read_expansions(self, which="multipole", state=0) -> np.ndarray:
         out = np.zeros(self.n_nodes * self.n_coefficients, dtype=np.float32)

@@ -150,6 +150,24 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
  * potential output and device-resident arrays). */
 int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args);
 
+/* Allocation-free variant of cdfmm_b200_evaluate (no counterpart in the
+ * reference).  For callers that cannot call cudaMalloc/cudaFree while they
+ * evaluate -- a host program capturing its evaluation loop into a CUDA graph,
+ * a framework whose memory pool owns the device memory, a real-time loop
+ * that cannot take the allocator's implicit synchronisation.  Same
+ * arguments and results as cdfmm_b200_evaluate, with these limits:
+ *  - moments and results must be device-resident (args->memory == 0);
+ *  - all per-call scratch (sorted moments, expansions, near field, tensor-
+ *    core operands) lives in one fixed 64 MiB device array built into the
+ *    library, so the plan's size times n_states must fit in it; larger calls
+ *    fail with CDFMM_B200_ERR_INVALID_ARGUMENT and a message giving the need;
+ *  - the first call on a device looks up that array's device address
+ *    (cudaGetSymbolAddress): make it before any stream capture starts;
+ *  - every call shares the array: calls whose GPU work overlaps race, so
+ *    order them on one stream.
+ * The plan itself is created (and allocated) by cdfmm_b200_plan_create. */
+int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args);
+
 /* Copies the FP32 multipole (which = 0) or local (which = 1) expansions of one
  * state of the last evaluate to host memory as out[node][coefficient], node in
  * flat level-wise Morton order and coefficients in the total-degree basis
