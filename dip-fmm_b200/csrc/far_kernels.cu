@@ -18,30 +18,39 @@ namespace {
 
 // ---------------------------------------------------------------------------
 // moments: user order [K][ns][3] (f32 / f64) -> sorted [ns][K] float4 / scale^3
-// (upstream src/far_field.cpp:248-275, src/cuda_fmm.cu:56-64).
+// (upstream src/far_field.cpp:248-275, src/cuda_fmm.cu:56-64).  A CTA takes
+// 32 consecutive user indices and 32 states at a time through a shared tile:
+// the reads are contiguous runs of each state's user array, the writes
+// contiguous runs of each sorted row (inv = user -> sorted index).
 template <typename T>
-__global__ void gather_moments_kernel(const T *__restrict__ user, const int *__restrict__ perm,
-                                      int ns, int K, double inv_scale, float inv_scale3_f,
-                                      float4 *__restrict__ mom) {
-  const long long total = static_cast<long long>(ns) * K;
-  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < total;
-       q += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const int j = static_cast<int>(q / K);
-    const int k = static_cast<int>(q - static_cast<long long>(j) * K);
-    const T *m = user + (static_cast<long long>(k) * ns + perm[j]) * 3;
-    float4 v;
-    if constexpr (sizeof(T) == 8) {
-      // Same arithmetic as the reference FP32 boundary: m / s / s / s in FP64.
-      v.x = static_cast<float>(static_cast<double>(m[0]) * inv_scale * inv_scale * inv_scale);
-      v.y = static_cast<float>(static_cast<double>(m[1]) * inv_scale * inv_scale * inv_scale);
-      v.z = static_cast<float>(static_cast<double>(m[2]) * inv_scale * inv_scale * inv_scale);
-    } else {
-      v.x = static_cast<float>(m[0]) * inv_scale3_f;
-      v.y = static_cast<float>(m[1]) * inv_scale3_f;
-      v.z = static_cast<float>(m[2]) * inv_scale3_f;
+__global__ void __launch_bounds__(256) gather_moments_kernel(const T *__restrict__ user, const int *__restrict__ inv,
+                                                             int ns, int K, double inv_scale, float inv_scale3_f,
+                                                             float4 *__restrict__ mom) {
+  __shared__ float tile[32][32 * 3 + 1]; // [user][state * 3 + component]
+  const int u0 = blockIdx.x * 32;
+  const int nu = min(32, ns - u0);
+  for (int kc = 0; kc < K; kc += 32) {
+    const int kn = min(32, K - kc);
+    for (int e = threadIdx.x; e < kn * nu * 3; e += blockDim.x) {
+      const int k = e / (nu * 3);
+      const int r = e - k * nu * 3;
+      const int t = r / 3;
+      const T v = user[(static_cast<long long>(kc + k) * ns + u0) * 3 + r];
+      float f;
+      if constexpr (sizeof(T) == 8)
+        f = static_cast<float>(static_cast<double>(v) * inv_scale * inv_scale * inv_scale); // m / s / s / s in FP64
+      else
+        f = static_cast<float>(v) * inv_scale3_f;
+      tile[t][3 * k + (r - 3 * t)] = f;
     }
-    v.w = 0.0F;
-    mom[q] = v;
+    __syncthreads();
+    for (int e = threadIdx.x; e < nu * kn; e += blockDim.x) {
+      const int t = e / kn;
+      const int k = e - t * kn;
+      mom[static_cast<long long>(inv[u0 + t]) * K + kc + k] =
+          make_float4(tile[t][3 * k], tile[t][3 * k + 1], tile[t][3 * k + 2], 0.0F);
+    }
+    __syncthreads();
   }
 }
 
@@ -65,53 +74,104 @@ __device__ inline void monomials(float dx, float dy, float dz, int q, float *out
 // ---------------------------------------------------------------------------
 // P2M (upstream docs/math.md P2M; src/static_operators.cpp:186-220):
 //   M_alpha = (-1)^|alpha| sum_j sum_{k: alpha_k > 0} m_jk d_j^(alpha-e_k)/(alpha-e_k)!
-// One CTA per leaf.  Accumulators for the leaf (n*K) live in shared memory,
-// each owned by one thread; sources are staged in chunks with their
-// monomials of degree <= p-1 precomputed once per source.
-__global__ void p2m_kernel(const float4 *__restrict__ src_rel, const float4 *__restrict__ mom,
-                           const int *__restrict__ src_off, const int8_t *__restrict__ basis,
-                           float *__restrict__ M, int n, int p, int K, int leaf_node_base, int chunk) {
-  extern __shared__ float smem[];
+// computed per leaf as three small GEMMs
+//   P_c[mu][s] = sum_j m_jcs d_j^mu / mu!        (|mu| <= p-1, s = state)
+//   M_alpha[s] = (-1)^|alpha| sum_{c: alpha_c > 0} P_c[alpha - e_c][s].
+// One CTA per leaf.  Sources are staged in chunks (monomials [j][mu] and
+// moments [j][s]); a thread owns a register tile of 4 consecutive mu x 4
+// states (s = kb, kb + Kq, ...; consecutive lanes take consecutive kb, so the
+// float4 moment loads are conflict-free and the monomial quad a broadcast)
+// and adds it into P in shared memory after each chunk.  States are handled
+// in blocks of Kb so P fits in shared memory for any K.
+constexpr int kP2mThreads = 256;
+constexpr int kP2mChunk = 32;
+
+__global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restrict__ src_rel,
+                                                          const float4 *__restrict__ mom,
+                                                          const int *__restrict__ src_off,
+                                                          const int8_t *__restrict__ basis, float *__restrict__ M,
+                                                          int n, int p, int K, int leaf_node_base, int Kb) {
+  extern __shared__ float4 p2m_smem[];
   const int nm1 = basis_size_d(p - 1);
-  float *acc = smem;                                  // [n*K], padded to 16 bytes
-  float *mono = acc + ((n * K + 3) & ~3);             // [chunk][nm1]
-  float4 *smom = reinterpret_cast<float4 *>(mono + ((chunk * nm1 + 3) & ~3)); // [chunk][K]
+  const int nm1p = (nm1 + 3) & ~3;
+  float4 *smom = p2m_smem;                                              // [chunk][Kc]
+  float *P = reinterpret_cast<float *>(smom + kP2mChunk * Kb);          // [3][nm1p][Kc]
+  float *mono = P + 3 * nm1p * Kb;                                      // [chunk][nm1p]
+  const int tid = threadIdx.x;
   const int leaf = blockIdx.x;
   const int s0 = src_off[leaf];
   const int s1 = src_off[leaf + 1];
-  const int items = n * K;
-  for (int q = threadIdx.x; q < items; q += blockDim.x) acc[q] = 0.0F;
-  for (int c0 = s0; c0 < s1; c0 += chunk) {
-    const int cn = min(chunk, s1 - c0);
-    __syncthreads();
-    for (int j = threadIdx.x; j < cn; j += blockDim.x) {
-      const float4 d = src_rel[c0 + j];
-      if (nm1 > 0) monomials(d.x, d.y, d.z, p - 1, mono + j * nm1);
-    }
-    for (int q = threadIdx.x; q < cn * K; q += blockDim.x) smom[q] = mom[static_cast<long long>(c0) * K + q];
-    __syncthreads();
-    for (int q = threadIdx.x; q < items; q += blockDim.x) {
-      const int a = q / K;
-      const int k = q - a * K;
-      const int ax = basis[4 * a], ay = basis[4 * a + 1], az = basis[4 * a + 2];
-      if (ax + ay + az == 0) continue;
-      const int ix = ax > 0 ? rank3(ax - 1, ay, az) : -1;
-      const int iy = ay > 0 ? rank3(ax, ay - 1, az) : -1;
-      const int iz = az > 0 ? rank3(ax, ay, az - 1) : -1;
-      float v = 0.0F;
-      for (int j = 0; j < cn; ++j) {
-        const float4 m = smom[j * K + k];
-        const float *mj = mono + j * nm1;
-        if (ix >= 0) v = fmaf(m.x, mj[ix], v);
-        if (iy >= 0) v = fmaf(m.y, mj[iy], v);
-        if (iz >= 0) v = fmaf(m.z, mj[iz], v);
+  float *out = M + static_cast<long long>(leaf_node_base + leaf) * n * K;
+  for (int kblk = 0; kblk < K; kblk += Kb) {
+    const int Kc = min(Kb, K - kblk);
+    const int Kq = (Kc + 3) >> 2;
+    const int tiles = (nm1p >> 2) * Kq;
+    for (int q = tid; q < 3 * nm1p * Kc; q += kP2mThreads) P[q] = 0.0F;
+    for (int c0 = s0; c0 < s1; c0 += kP2mChunk) {
+      const int cn = min(kP2mChunk, s1 - c0);
+      __syncthreads();
+      for (int j = tid; j < cn; j += kP2mThreads) {
+        const float4 d = src_rel[c0 + j];
+        if (nm1 > 0) monomials(d.x, d.y, d.z, p - 1, mono + j * nm1p);
+        for (int q = nm1; q < nm1p; ++q) mono[j * nm1p + q] = 0.0F;
       }
-      acc[q] += ((ax + ay + az) & 1) ? -v : v;
+      for (int q = tid; q < cn * Kc; q += kP2mThreads) {
+        const int j = q / Kc;
+        const int k = q - j * Kc;
+        smom[q] = mom[static_cast<long long>(c0 + j) * K + kblk + k];
+      }
+      __syncthreads();
+      for (int t = tid; t < tiles; t += kP2mThreads) {
+        const int mb = t / Kq;
+        const int kb = t - mb * Kq;
+        const int mu0 = mb * 4;
+        float acc[3][4][4];
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+#pragma unroll
+          for (int u = 0; u < 4; ++u)
+#pragma unroll
+            for (int kk = 0; kk < 4; ++kk) acc[c][u][kk] = 0.0F;
+        for (int j = 0; j < cn; ++j) {
+          const float4 mo = *reinterpret_cast<const float4 *>(mono + j * nm1p + mu0);
+          const float mv[4] = {mo.x, mo.y, mo.z, mo.w};
+#pragma unroll
+          for (int kk = 0; kk < 4; ++kk) {
+            const int k = kb + kk * Kq;
+            const float4 m = k < Kc ? smom[j * Kc + k] : make_float4(0, 0, 0, 0);
+#pragma unroll
+            for (int u = 0; u < 4; ++u) {
+              acc[0][u][kk] = fmaf(m.x, mv[u], acc[0][u][kk]);
+              acc[1][u][kk] = fmaf(m.y, mv[u], acc[1][u][kk]);
+              acc[2][u][kk] = fmaf(m.z, mv[u], acc[2][u][kk]);
+            }
+          }
+        }
+#pragma unroll
+        for (int kk = 0; kk < 4; ++kk) {
+          const int k = kb + kk * Kq;
+          if (k < Kc) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c)
+#pragma unroll
+              for (int u = 0; u < 4; ++u) P[(c * nm1p + mu0 + u) * Kc + k] += acc[c][u][kk];
+          }
+        }
+      }
     }
+    __syncthreads();
+    for (int q = tid; q < n * Kc; q += kP2mThreads) {
+      const int a = q / Kc;
+      const int k = q - a * Kc;
+      const int ax = basis[4 * a], ay = basis[4 * a + 1], az = basis[4 * a + 2];
+      float v = 0.0F;
+      if (ax > 0) v += P[(0 * nm1p + rank3(ax - 1, ay, az)) * Kc + k];
+      if (ay > 0) v += P[(1 * nm1p + rank3(ax, ay - 1, az)) * Kc + k];
+      if (az > 0) v += P[(2 * nm1p + rank3(ax, ay, az - 1)) * Kc + k];
+      out[static_cast<long long>(a) * K + kblk + k] = ((ax + ay + az) & 1) ? -v : v;
+    }
+    __syncthreads();
   }
-  __syncthreads();
-  float *out = M + static_cast<long long>(leaf_node_base + leaf) * items;
-  for (int q = threadIdx.x; q < items; q += blockDim.x) out[q] = acc[q];
 }
 
 // ---------------------------------------------------------------------------
@@ -197,84 +257,237 @@ __global__ void __launch_bounds__(256) l2l_kernel(float *__restrict__ L, const i
 
 // ---------------------------------------------------------------------------
 // L2P + combine + unsort (upstream docs/math.md L2P; src/cuda_fmm.cu:503-516):
-//   phi = sum_b L_b dx^b/b!,  H_k = -sum_{b_k > 0} L_b dx^(b-e_k)/(b-e_k)!
+//   phi = sum_b L_b dx^b/b!,  H_c = -sum_{|mu| <= p-1} L_{mu+e_c} dx^mu/mu!
 // then result = far + near (near from the P2P kernel), phi times the root
 // width, written at the target's user index.  One CTA per leaf; the leaf's
-// local expansion (n*K) is staged in shared memory; a thread owns
-// (target, group of up to 4 states).
-__global__ void l2p_kernel(const float *__restrict__ L, const float4 *__restrict__ tgt_rel,
-                           const int *__restrict__ tgt_off, const int *__restrict__ tgt_perm,
-                           const float4 *__restrict__ near, int n, int p, int K, int nt,
-                           int leaf_node_base, unsigned output, int layout, float phi_scale,
-                           float *__restrict__ field, float *__restrict__ potential) {
-  extern __shared__ float sL[]; // [n][K]
+// local expansion (n x Kc states, a state block) and the monomials of up to
+// 32 targets ([b][t]) are staged in shared memory; a thread owns a register
+// tile of 4 targets x 4 consecutive states, reading float4 quads of both
+// (consecutive lanes take consecutive state quads of the same target quad:
+// conflict-free L loads, broadcast monomial loads).
+constexpr int kL2pThreads = 128;
+constexpr int kL2pTargets = 32;
+
+__device__ inline void monomials_strided(float dx, float dy, float dz, int q, float *out, int stride) {
+  float xa = 1.0F;
+  for (int a = 0; a <= q; ++a) {
+    float xb = xa;
+    for (int b = 0; a + b <= q; ++b) {
+      float xc = xb;
+      for (int c = 0; a + b + c <= q; ++c) {
+        out[rank3(a, b, c) * stride] = xc;
+        xc = xc * dz * kInvInt[c + 1];
+      }
+      xb = xb * dy * kInvInt[b + 1];
+    }
+    xa = xa * dx * kInvInt[a + 1];
+  }
+}
+
+__global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restrict__ L, const float4 *__restrict__ tgt_rel,
+                                                          const int *__restrict__ tgt_off, const int *__restrict__ tgt_perm,
+                                                          const float4 *__restrict__ near,
+                                                          const int8_t *__restrict__ basis, int n, int p, int K, int nt,
+                                                          int leaf_node_base, unsigned output, int layout,
+                                                          float phi_scale, float *__restrict__ field,
+                                                          float *__restrict__ potential, int Kb) {
+  extern __shared__ float4 l2p_smem[];
+  const int Kbp = (Kb + 3) & ~3;
+  float *sL = reinterpret_cast<float *>(l2p_smem);                 // [n][Kcp]
+  float *mono = sL + n * Kbp;                                      // [n][kL2pTargets]
+  short *sidx = reinterpret_cast<short *>(mono + n * kL2pTargets); // [nm1][3] rank of mu + e_c
+  const int tid = threadIdx.x;
+  const int leaf = blockIdx.x;
+  const int t0 = tgt_off[leaf];
+  const int t1 = tgt_off[leaf + 1];
+  if (t0 == t1) return;
+  const int nm1 = basis_size_d(p - 1);
+  for (int q = tid; q < nm1; q += kL2pThreads) {
+    const int a = basis[4 * q], b = basis[4 * q + 1], c = basis[4 * q + 2];
+    sidx[3 * q] = static_cast<short>(rank3(a + 1, b, c));
+    sidx[3 * q + 1] = static_cast<short>(rank3(a, b + 1, c));
+    sidx[3 * q + 2] = static_cast<short>(rank3(a, b, c + 1));
+  }
+  const bool want_phi = (output & 1u) != 0u;
+  const bool want_h = (output & 2u) != 0u;
+  const float *src = L + static_cast<long long>(leaf_node_base + leaf) * n * K;
+  for (int kblk = 0; kblk < K; kblk += Kb) {
+    const int Kc = min(Kb, K - kblk);
+    const int Kcp = (Kc + 3) & ~3;
+    const int Kq = Kcp >> 2;
+    __syncthreads();
+    for (int q = tid; q < n * Kcp; q += kL2pThreads) {
+      const int b = q / Kcp;
+      const int k = q - b * Kcp;
+      sL[q] = k < Kc ? src[static_cast<long long>(b) * K + kblk + k] : 0.0F;
+    }
+    for (int tc = t0; tc < t1; tc += kL2pTargets) {
+      const int tn = min(kL2pTargets, t1 - tc);
+      __syncthreads();
+      for (int t = tid; t < kL2pTargets; t += kL2pThreads) {
+        if (t < tn) {
+          const float4 d = tgt_rel[tc + t];
+          monomials_strided(d.x, d.y, d.z, p, mono + t, kL2pTargets);
+        } else {
+          for (int b = 0; b < n; ++b) mono[b * kL2pTargets + t] = 0.0F;
+        }
+      }
+      __syncthreads();
+      const int tiles = ((tn + 3) >> 2) * Kq;
+      for (int tile = tid; tile < tiles; tile += kL2pThreads) {
+        const int tq = tile / Kq;
+        const int kq = tile - tq * Kq;
+        float ph[4][4], hx[4][4], hy[4][4], hz[4][4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) ph[u][v] = hx[u][v] = hy[u][v] = hz[u][v] = 0.0F;
+        const float *mq = mono + 4 * tq;
+        const float *lq = sL + 4 * kq;
+        if (want_phi) {
+          for (int b = 0; b < n; ++b) {
+            const float4 mo = *reinterpret_cast<const float4 *>(mq + b * kL2pTargets);
+            const float4 l = *reinterpret_cast<const float4 *>(lq + b * Kcp);
+            const float mv[4] = {mo.x, mo.y, mo.z, mo.w};
+            const float lv[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+              for (int v = 0; v < 4; ++v) ph[u][v] = fmaf(mv[u], lv[v], ph[u][v]);
+          }
+        }
+        if (want_h) {
+          for (int mu = 0; mu < nm1; ++mu) {
+            const float4 mo = *reinterpret_cast<const float4 *>(mq + mu * kL2pTargets);
+            const float4 lx = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu] * Kcp);
+            const float4 ly = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu + 1] * Kcp);
+            const float4 lz = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu + 2] * Kcp);
+            const float mv[4] = {mo.x, mo.y, mo.z, mo.w};
+            const float xv[4] = {lx.x, lx.y, lx.z, lx.w};
+            const float yv[4] = {ly.x, ly.y, ly.z, ly.w};
+            const float zv[4] = {lz.x, lz.y, lz.z, lz.w};
+#pragma unroll
+            for (int u = 0; u < 4; ++u)
+#pragma unroll
+              for (int v = 0; v < 4; ++v) {
+                hx[u][v] = fmaf(mv[u], xv[v], hx[u][v]);
+                hy[u][v] = fmaf(mv[u], yv[v], hy[u][v]);
+                hz[u][v] = fmaf(mv[u], zv[v], hz[u][v]);
+              }
+          }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+          const int t = 4 * tq + u;
+          if (t >= tn) break;
+          const int i = tc + t;
+          const int usr = tgt_perm[i];
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const int kl = 4 * kq + v;
+            if (kl >= Kc) break;
+            const int k = kblk + kl;
+            const float4 nr = near[static_cast<long long>(i) * K + k];
+            const float rphi = want_phi ? (ph[u][v] + nr.x) * phi_scale : 0.0F;
+            const float rx = want_h ? nr.y - hx[u][v] : 0.0F;
+            const float ry = want_h ? nr.z - hy[u][v] : 0.0F;
+            const float rz = want_h ? nr.w - hz[u][v] : 0.0F;
+            const long long o = static_cast<long long>(k) * nt + usr;
+            if (layout == 1) {
+              reinterpret_cast<float4 *>(field)[o] = make_float4(rphi, rx, ry, rz);
+            } else {
+              if (want_h) {
+                field[3 * o] = rx;
+                field[3 * o + 1] = ry;
+                field[3 * o + 2] = rz;
+              }
+              if (want_phi && potential != nullptr) potential[o] = rphi;
+            }
+          }
+        }
+      }
+    }
+  }
+}
+
+// Position gradient of L = sum_k w_k . H_k (reverse mode; no counterpart in
+// the reference).  H_k = -grad phi_k, so dL/dx_m = -sum_k sum_l w_kl d_l d_m phi_k
+// and, from phi = sum_b L_b dx^b/b!,
+//   d_l d_m phi = sum_{|g| <= p-2} L_{g + e_l + e_m} dx^g/g!
+// (the exact derivative of the evaluated polynomial).  Four lanes share a
+// target and split its states (k = lane quarter mod 4); their sums are
+// combined with shuffles, then the near partial sums of the P2P gradient
+// kernel are added and the total is scaled to physical units.
+__global__ void __launch_bounds__(128) l2p_grad_kernel(const float *__restrict__ L, const float4 *__restrict__ tgt_rel,
+                                                       const int *__restrict__ tgt_off, const int *__restrict__ tgt_perm,
+                                                       const float4 *__restrict__ W, const float4 *__restrict__ gpart,
+                                                       int G, int n, int p, int K, int leaf_node_base,
+                                                       float inv_scale, float *__restrict__ out, int Kb) {
+  extern __shared__ float sLg[]; // [n][Kc], one state block
   const int leaf = blockIdx.x;
   const int t0 = tgt_off[leaf];
   const int t1 = tgt_off[leaf + 1];
   if (t0 == t1) return;
   const float *src = L + static_cast<long long>(leaf_node_base + leaf) * n * K;
-  for (int q = threadIdx.x; q < n * K; q += blockDim.x) sL[q] = src[q];
-  __syncthreads();
-  const bool want_phi = (output & 1u) != 0u;
-  const bool want_h = (output & 2u) != 0u;
-  const int groups = (K + 3) / 4;
-  const int items = (t1 - t0) * groups;
-  for (int it = threadIdx.x; it < items; it += blockDim.x) {
-    const int g = it / (t1 - t0);
-    const int i = t0 + (it - g * (t1 - t0));
-    const int kb = g * 4;
-    const int kn = min(4, K - kb);
+  const int items = (t1 - t0) * 4;
+  for (int base = 0; base < items; base += blockDim.x) {
+    const int it = base + threadIdx.x;
+    const bool valid = it < items;
+    const int i = t0 + (valid ? it >> 2 : 0);
+    const int q4 = it & 3;
     const float4 d = tgt_rel[i];
-    float phi[4] = {0, 0, 0, 0}, hx[4] = {0, 0, 0, 0}, hy[4] = {0, 0, 0, 0}, hz[4] = {0, 0, 0, 0};
-    float xa = 1.0F;
-    for (int a = 0; a <= p; ++a) {
-      float xb = xa;
-      for (int b = 0; a + b <= p; ++b) {
-        float xc = xb;
-        for (int c = 0; a + b + c <= p; ++c) {
-          const int deg = a + b + c;
-          const float *l0 = sL + rank3(a, b, c) * K + kb;
-          const float *lx = deg < p ? sL + rank3(a + 1, b, c) * K + kb : nullptr;
-          const float *ly = deg < p ? sL + rank3(a, b + 1, c) * K + kb : nullptr;
-          const float *lz = deg < p ? sL + rank3(a, b, c + 1) * K + kb : nullptr;
-#pragma unroll
-          for (int s = 0; s < 4; ++s) {
-            if (s < kn) {
-              if (want_phi) phi[s] = fmaf(l0[s], xc, phi[s]);
-              if (want_h && deg < p) {
-                hx[s] = fmaf(lx[s], xc, hx[s]);
-                hy[s] = fmaf(ly[s], xc, hy[s]);
-                hz[s] = fmaf(lz[s], xc, hz[s]);
-              }
+    float g0 = 0.0F, g1 = 0.0F, g2 = 0.0F;
+    for (int kblk = 0; kblk < K; kblk += Kb) {
+      const int Kc = min(Kb, K - kblk);
+      __syncthreads();
+      for (int q = threadIdx.x; q < n * Kc; q += blockDim.x) {
+        const int b = q / Kc;
+        sLg[q] = src[static_cast<long long>(b) * K + kblk + (q - b * Kc)];
+      }
+      __syncthreads();
+      if (!valid || p < 2) continue;
+      for (int kl = q4; kl < Kc; kl += 4) {
+        const float4 w = W[static_cast<long long>(i) * K + kblk + kl];
+        float xa = 1.0F;
+        for (int a = 0; a <= p - 2; ++a) {
+          float xb = xa;
+          for (int b = 0; a + b <= p - 2; ++b) {
+            float xc = xb;
+            for (int c = 0; a + b + c <= p - 2; ++c) {
+              const float lxx = sLg[rank3(a + 2, b, c) * Kc + kl];
+              const float lxy = sLg[rank3(a + 1, b + 1, c) * Kc + kl];
+              const float lxz = sLg[rank3(a + 1, b, c + 1) * Kc + kl];
+              const float lyy = sLg[rank3(a, b + 2, c) * Kc + kl];
+              const float lyz = sLg[rank3(a, b + 1, c + 1) * Kc + kl];
+              const float lzz = sLg[rank3(a, b, c + 2) * Kc + kl];
+              g0 = fmaf(-xc, fmaf(w.x, lxx, fmaf(w.y, lxy, w.z * lxz)), g0);
+              g1 = fmaf(-xc, fmaf(w.x, lxy, fmaf(w.y, lyy, w.z * lyz)), g1);
+              g2 = fmaf(-xc, fmaf(w.x, lxz, fmaf(w.y, lyz, w.z * lzz)), g2);
+              xc = xc * d.z * kInvInt[c + 1];
             }
+            xb = xb * d.y * kInvInt[b + 1];
           }
-          xc = xc * d.z * kInvInt[c + 1];
+          xa = xa * d.x * kInvInt[a + 1];
         }
-        xb = xb * d.y * kInvInt[b + 1];
       }
-      xa = xa * d.x * kInvInt[a + 1];
     }
-    const int u = tgt_perm[i];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-      if (s >= kn) break;
-      const int k = kb + s;
-      const float4 nr = near[static_cast<long long>(i) * K + k];
-      const float rphi = want_phi ? (phi[s] + nr.x) * phi_scale : 0.0F;
-      const float rx = want_h ? nr.y - hx[s] : 0.0F;
-      const float ry = want_h ? nr.z - hy[s] : 0.0F;
-      const float rz = want_h ? nr.w - hz[s] : 0.0F;
-      const long long o = static_cast<long long>(k) * nt + u;
-      if (layout == 1) {
-        reinterpret_cast<float4 *>(field)[o] = make_float4(rphi, rx, ry, rz);
-      } else {
-        if (want_h) {
-          field[3 * o] = rx;
-          field[3 * o + 1] = ry;
-          field[3 * o + 2] = rz;
-        }
-        if (want_phi && potential != nullptr) potential[o] = rphi;
+    for (int o = 1; o < 4; o <<= 1) {
+      g0 += __shfl_xor_sync(0xffffffffu, g0, o);
+      g1 += __shfl_xor_sync(0xffffffffu, g1, o);
+      g2 += __shfl_xor_sync(0xffffffffu, g2, o);
+    }
+    if (valid && q4 == 0) {
+      for (int gi = 0; gi < G; ++gi) {
+        const float4 v = gpart[static_cast<long long>(i) * G + gi];
+        g0 += v.x;
+        g1 += v.y;
+        g2 += v.z;
       }
+      const int u = tgt_perm[i];
+      out[3 * static_cast<long long>(u)] = g0 * inv_scale;
+      out[3 * static_cast<long long>(u) + 1] = g1 * inv_scale;
+      out[3 * static_cast<long long>(u) + 2] = g2 * inv_scale;
     }
   }
 }
@@ -285,31 +498,41 @@ __global__ void l2p_kernel(const float *__restrict__ L, const float4 *__restrict
 // Host launchers
 // ---------------------------------------------------------------------------
 
-void launch_gather_moments(const void *user, int dtype, const int *perm, int ns, int K,
+void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, int K,
                            double scale, float4 *mom, cudaStream_t s) {
   if (ns == 0) return;
-  const long long total = static_cast<long long>(ns) * K;
-  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 16));
-  const double inv = 1.0 / scale;
-  const float inv3f = static_cast<float>(inv * inv * inv);
+  const int blocks = (ns + 31) / 32;
+  const double invs = 1.0 / scale;
+  const float inv3f = static_cast<float>(invs * invs * invs);
   if (dtype == 1)
-    gather_moments_kernel<double><<<blocks, 256, 0, s>>>(static_cast<const double *>(user), perm, ns, K, inv, inv3f, mom);
+    gather_moments_kernel<double><<<blocks, 256, 0, s>>>(static_cast<const double *>(user), inv, ns, K, invs, inv3f, mom);
   else
-    gather_moments_kernel<float><<<blocks, 256, 0, s>>>(static_cast<const float *>(user), perm, ns, K, inv, inv3f, mom);
+    gather_moments_kernel<float><<<blocks, 256, 0, s>>>(static_cast<const float *>(user), inv, ns, K, invs, inv3f, mom);
+}
+
+// State block of the P2M kernel for K states: the largest of 64, 32, ...
+// (<= K) whose shared memory stays within 100 KB (two CTAs per SM).
+static int p2m_state_block(int p, int K) {
+  int Kb = std::min(K, 64);
+  while (Kb > 4 && p2m_smem_bytes(0, p, Kb, 0) > 100 * 1024) Kb = (Kb + 1) / 2;
+  return Kb;
 }
 
 size_t p2m_smem_bytes(int n, int p, int K, int chunk) {
-  const int nm1 = basis_size_d(p - 1);
-  return sizeof(float) * (((static_cast<size_t>(n) * K + 3) & ~static_cast<size_t>(3)) + ((chunk * nm1 + 3) & ~3)) +
-         sizeof(float4) * static_cast<size_t>(chunk) * K;
+  (void)n;
+  (void)chunk;
+  const int nm1p = (basis_size_d(p - 1) + 3) & ~3;
+  const size_t Kb = static_cast<size_t>(std::min(K, 64));
+  return sizeof(float4) * kP2mChunk * Kb + sizeof(float) * (3 * nm1p * Kb + static_cast<size_t>(kP2mChunk) * nm1p);
 }
 
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
                 float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s) {
+  (void)chunk;
   const int leaves = 1 << (3 * depth);
-  const size_t smem = p2m_smem_bytes(n, p, K, chunk);
-  p2m_kernel<<<leaves, 128, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K,
-                                       level_offset_d(depth), chunk);
+  const int Kb = p2m_state_block(p, K);
+  const size_t smem = p2m_smem_bytes(n, p, Kb, 0);
+  p2m_kernel<<<leaves, kP2mThreads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb);
 }
 
 static size_t pair_smem(int n, int n_pairs) {
@@ -332,17 +555,37 @@ void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *co
                                                                               child_level, n_pairs);
 }
 
+size_t l2p_smem_bytes(int n, int p, int Kb) {
+  const int Kbp = (Kb + 3) & ~3;
+  return sizeof(float) * (static_cast<size_t>(n) * Kbp + static_cast<size_t>(n) * kL2pTargets) +
+         sizeof(short) * 3 * static_cast<size_t>(basis_size_d(p - 1)) + 16;
+}
+
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
-                const float4 *near, int n, int p, int K, int nt, int depth, unsigned output,
+                const float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
                 int layout, float phi_scale, float *field, float *potential, cudaStream_t s) {
   const int leaves = 1 << (3 * depth);
-  const size_t smem = sizeof(float) * static_cast<size_t>(n) * K;
-  l2p_kernel<<<leaves, 128, smem, s>>>(L, tgt_rel, tgt_off, tgt_perm, near, n, p, K, nt,
-                                       level_offset_d(depth), output, layout, phi_scale, field,
-                                       potential);
+  int Kb = std::min(K, 64);
+  while (Kb > 4 && l2p_smem_bytes(n, p, Kb) > 60 * 1024) Kb = (Kb + 1) / 2;
+  const size_t smem = l2p_smem_bytes(n, p, Kb);
+  l2p_kernel<<<leaves, kL2pThreads, smem, s>>>(L, tgt_rel, tgt_off, tgt_perm, near, basis, n, p, K, nt,
+                                               level_offset_d(depth), output, layout, phi_scale, field, potential, Kb);
+}
+
+void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
+                     const float4 *W, const float4 *gpart, int G, int n, int p, int K, int nt, int depth,
+                     float inv_scale, float *out, cudaStream_t s) {
+  if (nt == 0) return;
+  const int leaves = 1 << (3 * depth);
+  int Kb = std::min(K, 64);
+  while (Kb > 4 && sizeof(float) * static_cast<size_t>(n) * Kb > 48 * 1024) Kb = (Kb + 1) / 2;
+  const size_t smem = sizeof(float) * static_cast<size_t>(n) * Kb;
+  l2p_grad_kernel<<<leaves, 128, smem, s>>>(L, tgt_rel, tgt_off, tgt_perm, W, gpart, G, n, p, K, level_offset_d(depth),
+                                            inv_scale, out, Kb);
 }
 
 void configure_far_kernels(size_t max_smem) {
+  allow_dynamic_smem(l2p_grad_kernel, max_smem);
   allow_dynamic_smem(p2m_kernel, max_smem);
   allow_dynamic_smem(l2p_kernel, max_smem);
   allow_dynamic_smem(m2m_kernel, max_smem);

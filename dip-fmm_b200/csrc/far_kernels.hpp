@@ -9,7 +9,8 @@
 
 namespace cdfmm_b200 {
 
-void launch_gather_moments(const void *user, int dtype, const int *perm, int ns, int K,
+// inv: user index -> sorted index.
+void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, int K,
                            double scale, float4 *mom, cudaStream_t s);
 size_t p2m_smem_bytes(int n, int p, int K, int chunk);
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
@@ -18,8 +19,9 @@ void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *co
                 int parent_level, int n_pairs, cudaStream_t s);
 void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
                 int child_level, int n_pairs, cudaStream_t s);
+size_t l2p_smem_bytes(int n, int p, int Kb);
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
-                const float4 *near, int n, int p, int K, int nt, int depth, unsigned output,
+                const float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
                 int layout, float phi_scale, float *field, float *potential, cudaStream_t s);
 void configure_far_kernels(size_t max_smem);
 
@@ -35,6 +37,17 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s);
 void configure_p2p(size_t max_smem);
+// Position gradient of sum_k W_k . H_k, near part: partial sums per state
+// group, gpart[nt][p2p_grad_groups(K)] (normalised units, 1/(4 pi) applied).
+int p2p_grad_groups(int K);
+void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
+                     const int *tgt_off, const int *self_idx, int depth, int K, const float4 *W, float4 *gpart,
+                     cudaStream_t s);
+// Far part (second derivatives of the leaf local expansions) plus the near
+// partial sums, scaled by inv_scale, written as out[user target][3].
+void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
+                     const float4 *W, const float4 *gpart, int G, int n, int p, int K, int nt, int depth,
+                     float inv_scale, float *out, cudaStream_t s);
 
 // FP64 direct sum (validation reference).
 void launch_direct_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,

@@ -95,6 +95,8 @@ struct cdfmm_b200_plan {
   int *tgt_off = nullptr;      // [n_leaves + 1]
   int *src_perm = nullptr;     // [ns] sorted -> user
   int *tgt_perm = nullptr;     // [nt]
+  int *src_inv = nullptr;      // [ns] user -> sorted
+  int *tgt_inv = nullptr;      // [nt]
   int *self_idx = nullptr;     // [nt] sorted target -> sorted source, -1 none
 
   // operators (device)
@@ -113,9 +115,10 @@ struct cdfmm_b200_plan {
   // tensor-core M2L (split BF16): availability, shapes, buffers, tiles
   bool tc_supported = false;
   int tc_Kpad = 0, tc_Npad = 0, tc_stages = 0, tc_Kp_max = 0;
+  int tc_m_tiles = 1, tc_acc_stride = 0; // accumulators per CTA, TMEM columns apart
   uint32_t tc_tmem_cols = 0;
   void *tc_a_hi = nullptr, *tc_a_lo = nullptr; // [boxes + 1][Kp_max * Kpad] BF16
-  void *tc_b = nullptr;                        // [343][2][Npad * Kpad] BF16
+  void *tc_b = nullptr;                        // [343][Kpad/32][2][Npad * 32] BF16
   int4 *tc_tiles = nullptr;
   size_t tc_tiles_capacity = 0;
   int tc_tiles_Kp = 0, tc_n_tiles = 0;
@@ -131,6 +134,21 @@ struct cdfmm_b200_plan {
   size_t stage_in_bytes = 0;
   void *stage_out = nullptr;   // device results before D2H
   size_t stage_out_bytes = 0;
+
+  // reverse mode: host copy of the sorted geometry (to build the transposed
+  // plan on first use), that plan -- its sources are this plan's targets and
+  // vice versa -- and the buffers of the position gradient
+  std::vector<double> h_src_pos, h_tgt_pos;    // [n][3] Morton-sorted
+  std::vector<int> h_src_perm, h_tgt_perm, h_src_off, h_tgt_off;
+  std::vector<int> h_self;                     // sorted self map as last set (empty: none)
+  int self_version = 0;                        // bumped by every set_self_indices
+  cdfmm_b200_plan *adjoint = nullptr;
+  int adjoint_self_version = -1;
+  float4 *wbuf = nullptr;                      // [nt][K] sorted dL/dH weights
+  float4 *gpart = nullptr;                     // [nt][groups] near gradient partial sums
+  size_t wbuf_count = 0, gpart_count = 0;
+  void *stage_grad = nullptr;                  // device staging of host gradient inputs / outputs
+  size_t stage_grad_bytes = 0;
 
   cdfmm_b200_stats stats{};
 };

@@ -14,18 +14,20 @@
 // product), then L = 2^(l(|beta|+1)) D in the epilogue (upstream math:
 // docs/math.md "M2L normalisation and cross-level reuse").
 //
-// Data movement: one thread issues bulk async copies (cp.async.bulk, TMA
-// engine) of each source box's K-row block (contiguous, already in the
-// canonical no-swizzle K-major core-matrix layout written by the pack kernel)
-// and of the offset's B tile (pre-tiled on the host), completing on an
-// mbarrier; the same thread issues tcgen05.mma from shared memory into the
-// TMEM accumulator and commits to a second mbarrier that frees the stage.
-// Stages are double buffered so copies of offset o+1 overlap the MMAs of o.
+// Data movement: a producer warp issues bulk async copies (cp.async.bulk, TMA
+// engine) of each source box's rows (contiguous, already in the canonical
+// no-swizzle K-major core-matrix layout written by the pack kernel) and of the
+// offset's B tile (pre-tiled on the host), completing on the stage's "full"
+// mbarrier; one thread issues tcgen05.mma from shared memory into the TMEM
+// accumulators and commits to the stage's "empty" mbarrier, which frees it.
+// A pipeline unit is one offset and one 32-wide alpha chunk, so 4-8 stages
+// fit in shared memory and copies run several units ahead of the MMAs.
 // Every wait is bounded: on expiry the kernel records an error code, stops
 // issuing, drains what it issued, frees its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cstdint>
 
 #include "far_kernels.hpp"
@@ -38,6 +40,7 @@ namespace {
 
 constexpr int kTcThreads = 128;
 constexpr uint32_t kWaitLimit = 1u << 26; // ~2 s with the back-off below
+constexpr int kKChunk = 32;               // alphas per pipeline unit
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
   return static_cast<uint32_t>(__cvta_generic_to_shared(p));
@@ -125,30 +128,47 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Pipeline unit = (offset, alpha chunk of kKChunk = 32, the last chunk
+// possibly 16 wide): up to two MMA k-steps on each of the CTA's m_tiles
+// accumulators, which share the unit's B tile.  Shared-memory operand layout
+// of a chunk of width w (no swizzle, K-major, 8x16-byte core matrices):
+//   [row group][w/8 column blocks][8 rows][8 alphas]  -> LBO 128 B, SBO w*16 B
+// for A (128 rows per M tile) and for B (Npad rows = betas).  Stage =
+// [A_hi x m_tiles][A_lo x m_tiles][B_hi][B_lo].  Global operands hold each
+// chunk in the same order, so one source box's rows of one chunk are one
+// contiguous bulk copy; lanes of the producer warp issue a unit's copies in
+// parallel.
 __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x;
+  const int lane = tid & 31;
   const int4 tile = args.tiles[blockIdx.x];
   const int level = tile.x;
   const int cls = tile.y;
   const int p_first = tile.z; // first parent (Morton index at level-1) of this tile
-  const int count = tile.w;   // targets in this tile (<= T)
+  const int count = tile.w;   // targets in this tile (<= m_tiles * 128 / Kp)
   const int cx = cls & 1, cy = (cls >> 1) & 1, cz = (cls >> 2) & 1;
   const int side = 1 << level;
+  const int S = args.stages;
+  const int MT = args.m_tiles;
+  const int T = 128 / args.Kp;                                      // targets per M tile
+  const int m_active = (count + T - 1) / T;
+  const int nkc = (args.Kpad + kKChunk - 1) / kKChunk;
 
-  const uint32_t a_bytes = 128u * static_cast<uint32_t>(args.Kpad) * 2u;
-  const uint32_t b_bytes = static_cast<uint32_t>(args.Npad) * static_cast<uint32_t>(args.Kpad) * 2u;
+  const uint32_t a_tile = 128u * kKChunk * 2u;                      // one M tile, one of hi / lo
+  const uint32_t a_bytes = a_tile * static_cast<uint32_t>(MT);
+  const uint32_t b_bytes = static_cast<uint32_t>(args.Npad) * kKChunk * 2u;
   const uint32_t stage_bytes = 2u * a_bytes + 2u * b_bytes;
   uint8_t *stage0 = smem;
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + args.stages * stage_bytes);
-  uint64_t *empty = full + args.stages;
-  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(empty + args.stages);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + S * stage_bytes);
+  uint64_t *empty = full + S;
+  uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(empty + S);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
-  int *tgt_node = abort_flag + 1; // [T]
-  int *tgt_xyz = tgt_node + 16;   // [T] packed coordinates
+  int *tgt_node = abort_flag + 1;            // [kTcMaxTargets]
+  int *tgt_xyz = tgt_node + kTcMaxTargets;   // [kTcMaxTargets] packed coordinates
 
-  // Zero both stages' A buffers once: rows beyond count*Kp stay zero.
-  for (uint32_t q = tid; q < args.stages * stage_bytes / 16u; q += kTcThreads)
+  // Zero every stage once: A rows beyond a tile's targets are never written.
+  for (uint32_t q = tid; q < S * stage_bytes / 16u; q += kTcThreads)
     reinterpret_cast<uint4 *>(stage0)[q] = make_uint4(0, 0, 0, 0);
   if (tid < count) {
     int px, py, pz;
@@ -158,7 +178,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     tgt_xyz[tid] = tx | (ty << 10) | (tz << 20);
   }
   if (tid == 0) {
-    for (int s = 0; s < args.stages; ++s) {
+    for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
       mbar_init(&empty[s], 1);
     }
@@ -175,111 +195,142 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
+  const int units = 189 * nkc;
 
-  if (tid == 0) {
-    const uint32_t idesc = instr_desc_bf16(args.Npad);
-    const uint32_t sbo = static_cast<uint32_t>(args.Kpad) * 16u;
-    const int ksteps = args.Kpad / 16;
-    const uint32_t expect = 2u * static_cast<uint32_t>(count) * args.box_bytes + 2u * b_bytes;
-    // the 189 offsets of this class in a fixed order
-    int units = 0;
-    int o_list[189];
-    for (int oz = cz - 3; oz <= cz + 2; ++oz)
-      for (int oy = cy - 3; oy <= cy + 2; ++oy)
-        for (int ox = cx - 3; ox <= cx + 2; ++ox) {
-          if (ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1) continue;
-          o_list[units++] = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
+  if (tid >= 32 && tid < 64) {
+    // Producer warp: bulk copies of (offset, chunk) operands into stage u % S.
+    const size_t btile = static_cast<size_t>(args.Npad) * kKChunk * 2u; // stride of one B chunk tile
+    int produced = 0;
+    int slot = 0, ox = 0, oy = 0, oz = 0;
+    int o_next = 0; // position in the class's offset enumeration (x fastest)
+    for (int u = 0; u < units; ++u) {
+      const int s = u % S;
+      int ok = 1;
+      if (lane == 0) {
+        if (u >= S && !mbar_wait(&empty[s], ((u / S) - 1) & 1)) {
+          *abort_flag = 1;
+          atomicExch(args.error_flag, 1);
         }
-    bool ok = true;
-    uint32_t accumulate = 0;
-    int issued = 0; // units whose MMAs were committed
-    for (int step = 0; step < units + args.stages - 1 && ok; ++step) {
-      if (step < units) { // produce unit `step`
-        const int s = step % args.stages;
-        if (step >= args.stages) ok = mbar_wait(&empty[s], ((step / args.stages) - 1) & 1);
-        if (!ok) break;
-        const int slot = o_list[step];
-        const int ox = slot / 49 - 3, oy = (slot / 7) % 7 - 3, oz = slot % 7 - 3;
-        uint8_t *st = stage0 + s * stage_bytes;
-        mbar_expect_tx(&full[s], expect);
-        for (int t = 0; t < count; ++t) {
+        ok = *reinterpret_cast<volatile int *>(abort_flag) == 0;
+      }
+      ok = __shfl_sync(0xffffffffu, ok, 0);
+      if (!ok) break;
+      const int kc = u % nkc;
+      if (kc == 0) {
+        // Next list2 offset of class (cx, cy, cz): o in [c-3, c+2]^3 minus |o| <= 1.
+        for (;;) {
+          const int i = o_next++;
+          ox = cx - 3 + i % 6;
+          oy = cy - 3 + (i / 6) % 6;
+          oz = cz - 3 + i / 36;
+          if (!(ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1)) break;
+        }
+        slot = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
+      }
+      const int kcw = min(kKChunk, args.Kpad - kc * kKChunk);
+      const uint32_t box_chunk = static_cast<uint32_t>(args.Kp * kcw * 2); // one box's rows of this chunk
+      uint8_t *st = stage0 + s * stage_bytes;
+      const int n_a = count * 2;
+      if (lane == 0)
+        mbar_expect_tx(&full[s], static_cast<uint32_t>(n_a) * box_chunk + 2u * static_cast<uint32_t>(args.Npad) * kcw * 2u);
+      __syncwarp();
+      for (int c = lane; c < n_a + 2; c += 32) {
+        if (c < n_a) {
+          const int h = c & 1;
+          const int t = c >> 1;
+          const int m = t / T;
           const int xyz = tgt_xyz[t];
           const int sx = (xyz & 1023) - ox, sy = ((xyz >> 10) & 1023) - oy, sz = ((xyz >> 20) & 1023) - oz;
           int src = args.zero_node;
           if (sx >= 0 && sy >= 0 && sz >= 0 && sx < side && sy < side && sz < side)
             src = level_offset_d(level) + static_cast<int>(morton3(sx, sy, sz)) - args.node_base;
-          const size_t off = static_cast<size_t>(src) * args.box_bytes;
-          bulk_g2s(st + t * args.box_bytes, args.a_hi + off, args.box_bytes, &full[s]);
-          bulk_g2s(st + a_bytes + t * args.box_bytes, args.a_lo + off, args.box_bytes, &full[s]);
+          const size_t goff = static_cast<size_t>(src) * args.box_bytes +
+                              static_cast<size_t>(kc) * static_cast<size_t>(args.Kp * kKChunk * 2);
+          const uint32_t soff = static_cast<uint32_t>(h) * a_bytes + static_cast<uint32_t>(m) * a_tile +
+                                static_cast<uint32_t>(t - m * T) * box_chunk;
+          bulk_g2s(st + soff, (h ? args.a_lo : args.a_hi) + goff, box_chunk, &full[s]);
+        } else {
+          const int h = c - n_a;
+          const uint8_t *bsrc = args.b_tiles + (static_cast<size_t>(slot) * nkc + kc) * 2u * btile + h * btile;
+          bulk_g2s(st + 2 * a_bytes + h * b_bytes, bsrc, static_cast<uint32_t>(args.Npad) * kcw * 2u, &full[s]);
         }
-        const uint8_t *bsrc = args.b_tiles + static_cast<size_t>(slot) * 2u * b_bytes;
-        bulk_g2s(st + 2 * a_bytes, bsrc, b_bytes, &full[s]);
-        bulk_g2s(st + 2 * a_bytes + b_bytes, bsrc + b_bytes, b_bytes, &full[s]);
       }
-      const int c = step - (args.stages - 1);
-      if (c >= 0) { // consume unit c
-        const int s = c % args.stages;
-        ok = mbar_wait(&full[s], (c / args.stages) & 1);
-        if (!ok) break;
-        tc_fence_after();
-        const uint32_t a_hi = smem_u32(stage0 + s * stage_bytes);
-        const uint32_t a_lo = a_hi + a_bytes;
-        const uint32_t b_hi = a_hi + 2 * a_bytes;
-        const uint32_t b_lo = b_hi + b_bytes;
-        for (int ks = 0; ks < ksteps; ++ks) {
-          const uint32_t koff = static_cast<uint32_t>(ks) * 256u;
-          const uint64_t dah = smem_desc(a_hi + koff, 128u, sbo);
-          const uint64_t dal = smem_desc(a_lo + koff, 128u, sbo);
-          const uint64_t dbh = smem_desc(b_hi + koff, 128u, sbo);
-          const uint64_t dbl = smem_desc(b_lo + koff, 128u, sbo);
-          mma_bf16(tmem, dah, dbh, idesc, accumulate);
-          accumulate = 1;
-          mma_bf16(tmem, dah, dbl, idesc, 1);
-          mma_bf16(tmem, dal, dbh, idesc, 1);
-        }
-        mma_commit(&empty[s]);
-        issued = c + 1;
-      }
+      __syncwarp();
+      produced = u + 1;
     }
-    if (!ok) {
-      *abort_flag = 1;
-      atomicExch(args.error_flag, 1);
+    if (lane == 0 && *reinterpret_cast<volatile int *>(abort_flag)) {
+      // Abort: wait (bounded) for this warp's copies still in flight.
+      for (int u = max(0, produced - S); u < produced; ++u) mbar_wait(&full[u % S], (u / S) & 1);
     }
-    // The last commit arrives once every MMA issued before it has completed.
-    if (issued > 0) {
-      const int last = issued - 1;
-      if (!mbar_wait(&empty[last % args.stages], (last / args.stages) & 1)) {
+  } else if (tid == 0) {
+    // MMA issuer: waits for each unit's operands, issues its MMAs, commits
+    // to the unit's empty barrier (arrives when those MMAs completed).
+    const uint32_t idesc = instr_desc_bf16(args.Npad);
+    uint32_t accumulate = 0;
+    int issued = 0;
+    for (int u = 0; u < units; ++u) {
+      const int s = u % S;
+      if (!mbar_wait(&full[s], (u / S) & 1)) {
         *abort_flag = 1;
         atomicExch(args.error_flag, 2);
+        break;
       }
+      tc_fence_after();
+      const int kc = u % nkc;
+      const int kcw = min(kKChunk, args.Kpad - kc * kKChunk);
+      const uint32_t sbo = static_cast<uint32_t>(kcw) * 16u;
+      const uint32_t a_hi = smem_u32(stage0 + s * stage_bytes);
+      const uint32_t a_lo = a_hi + a_bytes;
+      const uint32_t b_hi = a_hi + 2 * a_bytes;
+      const uint32_t b_lo = b_hi + b_bytes;
+      for (int ks = 0; ks < kcw / 16; ++ks) {
+        const uint64_t dbh = smem_desc(b_hi + ks * 256u, 128u, sbo);
+        const uint64_t dbl = smem_desc(b_lo + ks * 256u, 128u, sbo);
+        for (int m = 0; m < m_active; ++m) {
+          const uint32_t d = tmem + static_cast<uint32_t>(m * args.acc_stride);
+          const uint64_t dah = smem_desc(a_hi + m * a_tile + ks * 256u, 128u, sbo);
+          const uint64_t dal = smem_desc(a_lo + m * a_tile + ks * 256u, 128u, sbo);
+          mma_bf16(d, dah, dbh, idesc, accumulate);
+          mma_bf16(d, dah, dbl, idesc, 1);
+          mma_bf16(d, dal, dbh, idesc, 1);
+        }
+        accumulate = 1;
+      }
+      mma_commit(&empty[s]);
+      issued = u + 1;
     }
-    // Drain copies that were issued but never consumed (only after an abort).
-    if (*abort_flag) {
-      for (int u = issued; u < units && u < issued + args.stages; ++u) mbar_wait(&full[u % args.stages], (u / args.stages) & 1);
+    // The last commit arrives once every MMA issued before it has completed.
+    if (issued > 0 && !mbar_wait(&empty[(issued - 1) % S], ((issued - 1) / S) & 1)) {
+      *abort_flag = 1;
+      atomicExch(args.error_flag, 3);
     }
   }
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
 
-  // Epilogue: warp w owns TMEM lanes 32w..32w+31 (rows); scale by D_L and store.
+  // Epilogue: warp w owns TMEM lanes 32w..32w+31 (rows of every M tile);
+  // scale by D_L and store.
   if (*abort_flag == 0) {
     const int warp = tid >> 5;
     const int row = tid;
-    const int tt = row / args.Kp;
-    const int k = row - tt * args.Kp;
-    const bool valid = tt < count && k < args.K;
-    const int node = valid ? tgt_node[tt] : 0;
-    const long long base = static_cast<long long>(node) * args.n * args.K + k;
+    const int tr = row / args.Kp;
+    const int k = row - tr * args.Kp;
     const float *sl = args.scale_l + level * args.n;
-    for (int c0 = 0; c0 < args.Npad; c0 += 16) {
-      float v[16];
-      tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(c0), v);
-      if (valid) {
+    for (int m = 0; m < m_active; ++m) {
+      const int tt = m * T + tr;
+      const bool valid = tr < T && tt < count && k < args.K;
+      const int node = valid ? tgt_node[tt] : 0;
+      const long long base = static_cast<long long>(node) * args.n * args.K + k;
+      for (int c0 = 0; c0 < args.Npad; c0 += 16) {
+        float v[16];
+        tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(m * args.acc_stride + c0), v);
+        if (valid) {
 #pragma unroll
-        for (int j = 0; j < 16; ++j) {
-          const int b = c0 + j;
-          if (b < args.n) args.L[base + static_cast<long long>(b) * args.K] = v[j] * sl[b];
+          for (int j = 0; j < 16; ++j) {
+            const int b = c0 + j;
+            if (b < args.n) args.L[base + static_cast<long long>(b) * args.K] = v[j] * sl[b];
+          }
         }
       }
     }
@@ -292,28 +343,30 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   }
 }
 
-// Pack: scaled multipoles of levels 2..depth -> BF16 hi/lo boxes
-// [box][Kp/8][Kpad/8][8 rows][8 alphas] (rows = states), the no-swizzle
-// K-major core-matrix layout the MMA reads directly.  One extra all-zero box
+// Pack: scaled multipoles of levels 2..depth -> BF16 hi/lo boxes.  A box is
+// Kp rows (states) x Kpad alphas stored chunk by chunk (32 alphas; the last
+// chunk may be 16), each chunk as [Kp/8 row groups][w/8 column blocks][8][8]
+// so one box's rows of one chunk are contiguous.  One extra all-zero box
 // (index n_boxes) stands for sources outside the grid.
 __global__ void m2l_pack_kernel(const float *__restrict__ M, const float *__restrict__ scale_m,
-                                const int8_t *__restrict__ basis, __nv_bfloat16 *__restrict__ hi,
-                                __nv_bfloat16 *__restrict__ lo, int n, int K, int Kp, int Kpad, int depth,
-                                int node_base, int n_boxes) {
+                                __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo, int n, int K, int Kp,
+                                int Kpad, int depth, int node_base, int n_boxes) {
   const long long per_box = static_cast<long long>(Kp) * Kpad;
   const long long total = (static_cast<long long>(n_boxes) + 1) * per_box;
   for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < total;
        q += static_cast<long long>(gridDim.x) * blockDim.x) {
     const long long box = q / per_box;
     const int e = static_cast<int>(q - box * per_box);
-    // e enumerates [rg][cj][r8][a8]
-    const int a8 = e & 7;
-    const int r8 = (e >> 3) & 7;
-    const int rest = e >> 6;
-    const int cj = rest % (Kpad / 8);
-    const int rg = rest / (Kpad / 8);
+    const int kc = e / (Kp * kKChunk);
+    const int rem = e - kc * Kp * kKChunk;
+    const int ncj = min(kKChunk, Kpad - kc * kKChunk) / 8;
+    const int a8 = rem & 7;
+    const int r8 = (rem >> 3) & 7;
+    const int x = rem >> 6;
+    const int cjl = x % ncj;
+    const int rg = x / ncj;
     const int k = rg * 8 + r8;
-    const int a = cj * 8 + a8;
+    const int a = kc * kKChunk + cjl * 8 + a8;
     float v = 0.0F;
     if (box < n_boxes && k < K && a < n) {
       const int node = node_base + static_cast<int>(box);
@@ -329,33 +382,40 @@ __global__ void m2l_pack_kernel(const float *__restrict__ M, const float *__rest
 
 } // namespace
 
-size_t m2l_tc_smem_bytes(int Kpad, int Npad, int stages) {
-  const size_t a = 128u * static_cast<size_t>(Kpad) * 2u;
-  const size_t b = static_cast<size_t>(Npad) * Kpad * 2u;
-  return static_cast<size_t>(stages) * (2 * a + 2 * b) + 2 * stages * sizeof(uint64_t) + 8 + 32 * sizeof(int) + 1024;
+size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages) {
+  const size_t a = 128u * kKChunk * 2u * static_cast<size_t>(m_tiles);
+  const size_t b = static_cast<size_t>(Npad) * kKChunk * 2u;
+  return static_cast<size_t>(stages) * (2 * a + 2 * b) + 2 * stages * sizeof(uint64_t) + 8 +
+         2 * kTcMaxTargets * sizeof(int);
 }
 
 void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,
                      int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s) {
+  (void)basis;
   const long long total = (static_cast<long long>(n_boxes) + 1) * Kp * Kpad;
   const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 64));
-  m2l_pack_kernel<<<blocks, 256, 0, s>>>(M, scale_m, basis, static_cast<__nv_bfloat16 *>(hi),
+  m2l_pack_kernel<<<blocks, 256, 0, s>>>(M, scale_m, static_cast<__nv_bfloat16 *>(hi),
                                           static_cast<__nv_bfloat16 *>(lo), n, K, Kp, Kpad, depth, node_base, n_boxes);
 }
 
 void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s) {
   if (n_tiles == 0) return;
-  const size_t smem = m2l_tc_smem_bytes(args.Kpad, args.Npad, args.stages);
+  size_t smem = m2l_tc_smem_bytes(args.Npad, args.m_tiles, args.stages);
+  // More than half of TMEM per CTA: request enough shared memory that a
+  // second CTA never shares the SM (its tcgen05.alloc would wait for ours).
+  if (args.tmem_cols > 256) smem = std::max<size_t>(smem, 120 * 1024);
   m2l_tc_kernel<<<n_tiles, kTcThreads, smem, s>>>(args);
 }
 
 bool configure_m2l_tc(size_t max_smem) { return allow_dynamic_smem(m2l_tc_kernel, max_smem); }
 
-// Host: B tiles [slot][hi, lo][Npad/8][Kpad/8][8][8] BF16 from FP64 matrices
-// T[slot][alpha][beta] (symmetric in alpha, beta).
+// Host: B tiles [slot][alpha chunk][hi, lo][Npad x 32 stride] BF16 from FP64
+// matrices T[slot][alpha][beta] (symmetric in alpha, beta); a chunk of width w
+// is stored as [beta group][w/8 column blocks][8 betas][8 alphas].
 std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, int Npad, int Kpad) {
-  const size_t tile = static_cast<size_t>(Npad) * Kpad;
-  std::vector<uint16_t> out(343 * 2 * tile, 0);
+  const int nkc = (Kpad + kKChunk - 1) / kKChunk;
+  const size_t btile = static_cast<size_t>(Npad) * kKChunk;
+  std::vector<uint16_t> out(static_cast<size_t>(343) * nkc * 2 * btile, 0);
   auto bf16_bits = [](float f) -> uint16_t {
     const __nv_bfloat16 h = __float2bfloat16_rn(f);
     uint16_t b;
@@ -364,14 +424,17 @@ std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, in
   };
   for (int slot = 0; slot < 343; ++slot) {
     const double *Ts = T64.data() + static_cast<size_t>(slot) * n * n;
-    uint16_t *hi = out.data() + static_cast<size_t>(slot) * 2 * tile;
-    uint16_t *lo = hi + tile;
     for (int beta = 0; beta < n; ++beta)
       for (int alpha = 0; alpha < n; ++alpha) {
         const double v = Ts[static_cast<size_t>(alpha) * n + beta];
         const __nv_bfloat16 h = __float2bfloat16_rn(static_cast<float>(v));
         const float l = static_cast<float>(v - static_cast<double>(__bfloat162float(h)));
-        const size_t at = ((static_cast<size_t>(beta / 8) * (Kpad / 8) + alpha / 8) * 8 + beta % 8) * 8 + alpha % 8;
+        const int kc = alpha / kKChunk;
+        const int al = alpha - kc * kKChunk;
+        const int ncj = std::min(kKChunk, Kpad - kc * kKChunk) / 8;
+        uint16_t *hi = out.data() + (static_cast<size_t>(slot) * nkc + kc) * 2 * btile;
+        uint16_t *lo = hi + btile;
+        const size_t at = ((static_cast<size_t>(beta / 8) * ncj + al / 8) * 8 + beta % 8) * 8 + al % 8;
         hi[at] = bf16_bits(static_cast<float>(v));
         lo[at] = bf16_bits(l);
       }

@@ -11,9 +11,9 @@
 namespace cdfmm_b200 {
 
 struct TcArgs {
-  const uint8_t *a_hi;     // packed BF16 hi boxes [box][Kp rows][Kpad] (core-matrix tiled)
+  const uint8_t *a_hi;     // packed BF16 hi boxes [box][32-alpha chunk][Kp/8][w/8][8][8]
   const uint8_t *a_lo;     // packed BF16 lo boxes
-  const uint8_t *b_tiles;  // [343 slots][hi, lo][Npad x Kpad] (core-matrix tiled)
+  const uint8_t *b_tiles;  // [343 slots][32-alpha chunk][hi, lo][Npad/8][w/8][8][8]
   const int4 *tiles;       // per CTA: (level, class, first parent Morton index, target count)
   const float *scale_l;    // [depth+1][n] exact powers of two
   float *L;                // [node][n][K] FP32 locals (overwritten)
@@ -22,11 +22,16 @@ struct TcArgs {
   int node_base;           // flat node index of packed box 0
   int zero_node;           // packed index of the all-zero box
   int stages;
+  int m_tiles;             // 128-row accumulators per CTA sharing each B tile
+  int acc_stride;          // TMEM columns between accumulators (multiple of 32)
   uint32_t tmem_cols;
   uint32_t box_bytes;      // Kp * Kpad * 2
 };
 
-size_t m2l_tc_smem_bytes(int Kpad, int Npad, int stages);
+// Largest target count of one CTA: m_tiles (<= 4) x 128 / Kp with Kp >= 8.
+constexpr int kTcMaxTargets = 64;
+
+size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages);
 void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,
                      int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s);
 void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s);

@@ -15,6 +15,7 @@
 // block does (src/static_operators.cpp:435-446).
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 
 #include "far_kernels.hpp"
@@ -178,97 +179,275 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
   }
 }
 
-// K > 1: a thread owns (target, group of KG states); per staged source the
-// geometry is computed once and applied to the KG states.  Lanes of a warp
-// share the state group, so moment reads are shared-memory broadcasts.
-template <int KG, bool PHI>
-__global__ void __launch_bounds__(256) p2p_kn_kernel(const float4 *__restrict__ src_rel,
-                                                     const float4 *__restrict__ mom,
-                                                     const int *__restrict__ src_off,
-                                                     const float4 *__restrict__ tgt_rel,
-                                                     const int *__restrict__ tgt_off,
-                                                     const int *__restrict__ self_idx, int depth,
-                                                     int K, int chunk, float4 *__restrict__ near) {
-  extern __shared__ float4 dyn[];
-  float4 *sPos = dyn;          // [chunk]
-  float4 *sMom = dyn + chunk;  // [chunk][K]
+// K > 1.  One CTA per target leaf.  Work items are (target, group of KG
+// states); a lane owns one item and computes a pair's geometry once --
+// r, v = 1/|r|^3, u = 3 r / |r|^5, w = |r|^2 / 3 -- applying it to its KG
+// states:
+//   s = m.u,  phi += s w,  H += s r - v m          (10 FP ops per pair-state)
+// A self pair gets u = v = w = 0; a coincident non-self pair gives u = NaN
+// (0 * inf), hence NaN results, as in the reference.
+//
+// Load balance: the items of a leaf are processed in rounds of 256; a round
+// with r < 256 items gives each item F = 2^j <= min(8, 256 / r) lanes that
+// split the sources (lane f takes sources f, f + F, ...) and are summed with
+// warp shuffles at the end of the round, so a leaf whose target count is not
+// a multiple of 32 does not leave most lanes idle in its last round.
+//
+// Staging: the neighbourhood positions (relative to this leaf's centre) and
+// sorted source indices are staged once; the moments of the round's state
+// window stream through a double-buffered cp.async pipeline in chunks of
+// kChunkB sources.  Within a moment row, state k sits at k + k/8 (one pad
+// float4 per 8 states), so lanes of one warp that read the same source for
+// two state groups hit different banks; the row stride Kr is 1 mod 8 (in
+// float4) so the F lanes of one item, reading different sources, do too.
+constexpr int kChunkB = 32;         // sources per moment chunk
+constexpr int kNeighbourCap = 1024; // staged neighbourhood size per pass
+constexpr int kStateBlock = 64;     // states per state block (bounds shared memory)
+constexpr int kKbThreads = 256;
+
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+
+// Shared-memory position of state k within a staged moment row, and the row
+// stride for a window of Kw states (1 mod 8 float4).
+__device__ __forceinline__ int mrow_pos(int k) { return k + (k >> 3); }
+__device__ __forceinline__ int mrow_stride(int Kw) { return ((Kw + (Kw - 1) / 8 + 6) / 8) * 8 + 1; }
+
+// Sources q = qbeg, qbeg + F, ... < sn of one staged chunk; m_row0 points at
+// this item's first state in source row 0 (its KG states are contiguous:
+// groups start at multiples of 8), rows Kr float4 apart.  FULL: all KG states
+// valid (no per-state predicate).
+template <int KG, bool PHI, bool FULL>
+__device__ __forceinline__ void p2p_kb_chunk(const float4 &ti, int self, const float4 *sPos, const int *sIdx,
+                                             const float4 *m_row0, int Kr, int qbeg, int sn, int F, int kvalid,
+                                             float (&acc)[KG][4]) {
+#pragma unroll 2
+  for (int q = qbeg; q < sn; q += F) {
+    const float4 s = sPos[q];
+    const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const bool is_self = sIdx[q] == self;
+    const float rinv = is_self ? 0.0F : rsqrtf(r2);
+    const float v = rinv * rinv * rinv;
+    const float f = 3.0F * v * rinv * rinv;
+    const float ux = f * dx, uy = f * dy, uz = f * dz;
+    const float w = is_self ? 0.0F : r2 * (1.0F / 3.0F);
+    const float4 *mq = m_row0 + q * Kr;
+#pragma unroll
+    for (int st = 0; st < KG; ++st) {
+      if (FULL || st < kvalid) {
+        const float4 m = mq[st];
+        const float sd = fmaf(m.x, ux, fmaf(m.y, uy, m.z * uz));
+        if (PHI) acc[st][0] = fmaf(sd, w, acc[st][0]);
+        acc[st][1] = fmaf(-v, m.x, fmaf(sd, dx, acc[st][1]));
+        acc[st][2] = fmaf(-v, m.y, fmaf(sd, dy, acc[st][2]));
+        acc[st][3] = fmaf(-v, m.z, fmaf(sd, dz, acc[st][3]));
+      }
+    }
+  }
+}
+
+// Position gradient of w.H for a target over one staged chunk (summed over
+// the item's KG states): with a = m.r, b = w.r, f5 = 3/|r|^5, f7 = 15/|r|^7,
+//   grad_x [w.K(r) m] = f5 [b m + a w + (w.m) r] - f7 a b r       (times 1/(4 pi))
+// accumulated per pair as g += f5 V + (f5 C - f7 P) r with V = sum(b m + a w),
+// C = sum(w.m), P = sum(a b) over the states.  Self pairs give zero; a
+// coincident non-self pair gives NaN like the forward field.
+template <int KG, bool FULL>
+__device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const float4 *sPos, const int *sIdx,
+                                               const float4 *m_row0, int Kr, int qbeg, int sn, int F, int kvalid,
+                                               const float (&w)[KG][3], float (&g)[3]) {
+#pragma unroll 2
+  for (int q = qbeg; q < sn; q += F) {
+    const float4 s = sPos[q];
+    const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const bool is_self = sIdx[q] == self;
+    const float rinv = is_self ? 0.0F : rsqrtf(r2);
+    const float r2inv = rinv * rinv;
+    const float f5 = 3.0F * r2inv * r2inv * rinv;
+    const float f7 = 5.0F * f5 * r2inv;
+    const float4 *mq = m_row0 + q * Kr;
+    float vx = 0.0F, vy = 0.0F, vz = 0.0F, C = 0.0F, P = 0.0F;
+#pragma unroll
+    for (int st = 0; st < KG; ++st) {
+      if (FULL || st < kvalid) {
+        const float4 m = mq[st];
+        const float a = fmaf(m.x, dx, fmaf(m.y, dy, m.z * dz));
+        const float b = fmaf(w[st][0], dx, fmaf(w[st][1], dy, w[st][2] * dz));
+        C = fmaf(w[st][0], m.x, fmaf(w[st][1], m.y, fmaf(w[st][2], m.z, C)));
+        P = fmaf(a, b, P);
+        vx = fmaf(b, m.x, fmaf(a, w[st][0], vx));
+        vy = fmaf(b, m.y, fmaf(a, w[st][1], vy));
+        vz = fmaf(b, m.z, fmaf(a, w[st][2], vz));
+      }
+    }
+    const float coef = fmaf(f5, C, -f7 * P);
+    g[0] = fmaf(f5, vx, fmaf(coef, dx, g[0]));
+    g[1] = fmaf(f5, vy, fmaf(coef, dy, g[1]));
+    g[2] = fmaf(f5, vz, fmaf(coef, dz, g[2]));
+  }
+}
+
+// MODE 0: field; 1: field and potential (near[nt][K] = (phi, H) / 4 pi);
+// 2: position gradient of sum_k w_k . H_k, partial sums per state group
+//    gpart[nt][G] (G = ceil(K / KG)) from the weights W[nt][K].
+template <int KG, int MODE>
+__global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__restrict__ src_rel,
+                                                              const float4 *__restrict__ mom,
+                                                              const int *__restrict__ src_off,
+                                                              const float4 *__restrict__ tgt_rel,
+                                                              const int *__restrict__ tgt_off,
+                                                              const int *__restrict__ self_idx, int depth, int K,
+                                                              float4 *__restrict__ near,
+                                                              const float4 *__restrict__ W) {
+  constexpr bool PHI = MODE == 1;
+  constexpr bool GRAD = MODE == 2;
+  extern __shared__ float4 dynb[];
+  float4 *sPos = dynb;                                            // [kNeighbourCap]
+  int *sIdx = reinterpret_cast<int *>(sPos + kNeighbourCap);      // [kNeighbourCap]
+  float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [2][kChunkB][Kr <= kStateBlock + 9]
   __shared__ Neighbours nb;
   const int leaf = blockIdx.x;
   const int t0 = tgt_off[leaf];
-  const int t1 = tgt_off[leaf + 1];
-  if (t0 == t1) return;
+  const int nt = tgt_off[leaf + 1] - t0;
+  if (nt == 0) return;
   if (threadIdx.x == 0) build_neighbours(nb, leaf, depth, src_off);
   __syncthreads();
   const int total = nb.prefix[nb.count];
-  const int nt_leaf = t1 - t0;
-  const int groups = (K + KG - 1) / KG;
-  const int items = nt_leaf * groups;
-  for (int base = 0; base < items; base += blockDim.x) {
-    const int item = base + threadIdx.x;
-    const bool active = item < items;
-    const int g = active ? item / nt_leaf : 0;
-    const int i = t0 + (active ? item - g * nt_leaf : 0);
-    const int kb = g * KG;
-    const float4 ti = tgt_rel[i];
-    const int self = self_idx != nullptr ? self_idx[i] : -1;
-    float acc[KG][4];
+  const int tid = threadIdx.x;
+  bool staged = false; // positions of the single pass already in shared memory
+  for (int kblk = 0; kblk < K; kblk += kStateBlock) {
+    const int Kc = min(kStateBlock, K - kblk);
+    const int G = (Kc + KG - 1) / KG;
+    const int items = nt * G;
+    for (int ib = 0; ib < items; ib += kKbThreads) {
+      const int r = min(kKbThreads, items - ib);
+      int F = 1;
+      while (F < 8 && 2 * F * r <= kKbThreads) F <<= 1;
+      const int li = tid / F;
+      const int f = tid - li * F;
+      const bool valid = li < r;
+      const int item = ib + (valid ? li : 0);
+      const int g = item / nt;
+      const int t = item - g * nt;
+      const int kb = g * KG;                 // within the state block
+      const int kvalid = min(KG, Kc - kb);
+      const int k_lo = (ib / nt) * KG;       // the round's state window [k_lo, k_hi)
+      const int k_hi = min(Kc, ((ib + r - 1) / nt + 1) * KG);
+      const int Kw = k_hi - k_lo;
+      const int Kr = mrow_stride(Kw);
+      const int i = t0 + t;
+      const float4 ti = tgt_rel[i];
+      const int self = self_idx != nullptr ? self_idx[i] : -1;
+      float acc[KG][4];
 #pragma unroll
-    for (int s = 0; s < KG; ++s) acc[s][0] = acc[s][1] = acc[s][2] = acc[s][3] = 0.0F;
-    for (int sc = 0; sc < total; sc += chunk) {
-      const int sn = min(chunk, total - sc);
-      __syncthreads();
-      for (int q = threadIdx.x; q < sn; q += blockDim.x) {
-        float4 pos;
-        int j;
-        stage_source(nb, sc + q, src_rel, pos, j);
-        sPos[q] = pos;
-      }
-      __syncthreads();
-      for (int q = threadIdx.x; q < sn * K; q += blockDim.x) {
-        const int qs = q / K;
-        const int k = q - qs * K;
-        sMom[q] = mom[static_cast<long long>(__float_as_int(sPos[qs].w)) * K + k];
-      }
-      __syncthreads();
-      if (active) {
-        for (int q = 0; q < sn; ++q) {
-          const float4 s = sPos[q];
-          const float dx = ti.x - s.x;
-          const float dy = ti.y - s.y;
-          const float dz = ti.z - s.z;
-          float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-          r2 = (__float_as_int(s.w) == self) ? __int_as_float(0x7f800000) : r2;
-          const float rinv = rsqrtf(r2);
-          const float rinv2 = rinv * rinv;
-          const float rinv3 = rinv2 * rinv;
-          const float a3 = 3.0F * rinv2;
-          const float4 *mq = sMom + q * K + kb;
+      for (int st = 0; st < KG; ++st) acc[st][0] = acc[st][1] = acc[st][2] = acc[st][3] = 0.0F;
+      float wreg[KG][3];
+      float gacc[3] = {0.0F, 0.0F, 0.0F};
+      if constexpr (GRAD) {
 #pragma unroll
-          for (int s2 = 0; s2 < KG; ++s2) {
-            if (kb + s2 < K) {
-              const float4 m = mq[s2];
-              const float mr = fmaf(m.x, dx, fmaf(m.y, dy, m.z * dz));
-              if (PHI) acc[s2][0] = fmaf(mr, rinv3, acc[s2][0]);
-              const float a = a3 * mr;
-              acc[s2][1] = fmaf(rinv3, fmaf(a, dx, -m.x), acc[s2][1]);
-              acc[s2][2] = fmaf(rinv3, fmaf(a, dy, -m.y), acc[s2][2]);
-              acc[s2][3] = fmaf(rinv3, fmaf(a, dz, -m.z), acc[s2][3]);
+        for (int st = 0; st < KG; ++st) {
+          const float4 wv = st < kvalid ? W[static_cast<long long>(i) * K + kblk + kb + st] : make_float4(0, 0, 0, 0);
+          wreg[st][0] = wv.x;
+          wreg[st][1] = wv.y;
+          wreg[st][2] = wv.z;
+        }
+      }
+      for (int pass = 0; pass < total; pass += kNeighbourCap) {
+        const int pn = min(kNeighbourCap, total - pass);
+        if (!staged || total > kNeighbourCap) {
+          __syncthreads();
+          for (int q = tid; q < pn; q += kKbThreads) {
+            float4 pos;
+            int j;
+            stage_source(nb, pass + q, src_rel, pos, j);
+            sPos[q] = pos;
+            sIdx[q] = j;
+          }
+          __syncthreads();
+          staged = true;
+        }
+        const int chunks = (pn + kChunkB - 1) / kChunkB;
+        // Copy element e = q * Kw + k of a chunk; each thread walks e = tid,
+        // tid + 256, ... incrementally (no division in the loop).
+        const int cq0 = tid / Kw, ck0 = tid - cq0 * Kw;
+        const int cqs = kKbThreads / Kw, cks = kKbThreads - cqs * Kw;
+        auto issue = [&](int c) {
+          const int q0 = c * kChunkB;
+          const int sn = min(kChunkB, pn - q0);
+          float4 *dst = sMom + (c & 1) * kChunkB * Kr;
+          int q = cq0, k = ck0;
+          while (q < sn) {
+            cp_async16(dst + q * Kr + mrow_pos(k), mom + static_cast<long long>(sIdx[q0 + q]) * K + kblk + k_lo + k);
+            q += cqs;
+            k += cks;
+            if (k >= Kw) {
+              k -= Kw;
+              ++q;
             }
           }
+          cp_async_commit();
+        };
+        issue(0);
+        for (int c = 0; c < chunks; ++c) {
+          if (c + 1 < chunks)
+            issue(c + 1);
+          else
+            cp_async_commit(); // one group per iteration keeps the wait count uniform
+          cp_async_wait<1>();
+          __syncthreads();
+          const int q0 = c * kChunkB;
+          const int sn = min(kChunkB, pn - q0);
+          if (valid) {
+            const float4 *m_row0 = sMom + (c & 1) * kChunkB * Kr + mrow_pos(kb - k_lo);
+            if constexpr (GRAD) {
+              if (kvalid == KG)
+                p2p_grad_chunk<KG, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg, gacc);
+              else
+                p2p_grad_chunk<KG, false>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg, gacc);
+            } else {
+              if (kvalid == KG)
+                p2p_kb_chunk<KG, PHI, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc);
+              else
+                p2p_kb_chunk<KG, PHI, false>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc);
+            }
+          }
+          __syncthreads();
         }
       }
-    }
-    if (active) {
+      if constexpr (GRAD) {
+        for (int o = 1; o < F; o <<= 1)
 #pragma unroll
-      for (int s2 = 0; s2 < KG; ++s2) {
-        if (kb + s2 < K) {
-          near[static_cast<long long>(i) * K + kb + s2] =
-              make_float4(acc[s2][0] * kInvFourPiF, acc[s2][1] * kInvFourPiF,
-                          acc[s2][2] * kInvFourPiF, acc[s2][3] * kInvFourPiF);
-        }
+          for (int c = 0; c < 3; ++c) gacc[c] += __shfl_xor_sync(0xffffffffu, gacc[c], o);
+        if (valid && f == 0)
+          near[static_cast<long long>(i) * ((K + KG - 1) / KG) + kblk / KG + g] =
+              make_float4(gacc[0] * kInvFourPiF, gacc[1] * kInvFourPiF, gacc[2] * kInvFourPiF, 0.0F);
+        continue;
+      }
+      if (F > 1) {
+#pragma unroll
+        for (int st = 0; st < KG; ++st)
+#pragma unroll
+          for (int c = 0; c < 4; ++c)
+            for (int o = 1; o < F; o <<= 1) acc[st][c] += __shfl_xor_sync(0xffffffffu, acc[st][c], o);
+      }
+      if (valid && f == 0) {
+        float4 *out = near + static_cast<long long>(i) * K + kblk + kb;
+#pragma unroll
+        for (int st = 0; st < KG; ++st)
+          if (st < kvalid)
+            out[st] = make_float4(acc[st][0] * kInvFourPiF, acc[st][1] * kInvFourPiF, acc[st][2] * kInvFourPiF,
+                                  acc[st][3] * kInvFourPiF);
       }
     }
-    __syncthreads();
   }
 }
 
@@ -330,18 +509,28 @@ __global__ void __launch_bounds__(256) direct_fp64_kernel(const double *__restri
   }
 }
 
+size_t p2p_kb_smem_bytes(int K) {
+  const int Kc = std::min(K, kStateBlock);
+  const int Kr = ((Kc + (Kc - 1) / 8 + 6) / 8) * 8 + 1; // mrow_stride(Kc), the widest window
+  return sizeof(float4) * kNeighbourCap + sizeof(int) * kNeighbourCap +
+         sizeof(float4) * 2 * kChunkB * static_cast<size_t>(Kr);
+}
+
 template <int KG>
-void launch_kn(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
-               const int *tgt_off, const int *self_idx, int depth, int K, bool want_phi,
-               float4 *near, cudaStream_t s) {
+void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
+               const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
+               cudaStream_t s) {
   const int leaves = 1 << (3 * depth);
-  int chunk = static_cast<int>((96 * 1024) / (16 + 16 * static_cast<size_t>(K)));
-  chunk = std::max(8, std::min(256, chunk));
-  const size_t smem = sizeof(float4) * (static_cast<size_t>(chunk) + static_cast<size_t>(chunk) * K);
-  if (want_phi)
-    p2p_kn_kernel<KG, true><<<leaves, 256, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, chunk, near);
+  const size_t smem = p2p_kb_smem_bytes(K);
+  if (mode == 1)
+    p2p_kb_kernel<KG, 1><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K,
+                                                          near, W);
+  else if (mode == 2)
+    p2p_kb_kernel<KG, 2><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K,
+                                                          near, W);
   else
-    p2p_kn_kernel<KG, false><<<leaves, 256, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, chunk, near);
+    p2p_kb_kernel<KG, 0><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K,
+                                                          near, W);
 }
 
 } // namespace
@@ -355,18 +544,32 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
       p2p_k1_kernel<true><<<leaves, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, near);
     else
       p2p_k1_kernel<false><<<leaves, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, near);
-  } else if (K >= 8) {
-    launch_kn<8>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi, near, s);
   } else {
-    launch_kn<4>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi, near, s);
+    if (K >= 8)
+      launch_kb<8>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s);
+    else
+      launch_kb<4>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s);
   }
 }
 
+int p2p_grad_groups(int K) { return K >= 8 ? (K + 7) / 8 : (K + 3) / 4; }
+
+void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
+                     const int *tgt_off, const int *self_idx, int depth, int K, const float4 *W, float4 *gpart,
+                     cudaStream_t s) {
+  if (K >= 8)
+    launch_kb<8>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, 2, gpart, W, s);
+  else
+    launch_kb<4>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, 2, gpart, W, s);
+}
+
 void configure_p2p(size_t max_smem) {
-  allow_dynamic_smem(p2p_kn_kernel<8, true>, max_smem);
-  allow_dynamic_smem(p2p_kn_kernel<8, false>, max_smem);
-  allow_dynamic_smem(p2p_kn_kernel<4, true>, max_smem);
-  allow_dynamic_smem(p2p_kn_kernel<4, false>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<8, 0>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<8, 1>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<8, 2>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 0>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 1>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 2>, max_smem);
 }
 
 void launch_direct_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,

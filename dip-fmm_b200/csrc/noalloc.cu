@@ -71,8 +71,8 @@ cudaError_t scratch_address(int device, void **out) {
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
 // Tensor-core M2L work tiles, written on the device (no host copy, so the
-// call stays capturable): per level from `depth` down to 2, per parity
-// class, runs of T = 128 / Kp consecutive parents (same order as the plan's).
+// call stays capturable): per level from `depth` down to 2, runs of T
+// consecutive parents, the 8 parity classes of a run adjacent (the plan's order).
 __global__ void noalloc_tiles_kernel(int4 *tiles, int depth, int T, int n_tiles) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;
   if (q >= n_tiles) return;
@@ -81,8 +81,8 @@ __global__ void noalloc_tiles_kernel(int4 *tiles, int depth, int T, int n_tiles)
     const int parents = 1 << (3 * (level - 1));
     const int per_class = (parents + T - 1) / T;
     if (rest < 8 * per_class) {
-      const int cls = rest / per_class;
-      const int p0 = (rest - cls * per_class) * T;
+      const int cls = rest & 7;
+      const int p0 = (rest >> 3) * T;
       tiles[q] = make_int4(level, cls, p0, min(T, parents - p0));
       return;
     }
@@ -127,7 +127,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   const int Kp = round_up(K, 8);
   const int node_base = level_offset(2);
   const int boxes = plan->n_nodes - node_base;
-  const int T = 128 / Kp;
+  const int T = plan->tc_m_tiles * (128 / Kp);
   int n_tiles = 0;
   if (use_tc)
     for (int level = plan->depth; level >= 2; --level) n_tiles += 8 * (((1 << (3 * (level - 1))) + T - 1) / T);
@@ -171,7 +171,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   if (e != cudaSuccess) return noalloc_fail(plan, CDFMM_B200_ERR_RUNTIME, std::string("scratch: ") + cudaGetErrorString(e));
   if (n_tiles > 0) noalloc_tiles_kernel<<<(n_tiles + 127) / 128, 128, 0, s>>>(dtiles, plan->depth, T, n_tiles);
 
-  launch_gather_moments(a->moments, a->moments_dtype, plan->src_perm, plan->ns, K, plan->scale, mom, s);
+  launch_gather_moments(a->moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, mom, s);
   cudaEventRecord(plan->ev_fork, s);
   cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0);
   launch_p2p(plan->src_rel, mom, plan->src_off, plan->tgt_rel, plan->tgt_off, plan->has_self ? plan->self_idx : nullptr,
@@ -198,6 +198,8 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
     ta.node_base = node_base;
     ta.zero_node = boxes;
     ta.stages = plan->tc_stages;
+    ta.m_tiles = plan->tc_m_tiles;
+    ta.acc_stride = plan->tc_acc_stride;
     ta.tmem_cols = plan->tc_tmem_cols;
     ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
     launch_m2l_tc(ta, n_tiles, s);
@@ -208,7 +210,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   for (int level = 3; level <= plan->depth; ++level)
     launch_l2l(L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level, static_cast<int>(plan->ops.l2l_pair_g.size()), s);
   cudaStreamWaitEvent(s, plan->ev_join, 0);
-  launch_l2p(L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, near, n, plan->p, K, plan->nt, plan->depth, a->output,
+  launch_l2p(L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, near, plan->basis, n, plan->p, K, plan->nt, plan->depth, a->output,
              a->layout, plan->phi_scale, a->field, a->potential, s);
   e = cudaGetLastError();
   if (e == cudaSuccess && a->synchronize) e = cudaStreamSynchronize(s);

@@ -59,15 +59,28 @@ template <typename T> void upload(T *dst, const T *src, size_t count, uint64_t &
   bytes += count * sizeof(T);
 }
 
+// Grows a device buffer to at least `need` elements (contents not kept).
+template <typename T> T *grow(T *&buf, size_t &have, size_t need, const char *what) {
+  if (have < need) {
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    have = 0;
+    check(cudaMalloc(reinterpret_cast<void **>(&buf), need * sizeof(T)), what);
+    have = need;
+  }
+  return buf;
+}
+
 void free_plan(cdfmm_b200_plan *p) {
   if (p == nullptr) return;
-  void *ptrs[] = {p->src_rel, p->tgt_rel, p->src_off, p->tgt_off, p->src_perm, p->tgt_perm,
+  void *ptrs[] = {p->src_rel, p->tgt_rel, p->src_off, p->tgt_off, p->src_perm, p->tgt_perm, p->src_inv, p->tgt_inv,
                   p->self_idx, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
-                  p->tc_b, p->tc_tiles, p->error_flag};
+                  p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
+  if (p->adjoint != nullptr) free_plan(p->adjoint);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   if (p->ev_join) cudaEventDestroy(p->ev_join);
   for (cudaEvent_t &e : p->ev_t)
@@ -204,6 +217,18 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     plan->scale = 2.0 * desc->root_half_width;
     plan->inv_scale3 = static_cast<float>(1.0 / (plan->scale * plan->scale * plan->scale));
     plan->phi_scale = static_cast<float>(plan->scale);
+    // Host copy of the geometry: the transposed (reverse-mode) plan is built
+    // from it on the first backward call.
+    if (plan->ns > 0) {
+      plan->h_src_pos.assign(desc->sorted_source_positions, desc->sorted_source_positions + 3 * static_cast<size_t>(plan->ns));
+      plan->h_src_perm.assign(desc->source_permutation, desc->source_permutation + plan->ns);
+    }
+    if (plan->nt > 0) {
+      plan->h_tgt_pos.assign(desc->sorted_target_positions, desc->sorted_target_positions + 3 * static_cast<size_t>(plan->nt));
+      plan->h_tgt_perm.assign(desc->target_permutation, desc->target_permutation + plan->nt);
+    }
+    plan->h_src_off.assign(desc->leaf_source_offsets, desc->leaf_source_offsets + n_leaves + 1);
+    plan->h_tgt_off.assign(desc->leaf_target_offsets, desc->leaf_target_offsets + n_leaves + 1);
 
     HostOperators &ops = plan->ops;
     ops = build_host_operators(plan->p, plan->depth, 16);
@@ -246,6 +271,22 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     upload(plan->tgt_off, desc->leaf_target_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
     upload(plan->src_perm, desc->source_permutation, static_cast<size_t>(plan->ns), h2d);
     upload(plan->tgt_perm, desc->target_permutation, static_cast<size_t>(plan->nt), h2d);
+    {
+      std::vector<int> inv(static_cast<size_t>(std::max(plan->ns, plan->nt)), -1);
+      for (int j = 0; j < plan->ns; ++j) {
+        require(inv[static_cast<size_t>(desc->source_permutation[j])] < 0, "source_permutation is not a permutation");
+        inv[static_cast<size_t>(desc->source_permutation[j])] = j;
+      }
+      plan->src_inv = dalloc<int>(plan->ns, bytes);
+      upload(plan->src_inv, inv.data(), static_cast<size_t>(plan->ns), h2d);
+      std::fill(inv.begin(), inv.end(), -1);
+      for (int j = 0; j < plan->nt; ++j) {
+        require(inv[static_cast<size_t>(desc->target_permutation[j])] < 0, "target_permutation is not a permutation");
+        inv[static_cast<size_t>(desc->target_permutation[j])] = j;
+      }
+      plan->tgt_inv = dalloc<int>(plan->nt, bytes);
+      upload(plan->tgt_inv, inv.data(), static_cast<size_t>(plan->nt), h2d);
+    }
 
     // operators
     std::vector<int8_t> basis(static_cast<size_t>(n) * 4);
@@ -378,9 +419,8 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     configure_p2p(smem);
     plan->p2m_chunk = 64;
     while (plan->p2m_chunk > 8 && p2m_smem_bytes(n, plan->p, static_cast<int>(K), plan->p2m_chunk) > smem) plan->p2m_chunk /= 2;
-    require(p2m_smem_bytes(n, plan->p, static_cast<int>(K), plan->p2m_chunk) <= smem &&
-                sizeof(float) * static_cast<size_t>(n) * K <= smem,
-            "order and max_states exceed the shared-memory budget of one CTA");
+    require(p2m_smem_bytes(n, plan->p, 4, plan->p2m_chunk) <= smem && l2p_smem_bytes(n, plan->p, 4) <= smem,
+            "order exceeds the shared-memory budget of one CTA");
     check(cudaDeviceSynchronize(), "plan upload");
     plan->error_flag = dalloc<int>(1, bytes);
     check(cudaMemset(plan->error_flag, 0, sizeof(int)), "cudaMemset");
@@ -392,17 +432,23 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
       cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, plan->device);
       const int Kpad = round_up(n, 16);
       const int Npad = round_up(n, 16);
+      // Two 128-row accumulators per CTA share each B tile (halving its
+      // traffic); pipeline stages fill the remaining shared memory.
+      const int acc_stride = round_up(Npad, 32);
+      const int m_tiles = 2 * acc_stride <= 512 ? 2 : 1;
       int stages = 0;
-      while (stages < 4 && m2l_tc_smem_bytes(Kpad, Npad, stages + 1) <= std::min<size_t>(smem, 210 * 1024)) ++stages;
-      plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 1 &&
+      while (stages < 8 && m2l_tc_smem_bytes(Npad, m_tiles, stages + 1) <= std::min<size_t>(smem, 224 * 1024)) ++stages;
+      plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 2 &&
                            desc->m2l_mode != CDFMM_B200_M2L_FP32 && desc->max_states >= 1 &&
                            configure_m2l_tc(smem);
       if (plan->tc_supported) {
         plan->tc_Kpad = Kpad;
         plan->tc_Npad = Npad;
         plan->tc_stages = stages;
+        plan->tc_m_tiles = m_tiles;
+        plan->tc_acc_stride = acc_stride;
         uint32_t cols = 32;
-        while (cols < static_cast<uint32_t>(Npad)) cols <<= 1;
+        while (cols < static_cast<uint32_t>(m_tiles * acc_stride)) cols <<= 1;
         plan->tc_tmem_cols = cols;
         plan->tc_Kp_max = round_up(std::min(plan->max_states, 128), 8);
         const size_t boxes = static_cast<size_t>(plan->n_nodes - level_offset(2)) + 1;
@@ -447,8 +493,10 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
   if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
   try {
     check(cudaSetDevice(plan->device), "cudaSetDevice");
+    plan->self_version += 1;
     if (sorted_self == nullptr) {
       plan->has_self = false;
+      plan->h_self.clear();
       return CDFMM_B200_OK;
     }
     for (int i = 0; i < plan->nt; ++i)
@@ -456,11 +504,97 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
     check(cudaDeviceSynchronize(), "sync");
     if (plan->nt > 0)
       check(cudaMemcpy(plan->self_idx, sorted_self, sizeof(int) * plan->nt, cudaMemcpyHostToDevice), "cudaMemcpy");
+    plan->h_self.assign(sorted_self, sorted_self + plan->nt);
     plan->has_self = true;
     return CDFMM_B200_OK;
   } catch (const AbiError &e) {
     return fail(plan, e.code, e.what());
   }
+}
+
+// Upward and downward far-field passes for K states whose sorted, scaled
+// moments are in plan->mom: P2M, M2M, M2L (tensor cores or FP32 SIMT), L2L,
+// leaving the leaf local expansions in plan->L.  Returns the launch count.
+static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing) {
+  const int n = plan->n;
+  int launches = 0;
+    launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
+               plan->p2m_chunk, s);
+    ++launches;
+    if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
+    for (int level = plan->depth - 1; level >= 0; --level) {
+      launch_m2m(plan->M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level,
+                 static_cast<int>(plan->ops.m2m_pair_g.size()), s);
+      ++launches;
+    }
+    if (timing) check(cudaEventRecord(plan->ev_t[3], s), "event");
+    const bool use_tc = plan->depth >= 2 && plan->tc_supported && K <= 128 &&
+                        (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || (plan->m2l_mode == CDFMM_B200_M2L_AUTO && K >= 8));
+    if (use_tc) {
+      const int Kp = round_up(K, 8);
+      if (plan->tc_tiles_Kp != Kp) {
+        // Work tiles: per level (deepest first), runs of T = m_tiles * (128 / Kp)
+        // consecutive parents in Morton order, the 8 parity classes of a run
+        // adjacent so that CTAs running together read the same source boxes
+        // (the run's parents' neighbours' children) from L2.
+        const int T = plan->tc_m_tiles * (128 / Kp);
+        std::vector<int4> tiles;
+        for (int level = plan->depth; level >= 2; --level) {
+          const int parents = 1 << (3 * (level - 1));
+          for (int p0 = 0; p0 < parents; p0 += T)
+            for (int cls = 0; cls < 8; ++cls) tiles.push_back(make_int4(level, cls, p0, std::min(T, parents - p0)));
+        }
+        check(cudaStreamSynchronize(s), "sync");
+        if (plan->tc_tiles_capacity < tiles.size()) {
+          if (plan->tc_tiles) cudaFree(plan->tc_tiles);
+          plan->tc_tiles = nullptr;
+          plan->tc_tiles_capacity = 0;
+          check(cudaMalloc(&plan->tc_tiles, tiles.size() * sizeof(int4)), "cudaMalloc tiles");
+          plan->tc_tiles_capacity = tiles.size();
+        }
+        check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
+        plan->tc_tiles_Kp = Kp;
+        plan->tc_n_tiles = static_cast<int>(tiles.size());
+      }
+      const int node_base = level_offset(2);
+      const int boxes = plan->n_nodes - node_base;
+      launch_m2l_pack(plan->M, plan->scale_m, plan->basis, plan->tc_a_hi, plan->tc_a_lo, n, K, Kp, plan->tc_Kpad,
+                      plan->depth, node_base, boxes, s);
+      TcArgs ta{};
+      ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
+      ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
+      ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b);
+      ta.tiles = plan->tc_tiles;
+      ta.scale_l = plan->scale_l;
+      ta.L = plan->L;
+      ta.error_flag = plan->error_flag;
+      ta.n = n;
+      ta.K = K;
+      ta.Kp = Kp;
+      ta.Kpad = plan->tc_Kpad;
+      ta.Npad = plan->tc_Npad;
+      ta.node_base = node_base;
+      ta.zero_node = boxes;
+      ta.stages = plan->tc_stages;
+      ta.m_tiles = plan->tc_m_tiles;
+      ta.acc_stride = plan->tc_acc_stride;
+      ta.tmem_cols = plan->tc_tmem_cols;
+      ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
+      launch_m2l_tc(ta, plan->tc_n_tiles, s);
+      launches += 2;
+    } else if (plan->depth >= 2) {
+      launch_m2l_simt(plan->M, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles,
+                      plan->n_tiles, n, plan->ops.m2l_ld, K, s);
+      ++launches;
+    }
+    plan->last_m2l_tc = use_tc;
+    if (timing) check(cudaEventRecord(plan->ev_t[4], s), "event");
+    for (int level = 3; level <= plan->depth; ++level) {
+      launch_l2l(plan->L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level,
+                 static_cast<int>(plan->ops.l2l_pair_g.size()), s);
+      ++launches;
+    }
+  return launches;
 }
 
 int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
@@ -530,7 +664,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       potential = out_phi_bytes > 0 ? reinterpret_cast<float *>(static_cast<char *>(plan->stage_out) + out_field_bytes) : nullptr;
     }
 
-    launch_gather_moments(moments, a->moments_dtype, plan->src_perm, plan->ns, K, plan->scale, plan->mom, s);
+    launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s);
     launches += plan->ns > 0 ? 1 : 0;
     if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
 
@@ -551,82 +685,11 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     if (!timing) check(cudaEventRecord(plan->ev_join, ns), "event");
 
     // far field
-    launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
-               plan->p2m_chunk, s);
-    ++launches;
-    if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
-    for (int level = plan->depth - 1; level >= 0; --level) {
-      launch_m2m(plan->M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level,
-                 static_cast<int>(plan->ops.m2m_pair_g.size()), s);
-      ++launches;
-    }
-    if (timing) check(cudaEventRecord(plan->ev_t[3], s), "event");
-    const bool use_tc = plan->depth >= 2 && plan->tc_supported && K <= 128 &&
-                        (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || (plan->m2l_mode == CDFMM_B200_M2L_AUTO && K >= 8));
-    if (use_tc) {
-      const int Kp = round_up(K, 8);
-      if (plan->tc_tiles_Kp != Kp) {
-        // Work tiles: per level (deepest first) and parity class, runs of
-        // T = 128 / Kp targets (consecutive parents in Morton order).
-        const int T = 128 / Kp;
-        std::vector<int4> tiles;
-        for (int level = plan->depth; level >= 2; --level) {
-          const int parents = 1 << (3 * (level - 1));
-          for (int cls = 0; cls < 8; ++cls)
-            for (int p0 = 0; p0 < parents; p0 += T) tiles.push_back(make_int4(level, cls, p0, std::min(T, parents - p0)));
-        }
-        check(cudaStreamSynchronize(s), "sync");
-        if (plan->tc_tiles_capacity < tiles.size()) {
-          if (plan->tc_tiles) cudaFree(plan->tc_tiles);
-          plan->tc_tiles = nullptr;
-          plan->tc_tiles_capacity = 0;
-          check(cudaMalloc(&plan->tc_tiles, tiles.size() * sizeof(int4)), "cudaMalloc tiles");
-          plan->tc_tiles_capacity = tiles.size();
-        }
-        check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
-        plan->tc_tiles_Kp = Kp;
-        plan->tc_n_tiles = static_cast<int>(tiles.size());
-      }
-      const int node_base = level_offset(2);
-      const int boxes = plan->n_nodes - node_base;
-      launch_m2l_pack(plan->M, plan->scale_m, plan->basis, plan->tc_a_hi, plan->tc_a_lo, n, K, Kp, plan->tc_Kpad,
-                      plan->depth, node_base, boxes, s);
-      TcArgs ta{};
-      ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
-      ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
-      ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b);
-      ta.tiles = plan->tc_tiles;
-      ta.scale_l = plan->scale_l;
-      ta.L = plan->L;
-      ta.error_flag = plan->error_flag;
-      ta.n = n;
-      ta.K = K;
-      ta.Kp = Kp;
-      ta.Kpad = plan->tc_Kpad;
-      ta.Npad = plan->tc_Npad;
-      ta.node_base = node_base;
-      ta.zero_node = boxes;
-      ta.stages = plan->tc_stages;
-      ta.tmem_cols = plan->tc_tmem_cols;
-      ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
-      launch_m2l_tc(ta, plan->tc_n_tiles, s);
-      launches += 2;
-    } else if (plan->depth >= 2) {
-      launch_m2l_simt(plan->M, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles,
-                      plan->n_tiles, n, plan->ops.m2l_ld, K, s);
-      ++launches;
-    }
-    plan->last_m2l_tc = use_tc;
-    if (timing) check(cudaEventRecord(plan->ev_t[4], s), "event");
-    for (int level = 3; level <= plan->depth; ++level) {
-      launch_l2l(plan->L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level,
-                 static_cast<int>(plan->ops.l2l_pair_g.size()), s);
-      ++launches;
-    }
+    launches += enqueue_far(plan, K, s, timing);
     if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
     if (!timing) check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
     if (timing) check(cudaEventRecord(plan->ev_t[6], s), "event");
-    launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->near, n, plan->p, K, plan->nt,
+    launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->near, plan->basis, n, plan->p, K, plan->nt,
                plan->depth, a->output, a->layout, plan->phi_scale, field, potential, s);
     ++launches;
     check(cudaGetLastError(), "kernel launch");
@@ -675,6 +738,160 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     plan->last_K = K;
     plan->stats.evaluations += 1;
     plan->stats.kernel_launches_last = static_cast<uint64_t>(launches);
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(plan, e.code, e.what());
+  } catch (const std::exception &e) {
+    return fail(plan, CDFMM_B200_ERR_RUNTIME, e.what());
+  }
+}
+
+// The transposed plan: sources and targets swapped, self map inverted.  The
+// exact transpose of the evaluated (discrete) FMM is the same FMM with the
+// two point sets exchanged: the M2L matrices satisfy T_o = T_o^t and
+// T_-o = S T_o S (S = diag((-1)^|alpha|)), P2M/L2P and M2M/L2L are transposes
+// of each other up to S and a sign, list1 and list2 are symmetric relations in
+// the uniform tree, and the dipole pair tensor is symmetric and even in r.
+static void ensure_adjoint(cdfmm_b200_plan *plan) {
+  if (plan->adjoint == nullptr) {
+    cdfmm_b200_plan_desc d{};
+    d.struct_size = sizeof d;
+    d.n_sources = plan->nt;
+    d.n_targets = plan->ns;
+    d.order = plan->p;
+    d.depth = plan->depth;
+    d.max_states = plan->max_states;
+    d.m2l_mode = plan->m2l_mode;
+    d.device = plan->device;
+    for (int a = 0; a < 3; ++a) d.root_centre[a] = plan->root_centre[a];
+    d.root_half_width = plan->root_half_width;
+    d.sorted_source_positions = plan->h_tgt_pos.data();
+    d.sorted_target_positions = plan->h_src_pos.data();
+    d.source_permutation = plan->h_tgt_perm.data();
+    d.target_permutation = plan->h_src_perm.data();
+    d.leaf_source_offsets = plan->h_tgt_off.data();
+    d.leaf_target_offsets = plan->h_src_off.data();
+    cdfmm_b200_plan *adj = nullptr;
+    const int rc = cdfmm_b200_plan_create(&d, &adj);
+    if (rc != CDFMM_B200_OK)
+      throw AbiError(rc, std::string("transposed plan: ") + cdfmm_b200_last_error(nullptr));
+    plan->adjoint = adj;
+    plan->adjoint_self_version = -1;
+  }
+  if (plan->adjoint_self_version != plan->self_version) {
+    int rc = CDFMM_B200_OK;
+    if (plan->h_self.empty()) {
+      rc = cdfmm_b200_set_self_indices(plan->adjoint, nullptr);
+    } else {
+      std::vector<int> inv(static_cast<size_t>(plan->ns), -1);
+      for (int t = 0; t < plan->nt; ++t) {
+        const int j = plan->h_self[static_cast<size_t>(t)];
+        if (j < 0) continue;
+        require(inv[static_cast<size_t>(j)] < 0,
+                "backward needs a one-to-one self map (two targets name the same self source)");
+        inv[static_cast<size_t>(j)] = t;
+      }
+      rc = cdfmm_b200_set_self_indices(plan->adjoint, inv.data());
+    }
+    if (rc != CDFMM_B200_OK) throw AbiError(rc, cdfmm_b200_last_error(plan->adjoint));
+    plan->adjoint_self_version = plan->self_version;
+  }
+}
+
+int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  try {
+    require(a != nullptr, "args is NULL");
+    require(a->struct_size == static_cast<int32_t>(sizeof(cdfmm_b200_backward_args)), "args.struct_size mismatch");
+    require(a->n_states >= 1 && a->n_states <= plan->max_states, "n_states must be in [1, max_states]");
+    require(a->grad_moments != nullptr || a->grad_target_positions != nullptr,
+            "request grad_moments and/or grad_target_positions");
+    require(plan->nt == 0 || a->grad_field != nullptr, "grad_field is NULL");
+    const bool want_x = a->grad_target_positions != nullptr;
+    if (want_x) {
+      require(plan->ns == 0 || a->moments != nullptr, "grad_target_positions needs the forward moments");
+      require(a->moments_dtype == 0 || a->moments_dtype == 1, "moments_dtype must be 0 (float32) or 1 (float64)");
+    }
+    check(cudaSetDevice(plan->device), "cudaSetDevice");
+    (void)cudaGetLastError();
+    const int K = a->n_states;
+    cudaStream_t s = static_cast<cudaStream_t>(a->stream);
+    const bool host_in = (a->memory & CDFMM_B200_MOMENTS_ON_HOST) != 0u;
+    const bool host_out = (a->memory & CDFMM_B200_RESULTS_ON_HOST) != 0u;
+
+    if (a->grad_moments != nullptr) {
+      // dL/dm = A^t dL/dH: the transposed plan evaluated on the weights.
+      ensure_adjoint(plan);
+      cdfmm_b200_eval_args e{};
+      e.moments = a->grad_field;
+      e.moments_dtype = 0;
+      e.n_states = K;
+      e.output = CDFMM_B200_OUTPUT_FIELD;
+      e.layout = CDFMM_B200_LAYOUT_SEPARATE;
+      e.field = a->grad_moments;
+      e.memory = a->memory;
+      e.stream = a->stream;
+      e.synchronize = 0;
+      const int rc = cdfmm_b200_evaluate(plan->adjoint, &e);
+      if (rc != CDFMM_B200_OK) throw AbiError(rc, std::string("transposed evaluate: ") + cdfmm_b200_last_error(plan->adjoint));
+    }
+
+    if (want_x && plan->nt > 0) {
+      // dL/dx_target: forward moments -> leaf locals (far pass), then the P2P
+      // gradient partial sums and the L2P second-derivative kernel.
+      const size_t mom_in_bytes = static_cast<size_t>(K) * plan->ns * 3 * (a->moments_dtype == 1 ? 8 : 4);
+      const size_t w_in_bytes = static_cast<size_t>(K) * plan->nt * 3 * sizeof(float);
+      const size_t out_bytes = static_cast<size_t>(plan->nt) * 3 * sizeof(float);
+      const void *moments = a->moments;
+      const void *weights = a->grad_field;
+      float *out = a->grad_target_positions;
+      if (host_in || host_out) {
+        const size_t need = (host_in ? mom_in_bytes + w_in_bytes : 0) + (host_out ? out_bytes : 0) + 64;
+        char *stage = grow(reinterpret_cast<char *&>(plan->stage_grad), plan->stage_grad_bytes, need, "cudaMalloc staging");
+        size_t off = 0;
+        if (host_in) {
+          if (mom_in_bytes > 0)
+            check(cudaMemcpyAsync(stage, a->moments, mom_in_bytes, cudaMemcpyHostToDevice, s), "H2D moments");
+          check(cudaMemcpyAsync(stage + mom_in_bytes, a->grad_field, w_in_bytes, cudaMemcpyHostToDevice, s),
+                "H2D grad_field");
+          plan->stats.evaluation_h2d_bytes += mom_in_bytes + w_in_bytes;
+          plan->stats.evaluation_h2d_calls += mom_in_bytes > 0 ? 2 : 1;
+          moments = stage;
+          weights = stage + mom_in_bytes;
+          off = (mom_in_bytes + w_in_bytes + 15) & ~static_cast<size_t>(15);
+        }
+        if (host_out) out = reinterpret_cast<float *>(stage + off);
+      }
+      const int G = p2p_grad_groups(K);
+      float4 *W = grow(plan->wbuf, plan->wbuf_count, static_cast<size_t>(plan->nt) * K, "cudaMalloc weights");
+      float4 *gpart = grow(plan->gpart, plan->gpart_count, static_cast<size_t>(plan->nt) * G, "cudaMalloc partials");
+      launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s);
+      launch_gather_moments(weights, 0, plan->tgt_inv, plan->nt, K, 1.0, W, s);
+      enqueue_far(plan, K, s, false);
+      launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
+                      plan->has_self ? plan->self_idx : nullptr, plan->depth, K, W, gpart, s);
+      launch_l2p_grad(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, W, gpart, G, plan->n, plan->p, K,
+                      plan->nt, plan->depth, static_cast<float>(1.0 / plan->scale), out, s);
+      check(cudaGetLastError(), "kernel launch");
+      if (host_out) {
+        check(cudaMemcpyAsync(a->grad_target_positions, out, out_bytes, cudaMemcpyDeviceToHost, s), "D2H gradient");
+        plan->stats.evaluation_d2h_bytes += out_bytes;
+        plan->stats.evaluation_d2h_calls += 1;
+      }
+    }
+    if (a->synchronize || host_in || host_out) {
+      check(cudaStreamSynchronize(s), "backward");
+      int flag = 0;
+      check(cudaMemcpy(&flag, plan->error_flag, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+      if (flag == 0 && plan->adjoint != nullptr)
+        check(cudaMemcpy(&flag, plan->adjoint->error_flag, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
+      if (flag != 0) {
+        cudaMemset(plan->error_flag, 0, sizeof(int));
+        if (plan->adjoint != nullptr) cudaMemset(plan->adjoint->error_flag, 0, sizeof(int));
+        throw AbiError(CDFMM_B200_ERR_TIMEOUT, "tensor-core M2L: a bounded wait expired (code " + std::to_string(flag) +
+                                                   "); results are invalid");
+      }
+    }
     return CDFMM_B200_OK;
   } catch (const AbiError &e) {
     return fail(plan, e.code, e.what());

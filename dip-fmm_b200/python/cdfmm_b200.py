@@ -40,7 +40,7 @@ EXPORTED = (
     "cdfmm_b200_plan_destroy", "cdfmm_b200_set_self_indices", "cdfmm_b200_evaluate",
     "cdfmm_b200_read_expansions", "cdfmm_b200_set_timing", "cdfmm_b200_get_stats",
     "cdfmm_b200_direct_fp64", "cdfmm_b200_m2l_matrix", "cdfmm_b200_last_error",
-    "cdfmm_b200_evaluate_noalloc",
+    "cdfmm_b200_evaluate_noalloc", "cdfmm_b200_backward",
 )
 
 # Scratch capacity of cdfmm_b200_evaluate_noalloc (bytes).
@@ -64,6 +64,15 @@ class EvalArgs(ctypes.Structure):
         ("moments", ctypes.c_void_p), ("moments_dtype", ctypes.c_int32), ("n_states", ctypes.c_int32),
         ("output", ctypes.c_uint32), ("layout", ctypes.c_int32), ("field", ctypes.c_void_p),
         ("potential", ctypes.c_void_p), ("memory", ctypes.c_uint32), ("stream", ctypes.c_void_p),
+        ("synchronize", ctypes.c_int32),
+    ]
+
+
+class BackwardArgs(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("n_states", ctypes.c_int32), ("grad_field", ctypes.c_void_p),
+        ("moments", ctypes.c_void_p), ("moments_dtype", ctypes.c_int32), ("grad_moments", ctypes.c_void_p),
+        ("grad_target_positions", ctypes.c_void_p), ("memory", ctypes.c_uint32), ("stream", ctypes.c_void_p),
         ("synchronize", ctypes.c_int32),
     ]
 
@@ -112,6 +121,7 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_set_self_indices.argtypes = [vp, vp]
     lib.cdfmm_b200_evaluate.argtypes = [vp, ctypes.POINTER(EvalArgs)]
     lib.cdfmm_b200_evaluate_noalloc.argtypes = [vp, ctypes.POINTER(EvalArgs)]
+    lib.cdfmm_b200_backward.argtypes = [vp, ctypes.POINTER(BackwardArgs)]
     lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
     lib.cdfmm_b200_set_timing.argtypes = [vp, i32]
     lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -303,8 +313,95 @@ class DevicePlan:
         a.synchronize = 1 if synchronize else 0
         _check(library().cdfmm_b200_evaluate_noalloc(self._h, ctypes.byref(a)), self._h)
 
+    def backward(self, grad_field, moments=None, grad_moments=None, grad_target_positions=None,
+                 want_moments=True, want_positions=False, stream=None, synchronize=True, memory=None):
+        """Reverse mode of `evaluate` for L = sum w . H with w = grad_field
+        (K, n_targets, 3) float32: returns {"moments": dL/dm (K, n_sources, 3),
+        "positions": dL/dx_target (n_targets, 3), summed over states}.
+        `moments` (the forward ones) are needed for the position gradient.
+        numpy inputs give numpy outputs; for tensors the caller supplies the
+        outputs it asks for."""
+        is_tensor = hasattr(grad_field, "data_ptr")
+        if is_tensor:
+            K = int(grad_field.shape[0]) if len(grad_field.shape) == 3 else 1
+            if memory is None:
+                memory = 0 if getattr(grad_field, "is_cuda", False) else MOMENTS_ON_HOST | RESULTS_ON_HOST
+        else:
+            grad_field = np.ascontiguousarray(grad_field, dtype=np.float32)
+            K = grad_field.shape[0] if grad_field.ndim == 3 else 1
+            memory = MOMENTS_ON_HOST | RESULTS_ON_HOST
+            if moments is not None:
+                moments = np.ascontiguousarray(moments)
+                if moments.dtype not in (np.float32, np.float64):
+                    moments = moments.astype(np.float64)
+            if want_moments and grad_moments is None:
+                grad_moments = np.zeros((K, self.n_sources, 3), dtype=np.float32)
+            if want_positions and grad_target_positions is None:
+                grad_target_positions = np.zeros((self.n_targets, 3), dtype=np.float32)
+        a = BackwardArgs()
+        a.struct_size = ctypes.sizeof(BackwardArgs)
+        a.n_states = K
+        a.grad_field = _ptr(grad_field).value
+        a.moments = _ptr(moments).value if moments is not None else None
+        a.moments_dtype = 1 if moments is not None and str(moments.dtype).endswith("float64") else 0
+        a.grad_moments = _ptr(grad_moments).value if (want_moments and grad_moments is not None) else None
+        a.grad_target_positions = (_ptr(grad_target_positions).value
+                                   if (want_positions and grad_target_positions is not None) else None)
+        a.memory = memory
+        a.stream = stream
+        a.synchronize = 1 if synchronize else 0
+        _check(library().cdfmm_b200_backward(self._h, ctypes.byref(a)), self._h)
+        return {"moments": grad_moments if want_moments else None,
+                "positions": grad_target_positions if want_positions else None}
+
     def read_expansions(self, which="multipole", state=0) -> np.ndarray:
         out = np.zeros(self.n_nodes * self.n_coefficients, dtype=np.float32)
         w = 0 if which == "multipole" else 1
         _check(library().cdfmm_b200_read_expansions(self._h, w, state, _ptr(out), out.size), self._h)
         return out.reshape(self.n_nodes, self.n_coefficients)
+
+
+def dipole_field(plan: DevicePlan, moments, target_positions=None):
+    """Differentiable field H = FMM(moments) on `plan`'s fixed geometry.
+
+    moments: CUDA float32 tensor (K, n_sources, 3) (or (n_sources, 3));
+    target_positions: optional CUDA tensor (n_targets, 3) holding the plan's
+    target positions (user order).  It is not read -- the geometry is the
+    plan's -- but gradients flow to it: dL/dx = sum over states of the
+    position gradient.  Returns (K, n_targets, 3) float32 (squeezed like the
+    input).  torch.autograd.Function wrapper of cdfmm_b200_evaluate /
+    cdfmm_b200_backward, on the current CUDA stream, no host copies.
+    """
+    import torch
+
+    class _DipoleField(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, m, x):
+            squeeze = m.dim() == 2
+            m3 = (m.unsqueeze(0) if squeeze else m).contiguous()
+            if m3.dtype != torch.float32:
+                m3 = m3.float()
+            H = torch.empty((m3.shape[0], plan.n_targets, 3), dtype=torch.float32, device=m3.device)
+            plan.evaluate(m3, output="field", field=H, stream=torch.cuda.current_stream(m3.device).cuda_stream,
+                          synchronize=False)
+            ctx.save_for_backward(m3)
+            ctx.squeeze = squeeze
+            return H.squeeze(0) if squeeze else H
+
+        @staticmethod
+        def backward(ctx, gH):
+            (m3,) = ctx.saved_tensors
+            g3 = (gH.unsqueeze(0) if ctx.squeeze else gH).contiguous().float()
+            want_m = ctx.needs_input_grad[0]
+            want_x = ctx.needs_input_grad[1]
+            gm = torch.empty_like(m3) if want_m else None
+            gx = torch.empty((plan.n_targets, 3), dtype=torch.float32, device=m3.device) if want_x else None
+            if want_m or want_x:
+                plan.backward(g3, moments=m3, grad_moments=gm, grad_target_positions=gx, want_moments=want_m,
+                              want_positions=want_x, stream=torch.cuda.current_stream(m3.device).cuda_stream,
+                              synchronize=False)
+            if gm is not None and ctx.squeeze:
+                gm = gm.squeeze(0)
+            return gm, gx
+
+    return _DipoleField.apply(moments, target_positions)

@@ -168,6 +168,33 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args)
  * The plan itself is created (and allocated) by cdfmm_b200_plan_create. */
 int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args);
 
+/* Reverse mode (no counterpart in the reference, whose evaluate is not
+ * differentiable).  For a loss L = sum_k sum_i w_ik . H_ik of the field of
+ * cdfmm_b200_evaluate, with w = dL/dH given:
+ *  - grad_moments[k][j][c] = dL/dm_jkc, the exact transpose of the evaluated
+ *    (discrete, FP32) FMM applied to w: the same FMM with sources and targets
+ *    exchanged, run by a transposed plan that the first call builds (it
+ *    needs a one-to-one self map);
+ *  - grad_target_positions[i][c] = dL/dx_ic summed over the states, from the
+ *    second derivatives of the leaf local expansions (one Taylor order beyond
+ *    L2P) and the analytic gradient of the list1 pair field; this needs the
+ *    forward moments, whose far pass is recomputed.
+ * Arrays use user order and physical units like cdfmm_b200_evaluate. */
+typedef struct cdfmm_b200_backward_args {
+  int32_t struct_size;          /* sizeof(cdfmm_b200_backward_args) */
+  int32_t n_states;             /* K, 1..max_states */
+  const float *grad_field;      /* [n_states][n_targets][3] dL/dH */
+  const void *moments;          /* [n_states][n_sources][3] forward moments (for grad_target_positions) */
+  int32_t moments_dtype;        /* 0 = float32, 1 = float64 */
+  float *grad_moments;          /* [n_states][n_sources][3] output, or NULL */
+  float *grad_target_positions; /* [n_targets][3] output (sum over states), or NULL */
+  uint32_t memory;              /* MOMENTS_ON_HOST: grad_field and moments on the host;
+                                   RESULTS_ON_HOST: the outputs on the host */
+  void *stream;                 /* cudaStream_t; NULL = the legacy default stream */
+  int32_t synchronize;          /* nonzero: return only after the outputs are complete */
+} cdfmm_b200_backward_args;
+int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *args);
+
 /* Copies the FP32 multipole (which = 0) or local (which = 1) expansions of one
  * state of the last evaluate to host memory as out[node][coefficient], node in
  * flat level-wise Morton order and coefficients in the total-degree basis

@@ -43,6 +43,7 @@ def library() -> ctypes.CDLL:
     lib.oracle_tree.restype = i
     lib.oracle_lists.argtypes = [i, P(i), P(i), P(i), P(i)]
     lib.oracle_direct.argtypes = [i, P(d), P(d), i, P(d), P(i), i, P(d), P(d)]
+    lib.oracle_direct_grad.argtypes = [i, P(d), P(d), i, P(d), P(i), P(d), P(d)]
     lib.oracle_fmm.argtypes = [i, P(d), i, P(d), i, i, i, P(d), d, P(d), P(i), i, P(d), P(d), P(d), P(d)]
     lib.oracle_fmm.restype = i
     _LIB = lib
@@ -131,6 +132,16 @@ def direct(sources, moments, targets, self_indices=None, flags=3):
     ids = _i32(self_indices)
     lib.oracle_direct(len(s), _dp(s), _dp(m), len(t), _dp(t), _ip(ids), flags, _dp(phi), _dp(H))
     return phi, H
+
+
+def direct_grad(sources, moments, targets, weights, self_indices=None):
+    """FP64 direct gradient of L = sum_i w_i . H_i w.r.t. the target positions."""
+    lib = library()
+    s, m, t = _f64(sources).reshape(-1, 3), _f64(moments).reshape(-1, 3), _f64(targets).reshape(-1, 3)
+    w = _f64(weights).reshape(-1, 3)
+    g = np.zeros((len(t), 3))
+    lib.oracle_direct_grad(len(s), _dp(s), _dp(m), len(t), _dp(t), _ip(_i32(self_indices)), _dp(w), _dp(g))
+    return g
 
 
 def fmm(sources, targets, moments, order, depth, identities=None, flags=3, root_centre=None,

@@ -388,6 +388,35 @@ void oracle_direct(int ns, const double *src, const double *mom, int nt, const d
   }
 }
 
+/* Position gradient of L = sum_i w_i . H_i (direct sum, FP64) with respect
+ * to the target positions.  The reference has no reverse mode; this is the
+ * analytic derivative of the pair field of pair_add:
+ *   grad_t [w . H_pair] = (3/|r|^5)[(w.r) m + (m.r) w + (w.m) r] - 15 (m.r)(w.r) r / |r|^7
+ * (times 1/(4 pi)), summed over sources j != self[i]. */
+void oracle_direct_grad(int ns, const double *src, const double *mom, int nt, const double *tgt, const int *self,
+                        const double *w, double *g) {
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < nt; ++i) {
+    double acc[3] = {0.0, 0.0, 0.0};
+    const int me = self != NULL ? self[i] : -1;
+    const double *wi = w + 3 * i;
+    for (int j = 0; j < ns; ++j) {
+      if (j == me) continue;
+      const double *m = mom + 3 * j;
+      const double r[3] = {tgt[3 * i] - src[3 * j], tgt[3 * i + 1] - src[3 * j + 1], tgt[3 * i + 2] - src[3 * j + 2]};
+      const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      const double rinv = 1.0 / sqrt(r2);
+      const double rinv5 = rinv * rinv * rinv * rinv * rinv;
+      const double a = m[0] * r[0] + m[1] * r[1] + m[2] * r[2];
+      const double b = wi[0] * r[0] + wi[1] * r[1] + wi[2] * r[2];
+      const double c = wi[0] * m[0] + wi[1] * m[1] + wi[2] * m[2];
+      for (int d = 0; d < 3; ++d)
+        acc[d] += 3.0 * rinv5 * (b * m[d] + a * wi[d] + c * r[d]) - 15.0 * rinv5 * rinv * rinv * a * b * r[d];
+    }
+    for (int d = 0; d < 3; ++d) g[3 * i + d] = acc[d] * ORACLE_INV_4PI;
+  }
+}
+
 /* ------------------------------------------------------------------ FMM */
 typedef struct {
   int level;
