@@ -20,7 +20,9 @@ Reported beside `value` (device-resident inputs):
   rel_l2_*      accuracy of state 0 vs the FP64 direct sum on 16,384 targets;
   roofline      dominant kernel: algorithmic work / CUDA-event duration;
   cpu_baseline  the reference CpuStatic (oracle/_ref, built from the upstream
-                sources) on the host cores, on a bounded sample.
+                sources) on the host cores, on a bounded sample;
+  backward      reverse mode on the same workload: device time of the field
+                forward and of the backward (dL/dmoments + dL/dtarget-positions).
 --impl reference times the reference CpuStatic path (FP32, field+potential)
 on the host cores on that same bounded sample and prints the same line.
 """
@@ -67,6 +69,7 @@ def parse_args():
     ap.add_argument("--plain-states", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-backward", action="store_true")
     return ap.parse_args()
 
 
@@ -341,6 +344,40 @@ def b200_arm(args):
     plain_value = N * world / (ms_state_plain * 1e-3)
     plain_plan.close()
 
+    # Reverse mode on the same workload: the forward (field output) against
+    # the backward of L = sum w . H giving dL/dmoments (transposed plan) and
+    # dL/dtarget-positions, both device-timed on the bench stream.
+    backward = None
+    if not args.no_backward:
+        dW = torch.from_numpy(np.random.default_rng(args.seed + 3).normal(size=(K, N, 3)).astype(np.float32)).cuda()
+        gm = torch.empty_like(dm)
+        gx = torch.empty((N, 3), dtype=torch.float32, device="cuda")
+
+        def fwd():
+            plan.evaluate(dm, output="field", field=dH, stream=stream.cuda_stream, synchronize=False)
+
+        def bwd():
+            plan.backward(dW, moments=dm, grad_moments=gm, grad_target_positions=gx, want_moments=True,
+                          want_positions=True, stream=stream.cuda_stream, synchronize=False)
+
+        def timed(fn, reps):
+            fn()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(reps):
+                fn()
+            b.record(stream)
+            torch.cuda.synchronize()
+            return max_over_ranks(a.elapsed_time(b) / reps)
+
+        reps = max(1, args.steps)
+        ms_f = timed(fwd, reps)
+        ms_b = timed(bwd, reps)
+        backward = {"ms_forward_field": ms_f, "ms_backward": ms_b, "backward_over_forward": ms_b / ms_f,
+                    "outputs": "dL/dmoments (K x N x 3) + dL/dtarget_positions (N x 3), L = sum w.H"}
+        del dW, gm, gx
+
     if rank != 0:
         if dist is not None:
             dist.barrier()
@@ -386,6 +423,7 @@ def b200_arm(args):
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_state": ms_state_plain, "states_timed": ks,
                   "m2l": "fp32"},
         "batched_over_plain": value / plain_value,
+        "backward": backward,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:

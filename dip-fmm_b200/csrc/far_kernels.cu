@@ -86,6 +86,55 @@ __device__ inline void monomials(float dx, float dy, float dz, int q, float *out
 constexpr int kP2mThreads = 256;
 constexpr int kP2mChunk = 32;
 
+// Few states (K < 4): one thread per (alpha, state) accumulator, sources
+// staged in chunks with their monomials (the register tiles below would
+// leave most lanes idle).
+__global__ void __launch_bounds__(128) p2m_small_kernel(const float4 *__restrict__ src_rel,
+                                                        const float4 *__restrict__ mom,
+                                                        const int *__restrict__ src_off,
+                                                        const int8_t *__restrict__ basis, float *__restrict__ M,
+                                                        int n, int p, int K, int leaf_node_base) {
+  __shared__ float mono[kP2mChunk * 220];
+  __shared__ float4 smom[kP2mChunk * 3];
+  const int nm1 = basis_size_d(p - 1);
+  const int leaf = blockIdx.x;
+  const int s0 = src_off[leaf];
+  const int s1 = src_off[leaf + 1];
+  const int items = n * K;
+  float *out = M + static_cast<long long>(leaf_node_base + leaf) * items;
+  for (int base = 0; base < items; base += blockDim.x) {
+    const int q = base + threadIdx.x;
+    const bool valid = q < items;
+    const int a = valid ? q / K : 0;
+    const int k = valid ? q - a * K : 0;
+    const int ax = basis[4 * a], ay = basis[4 * a + 1], az = basis[4 * a + 2];
+    const int ix = ax > 0 ? rank3(ax - 1, ay, az) : -1;
+    const int iy = ay > 0 ? rank3(ax, ay - 1, az) : -1;
+    const int iz = az > 0 ? rank3(ax, ay, az - 1) : -1;
+    float v = 0.0F;
+    for (int c0 = s0; c0 < s1; c0 += kP2mChunk) {
+      const int cn = min(kP2mChunk, s1 - c0);
+      __syncthreads();
+      for (int j = threadIdx.x; j < cn; j += blockDim.x) {
+        const float4 d = src_rel[c0 + j];
+        if (nm1 > 0) monomials(d.x, d.y, d.z, p - 1, mono + j * nm1);
+      }
+      for (int e = threadIdx.x; e < cn * K; e += blockDim.x) smom[e] = mom[static_cast<long long>(c0) * K + e];
+      __syncthreads();
+      if (valid) {
+        for (int j = 0; j < cn; ++j) {
+          const float4 m = smom[j * K + k];
+          const float *mj = mono + j * nm1;
+          if (ix >= 0) v = fmaf(m.x, mj[ix], v);
+          if (iy >= 0) v = fmaf(m.y, mj[iy], v);
+          if (iz >= 0) v = fmaf(m.z, mj[iz], v);
+        }
+      }
+    }
+    if (valid) out[q] = ((ax + ay + az) & 1) ? -v : v;
+  }
+}
+
 __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restrict__ src_rel,
                                                           const float4 *__restrict__ mom,
                                                           const int *__restrict__ src_off,
@@ -256,10 +305,13 @@ __global__ void __launch_bounds__(256) l2l_kernel(float *__restrict__ L, const i
 }
 
 // ---------------------------------------------------------------------------
-// L2P + combine + unsort (upstream docs/math.md L2P; src/cuda_fmm.cu:503-516):
+// L2P + combine (upstream docs/math.md L2P; src/cuda_fmm.cu:503-516):
 //   phi = sum_b L_b dx^b/b!,  H_c = -sum_{|mu| <= p-1} L_{mu+e_c} dx^mu/mu!
 // then result = far + near (near from the P2P kernel), phi times the root
-// width, written at the target's user index.  One CTA per leaf; the leaf's
+// width, written back over near[target][state] (sorted order); the unsort
+// kernel below moves it to user order with contiguous writes.  (Writing user
+// order here would scatter 4-byte stores over the whole output.)  One CTA
+// per leaf; the leaf's
 // local expansion (n x Kc states, a state block) and the monomials of up to
 // 32 targets ([b][t]) are staged in shared memory; a thread owns a register
 // tile of 4 targets x 4 consecutive states, reading float4 quads of both
@@ -285,12 +337,10 @@ __device__ inline void monomials_strided(float dx, float dy, float dz, int q, fl
 }
 
 __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restrict__ L, const float4 *__restrict__ tgt_rel,
-                                                          const int *__restrict__ tgt_off, const int *__restrict__ tgt_perm,
-                                                          const float4 *__restrict__ near,
-                                                          const int8_t *__restrict__ basis, int n, int p, int K, int nt,
-                                                          int leaf_node_base, unsigned output, int layout,
-                                                          float phi_scale, float *__restrict__ field,
-                                                          float *__restrict__ potential, int Kb) {
+                                                          const int *__restrict__ tgt_off, float4 *__restrict__ near,
+                                                          const int8_t *__restrict__ basis, int n, int p, int K,
+                                                          int leaf_node_base, unsigned output, float phi_scale,
+                                                          int Kb) {
   extern __shared__ float4 l2p_smem[];
   const int Kbp = (Kb + 3) & ~3;
   float *sL = reinterpret_cast<float *>(l2p_smem);                 // [n][Kcp]
@@ -381,32 +431,130 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
           const int t = 4 * tq + u;
           if (t >= tn) break;
           const int i = tc + t;
-          const int usr = tgt_perm[i];
 #pragma unroll
           for (int v = 0; v < 4; ++v) {
             const int kl = 4 * kq + v;
             if (kl >= Kc) break;
             const int k = kblk + kl;
-            const float4 nr = near[static_cast<long long>(i) * K + k];
-            const float rphi = want_phi ? (ph[u][v] + nr.x) * phi_scale : 0.0F;
-            const float rx = want_h ? nr.y - hx[u][v] : 0.0F;
-            const float ry = want_h ? nr.z - hy[u][v] : 0.0F;
-            const float rz = want_h ? nr.w - hz[u][v] : 0.0F;
-            const long long o = static_cast<long long>(k) * nt + usr;
-            if (layout == 1) {
-              reinterpret_cast<float4 *>(field)[o] = make_float4(rphi, rx, ry, rz);
-            } else {
-              if (want_h) {
-                field[3 * o] = rx;
-                field[3 * o + 1] = ry;
-                field[3 * o + 2] = rz;
-              }
-              if (want_phi && potential != nullptr) potential[o] = rphi;
-            }
+            float4 *nr = near + static_cast<long long>(i) * K + k;
+            const float4 nv = *nr;
+            *nr = make_float4(want_phi ? (ph[u][v] + nv.x) * phi_scale : 0.0F, want_h ? nv.y - hx[u][v] : 0.0F,
+                              want_h ? nv.z - hy[u][v] : 0.0F, want_h ? nv.w - hz[u][v] : 0.0F);
           }
         }
       }
     }
+  }
+}
+
+// Few states (K < 4): one thread per (target, state), writing user order
+// directly.
+__global__ void __launch_bounds__(128) l2p_small_kernel(const float *__restrict__ L, const float4 *__restrict__ tgt_rel,
+                                                        const int *__restrict__ tgt_off, const int *__restrict__ tgt_perm,
+                                                        const float4 *__restrict__ near, int n, int p, int K, int nt,
+                                                        int leaf_node_base, unsigned output, int layout,
+                                                        float phi_scale, float *__restrict__ field,
+                                                        float *__restrict__ potential) {
+  __shared__ float sL[286 * 3];
+  const int leaf = blockIdx.x;
+  const int t0 = tgt_off[leaf];
+  const int t1 = tgt_off[leaf + 1];
+  if (t0 == t1) return;
+  const float *src = L + static_cast<long long>(leaf_node_base + leaf) * n * K;
+  for (int q = threadIdx.x; q < n * K; q += blockDim.x) sL[q] = src[q];
+  __syncthreads();
+  const bool want_phi = (output & 1u) != 0u;
+  const bool want_h = (output & 2u) != 0u;
+  for (int it = threadIdx.x; it < (t1 - t0) * K; it += blockDim.x) {
+    const int k = it / (t1 - t0);
+    const int i = t0 + (it - k * (t1 - t0));
+    const float4 d = tgt_rel[i];
+    float phi = 0.0F, hx = 0.0F, hy = 0.0F, hz = 0.0F;
+    float xa = 1.0F;
+    for (int a = 0; a <= p; ++a) {
+      float xb = xa;
+      for (int b = 0; a + b <= p; ++b) {
+        float xc = xb;
+        for (int c = 0; a + b + c <= p; ++c) {
+          const int deg = a + b + c;
+          if (want_phi) phi = fmaf(sL[rank3(a, b, c) * K + k], xc, phi);
+          if (want_h && deg < p) {
+            hx = fmaf(sL[rank3(a + 1, b, c) * K + k], xc, hx);
+            hy = fmaf(sL[rank3(a, b + 1, c) * K + k], xc, hy);
+            hz = fmaf(sL[rank3(a, b, c + 1) * K + k], xc, hz);
+          }
+          xc = xc * d.z * kInvInt[c + 1];
+        }
+        xb = xb * d.y * kInvInt[b + 1];
+      }
+      xa = xa * d.x * kInvInt[a + 1];
+    }
+    const float4 nr = near[static_cast<long long>(i) * K + k];
+    const float rphi = want_phi ? (phi + nr.x) * phi_scale : 0.0F;
+    const float rx = want_h ? nr.y - hx : 0.0F;
+    const float ry = want_h ? nr.z - hy : 0.0F;
+    const float rz = want_h ? nr.w - hz : 0.0F;
+    const long long o = static_cast<long long>(k) * nt + tgt_perm[i];
+    if (layout == 1) {
+      reinterpret_cast<float4 *>(field)[o] = make_float4(rphi, rx, ry, rz);
+    } else {
+      if (want_h) {
+        field[3 * o] = rx;
+        field[3 * o + 1] = ry;
+        field[3 * o + 2] = rz;
+      }
+      if (want_phi && potential != nullptr) potential[o] = rphi;
+    }
+  }
+}
+
+// Sorted results res[nt][K] (phi, Hx, Hy, Hz) -> user order: field[K][nt][3]
+// and potential[K][nt] (layout 0) or field[K][nt][4] (layout 1).  A CTA takes
+// 32 consecutive user indices and 32 states through a shared tile: the reads
+// are contiguous runs of each sorted row (inv = user -> sorted), the writes
+// contiguous runs of each state's user array.
+__global__ void __launch_bounds__(256) unsort_results_kernel(const float4 *__restrict__ res, const int *__restrict__ inv,
+                                                             int nt, int K, unsigned output, int layout,
+                                                             float *__restrict__ field, float *__restrict__ potential) {
+  __shared__ float4 tile[32][33];
+  const int u0 = blockIdx.x * 32;
+  const int nu = min(32, nt - u0);
+  const bool want_phi = (output & 1u) != 0u;
+  const bool want_h = (output & 2u) != 0u;
+  for (int kc = 0; kc < K; kc += 32) {
+    const int kn = min(32, K - kc);
+    for (int e = threadIdx.x; e < nu * kn; e += blockDim.x) {
+      const int t = e / kn;
+      const int k = e - t * kn;
+      tile[t][k] = res[static_cast<long long>(inv[u0 + t]) * K + kc + k];
+    }
+    __syncthreads();
+    if (layout == 1) {
+      for (int e = threadIdx.x; e < kn * nu; e += blockDim.x) {
+        const int k = e / nu;
+        const int t = e - k * nu;
+        reinterpret_cast<float4 *>(field)[static_cast<long long>(kc + k) * nt + u0 + t] = tile[t][k];
+      }
+    } else {
+      if (want_h) {
+        for (int e = threadIdx.x; e < kn * nu * 3; e += blockDim.x) {
+          const int k = e / (nu * 3);
+          const int r = e - k * nu * 3;
+          const int t = r / 3;
+          const int c = r - 3 * t;
+          const float4 v = tile[t][k];
+          field[(static_cast<long long>(kc + k) * nt + u0) * 3 + r] = c == 0 ? v.y : (c == 1 ? v.z : v.w);
+        }
+      }
+      if (want_phi && potential != nullptr) {
+        for (int e = threadIdx.x; e < kn * nu; e += blockDim.x) {
+          const int k = e / nu;
+          const int t = e - k * nu;
+          potential[static_cast<long long>(kc + k) * nt + u0 + t] = tile[t][k].x;
+        }
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -530,6 +678,10 @@ void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, co
                 float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s) {
   (void)chunk;
   const int leaves = 1 << (3 * depth);
+  if (K < 4) {
+    p2m_small_kernel<<<leaves, 128, 0, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth));
+    return;
+  }
   const int Kb = p2m_state_block(p, K);
   const size_t smem = p2m_smem_bytes(n, p, Kb, 0);
   p2m_kernel<<<leaves, kP2mThreads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb);
@@ -561,15 +713,22 @@ size_t l2p_smem_bytes(int n, int p, int Kb) {
          sizeof(short) * 3 * static_cast<size_t>(basis_size_d(p - 1)) + 16;
 }
 
-void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
-                const float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
+void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm, const int *tgt_inv,
+                float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
                 int layout, float phi_scale, float *field, float *potential, cudaStream_t s) {
+  if (nt == 0) return;
   const int leaves = 1 << (3 * depth);
+  if (K < 4) {
+    l2p_small_kernel<<<leaves, 128, 0, s>>>(L, tgt_rel, tgt_off, tgt_perm, near, n, p, K, nt, level_offset_d(depth),
+                                            output, layout, phi_scale, field, potential);
+    return;
+  }
   int Kb = std::min(K, 64);
   while (Kb > 4 && l2p_smem_bytes(n, p, Kb) > 60 * 1024) Kb = (Kb + 1) / 2;
   const size_t smem = l2p_smem_bytes(n, p, Kb);
-  l2p_kernel<<<leaves, kL2pThreads, smem, s>>>(L, tgt_rel, tgt_off, tgt_perm, near, basis, n, p, K, nt,
-                                               level_offset_d(depth), output, layout, phi_scale, field, potential, Kb);
+  l2p_kernel<<<leaves, kL2pThreads, smem, s>>>(L, tgt_rel, tgt_off, near, basis, n, p, K, level_offset_d(depth), output,
+                                               phi_scale, Kb);
+  unsort_results_kernel<<<(nt + 31) / 32, 256, 0, s>>>(near, tgt_inv, nt, K, output, layout, field, potential);
 }
 
 void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,

@@ -20,8 +20,10 @@ void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *co
 void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
                 int child_level, int n_pairs, cudaStream_t s);
 size_t l2p_smem_bytes(int n, int p, int Kb);
-void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,
-                const float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
+// L2P + combine; K >= 4 writes the sorted results over `near` and then unsorts
+// them to user order (2 launches), K < 4 writes user order directly.
+void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm, const int *tgt_inv,
+                float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
                 int layout, float phi_scale, float *field, float *potential, cudaStream_t s);
 void configure_far_kernels(size_t max_smem);
 

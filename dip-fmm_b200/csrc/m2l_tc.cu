@@ -138,6 +138,7 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
 // chunk in the same order, so one source box's rows of one chunk are one
 // contiguous bulk copy; lanes of the producer warp issue a unit's copies in
 // parallel.
+template <int MT>
 __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args) {
   extern __shared__ __align__(1024) uint8_t smem[];
   const int tid = threadIdx.x;
@@ -150,7 +151,6 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   const int cx = cls & 1, cy = (cls >> 1) & 1, cz = (cls >> 2) & 1;
   const int side = 1 << level;
   const int S = args.stages;
-  const int MT = args.m_tiles;
   const int T = 128 / args.Kp;                                      // targets per M tile
   const int m_active = (count + T - 1) / T;
   const int nkc = (args.Kpad + kKChunk - 1) / kKChunk;
@@ -264,40 +264,50 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     }
   } else if (tid == 0) {
     // MMA issuer: waits for each unit's operands, issues its MMAs, commits
-    // to the unit's empty barrier (arrives when those MMAs completed).
+    // to the unit's empty barrier (arrives when those MMAs completed).  The
+    // shared-memory descriptors are built once: a byte offset o < 256 KB is
+    // added to a descriptor as o >> 4 in its 14-bit start-address field.
     const uint32_t idesc = instr_desc_bf16(args.Npad);
+    const uint64_t desc_full = smem_desc(smem_u32(stage0), 128u, kKChunk * 16u); // SBO = chunk width * 16 B
+    const uint64_t desc_half = smem_desc(smem_u32(stage0), 128u, 16u * 16u);     // last chunk 16 wide
+    const uint64_t o_alo = a_bytes >> 4, o_bhi = (2u * a_bytes) >> 4, o_blo = (2u * a_bytes + b_bytes) >> 4;
     uint32_t accumulate = 0;
     int issued = 0;
+    int s = 0, kc = 0;
+    uint32_t phase = 0;
     for (int u = 0; u < units; ++u) {
-      const int s = u % S;
-      if (!mbar_wait(&full[s], (u / S) & 1)) {
+      if (!mbar_wait(&full[s], phase)) {
         *abort_flag = 1;
         atomicExch(args.error_flag, 2);
         break;
       }
       tc_fence_after();
-      const int kc = u % nkc;
       const int kcw = min(kKChunk, args.Kpad - kc * kKChunk);
-      const uint32_t sbo = static_cast<uint32_t>(kcw) * 16u;
-      const uint32_t a_hi = smem_u32(stage0 + s * stage_bytes);
-      const uint32_t a_lo = a_hi + a_bytes;
-      const uint32_t b_hi = a_hi + 2 * a_bytes;
-      const uint32_t b_lo = b_hi + b_bytes;
-      for (int ks = 0; ks < kcw / 16; ++ks) {
-        const uint64_t dbh = smem_desc(b_hi + ks * 256u, 128u, sbo);
-        const uint64_t dbl = smem_desc(b_lo + ks * 256u, 128u, sbo);
-        for (int m = 0; m < m_active; ++m) {
-          const uint32_t d = tmem + static_cast<uint32_t>(m * args.acc_stride);
-          const uint64_t dah = smem_desc(a_hi + m * a_tile + ks * 256u, 128u, sbo);
-          const uint64_t dal = smem_desc(a_lo + m * a_tile + ks * 256u, 128u, sbo);
-          mma_bf16(d, dah, dbh, idesc, accumulate);
-          mma_bf16(d, dah, dbl, idesc, 1);
-          mma_bf16(d, dal, dbh, idesc, 1);
+      const uint64_t base = (kcw == kKChunk ? desc_full : desc_half) + ((static_cast<uint32_t>(s) * stage_bytes) >> 4);
+#pragma unroll
+      for (int ks = 0; ks < kKChunk / 16; ++ks) {
+        if (ks * 16 < kcw) {
+          const uint64_t o = base + static_cast<uint64_t>(ks * 16); // 2 core matrices = 256 B
+#pragma unroll
+          for (int m = 0; m < MT; ++m) {
+            if (m < m_active) {
+              const uint32_t d = tmem + static_cast<uint32_t>(m * args.acc_stride);
+              const uint64_t ah = o + ((static_cast<uint32_t>(m) * a_tile) >> 4);
+              mma_bf16(d, ah, o + o_bhi, idesc, accumulate);
+              mma_bf16(d, ah, o + o_blo, idesc, 1);
+              mma_bf16(d, ah + o_alo, o + o_bhi, idesc, 1);
+            }
+          }
+          accumulate = 1;
         }
-        accumulate = 1;
       }
       mma_commit(&empty[s]);
       issued = u + 1;
+      if (++s == S) {
+        s = 0;
+        phase ^= 1u;
+      }
+      if (++kc == nkc) kc = 0;
     }
     // The last commit arrives once every MMA issued before it has completed.
     if (issued > 0 && !mbar_wait(&empty[(issued - 1) % S], ((issued - 1) / S) & 1)) {
@@ -404,10 +414,18 @@ void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s) {
   // More than half of TMEM per CTA: request enough shared memory that a
   // second CTA never shares the SM (its tcgen05.alloc would wait for ours).
   if (args.tmem_cols > 256) smem = std::max<size_t>(smem, 120 * 1024);
-  m2l_tc_kernel<<<n_tiles, kTcThreads, smem, s>>>(args);
+  if (args.m_tiles == 4)
+    m2l_tc_kernel<4><<<n_tiles, kTcThreads, smem, s>>>(args);
+  else if (args.m_tiles == 2)
+    m2l_tc_kernel<2><<<n_tiles, kTcThreads, smem, s>>>(args);
+  else
+    m2l_tc_kernel<1><<<n_tiles, kTcThreads, smem, s>>>(args);
 }
 
-bool configure_m2l_tc(size_t max_smem) { return allow_dynamic_smem(m2l_tc_kernel, max_smem); }
+bool configure_m2l_tc(size_t max_smem) {
+  return allow_dynamic_smem(m2l_tc_kernel<1>, max_smem) && allow_dynamic_smem(m2l_tc_kernel<2>, max_smem) &&
+         allow_dynamic_smem(m2l_tc_kernel<4>, max_smem);
+}
 
 // Host: B tiles [slot][alpha chunk][hi, lo][Npad x 32 stride] BF16 from FP64
 // matrices T[slot][alpha][beta] (symmetric in alpha, beta); a chunk of width w

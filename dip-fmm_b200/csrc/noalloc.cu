@@ -210,7 +210,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   for (int level = 3; level <= plan->depth; ++level)
     launch_l2l(L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level, static_cast<int>(plan->ops.l2l_pair_g.size()), s);
   cudaStreamWaitEvent(s, plan->ev_join, 0);
-  launch_l2p(L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, near, plan->basis, n, plan->p, K, plan->nt, plan->depth, a->output,
+  launch_l2p(L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, near, plan->basis, n, plan->p, K, plan->nt, plan->depth, a->output,
              a->layout, plan->phi_scale, a->field, a->potential, s);
   e = cudaGetLastError();
   if (e == cudaSuccess && a->synchronize) e = cudaStreamSynchronize(s);

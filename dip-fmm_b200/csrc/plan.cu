@@ -689,9 +689,9 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
     if (!timing) check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
     if (timing) check(cudaEventRecord(plan->ev_t[6], s), "event");
-    launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->near, plan->basis, n, plan->p, K, plan->nt,
+    launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis, n, plan->p, K, plan->nt,
                plan->depth, a->output, a->layout, plan->phi_scale, field, potential, s);
-    ++launches;
+    launches += (K >= 4 && plan->nt > 0) ? 2 : 1;
     check(cudaGetLastError(), "kernel launch");
     if (timing) check(cudaEventRecord(plan->ev_t[7], s), "event");
 
