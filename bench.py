@@ -22,7 +22,10 @@ Reported beside `value` (device-resident inputs):
   cpu_baseline  the reference CpuStatic (oracle/_ref, built from the upstream
                 sources) on the host cores, on a bounded sample;
   backward      reverse mode on the same workload: device time of the field
-                forward and of the backward (dL/dmoments + dL/dtarget-positions).
+                forward and of the backward (dL/dmoments + dL/dtarget-positions);
+  multi_geometry  48 clustered problems of uneven size (N log-uniform in
+                [8192, 524288], p = 6, one state each) evaluated by one CUDA
+                graph launch: total targets / launch time.
 --impl reference times the reference CpuStatic path (FP32, field+potential)
 on the host cores on that same bounded sample and prints the same line.
 """
@@ -70,6 +73,9 @@ def parse_args():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-backward", action="store_true")
+    ap.add_argument("--no-multi", action="store_true")
+    ap.add_argument("--no-lattice", action="store_true")
+    ap.add_argument("--multi-problems", type=int, default=48)
     return ap.parse_args()
 
 
@@ -378,6 +384,16 @@ def b200_arm(args):
                     "outputs": "dL/dmoments (K x N x 3) + dL/dtarget_positions (N x 3), L = sum w.H"}
         del dW, gm, gx
 
+    multi = None
+    if not args.no_multi and world == 1:
+        multi = multi_geometry_leg(args, stream, local)
+    lattice = None
+    if not args.no_lattice and world == 1:
+        lattice = lattice_leg(args, stream, local)
+    differentiable = None
+    if not args.no_backward and world == 1:
+        differentiable = differentiable_leg(args, stream, local)
+
     if rank != 0:
         if dist is not None:
             dist.barrier()
@@ -424,11 +440,199 @@ def b200_arm(args):
                   "m2l": "fp32"},
         "batched_over_plain": value / plain_value,
         "backward": backward,
+        "multi_geometry": multi,
+        "lattice_p8": lattice,
+        "differentiable_p8": differentiable,
     }
     print(json.dumps(line), flush=True)
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+def clustered_points(rng, n, clusters=8, sigma=0.05):
+    """n points from `clusters` isotropic Gaussians (sigma 0.05, centres
+    U[0.1, 0.9]^3); points outside the unit cube are rejected and redrawn."""
+    centres = rng.uniform(0.1, 0.9, (clusters, 3))
+    out = np.empty((0, 3))
+    while len(out) < n:
+        c = centres[rng.integers(0, clusters, size=2 * n)]
+        p = c + rng.normal(scale=sigma, size=c.shape)
+        out = np.concatenate([out, p[np.all((p >= 0.0) & (p < 1.0), axis=1)]])
+    return out[:n]
+
+
+def multi_geometry_leg(args, stream, local):
+    """Uneven multi-geometry batch: `--multi-problems` independent problems,
+    N log-uniform in [8192, 524288], clustered positions, depth
+    round(log8(N/32)), p = 6, unit random-direction moments, one state each,
+    field output, all evaluated by ONE CUDA graph launch (cdfmm_b200_batch)."""
+    import math
+
+    import cdfmm
+    import cdfmm_b200
+    import torch
+
+    rng = np.random.default_rng(args.seed + 77)
+    count = args.multi_problems
+    sizes = np.round(np.exp(rng.uniform(math.log(8192), math.log(524288), size=count))).astype(int)
+    t0 = time.perf_counter()
+    probs, items = [], []
+    for n in sizes:
+        n = int(n)
+        x = clustered_points(rng, n)
+        o = cdfmm.UniformTreeOptions()
+        o.max_level = max(1, int(round(math.log(n / 32.0, 8))))
+        tree = cdfmm.UniformTree(x, x, o)
+        plan = cdfmm_b200.DevicePlan.from_tree(tree, 6, max_states=1, device=local)
+        plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+        d = rng.normal(size=(1, n, 3))
+        d /= np.linalg.norm(d, axis=2, keepdims=True)
+        dm = torch.from_numpy(d.astype(np.float32)).cuda()
+        dH = torch.empty((1, n, 3), dtype=torch.float32, device="cuda")
+        probs.append((x, plan, d, dH))
+        items.append((plan, dm, dH, None))
+    setup_s = time.perf_counter() - t0
+    batch = cdfmm_b200.Batch(items, output="field")
+    for _ in range(3):
+        batch.launch(stream=stream.cuda_stream, synchronize=False)
+    torch.cuda.synchronize()
+    reps = max(3, args.steps)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        batch.launch(stream=stream.cuda_stream, synchronize=False)
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    # accuracy vs the FP64 direct sum: 4,096 sampled targets of the largest,
+    # the median-size and the smallest problem
+    order = np.argsort(sizes)
+    worst = 0.0
+    for idx in (order[-1], order[len(order) // 2], order[0]):
+        x, plan, d, dH = probs[int(idx)]
+        sub = np.random.default_rng(args.seed + 9).choice(len(x), size=min(len(x), 4096), replace=False)
+        _, H_ref = cdfmm_b200.direct_fp64(x, d[0], x[sub], sub, device=local)
+        H = dH[0].cpu().numpy()[sub]
+        worst = max(worst, float(np.sqrt(np.sum((H - H_ref) ** 2) / np.sum(H_ref ** 2))))
+    batch.close()
+    for _, plan, _, _ in probs:
+        plan.close()
+    total = int(sizes.sum())
+    return {"problems": count, "total_targets": total, "n_min": int(sizes.min()), "n_max": int(sizes.max()),
+            "order": 6, "states": 1, "output": "field", "graph_launches_per_step": 1, "ms_per_launch": ms,
+            "value": total / (ms * 1e-3), "unit": "target evals/s", "rel_l2_H_max_checked": worst,
+            "plan_setup_s": setup_s,
+            "data": "synthetic: 8 Gaussian clusters (sigma 0.05, centres U[0.1,0.9]^3, out-of-cube points redrawn)"}
+
+
+def lattice_leg(args, stream, local):
+    """Batched moments + split-precision M2L: a 64^3 lattice (spacing 1/64,
+    each coordinate jittered by U(-0.1, 0.1) spacings), N = 262,144, exactly
+    8 per leaf at depth 5, K = 64 states of i.i.d. N(0, 1) moments, p = 8,
+    field only, split-BF16 M2L on the tensor cores."""
+    import cdfmm
+    import cdfmm_b200
+    import torch
+
+    rng = np.random.default_rng(args.seed + 11)
+    g = np.stack(np.meshgrid(np.arange(64), np.arange(64), np.arange(64), indexing="ij"), axis=-1).reshape(-1, 3)
+    x = (g + rng.uniform(-0.1, 0.1, size=g.shape)) / 64.0
+    N, K, p, d = len(x), 64, 8, 5
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = d
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, p, max_states=K, device=local)
+    plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+    m = rng.normal(size=(K, N, 3)).astype(np.float32)
+    dm = torch.from_numpy(m).cuda()
+    dH = torch.empty((K, N, 3), dtype=torch.float32, device="cuda")
+
+    def run():
+        plan.evaluate(dm, output="field", field=dH, stream=stream.cuda_stream, synchronize=False)
+
+    for _ in range(3):
+        run()
+    torch.cuda.synchronize()
+    reps = max(3, args.steps)
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(reps):
+        run()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms = a.elapsed_time(b) / reps
+    sub = np.random.default_rng(args.seed + 12).choice(N, size=16384, replace=False)
+    _, H_ref = cdfmm_b200.direct_fp64(x, m[0].astype(np.float64), x[sub], sub, device=local)
+    H = dH[0].cpu().numpy()[sub]
+    rel = float(np.sqrt(np.sum((H - H_ref) ** 2) / np.sum(H_ref ** 2)))
+    st = plan.stats()
+    plan.close()
+    return {"workload": "64^3 jittered lattice, N=262144, p=8, depth 5, K=64, field only", "ms_per_step": ms,
+            "value": N * K / (ms * 1e-3), "unit": UNIT, "rel_l2_H": rel,
+            "m2l": ["auto", "fp32", "bf16x3"][st["m2l_mode_resolved"]],
+            "m2l_shape": {"accumulators_per_cta": st["m2l_tc_m_tiles"], "stages": st["m2l_tc_stages"]}}
+
+
+def differentiable_leg(args, stream, local):
+    """Differentiable FMM: N = 524,288 uniform, p = 8, depth 5, one state;
+    L = sum_i w_i . H_i with w_i ~ N(0, 1)^3; device time of the field forward
+    and of the backward (dL/dmoments + dL/dtarget-positions); the gradients
+    checked against the FP64 direct sums on 4,096 sampled points."""
+    import cdfmm
+    import cdfmm_b200
+    import torch
+
+    rng = np.random.default_rng(args.seed + 21)
+    N, p, d = 524288, 8, 5
+    x = rng.uniform(0.0, 1.0, size=(N, 3))
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = d
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, p, max_states=1, device=local)
+    plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+    m = unit_moments(rng, 1, N)
+    w = rng.normal(size=(1, N, 3)).astype(np.float32)
+    dm, dw = torch.from_numpy(m).cuda(), torch.from_numpy(w).cuda()
+    dH = torch.empty((1, N, 3), dtype=torch.float32, device="cuda")
+    gm = torch.empty_like(dm)
+    gx = torch.empty((N, 3), dtype=torch.float32, device="cuda")
+
+    def fwd():
+        plan.evaluate(dm, output="field", field=dH, stream=stream.cuda_stream, synchronize=False)
+
+    def bwd():
+        plan.backward(dw, moments=dm, grad_moments=gm, grad_target_positions=gx, want_moments=True,
+                      want_positions=True, stream=stream.cuda_stream, synchronize=False)
+
+    def timed(fn, reps):
+        for _ in range(2):
+            fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    reps = max(3, args.steps)
+    ms_f = timed(fwd, reps)
+    ms_b = timed(bwd, reps)
+    sub = np.random.default_rng(args.seed + 22).choice(N, size=4096, replace=False)
+    # dL/dm_j = field of the weights (as dipoles at the targets) at source j
+    _, gm_ref = cdfmm_b200.direct_fp64(x, w[0].astype(np.float64), x[sub], sub, device=local)
+    gx_ref = cdfmm_b200.direct_grad_fp64(x, m[0].astype(np.float64), x[sub], w[0][sub].astype(np.float64), sub,
+                                         device=local)
+    gm_s = gm[0].cpu().numpy()[sub]
+    gx_s = gx.cpu().numpy()[sub]
+    plan.close()
+    return {"workload": "uniform N=524288, p=8, depth 5, one state, L = sum w.H", "ms_forward_field": ms_f,
+            "ms_backward": ms_b, "backward_over_forward": ms_b / ms_f,
+            "rel_l2_grad_moments": float(np.sqrt(np.sum((gm_s - gm_ref) ** 2) / np.sum(gm_ref ** 2))),
+            "rel_l2_grad_positions": float(np.sqrt(np.sum((gx_s - gx_ref) ** 2) / np.sum(gx_ref ** 2))),
+            "checked": "4096 sampled points vs FP64 direct sums (transpose field; position gradient)"}
 
 
 def traffic_from_profiles(kernel):

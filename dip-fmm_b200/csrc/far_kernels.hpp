@@ -51,6 +51,10 @@ void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, 
                      const float4 *W, const float4 *gpart, int G, int n, int p, int K, int nt, int depth,
                      float inv_scale, float *out, cudaStream_t s);
 
+// FP64 direct position gradient of w . H (validation reference of the reverse mode).
+void launch_direct_grad_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,
+                             const int *self, const double *w, double *grad, cudaStream_t s);
+
 // FP64 direct sum (validation reference).
 void launch_direct_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,
                         const int *self, double *phi, double *field, cudaStream_t s);

@@ -509,6 +509,66 @@ __global__ void __launch_bounds__(256) direct_fp64_kernel(const double *__restri
   }
 }
 
+// FP64 direct position gradient of w_i . H_i (validation reference of the
+// reverse mode): g_i = sum_{j != self_i} (1/(4 pi)) { (3/|r|^5)[(w.r) m + (m.r) w
+// + (w.m) r] - 15 (m.r)(w.r) r / |r|^7 },  r = x_i - y_j.
+__global__ void __launch_bounds__(256) direct_grad_fp64_kernel(const double *__restrict__ src,
+                                                               const double *__restrict__ mom, int ns,
+                                                               const double *__restrict__ tgt, int nt,
+                                                               const int *__restrict__ self,
+                                                               const double *__restrict__ w,
+                                                               double *__restrict__ grad) {
+  __shared__ double sp[256][3];
+  __shared__ double sm[256][3];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = i < nt;
+  double x = 0, y = 0, z = 0, wx = 0, wy = 0, wz = 0;
+  int me = -1;
+  if (active) {
+    x = tgt[3 * i];
+    y = tgt[3 * i + 1];
+    z = tgt[3 * i + 2];
+    wx = w[3 * i];
+    wy = w[3 * i + 1];
+    wz = w[3 * i + 2];
+    me = self != nullptr ? self[i] : -1;
+  }
+  double gx = 0, gy = 0, gz = 0;
+  for (int s0 = 0; s0 < ns; s0 += 256) {
+    const int cnt = min(256, ns - s0);
+    __syncthreads();
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) {
+      for (int c = 0; c < 3; ++c) {
+        sp[q][c] = src[3 * (s0 + q) + c];
+        sm[q][c] = mom[3 * (s0 + q) + c];
+      }
+    }
+    __syncthreads();
+    if (active) {
+      for (int q = 0; q < cnt; ++q) {
+        if (s0 + q == me) continue;
+        const double rx = x - sp[q][0], ry = y - sp[q][1], rz = z - sp[q][2];
+        const double r2 = rx * rx + ry * ry + rz * rz;
+        const double rinv = 1.0 / sqrt(r2);
+        const double rinv5 = rinv * rinv * rinv * rinv * rinv;
+        const double a = sm[q][0] * rx + sm[q][1] * ry + sm[q][2] * rz;
+        const double b = wx * rx + wy * ry + wz * rz;
+        const double c = wx * sm[q][0] + wy * sm[q][1] + wz * sm[q][2];
+        const double f5 = 3.0 * rinv5, f7 = 15.0 * rinv5 * rinv * rinv * a * b;
+        gx += f5 * (b * sm[q][0] + a * wx + c * rx) - f7 * rx;
+        gy += f5 * (b * sm[q][1] + a * wy + c * ry) - f7 * ry;
+        gz += f5 * (b * sm[q][2] + a * wz + c * rz) - f7 * rz;
+      }
+    }
+  }
+  if (active) {
+    const double k = 1.0 / (4.0 * 3.14159265358979323846);
+    grad[3 * i] = gx * k;
+    grad[3 * i + 1] = gy * k;
+    grad[3 * i + 2] = gz * k;
+  }
+}
+
 size_t p2p_kb_smem_bytes(int K) {
   const int Kc = std::min(K, kStateBlock);
   const int Kr = ((Kc + (Kc - 1) / 8 + 6) / 8) * 8 + 1; // mrow_stride(Kc), the widest window
@@ -570,6 +630,12 @@ void configure_p2p(size_t max_smem) {
   allow_dynamic_smem(p2p_kb_kernel<4, 0>, max_smem);
   allow_dynamic_smem(p2p_kb_kernel<4, 1>, max_smem);
   allow_dynamic_smem(p2p_kb_kernel<4, 2>, max_smem);
+}
+
+void launch_direct_grad_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,
+                             const int *self, const double *w, double *grad, cudaStream_t s) {
+  if (nt == 0) return;
+  direct_grad_fp64_kernel<<<(nt + 255) / 256, 256, 0, s>>>(src, mom, ns, tgt, nt, self, w, grad);
 }
 
 void launch_direct_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,

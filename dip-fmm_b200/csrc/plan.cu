@@ -59,6 +59,13 @@ template <typename T> void upload(T *dst, const T *src, size_t count, uint64_t &
   bytes += count * sizeof(T);
 }
 
+// TMEM columns for m_tiles accumulators acc_stride apart (a power of two >= 32).
+uint32_t tmem_columns(int m_tiles, int acc_stride) {
+  uint32_t cols = 32;
+  while (cols < static_cast<uint32_t>(m_tiles * acc_stride)) cols <<= 1;
+  return cols;
+}
+
 // Grows a device buffer to at least `need` elements (contents not kept).
 template <typename T> T *grow(T *&buf, size_t &have, size_t need, const char *what) {
   if (have < need) {
@@ -432,14 +439,32 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
       cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, plan->device);
       const int Kpad = round_up(n, 16);
       const int Npad = round_up(n, 16);
-      // Two 128-row accumulators per CTA share each B tile (halving its
-      // traffic); pipeline stages fill the remaining shared memory.
+      // Pipeline shapes: 1, 2 or 4 128-row accumulators per CTA sharing each
+      // B tile, with as many stages as fit one CTA per SM, or half of that
+      // for two CTAs per SM.  Default: two accumulators, one CTA per SM; the
+      // AUTO mode times the candidates on first use for each K.
       const int acc_stride = round_up(Npad, 32);
-      const int m_tiles = 2 * acc_stride <= 512 ? 2 : 1;
-      int stages = 0;
-      while (stages < 8 && m2l_tc_smem_bytes(Npad, m_tiles, stages + 1) <= std::min<size_t>(smem, 224 * 1024)) ++stages;
-      plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 2 &&
-                           desc->m2l_mode != CDFMM_B200_M2L_FP32 && desc->max_states >= 1 &&
+      auto max_stages = [&](int mt, size_t budget) {
+        int st = 0;
+        while (st < 8 && m2l_tc_smem_bytes(Npad, mt, st + 1) <= budget) ++st;
+        return st;
+      };
+      const size_t one_cta = std::min<size_t>(smem, 224 * 1024), two_cta = 112 * 1024;
+      plan->tc_candidates.clear();
+      for (int mt : {2, 1, 4}) {
+        if (mt * acc_stride > 512) continue;
+        const int s1 = max_stages(mt, one_cta);
+        if (s1 >= 2) plan->tc_candidates.emplace_back(mt, s1);
+        const int s2 = max_stages(mt, two_cta);
+        if (s2 >= 2 && tmem_columns(mt, acc_stride) <= 256) plan->tc_candidates.emplace_back(mt, s2);
+      }
+      const int m_tiles = plan->tc_candidates.empty() ? 1 : plan->tc_candidates.front().first;
+      const int stages = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().second;
+      // AUTO uses the tensor cores from K = 8 states on: a plan that never
+      // evaluates 8 states at once does not allocate their operand buffers.
+      const bool wanted = desc->m2l_mode == CDFMM_B200_M2L_BF16X3 ||
+                          (desc->m2l_mode == CDFMM_B200_M2L_AUTO && desc->max_states >= 8);
+      plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 2 && wanted &&
                            configure_m2l_tc(smem);
       if (plan->tc_supported) {
         plan->tc_Kpad = Kpad;
@@ -447,9 +472,7 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
         plan->tc_stages = stages;
         plan->tc_m_tiles = m_tiles;
         plan->tc_acc_stride = acc_stride;
-        uint32_t cols = 32;
-        while (cols < static_cast<uint32_t>(m_tiles * acc_stride)) cols <<= 1;
-        plan->tc_tmem_cols = cols;
+        plan->tc_tmem_cols = tmem_columns(m_tiles, acc_stride);
         plan->tc_Kp_max = round_up(std::min(plan->max_states, 128), 8);
         const size_t boxes = static_cast<size_t>(plan->n_nodes - level_offset(2)) + 1;
         const size_t box_elems = static_cast<size_t>(plan->tc_Kp_max) * Kpad;
@@ -512,6 +535,82 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
   }
 }
 
+// Tensor-core M2L work tiles: per level (deepest first), runs of
+// T = m_tiles * (128 / Kp) consecutive parents in Morton order, the 8 parity
+// classes of a run adjacent so that CTAs running together read the same
+// source boxes (the run's parents' neighbours' children) from L2.
+static std::vector<int4> build_tc_tiles(int depth, int T) {
+  std::vector<int4> tiles;
+  for (int level = depth; level >= 2; --level) {
+    const int parents = 1 << (3 * (level - 1));
+    for (int p0 = 0; p0 < parents; p0 += T)
+      for (int cls = 0; cls < 8; ++cls) tiles.push_back(make_int4(level, cls, p0, std::min(T, parents - p0)));
+  }
+  return tiles;
+}
+
+static void upload_tc_tiles(cdfmm_b200_plan *plan, int Kp) {
+  const std::vector<int4> tiles = build_tc_tiles(plan->depth, plan->tc_m_tiles * (128 / Kp));
+  grow(plan->tc_tiles, plan->tc_tiles_capacity, tiles.size(), "cudaMalloc tiles");
+  check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
+  plan->tc_tiles_Kp = Kp;
+  plan->tc_n_tiles = static_cast<int>(tiles.size());
+}
+
+// Autotuner of the tensor-core M2L pipeline shape (accumulators per CTA,
+// stages): times every candidate on this call's packed operands (device
+// events, second of two launches) and keeps the fastest.  Candidates trade B
+// reuse (more accumulators per CTA) against pipeline depth and two CTAs per
+// SM; all give bit-identical results (the per-row MMA sequence is the same).
+static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
+  const int Kp = round_up(K, 8);
+  const int node_base = level_offset(2);
+  TcArgs ta{};
+  ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
+  ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
+  ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b);
+  ta.scale_l = plan->scale_l;
+  ta.L = plan->L;
+  ta.error_flag = plan->error_flag;
+  ta.n = plan->n;
+  ta.K = K;
+  ta.Kp = Kp;
+  ta.Kpad = plan->tc_Kpad;
+  ta.Npad = plan->tc_Npad;
+  ta.node_base = node_base;
+  ta.zero_node = plan->n_nodes - node_base;
+  ta.acc_stride = plan->tc_acc_stride;
+  ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
+  float best = 0.0F;
+  int best_i = -1;
+  for (size_t c = 0; c < plan->tc_candidates.size(); ++c) {
+    const int mt = plan->tc_candidates[c].first;
+    const std::vector<int4> tiles = build_tc_tiles(plan->depth, mt * (128 / Kp));
+    grow(plan->tc_tiles, plan->tc_tiles_capacity, tiles.size(), "cudaMalloc tiles");
+    check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
+    ta.tiles = plan->tc_tiles;
+    ta.m_tiles = mt;
+    ta.stages = plan->tc_candidates[c].second;
+    ta.tmem_cols = tmem_columns(mt, plan->tc_acc_stride);
+    float ms = 0.0F;
+    for (int rep = 0; rep < 2; ++rep) {
+      check(cudaEventRecord(plan->ev_t[10], s), "event");
+      launch_m2l_tc(ta, static_cast<int>(tiles.size()), s);
+      check(cudaEventRecord(plan->ev_t[11], s), "event");
+      check(cudaEventSynchronize(plan->ev_t[11]), "autotune");
+      check(cudaEventElapsedTime(&ms, plan->ev_t[10], plan->ev_t[11]), "event");
+    }
+    if (best_i < 0 || ms < best) {
+      best = ms;
+      best_i = static_cast<int>(c);
+    }
+  }
+  plan->tc_m_tiles = plan->tc_candidates[static_cast<size_t>(best_i)].first;
+  plan->tc_stages = plan->tc_candidates[static_cast<size_t>(best_i)].second;
+  plan->tc_tmem_cols = tmem_columns(plan->tc_m_tiles, plan->tc_acc_stride);
+  plan->tc_tiles_Kp = 0; // rebuilt for the chosen shape by the caller
+}
+
 // Upward and downward far-field passes for K states whose sorted, scaled
 // moments are in plan->mom: P2M, M2M, M2L (tensor cores or FP32 SIMT), L2L,
 // leaving the leaf local expansions in plan->L.  Returns the launch count.
@@ -532,34 +631,15 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
                         (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || (plan->m2l_mode == CDFMM_B200_M2L_AUTO && K >= 8));
     if (use_tc) {
       const int Kp = round_up(K, 8);
-      if (plan->tc_tiles_Kp != Kp) {
-        // Work tiles: per level (deepest first), runs of T = m_tiles * (128 / Kp)
-        // consecutive parents in Morton order, the 8 parity classes of a run
-        // adjacent so that CTAs running together read the same source boxes
-        // (the run's parents' neighbours' children) from L2.
-        const int T = plan->tc_m_tiles * (128 / Kp);
-        std::vector<int4> tiles;
-        for (int level = plan->depth; level >= 2; --level) {
-          const int parents = 1 << (3 * (level - 1));
-          for (int p0 = 0; p0 < parents; p0 += T)
-            for (int cls = 0; cls < 8; ++cls) tiles.push_back(make_int4(level, cls, p0, std::min(T, parents - p0)));
-        }
-        check(cudaStreamSynchronize(s), "sync");
-        if (plan->tc_tiles_capacity < tiles.size()) {
-          if (plan->tc_tiles) cudaFree(plan->tc_tiles);
-          plan->tc_tiles = nullptr;
-          plan->tc_tiles_capacity = 0;
-          check(cudaMalloc(&plan->tc_tiles, tiles.size() * sizeof(int4)), "cudaMalloc tiles");
-          plan->tc_tiles_capacity = tiles.size();
-        }
-        check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
-        plan->tc_tiles_Kp = Kp;
-        plan->tc_n_tiles = static_cast<int>(tiles.size());
-      }
       const int node_base = level_offset(2);
       const int boxes = plan->n_nodes - node_base;
       launch_m2l_pack(plan->M, plan->scale_m, plan->basis, plan->tc_a_hi, plan->tc_a_lo, n, K, Kp, plan->tc_Kpad,
                       plan->depth, node_base, boxes, s);
+      if (plan->tc_tiles_Kp != Kp) {
+        check(cudaStreamSynchronize(s), "sync");
+        if (plan->m2l_mode == CDFMM_B200_M2L_AUTO && plan->tc_candidates.size() > 1) tune_m2l_tc(plan, K, s);
+        upload_tc_tiles(plan, Kp);
+      }
       TcArgs ta{};
       ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
       ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
@@ -582,6 +662,8 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
       ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
       launch_m2l_tc(ta, plan->tc_n_tiles, s);
       launches += 2;
+      plan->stats.m2l_tc_m_tiles = plan->tc_m_tiles;
+      plan->stats.m2l_tc_stages = plan->tc_stages;
     } else if (plan->depth >= 2) {
       launch_m2l_simt(plan->M, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles,
                       plan->n_tiles, n, plan->ops.m2l_ld, K, s);
@@ -933,6 +1015,55 @@ int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out) {
   if (plan == nullptr || out == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan and out must not be NULL");
   *out = plan->stats;
   return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_direct_grad_fp64(int32_t device, int32_t ns, const double *src, const double *mom, int32_t nt,
+                                const double *tgt, const int32_t *self, const double *weights, double *grad) {
+  void *buf[6] = {};
+  try {
+    require(ns >= 0 && nt >= 0, "negative population size");
+    require(ns == 0 || (src && mom), "source arrays are required");
+    require(nt == 0 || (tgt && weights && grad), "target positions, weights and grad are required");
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+      cudaGetLastError();
+      throw AbiError(CDFMM_B200_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    check(cudaSetDevice(device), "cudaSetDevice");
+    if (nt == 0) return CDFMM_B200_OK;
+    uint64_t bytes = 0, h2d = 0;
+    double *dsrc = dalloc<double>(3 * static_cast<size_t>(ns), bytes);
+    buf[0] = dsrc;
+    double *dmom = dalloc<double>(3 * static_cast<size_t>(ns), bytes);
+    buf[1] = dmom;
+    double *dtgt = dalloc<double>(3 * static_cast<size_t>(nt), bytes);
+    buf[2] = dtgt;
+    double *dw = dalloc<double>(3 * static_cast<size_t>(nt), bytes);
+    buf[3] = dw;
+    double *dg = dalloc<double>(3 * static_cast<size_t>(nt), bytes);
+    buf[4] = dg;
+    int *dself = nullptr;
+    if (self) {
+      dself = dalloc<int>(nt, bytes);
+      buf[5] = dself;
+      upload(dself, self, nt, h2d);
+    }
+    upload(dsrc, src, 3 * static_cast<size_t>(ns), h2d);
+    upload(dmom, mom, 3 * static_cast<size_t>(ns), h2d);
+    upload(dtgt, tgt, 3 * static_cast<size_t>(nt), h2d);
+    upload(dw, weights, 3 * static_cast<size_t>(nt), h2d);
+    launch_direct_grad_fp64(dsrc, dmom, ns, dtgt, nt, dself, dw, dg, nullptr);
+    check(cudaGetLastError(), "direct gradient kernel");
+    check(cudaDeviceSynchronize(), "direct gradient kernel");
+    check(cudaMemcpy(grad, dg, sizeof(double) * 3 * nt, cudaMemcpyDeviceToHost), "D2H");
+    for (void *b : buf)
+      if (b) cudaFree(b);
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    for (void *b : buf)
+      if (b) cudaFree(b);
+    return fail(nullptr, e.code, e.what());
+  }
 }
 
 int cdfmm_b200_direct_fp64(int32_t device, int32_t ns, const double *src, const double *mom, int32_t nt,

@@ -40,7 +40,8 @@ EXPORTED = (
     "cdfmm_b200_plan_destroy", "cdfmm_b200_set_self_indices", "cdfmm_b200_evaluate",
     "cdfmm_b200_read_expansions", "cdfmm_b200_set_timing", "cdfmm_b200_get_stats",
     "cdfmm_b200_direct_fp64", "cdfmm_b200_m2l_matrix", "cdfmm_b200_last_error",
-    "cdfmm_b200_evaluate_noalloc", "cdfmm_b200_backward",
+    "cdfmm_b200_evaluate_noalloc", "cdfmm_b200_backward", "cdfmm_b200_batch_create",
+    "cdfmm_b200_batch_launch", "cdfmm_b200_batch_destroy", "cdfmm_b200_direct_grad_fp64",
 )
 
 # Scratch capacity of cdfmm_b200_evaluate_noalloc (bytes).
@@ -86,6 +87,7 @@ class Stats(ctypes.Structure):
         ("m2l_interactions", ctypes.c_uint64), ("m2l_matrix_bytes", ctypes.c_uint64),
         ("p2p_pairs", ctypes.c_uint64), ("kernel_launches_last", ctypes.c_uint64),
         ("m2l_mode_resolved", ctypes.c_int32), ("timing_enabled", ctypes.c_int32),
+        ("m2l_tc_m_tiles", ctypes.c_int32), ("m2l_tc_stages", ctypes.c_int32),
         ("ms_gather", ctypes.c_double), ("ms_p2m", ctypes.c_double), ("ms_m2m", ctypes.c_double),
         ("ms_m2l", ctypes.c_double), ("ms_l2l", ctypes.c_double), ("ms_l2p", ctypes.c_double),
         ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
@@ -122,10 +124,15 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_evaluate.argtypes = [vp, ctypes.POINTER(EvalArgs)]
     lib.cdfmm_b200_evaluate_noalloc.argtypes = [vp, ctypes.POINTER(EvalArgs)]
     lib.cdfmm_b200_backward.argtypes = [vp, ctypes.POINTER(BackwardArgs)]
+    lib.cdfmm_b200_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(EvalArgs), i32, ctypes.POINTER(vp)]
+    lib.cdfmm_b200_batch_launch.argtypes = [vp, vp, i32]
+    lib.cdfmm_b200_batch_destroy.argtypes = [vp]
+    lib.cdfmm_b200_batch_destroy.restype = None
     lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
     lib.cdfmm_b200_set_timing.argtypes = [vp, i32]
     lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.cdfmm_b200_direct_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
+    lib.cdfmm_b200_direct_grad_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
     lib.cdfmm_b200_m2l_matrix.argtypes = [i32, vp, vp, u64]
     lib.cdfmm_b200_last_error.argtypes = [vp]
     lib.cdfmm_b200_last_error.restype = ctypes.c_char_p
@@ -175,6 +182,19 @@ def direct_fp64(sources, moments, targets, self_indices=None, device=0):
     _check(library().cdfmm_b200_direct_fp64(device, len(s), _ptr(s), _ptr(m), len(t), _ptr(t), _ptr(ids),
                                             _ptr(phi), _ptr(H)))
     return phi, H
+
+
+def direct_grad_fp64(sources, moments, targets, weights, self_indices=None, device=0):
+    """FP64 direct position gradient d/dx_i (w_i . H_i) on the device; (nt, 3)."""
+    s = np.ascontiguousarray(sources, dtype=np.float64).reshape(-1, 3)
+    m = np.ascontiguousarray(moments, dtype=np.float64).reshape(-1, 3)
+    t = np.ascontiguousarray(targets, dtype=np.float64).reshape(-1, 3)
+    w = np.ascontiguousarray(weights, dtype=np.float64).reshape(-1, 3)
+    ids = None if self_indices is None else np.ascontiguousarray(self_indices, dtype=np.int32)
+    g = np.zeros((len(t), 3))
+    _check(library().cdfmm_b200_direct_grad_fp64(device, len(s), _ptr(s), _ptr(m), len(t), _ptr(t), _ptr(ids),
+                                                 _ptr(w), _ptr(g)))
+    return g
 
 
 class DevicePlan:
@@ -359,6 +379,51 @@ class DevicePlan:
         w = 0 if which == "multipole" else 1
         _check(library().cdfmm_b200_read_expansions(self._h, w, state, _ptr(out), out.size), self._h)
         return out.reshape(self.n_nodes, self.n_coefficients)
+
+
+class Batch:
+    """Several plans (independent geometries) evaluated by one CUDA graph
+    launch (cdfmm_b200_batch_*).  `items` is a list of (plan, moments,
+    field, potential) with device tensors (moments (K, ns, 3); field
+    (K, nt, 3); potential (K, nt) or None); arguments are fixed here."""
+
+    def __init__(self, items, output="field", layout=LAYOUT_SEPARATE):
+        flags = {"field": OUTPUT_FIELD, "potential": OUTPUT_POTENTIAL, "both": OUTPUT_FIELD | OUTPUT_POTENTIAL}[output]
+        n = len(items)
+        plans = (ctypes.c_void_p * n)()
+        args = (EvalArgs * n)()
+        self._keep = []
+        for i, (plan, moments, field, potential) in enumerate(items):
+            plans[i] = plan._h.value if isinstance(plan._h, ctypes.c_void_p) else plan._h
+            a = args[i]
+            a.moments = _ptr(moments).value
+            a.moments_dtype = 1 if str(moments.dtype).endswith("float64") else 0
+            a.n_states = int(moments.shape[0]) if len(moments.shape) == 3 else 1
+            a.output = flags
+            a.layout = layout
+            a.field = _ptr(field).value if field is not None else None
+            a.potential = _ptr(potential).value if potential is not None else None
+            a.memory = 0
+            a.stream = None
+            a.synchronize = 0
+            self._keep.append((plan, moments, field, potential))
+        handle = ctypes.c_void_p()
+        _check(library().cdfmm_b200_batch_create(plans, args, n, ctypes.byref(handle)))
+        self._h = handle
+
+    def launch(self, stream=None, synchronize=True):
+        _check(library().cdfmm_b200_batch_launch(self._h, stream, 1 if synchronize else 0))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            library().cdfmm_b200_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
 
 def dipole_field(plan: DevicePlan, moments, target_positions=None):

@@ -119,6 +119,8 @@ typedef struct cdfmm_b200_stats {
   uint64_t kernel_launches_last; /* kernels launched by the last evaluate */
   int32_t m2l_mode_resolved;
   int32_t timing_enabled;
+  int32_t m2l_tc_m_tiles;        /* tensor-core M2L shape last used: accumulators per CTA */
+  int32_t m2l_tc_stages;         /*   and pipeline stages (chosen by the autotuner in AUTO mode) */
   double ms_gather, ms_p2m, ms_m2m, ms_m2l, ms_l2l, ms_l2p, ms_p2p, ms_total;
 } cdfmm_b200_stats;
 
@@ -195,6 +197,24 @@ typedef struct cdfmm_b200_backward_args {
 } cdfmm_b200_backward_args;
 int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *args);
 
+/* Multi-geometry batches (no counterpart in the reference, which evaluates
+ * one UniformFmm per call).  A batch evaluates `count` plans -- independent
+ * geometries of any sizes, each with its own arguments -- with ONE CUDA graph
+ * launch: cdfmm_b200_batch_create evaluates each plan once (building its
+ * work tiles and tuning its M2L), then captures all the evaluations into one
+ * graph whose per-geometry branches run concurrently.  Arguments are fixed at
+ * creation and must be device-resident (memory == 0); a plan appears at most
+ * once per batch and must not be evaluated by other calls while the batch is
+ * in use (the batch replays into the plan's own buffers); stage timing is
+ * switched off on the plans. */
+typedef struct cdfmm_b200_batch cdfmm_b200_batch;
+int cdfmm_b200_batch_create(cdfmm_b200_plan *const *plans, const cdfmm_b200_eval_args *args, int32_t count,
+                            cdfmm_b200_batch **out_batch);
+/* One graph launch on `stream` (NULL = legacy default stream); with
+ * synchronize nonzero, waits and checks the plans' device error flags. */
+int cdfmm_b200_batch_launch(cdfmm_b200_batch *batch, void *stream, int32_t synchronize);
+void cdfmm_b200_batch_destroy(cdfmm_b200_batch *batch);
+
 /* Copies the FP32 multipole (which = 0) or local (which = 1) expansions of one
  * state of the last evaluate to host memory as out[node][coefficient], node in
  * flat level-wise Morton order and coefficients in the total-degree basis
@@ -217,6 +237,13 @@ int cdfmm_b200_direct_fp64(int32_t device, int32_t n_sources, const double *sour
                            const double *target_positions, const int32_t *self_indices,
                            double *phi, double *field);
 
+/* FP64 O(N*M) direct position gradient: grad[i] = d/dx_i (weights_i . H_i) with
+ * explicit self exclusion (no counterpart in the reference; the validation
+ * reference of cdfmm_b200_backward's grad_target_positions).  Host arrays in
+ * user order; self_indices may be NULL. */
+int cdfmm_b200_direct_grad_fp64(int32_t device, int32_t n_sources, const double *source_positions,
+                                const double *moments, int32_t n_targets, const double *target_positions,
+                                const int32_t *self_indices, const double *weights, double *grad);
 /* The FP64 M2L matrix the plan generates for translation R = target centre -
  * source centre: out[beta + n*alpha] = D^{alpha+beta} G(R), n = (p+1)(p+2)(p+3)/6
  * (the reference's build_static_m2l_matrix, src/static_operators.cpp:159-184,

@@ -211,3 +211,16 @@ def test_backward_argument_errors():
     with pytest.raises(ValueError, match="one-to-one"):
         plan.backward(w)
     plan.close()
+
+
+@pytest.mark.gpu
+def test_device_fp64_direct_gradient_matches_oracle():
+    rng = np.random.default_rng(77)
+    src = rng.uniform(0, 1, (3000, 3))
+    tgt = rng.uniform(0, 1, (500, 3))
+    m = rng.normal(size=(3000, 3))
+    w = rng.normal(size=(500, 3))
+    self_idx = rng.integers(-1, 3000, size=500).astype(np.int32)
+    g = cdfmm_b200.direct_grad_fp64(src, m, tgt, w, self_idx)
+    ref = oracle.direct_grad(src, m, tgt, w, self_idx)
+    assert oracle.rel_l2(g, ref) < 1e-12
