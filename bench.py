@@ -431,6 +431,8 @@ def b200_arm(args):
         "config": {"workload": f"uniform N={N} dipoles, p={p}, depth {d}, K={K} states per step, field+potential",
                    "n_dipoles": N, "order": p, "depth": d, "states_per_step": K, "output": "field+potential",
                    "m2l": ["auto", "fp32", "bf16x3"][st["m2l_mode_resolved"]],
+                   "m2l_shape": {"accumulators_per_cta": st["m2l_tc_m_tiles"], "stages": st["m2l_tc_stages"],
+                                 "chosen_by": "autotuner"},
                    "l2": f"inputs larger than L2 ({dm.numel() * 4 / 2**20:.0f} MiB of moments per step)",
                    "parallelism": "replicas (independent states per GPU)" if world > 1 else "single GPU"},
         "rel_l2_H": rel_h, "rel_l2_phi": rel_phi,
@@ -505,6 +507,19 @@ def multi_geometry_leg(args, stream, local):
     b.record(stream)
     torch.cuda.synchronize()
     ms = a.elapsed_time(b) / reps
+    # the same problems evaluated one call after another (no graph)
+    def sequential():
+        for plan, dm, dH, _ in items:
+            plan.evaluate(dm, output="field", field=dH, stream=stream.cuda_stream, synchronize=False)
+
+    sequential()
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(reps):
+        sequential()
+    b.record(stream)
+    torch.cuda.synchronize()
+    ms_seq = a.elapsed_time(b) / reps
     # accuracy vs the FP64 direct sum: 4,096 sampled targets of the largest,
     # the median-size and the smallest problem
     order = np.argsort(sizes)
@@ -521,6 +536,7 @@ def multi_geometry_leg(args, stream, local):
     total = int(sizes.sum())
     return {"problems": count, "total_targets": total, "n_min": int(sizes.min()), "n_max": int(sizes.max()),
             "order": 6, "states": 1, "output": "field", "graph_launches_per_step": 1, "ms_per_launch": ms,
+            "ms_sequential_calls": ms_seq,
             "value": total / (ms * 1e-3), "unit": "target evals/s", "rel_l2_H_max_checked": worst,
             "plan_setup_s": setup_s,
             "data": "synthetic: 8 Gaussian clusters (sigma 0.05, centres U[0.1,0.9]^3, out-of-cube points redrawn)"}
