@@ -210,6 +210,29 @@ def reference_arm(args):
     print(json.dumps(line), flush=True)
 
 
+# ------------------------------------------------------- ranks (replicas)
+def rank_moment_seed(seed, rank):
+    """Replicas: every rank evaluates its own K states (seeded by rank) on the
+    same geometry; no data-path collective."""
+    return seed + 1000 * (rank + 1)
+
+
+def reduce_max_over_ranks(v, dist, device):
+    """Max of a per-rank time over all ranks (the job's step time)."""
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(units_per_rank, world, ms_step):
+    """Aggregate throughput: the units all ranks processed / the max step time."""
+    return units_per_rank * world / (ms_step * 1e-3)
+
+
 # --------------------------------------------------------------------- B200
 def b200_arm(args):
     import torch
@@ -242,7 +265,7 @@ def b200_arm(args):
     sorted_self = np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)]
     plan = cdfmm_b200.DevicePlan.from_tree(tree, p, max_states=K, m2l_mode=mode, device=local)
     plan.set_self_indices(sorted_self)
-    moments = unit_moments(np.random.default_rng(args.seed + 1000 * (rank + 1)), K, N)
+    moments = unit_moments(np.random.default_rng(rank_moment_seed(args.seed, rank)), K, N)
     # A dedicated stream: torch's events and our kernels are ordered on it.
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
@@ -258,11 +281,7 @@ def b200_arm(args):
             dist.barrier()
 
     def max_over_ranks(v):
-        if dist is None:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max_over_ranks(v, dist, "cuda")
 
     for _ in range(max(args.warmup, 0)):
         step()
@@ -280,7 +299,7 @@ def b200_arm(args):
     barrier()
     clock_info = clocks.stop()
     ms_step = max_over_ranks(e0.elapsed_time(e1) / args.steps)
-    value = N * K * world / (ms_step * 1e-3)
+    value = whole_job_rate(N * K, world, ms_step)
     launches = plan.stats()["kernel_launches_last"] * args.steps
 
     # accuracy of state 0 (FP64 direct sum on a 16,384-target subsample)

@@ -25,7 +25,7 @@ namespace {
 template <typename T>
 __global__ void __launch_bounds__(256) gather_moments_kernel(const T *__restrict__ user, const int *__restrict__ inv,
                                                              int ns, int K, double inv_scale, float inv_scale3_f,
-                                                             float4 *__restrict__ mom) {
+                                                             bool paired, float4 *__restrict__ mom) {
   __shared__ float tile[32][32 * 3 + 1]; // [user][state * 3 + component]
   const int u0 = blockIdx.x * 32;
   const int nu = min(32, ns - u0);
@@ -44,11 +44,27 @@ __global__ void __launch_bounds__(256) gather_moments_kernel(const T *__restrict
       tile[t][3 * k + (r - 3 * t)] = f;
     }
     __syncthreads();
-    for (int e = threadIdx.x; e < nu * kn; e += blockDim.x) {
-      const int t = e / kn;
-      const int k = e - t * kn;
-      mom[static_cast<long long>(inv[u0 + t]) * K + kc + k] =
-          make_float4(tile[t][3 * k], tile[t][3 * k + 1], tile[t][3 * k + 2], 0.0F);
+    if (paired) {
+      // state pairs (k, k+1) as (x_k, x_k1, y_k, y_k1), (z_k, z_k1, 0, 0); a
+      // missing partner (K odd) is zero
+      const int kp = (kn + 1) >> 1;
+      const int row = (K + 1) & ~1;
+      for (int e = threadIdx.x; e < nu * kp; e += blockDim.x) {
+        const int t = e / kp;
+        const int k = 2 * (e - t * kp);
+        const bool b = k + 1 < kn;
+        float4 *dst = mom + static_cast<long long>(inv[u0 + t]) * row + kc + k;
+        dst[0] = make_float4(tile[t][3 * k], b ? tile[t][3 * k + 3] : 0.0F, tile[t][3 * k + 1],
+                             b ? tile[t][3 * k + 4] : 0.0F);
+        dst[1] = make_float4(tile[t][3 * k + 2], b ? tile[t][3 * k + 5] : 0.0F, 0.0F, 0.0F);
+      }
+    } else {
+      for (int e = threadIdx.x; e < nu * kn; e += blockDim.x) {
+        const int t = e / kn;
+        const int k = e - t * kn;
+        mom[static_cast<long long>(inv[u0 + t]) * K + kc + k] =
+            make_float4(tile[t][3 * k], tile[t][3 * k + 1], tile[t][3 * k + 2], 0.0F);
+      }
     }
     __syncthreads();
   }
@@ -166,8 +182,12 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
       }
       for (int q = tid; q < cn * Kc; q += kP2mThreads) {
         const int j = q / Kc;
-        const int k = q - j * Kc;
-        smom[q] = mom[static_cast<long long>(c0 + j) * K + kblk + k];
+        const int k = kblk + q - j * Kc;
+        // paired layout (K >= 4): state k is component k & 1 of its pair
+        const float4 *row = mom + static_cast<long long>(c0 + j) * ((K + 1) & ~1);
+        const float4 a = row[k & ~1], b = row[k | 1];
+        const bool odd = (k & 1) != 0;
+        smom[q] = make_float4(odd ? a.y : a.x, odd ? a.w : a.z, odd ? b.y : b.x, 0.0F);
       }
       __syncthreads();
       for (int t = tid; t < tiles; t += kP2mThreads) {
@@ -647,15 +667,17 @@ __global__ void __launch_bounds__(128) l2p_grad_kernel(const float *__restrict__
 // ---------------------------------------------------------------------------
 
 void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, int K,
-                           double scale, float4 *mom, cudaStream_t s) {
+                           double scale, float4 *mom, cudaStream_t s, bool paired) {
   if (ns == 0) return;
   const int blocks = (ns + 31) / 32;
   const double invs = 1.0 / scale;
   const float inv3f = static_cast<float>(invs * invs * invs);
   if (dtype == 1)
-    gather_moments_kernel<double><<<blocks, 256, 0, s>>>(static_cast<const double *>(user), inv, ns, K, invs, inv3f, mom);
+    gather_moments_kernel<double><<<blocks, 256, 0, s>>>(static_cast<const double *>(user), inv, ns, K, invs, inv3f,
+                                                         paired, mom);
   else
-    gather_moments_kernel<float><<<blocks, 256, 0, s>>>(static_cast<const float *>(user), inv, ns, K, invs, inv3f, mom);
+    gather_moments_kernel<float><<<blocks, 256, 0, s>>>(static_cast<const float *>(user), inv, ns, K, invs, inv3f,
+                                                        paired, mom);
 }
 
 // State block of the P2M kernel for K states: the largest of 64, 32, ...

@@ -9,9 +9,17 @@
 
 namespace cdfmm_b200 {
 
-// inv: user index -> sorted index.
+// Sorted moments: for K >= 4 states, pairs of states are interleaved so the
+// near field can use packed FP32x2 arithmetic: a row of round_up(K, 2) float4
+// holds, per pair (k, k+1), (x_k, x_k1, y_k, y_k1) then (z_k, z_k1, 0, 0).  For
+// K < 4 a row is K float4 (x, y, z, 0).
+inline bool moments_paired(int K) { return K >= 4; }
+inline int moment_row(int K) { return moments_paired(K) ? (K + 1) & ~1 : K; }
+
+// inv: user index -> sorted index; paired: write the paired layout (used for
+// the moments of K >= 4 states; gradient weights are always plain).
 void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, int K,
-                           double scale, float4 *mom, cudaStream_t s);
+                           double scale, float4 *mom, cudaStream_t s, bool paired);
 size_t p2m_smem_bytes(int n, int p, int K, int chunk);
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
                 float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s);

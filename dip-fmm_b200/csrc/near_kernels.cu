@@ -254,13 +254,52 @@ __device__ __forceinline__ void p2p_kb_chunk(const float4 &ti, int self, const f
   }
 }
 
+// Paired states (K >= 4): the staged row holds state pairs as
+// (x_a, x_b, y_a, y_b), (z_a, z_b, 0, 0) and the per-state arithmetic runs on
+// packed FP32x2 FMAs, one instruction for two states (same FP32 throughput,
+// half the issue slots).
+template <int KG, bool PHI, bool FULL>
+__device__ __forceinline__ void p2p_kb_chunk_x2(const float4 &ti, int self, const float4 *sPos, const int *sIdx,
+                                                const float4 *m_row0, int Kr, int qbeg, int sn, int F, int kvalid,
+                                                float2 (&acc)[KG / 2][4]) {
+#pragma unroll 2
+  for (int q = qbeg; q < sn; q += F) {
+    const float4 s = sPos[q];
+    const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
+    const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
+    const bool is_self = sIdx[q] == self;
+    const float rinv = is_self ? 0.0F : rsqrtf(r2);
+    const float v = rinv * rinv * rinv;
+    const float f = 3.0F * v * rinv * rinv;
+    const float w = is_self ? 0.0F : r2 * (1.0F / 3.0F);
+    const float2 UX = make_float2(f * dx, f * dx), UY = make_float2(f * dy, f * dy), UZ = make_float2(f * dz, f * dz);
+    const float2 DX = make_float2(dx, dx), DY = make_float2(dy, dy), DZ = make_float2(dz, dz);
+    const float2 NV = make_float2(-v, -v), W2 = make_float2(w, w);
+    const float4 *mq = m_row0 + q * Kr;
+#pragma unroll
+    for (int pr = 0; pr < KG / 2; ++pr) {
+      if (FULL || 2 * pr < kvalid) {
+        const float4 a = mq[2 * pr], b = mq[2 * pr + 1];
+        const float2 X = make_float2(a.x, a.y), Y = make_float2(a.z, a.w), Z = make_float2(b.x, b.y);
+        float2 sd = __fmul2_rn(X, UX);
+        sd = __ffma2_rn(Y, UY, sd);
+        sd = __ffma2_rn(Z, UZ, sd);
+        if (PHI) acc[pr][0] = __ffma2_rn(sd, W2, acc[pr][0]);
+        acc[pr][1] = __ffma2_rn(NV, X, __ffma2_rn(sd, DX, acc[pr][1]));
+        acc[pr][2] = __ffma2_rn(NV, Y, __ffma2_rn(sd, DY, acc[pr][2]));
+        acc[pr][3] = __ffma2_rn(NV, Z, __ffma2_rn(sd, DZ, acc[pr][3]));
+      }
+    }
+  }
+}
+
 // Position gradient of w.H for a target over one staged chunk (summed over
 // the item's KG states): with a = m.r, b = w.r, f5 = 3/|r|^5, f7 = 15/|r|^7,
 //   grad_x [w.K(r) m] = f5 [b m + a w + (w.m) r] - f7 a b r       (times 1/(4 pi))
 // accumulated per pair as g += f5 V + (f5 C - f7 P) r with V = sum(b m + a w),
 // C = sum(w.m), P = sum(a b) over the states.  Self pairs give zero; a
 // coincident non-self pair gives NaN like the forward field.
-template <int KG, bool FULL>
+template <int KG, bool FULL, bool PAIRED>
 __device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const float4 *sPos, const int *sIdx,
                                                const float4 *m_row0, int Kr, int qbeg, int sn, int F, int kvalid,
                                                const float (&w)[KG][3], float (&g)[3]) {
@@ -279,7 +318,13 @@ __device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const
 #pragma unroll
     for (int st = 0; st < KG; ++st) {
       if (FULL || st < kvalid) {
-        const float4 m = mq[st];
+        float4 m;
+        if constexpr (PAIRED) {
+          const float4 pa = mq[st & ~1], pb = mq[st | 1];
+          m = (st & 1) ? make_float4(pa.y, pa.w, pb.y, 0.0F) : make_float4(pa.x, pa.z, pb.x, 0.0F);
+        } else {
+          m = mq[st];
+        }
         const float a = fmaf(m.x, dx, fmaf(m.y, dy, m.z * dz));
         const float b = fmaf(w[st][0], dx, fmaf(w[st][1], dy, w[st][2] * dz));
         C = fmaf(w[st][0], m.x, fmaf(w[st][1], m.y, fmaf(w[st][2], m.z, C)));
@@ -298,8 +343,10 @@ __device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const
 
 // MODE 0: field; 1: field and potential (near[nt][K] = (phi, H) / 4 pi);
 // 2: position gradient of sum_k w_k . H_k, partial sums per state group
-//    gpart[nt][G] (G = ceil(K / KG)) from the weights W[nt][K].
-template <int KG, int MODE>
+//    gpart[nt][G] (G = ceil(K / KG)) from the weights W[nt][K] (plain layout).
+// PAIRED: the sorted moments use the paired layout (rows of round_up(K, 2)
+// float4), K >= 4.
+template <int KG, int MODE, bool PAIRED>
 __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__restrict__ src_rel,
                                                               const float4 *__restrict__ mom,
                                                               const int *__restrict__ src_off,
@@ -342,14 +389,18 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
       const int kvalid = min(KG, Kc - kb);
       const int k_lo = (ib / nt) * KG;       // the round's state window [k_lo, k_hi)
       const int k_hi = min(Kc, ((ib + r - 1) / nt + 1) * KG);
-      const int Kw = k_hi - k_lo;
+      const int Kw = PAIRED ? (k_hi - k_lo + 1) & ~1 : k_hi - k_lo; // staged float4 units per source
       const int Kr = mrow_stride(Kw);
+      const int mrow = PAIRED ? (K + 1) & ~1 : K;                   // global row length (float4)
       const int i = t0 + t;
       const float4 ti = tgt_rel[i];
       const int self = self_idx != nullptr ? self_idx[i] : -1;
       float acc[KG][4];
 #pragma unroll
       for (int st = 0; st < KG; ++st) acc[st][0] = acc[st][1] = acc[st][2] = acc[st][3] = 0.0F;
+      float2 acc2[KG / 2][4];
+#pragma unroll
+      for (int pr = 0; pr < KG / 2; ++pr) acc2[pr][0] = acc2[pr][1] = acc2[pr][2] = acc2[pr][3] = make_float2(0, 0);
       float wreg[KG][3];
       float gacc[3] = {0.0F, 0.0F, 0.0F};
       if constexpr (GRAD) {
@@ -386,7 +437,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
           float4 *dst = sMom + (c & 1) * kChunkB * Kr;
           int q = cq0, k = ck0;
           while (q < sn) {
-            cp_async16(dst + q * Kr + mrow_pos(k), mom + static_cast<long long>(sIdx[q0 + q]) * K + kblk + k_lo + k);
+            cp_async16(dst + q * Kr + mrow_pos(k), mom + static_cast<long long>(sIdx[q0 + q]) * mrow + kblk + k_lo + k);
             q += cqs;
             k += cks;
             if (k >= Kw) {
@@ -410,9 +461,16 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
             const float4 *m_row0 = sMom + (c & 1) * kChunkB * Kr + mrow_pos(kb - k_lo);
             if constexpr (GRAD) {
               if (kvalid == KG)
-                p2p_grad_chunk<KG, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg, gacc);
+                p2p_grad_chunk<KG, true, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
+                                                 gacc);
               else
-                p2p_grad_chunk<KG, false>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg, gacc);
+                p2p_grad_chunk<KG, false, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
+                                                  gacc);
+            } else if constexpr (PAIRED) {
+              if (kvalid == KG)
+                p2p_kb_chunk_x2<KG, PHI, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc2);
+              else
+                p2p_kb_chunk_x2<KG, PHI, false>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc2);
             } else {
               if (kvalid == KG)
                 p2p_kb_chunk<KG, PHI, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc);
@@ -431,6 +489,12 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
           near[static_cast<long long>(i) * ((K + KG - 1) / KG) + kblk / KG + g] =
               make_float4(gacc[0] * kInvFourPiF, gacc[1] * kInvFourPiF, gacc[2] * kInvFourPiF, 0.0F);
         continue;
+      }
+      if constexpr (PAIRED) {
+#pragma unroll
+        for (int st = 0; st < KG; ++st)
+#pragma unroll
+          for (int c = 0; c < 4; ++c) acc[st][c] = (st & 1) ? acc2[st >> 1][c].y : acc2[st >> 1][c].x;
       }
       if (F > 1) {
 #pragma unroll
@@ -570,27 +634,40 @@ __global__ void __launch_bounds__(256) direct_grad_fp64_kernel(const double *__r
 }
 
 size_t p2p_kb_smem_bytes(int K) {
-  const int Kc = std::min(K, kStateBlock);
-  const int Kr = ((Kc + (Kc - 1) / 8 + 6) / 8) * 8 + 1; // mrow_stride(Kc), the widest window
+  const int Kc = (std::min(K, kStateBlock) + 1) & ~1;   // widest window (paired rows round up)
+  const int Kr = ((Kc + (Kc - 1) / 8 + 6) / 8) * 8 + 1; // mrow_stride(Kc)
   return sizeof(float4) * kNeighbourCap + sizeof(int) * kNeighbourCap +
          sizeof(float4) * 2 * kChunkB * static_cast<size_t>(Kr);
 }
 
-template <int KG>
+template <int KG, bool PAIRED>
 void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
                cudaStream_t s) {
   const int leaves = 1 << (3 * depth);
   const size_t smem = p2p_kb_smem_bytes(K);
   if (mode == 1)
-    p2p_kb_kernel<KG, 1><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K,
-                                                          near, W);
+    p2p_kb_kernel<KG, 1, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
+                                                                  depth, K, near, W);
   else if (mode == 2)
-    p2p_kb_kernel<KG, 2><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K,
-                                                          near, W);
+    p2p_kb_kernel<KG, 2, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
+                                                                  depth, K, near, W);
   else
-    p2p_kb_kernel<KG, 0><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K,
-                                                          near, W);
+    p2p_kb_kernel<KG, 0, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
+                                                                  depth, K, near, W);
+}
+
+// K >= 8: groups of 8 states, paired layout; 4 <= K < 8: groups of 4, paired;
+// K = 2, 3: groups of 4, plain layout.
+void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
+                   const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
+                   cudaStream_t s) {
+  if (K >= 8)
+    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s);
+  else if (K >= 4)
+    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s);
+  else
+    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s);
 }
 
 } // namespace
@@ -605,10 +682,7 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
     else
       p2p_k1_kernel<false><<<leaves, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, near);
   } else {
-    if (K >= 8)
-      launch_kb<8>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s);
-    else
-      launch_kb<4>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s);
+    launch_kb_any(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s);
   }
 }
 
@@ -617,19 +691,19 @@ int p2p_grad_groups(int K) { return K >= 8 ? (K + 7) / 8 : (K + 3) / 4; }
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                      const int *tgt_off, const int *self_idx, int depth, int K, const float4 *W, float4 *gpart,
                      cudaStream_t s) {
-  if (K >= 8)
-    launch_kb<8>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, 2, gpart, W, s);
-  else
-    launch_kb<4>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, 2, gpart, W, s);
+  launch_kb_any(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, 2, gpart, W, s);
 }
 
 void configure_p2p(size_t max_smem) {
-  allow_dynamic_smem(p2p_kb_kernel<8, 0>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<8, 1>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<8, 2>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 0>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 1>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 2>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<8, 0, true>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<8, 1, true>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<8, 2, true>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 0, true>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 1, true>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 2, true>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 0, false>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 1, false>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<4, 2, false>, max_smem);
 }
 
 void launch_direct_grad_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,

@@ -132,7 +132,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   if (use_tc)
     for (int level = plan->depth; level >= 2; --level) n_tiles += 8 * (((1 << (3 * (level - 1))) + T - 1) / T);
   // Carve the scratch regions (each 256-byte aligned).
-  const size_t mom_bytes = align256(sizeof(float4) * static_cast<size_t>(plan->ns) * K);
+  const size_t mom_bytes = align256(sizeof(float4) * static_cast<size_t>(plan->ns) * moment_row(K));
   const size_t exp_bytes = align256(sizeof(float) * static_cast<size_t>(plan->n_nodes) * n * K);
   const size_t near_bytes = align256(sizeof(float4) * static_cast<size_t>(plan->nt) * K);
   const size_t pack_bytes = use_tc ? align256(static_cast<size_t>(boxes + 1) * Kp * plan->tc_Kpad * 2) : 0;
@@ -171,7 +171,8 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   if (e != cudaSuccess) return noalloc_fail(plan, CDFMM_B200_ERR_RUNTIME, std::string("scratch: ") + cudaGetErrorString(e));
   if (n_tiles > 0) noalloc_tiles_kernel<<<(n_tiles + 127) / 128, 128, 0, s>>>(dtiles, plan->depth, T, n_tiles);
 
-  launch_gather_moments(a->moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, mom, s);
+  launch_gather_moments(a->moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, mom, s,
+                        moments_paired(K));
   cudaEventRecord(plan->ev_fork, s);
   cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0);
   launch_p2p(plan->src_rel, mom, plan->src_off, plan->tgt_rel, plan->tgt_off, plan->has_self ? plan->self_idx : nullptr,

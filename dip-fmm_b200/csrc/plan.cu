@@ -412,7 +412,7 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
 
     // state buffers sized for max_states
     const size_t K = static_cast<size_t>(plan->max_states);
-    plan->mom = dalloc<float4>(static_cast<size_t>(plan->ns) * K, bytes);
+    plan->mom = dalloc<float4>(static_cast<size_t>(plan->ns) * ((K + 1) & ~static_cast<size_t>(1)), bytes); // paired rows
     plan->M = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
     plan->L = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
     plan->near = dalloc<float4>(static_cast<size_t>(plan->nt) * K, bytes);
@@ -746,7 +746,8 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       potential = out_phi_bytes > 0 ? reinterpret_cast<float *>(static_cast<char *>(plan->stage_out) + out_field_bytes) : nullptr;
     }
 
-    launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s);
+    launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s,
+                          moments_paired(K));
     launches += plan->ns > 0 ? 1 : 0;
     if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
 
@@ -947,8 +948,9 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
       const int G = p2p_grad_groups(K);
       float4 *W = grow(plan->wbuf, plan->wbuf_count, static_cast<size_t>(plan->nt) * K, "cudaMalloc weights");
       float4 *gpart = grow(plan->gpart, plan->gpart_count, static_cast<size_t>(plan->nt) * G, "cudaMalloc partials");
-      launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s);
-      launch_gather_moments(weights, 0, plan->tgt_inv, plan->nt, K, 1.0, W, s);
+      launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s,
+                          moments_paired(K));
+      launch_gather_moments(weights, 0, plan->tgt_inv, plan->nt, K, 1.0, W, s, false);
       enqueue_far(plan, K, s, false);
       launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
                       plan->has_self ? plan->self_idx : nullptr, plan->depth, K, W, gpart, s);
