@@ -86,6 +86,8 @@ struct cdfmm_b200_plan {
 
   cudaStream_t stream = nullptr;   // far-field / main stream
   cudaStream_t near_stream = nullptr;
+  cudaStream_t io_in = nullptr, io_out = nullptr;  // host-memory copies overlapping the evaluation
+  std::vector<cudaEvent_t> io_events;               // chunk pipeline events
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   cudaEvent_t ev_t[16] = {};
 
@@ -111,7 +113,8 @@ struct cdfmm_b200_plan {
   int n_tiles = 0;
   int8_t *basis = nullptr;     // [n][4] ax, ay, az, degree
   int p2m_chunk = 64;
-  int last_K = 0;
+  int last_K = 0;              // states whose expansions M, L hold (from state exp_state0)
+  int exp_state0 = 0;
 
   // tensor-core M2L (split BF16): availability, shapes, buffers, tiles
   bool tc_supported = false;

@@ -215,10 +215,13 @@ template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
 
-// Shared-memory position of state k within a staged moment row, and the row
-// stride for a window of Kw states (1 mod 8 float4).
-__device__ __forceinline__ int mrow_pos(int k) { return k + (k >> 3); }
-__device__ __forceinline__ int mrow_stride(int Kw) { return ((Kw + (Kw - 1) / 8 + 6) / 8) * 8 + 1; }
+// Shared-memory position of state k within a staged moment row (one pad
+// float4 after every group of KG states), and the row stride for a window of
+// Kw states (1 mod 8 float4).
+template <int KG> __host__ __device__ __forceinline__ int mrow_pos(int k) { return k + k / KG; }
+template <int KG> __host__ __device__ __forceinline__ int mrow_stride(int Kw) {
+  return ((Kw + (Kw - 1) / KG + 6) / 8) * 8 + 1;
+}
 
 // Sources q = qbeg, qbeg + F, ... < sn of one staged chunk; m_row0 points at
 // this item's first state in source row 0 (its KG states are contiguous:
@@ -390,7 +393,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
       const int k_lo = (ib / nt) * KG;       // the round's state window [k_lo, k_hi)
       const int k_hi = min(Kc, ((ib + r - 1) / nt + 1) * KG);
       const int Kw = PAIRED ? (k_hi - k_lo + 1) & ~1 : k_hi - k_lo; // staged float4 units per source
-      const int Kr = mrow_stride(Kw);
+      const int Kr = mrow_stride<KG>(Kw);
       const int mrow = PAIRED ? (K + 1) & ~1 : K;                   // global row length (float4)
       const int i = t0 + t;
       const float4 ti = tgt_rel[i];
@@ -437,7 +440,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
           float4 *dst = sMom + (c & 1) * kChunkB * Kr;
           int q = cq0, k = ck0;
           while (q < sn) {
-            cp_async16(dst + q * Kr + mrow_pos(k), mom + static_cast<long long>(sIdx[q0 + q]) * mrow + kblk + k_lo + k);
+            cp_async16(dst + q * Kr + mrow_pos<KG>(k), mom + static_cast<long long>(sIdx[q0 + q]) * mrow + kblk + k_lo + k);
             q += cqs;
             k += cks;
             if (k >= Kw) {
@@ -458,7 +461,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
           const int q0 = c * kChunkB;
           const int sn = min(kChunkB, pn - q0);
           if (valid) {
-            const float4 *m_row0 = sMom + (c & 1) * kChunkB * Kr + mrow_pos(kb - k_lo);
+            const float4 *m_row0 = sMom + (c & 1) * kChunkB * Kr + mrow_pos<KG>(kb - k_lo);
             if constexpr (GRAD) {
               if (kvalid == KG)
                 p2p_grad_chunk<KG, true, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
@@ -633,9 +636,9 @@ __global__ void __launch_bounds__(256) direct_grad_fp64_kernel(const double *__r
   }
 }
 
-size_t p2p_kb_smem_bytes(int K) {
-  const int Kc = (std::min(K, kStateBlock) + 1) & ~1;   // widest window (paired rows round up)
-  const int Kr = ((Kc + (Kc - 1) / 8 + 6) / 8) * 8 + 1; // mrow_stride(Kc)
+template <int KG> size_t p2p_kb_smem_bytes(int K) {
+  const int Kc = (std::min(K, kStateBlock) + 1) & ~1; // widest window (paired rows round up)
+  const int Kr = mrow_stride<KG>(Kc);
   return sizeof(float4) * kNeighbourCap + sizeof(int) * kNeighbourCap +
          sizeof(float4) * 2 * kChunkB * static_cast<size_t>(Kr);
 }
@@ -645,7 +648,7 @@ void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, con
                const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
                cudaStream_t s) {
   const int leaves = 1 << (3 * depth);
-  const size_t smem = p2p_kb_smem_bytes(K);
+  const size_t smem = p2p_kb_smem_bytes<KG>(K);
   if (mode == 1)
     p2p_kb_kernel<KG, 1, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
                                                                   depth, K, near, W);
@@ -657,8 +660,9 @@ void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, con
                                                                   depth, K, near, W);
 }
 
-// K >= 8: groups of 8 states, paired layout; 4 <= K < 8: groups of 4, paired;
-// K = 2, 3: groups of 4, plain layout.
+// K >= 8: groups of 8 states, paired layout; 4 <= K < 8: groups of 4,
+// paired; K = 2, 3: groups of 4, plain layout.  (Groups of 16 were measured
+// slower at K = 64: the accumulators no longer fit the register budget.)
 void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                    const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
                    cudaStream_t s) {

@@ -59,6 +59,18 @@ template <typename T> void upload(T *dst, const T *src, size_t count, uint64_t &
   bytes += count * sizeof(T);
 }
 
+// Grows a device buffer to at least `need` bytes (contents not kept).
+template <typename T> T *grow_bytes(T *&buf, size_t &have, size_t need, const char *what) {
+  if (have < need) {
+    if (buf) cudaFree(buf);
+    buf = nullptr;
+    have = 0;
+    check(cudaMalloc(reinterpret_cast<void **>(&buf), need), what);
+    have = need;
+  }
+  return buf;
+}
+
 // TMEM columns for m_tiles accumulators acc_stride apart (a power of two >= 32).
 uint32_t tmem_columns(int m_tiles, int acc_stride) {
   uint32_t cols = 32;
@@ -92,6 +104,10 @@ void free_plan(cdfmm_b200_plan *p) {
   if (p->ev_join) cudaEventDestroy(p->ev_join);
   for (cudaEvent_t &e : p->ev_t)
     if (e) cudaEventDestroy(e);
+  for (cudaEvent_t e : p->io_events)
+    if (e) cudaEventDestroy(e);
+  if (p->io_in) cudaStreamDestroy(p->io_in);
+  if (p->io_out) cudaStreamDestroy(p->io_out);
   if (p->near_stream) cudaStreamDestroy(p->near_stream);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
@@ -250,6 +266,8 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
 
     check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaStreamCreateWithFlags(&plan->near_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&plan->io_in, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&plan->io_out, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreateWithFlags(&plan->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
     check(cudaEventCreateWithFlags(&plan->ev_join, cudaEventDisableTiming), "cudaEventCreate");
     for (cudaEvent_t &e : plan->ev_t) check(cudaEventCreate(&e), "cudaEventCreate");
@@ -679,6 +697,48 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
   return launches;
 }
 
+// Enqueues one evaluation of K states on stream s: device-resident moments
+// ([K][ns][3], dtype) -> gather -> (list-1 P2P on the near stream || P2M, M2M,
+// M2L, L2L) -> L2P + combine + unsort into device results.  Returns the
+// kernel launch count.
+static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dtype, int K, unsigned output,
+                              int layout, float *field, float *potential, cudaStream_t s, bool timing) {
+  const bool want_phi = (output & CDFMM_B200_OUTPUT_POTENTIAL) != 0u;
+  int launches = 0;
+  if (timing) check(cudaEventRecord(plan->ev_t[0], s), "event");
+  launch_gather_moments(moments, dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s, moments_paired(K));
+  launches += plan->ns > 0 ? 1 : 0;
+  if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
+
+  // Near field on its own stream, concurrent with the far field.  With
+  // stage timing enabled it runs first on the main stream instead, so that
+  // each stage's events measure that stage alone.
+  cudaStream_t ns = timing ? s : plan->near_stream;
+  if (!timing) {
+    check(cudaEventRecord(plan->ev_fork, s), "event");
+    check(cudaStreamWaitEvent(ns, plan->ev_fork, 0), "wait");
+  }
+  if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
+  launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
+             plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi, plan->near, ns);
+  ++launches;
+  if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
+  if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
+  if (!timing) check(cudaEventRecord(plan->ev_join, ns), "event");
+
+  // far field
+  launches += enqueue_far(plan, K, s, timing);
+  if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
+  if (!timing) check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
+  if (timing) check(cudaEventRecord(plan->ev_t[6], s), "event");
+  launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis, plan->n,
+             plan->p, K, plan->nt, plan->depth, output, layout, plan->phi_scale, field, potential, s);
+  launches += (K >= 4 && plan->nt > 0) ? 2 : 1;
+  check(cudaGetLastError(), "kernel launch");
+  if (timing) check(cudaEventRecord(plan->ev_t[7], s), "event");
+  return launches;
+}
+
 int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
   if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
   try {
@@ -702,93 +762,106 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     (void)cudaGetLastError();
 
     const int K = a->n_states;
-    const int n = plan->n;
     // NULL is the legacy default stream, as everywhere in CUDA (a torch tensor
     // on the default stream and our kernels are then ordered).
     cudaStream_t s = static_cast<cudaStream_t>(a->stream);
     const bool host_in = (a->memory & CDFMM_B200_MOMENTS_ON_HOST) != 0u;
     const bool host_out = (a->memory & CDFMM_B200_RESULTS_ON_HOST) != 0u;
-    const size_t in_bytes = static_cast<size_t>(K) * plan->ns * 3 * (a->moments_dtype == 1 ? 8 : 4);
-    const size_t out_field_bytes = static_cast<size_t>(K) * plan->nt * sizeof(float) *
-                                   (a->layout == CDFMM_B200_LAYOUT_INTERLEAVED ? 4 : 3);
-    const size_t out_phi_bytes = (a->layout == CDFMM_B200_LAYOUT_SEPARATE && want_phi)
-                                     ? static_cast<size_t>(K) * plan->nt * sizeof(float) : 0;
+    const size_t in_state = static_cast<size_t>(plan->ns) * 3 * (a->moments_dtype == 1 ? 8 : 4);
+    const int width = a->layout == CDFMM_B200_LAYOUT_INTERLEAVED ? 4 : 3;
+    const size_t field_state = static_cast<size_t>(plan->nt) * sizeof(float) * width;
+    const bool field_out = want_h || a->layout == CDFMM_B200_LAYOUT_INTERLEAVED;
+    const size_t phi_state = (a->layout == CDFMM_B200_LAYOUT_SEPARATE && want_phi) ? static_cast<size_t>(plan->nt) * sizeof(float) : 0;
     const bool timing = plan->timing;
+
+    // Device staging of host arrays: [K][ns][3] moments; results field then potential.
+    const char *moments = static_cast<const char *>(a->moments);
+    if (host_in && in_state > 0) moments = grow_bytes(reinterpret_cast<char *&>(plan->stage_in), plan->stage_in_bytes, in_state * K, "cudaMalloc staging");
+    char *field = reinterpret_cast<char *>(a->field);
+    char *potential = reinterpret_cast<char *>(a->potential);
+    if (host_out) {
+      char *out = grow_bytes(reinterpret_cast<char *&>(plan->stage_out), plan->stage_out_bytes,
+                             (field_state + phi_state) * K + 16, "cudaMalloc staging");
+      field = out;
+      potential = phi_state > 0 ? out + field_state * K : nullptr;
+    }
+
+    // Host arrays and many states: states are cut into 64-state chunks so
+    // that the H2D copy of chunk c + 1 and the D2H copy of chunk c - 1 (on
+    // their own streams) overlap the evaluation of chunk c.  Below 128 states
+    // a call stays whole: per-state device time grows as chunks shrink (1.04,
+    // 1.16, 1.48 ms per state at 64, 32, 16 states on the 1M-point p = 6
+    // workload), which costs more than the copies the overlap would hide.
+    const int chunk = ((host_in || host_out) && !timing && K >= 128) ? 64 : K;
+    const int n_chunks = (K + chunk - 1) / chunk;
     int launches = 0;
-    if (timing) check(cudaEventRecord(plan->ev_t[0], s), "event");
-
-    const void *moments = a->moments;
-    if (host_in && in_bytes > 0) {
-      if (plan->stage_in_bytes < in_bytes) {
-        if (plan->stage_in) cudaFree(plan->stage_in);
-        plan->stage_in = nullptr;
-        plan->stage_in_bytes = 0;
-        check(cudaMalloc(&plan->stage_in, in_bytes), "cudaMalloc staging");
-        plan->stage_in_bytes = in_bytes;
+    if (n_chunks > 1) {
+      while (static_cast<int>(plan->io_events.size()) < 2 * n_chunks + 2) {
+        cudaEvent_t e;
+        check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
+        plan->io_events.push_back(e);
       }
-      check(cudaMemcpyAsync(plan->stage_in, a->moments, in_bytes, cudaMemcpyHostToDevice, s), "H2D moments");
-      plan->stats.evaluation_h2d_bytes += in_bytes;
-      plan->stats.evaluation_h2d_calls += 1;
-      moments = plan->stage_in;
-    }
-    float *field = a->field;
-    float *potential = a->potential;
-    if (host_out) {
-      const size_t need = out_field_bytes + out_phi_bytes;
-      if (plan->stage_out_bytes < need) {
-        if (plan->stage_out) cudaFree(plan->stage_out);
-        plan->stage_out = nullptr;
-        plan->stage_out_bytes = 0;
-        check(cudaMalloc(&plan->stage_out, need), "cudaMalloc staging");
-        plan->stage_out_bytes = need;
+      cudaEvent_t ev_start = plan->io_events[0], ev_end = plan->io_events[1];
+      check(cudaEventRecord(ev_start, s), "event");
+      check(cudaStreamWaitEvent(plan->io_in, ev_start, 0), "wait");
+      check(cudaStreamWaitEvent(plan->io_out, ev_start, 0), "wait");
+      for (int c = 0; c < n_chunks; ++c) {
+        const int k0 = c * chunk, kc = std::min(chunk, K - k0);
+        cudaEvent_t ev_in = plan->io_events[2 + 2 * c], ev_done = plan->io_events[3 + 2 * c];
+        if (host_in && in_state > 0) {
+          check(cudaMemcpyAsync(const_cast<char *>(moments) + in_state * k0, static_cast<const char *>(a->moments) + in_state * k0,
+                                in_state * kc, cudaMemcpyHostToDevice, plan->io_in), "H2D moments");
+          plan->stats.evaluation_h2d_bytes += in_state * kc;
+          plan->stats.evaluation_h2d_calls += 1;
+          check(cudaEventRecord(ev_in, plan->io_in), "event");
+          check(cudaStreamWaitEvent(s, ev_in, 0), "wait");
+        }
+        launches += enqueue_evaluation(plan, moments + in_state * k0, a->moments_dtype, kc, a->output, a->layout,
+                                       field ? reinterpret_cast<float *>(field + field_state * k0) : nullptr,
+                                       potential ? reinterpret_cast<float *>(potential + phi_state * k0) : nullptr, s, false);
+        if (host_out) {
+          check(cudaEventRecord(ev_done, s), "event");
+          check(cudaStreamWaitEvent(plan->io_out, ev_done, 0), "wait");
+          if (field_out && field_state > 0) {
+            check(cudaMemcpyAsync(reinterpret_cast<char *>(a->field) + field_state * k0, field + field_state * k0,
+                                  field_state * kc, cudaMemcpyDeviceToHost, plan->io_out), "D2H field");
+            plan->stats.evaluation_d2h_bytes += field_state * kc;
+            plan->stats.evaluation_d2h_calls += 1;
+          }
+          if (phi_state > 0) {
+            check(cudaMemcpyAsync(reinterpret_cast<char *>(a->potential) + phi_state * k0, potential + phi_state * k0,
+                                  phi_state * kc, cudaMemcpyDeviceToHost, plan->io_out), "D2H potential");
+            plan->stats.evaluation_d2h_bytes += phi_state * kc;
+            plan->stats.evaluation_d2h_calls += 1;
+          }
+        }
       }
-      field = static_cast<float *>(plan->stage_out);
-      potential = out_phi_bytes > 0 ? reinterpret_cast<float *>(static_cast<char *>(plan->stage_out) + out_field_bytes) : nullptr;
-    }
-
-    launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s,
-                          moments_paired(K));
-    launches += plan->ns > 0 ? 1 : 0;
-    if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
-
-    // Near field on its own stream, concurrent with the far field.  With
-    // stage timing enabled it runs first on the main stream instead, so that
-    // each stage's events measure that stage alone.
-    cudaStream_t ns = timing ? s : plan->near_stream;
-    if (!timing) {
-      check(cudaEventRecord(plan->ev_fork, s), "event");
-      check(cudaStreamWaitEvent(ns, plan->ev_fork, 0), "wait");
-    }
-    if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
-    launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
-               plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi, plan->near, ns);
-    ++launches;
-    if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
-    if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
-    if (!timing) check(cudaEventRecord(plan->ev_join, ns), "event");
-
-    // far field
-    launches += enqueue_far(plan, K, s, timing);
-    if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
-    if (!timing) check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
-    if (timing) check(cudaEventRecord(plan->ev_t[6], s), "event");
-    launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis, n, plan->p, K, plan->nt,
-               plan->depth, a->output, a->layout, plan->phi_scale, field, potential, s);
-    launches += (K >= 4 && plan->nt > 0) ? 2 : 1;
-    check(cudaGetLastError(), "kernel launch");
-    if (timing) check(cudaEventRecord(plan->ev_t[7], s), "event");
-
-    if (host_out) {
-      if (out_field_bytes > 0 && plan->nt > 0 && (want_h || a->layout == CDFMM_B200_LAYOUT_INTERLEAVED)) {
-        check(cudaMemcpyAsync(a->field, field, out_field_bytes, cudaMemcpyDeviceToHost, s), "D2H field");
-        plan->stats.evaluation_d2h_bytes += out_field_bytes;
-        plan->stats.evaluation_d2h_calls += 1;
+      check(cudaEventRecord(ev_end, plan->io_out), "event");
+      check(cudaStreamWaitEvent(s, ev_end, 0), "wait");
+      plan->exp_state0 = (n_chunks - 1) * chunk;
+      plan->last_K = K - plan->exp_state0;
+    } else {
+      if (host_in && in_state > 0) {
+        check(cudaMemcpyAsync(const_cast<char *>(moments), a->moments, in_state * K, cudaMemcpyHostToDevice, s), "H2D moments");
+        plan->stats.evaluation_h2d_bytes += in_state * K;
+        plan->stats.evaluation_h2d_calls += 1;
       }
-      if (out_phi_bytes > 0 && plan->nt > 0) {
-        check(cudaMemcpyAsync(a->potential, potential, out_phi_bytes, cudaMemcpyDeviceToHost, s), "D2H potential");
-        plan->stats.evaluation_d2h_bytes += out_phi_bytes;
-        plan->stats.evaluation_d2h_calls += 1;
+      launches += enqueue_evaluation(plan, moments, a->moments_dtype, K, a->output, a->layout,
+                                     reinterpret_cast<float *>(field), reinterpret_cast<float *>(potential), s, timing);
+      if (host_out) {
+        if (field_out && field_state > 0) {
+          check(cudaMemcpyAsync(a->field, field, field_state * K, cudaMemcpyDeviceToHost, s), "D2H field");
+          plan->stats.evaluation_d2h_bytes += field_state * K;
+          plan->stats.evaluation_d2h_calls += 1;
+        }
+        if (phi_state > 0) {
+          check(cudaMemcpyAsync(a->potential, potential, phi_state * K, cudaMemcpyDeviceToHost, s), "D2H potential");
+          plan->stats.evaluation_d2h_bytes += phi_state * K;
+          plan->stats.evaluation_d2h_calls += 1;
+        }
       }
+      plan->exp_state0 = 0;
+      plan->last_K = K;
     }
     if (a->synchronize || host_out || timing) {
       check(cudaStreamSynchronize(s), "evaluate");
@@ -818,7 +891,6 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       plan->stats.ms_l2p = ms(6, 7);
       plan->stats.ms_total = ms(0, 7);
     }
-    plan->last_K = K;
     plan->stats.evaluations += 1;
     plan->stats.kernel_launches_last = static_cast<uint64_t>(launches);
     return CDFMM_B200_OK;
@@ -891,7 +963,11 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
             "request grad_moments and/or grad_target_positions");
     require(plan->nt == 0 || a->grad_field != nullptr, "grad_field is NULL");
     const bool want_x = a->grad_target_positions != nullptr;
-    if (want_x) {
+    // The forward's sorted moments and leaf locals are still in the plan if
+    // no evaluate ran since and that one held all K states.
+    const bool reuse = a->forward_evaluation != 0 && a->forward_evaluation == plan->stats.evaluations &&
+                       plan->exp_state0 == 0 && plan->last_K == a->n_states;
+    if (want_x && !reuse) {
       require(plan->ns == 0 || a->moments != nullptr, "grad_target_positions needs the forward moments");
       require(a->moments_dtype == 0 || a->moments_dtype == 1, "moments_dtype must be 0 (float32) or 1 (float64)");
     }
@@ -922,7 +998,7 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
     if (want_x && plan->nt > 0) {
       // dL/dx_target: forward moments -> leaf locals (far pass), then the P2P
       // gradient partial sums and the L2P second-derivative kernel.
-      const size_t mom_in_bytes = static_cast<size_t>(K) * plan->ns * 3 * (a->moments_dtype == 1 ? 8 : 4);
+      const size_t mom_in_bytes = reuse ? 0 : static_cast<size_t>(K) * plan->ns * 3 * (a->moments_dtype == 1 ? 8 : 4);
       const size_t w_in_bytes = static_cast<size_t>(K) * plan->nt * 3 * sizeof(float);
       const size_t out_bytes = static_cast<size_t>(plan->nt) * 3 * sizeof(float);
       const void *moments = a->moments;
@@ -948,10 +1024,12 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
       const int G = p2p_grad_groups(K);
       float4 *W = grow(plan->wbuf, plan->wbuf_count, static_cast<size_t>(plan->nt) * K, "cudaMalloc weights");
       float4 *gpart = grow(plan->gpart, plan->gpart_count, static_cast<size_t>(plan->nt) * G, "cudaMalloc partials");
-      launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s,
-                          moments_paired(K));
+      if (!reuse)
+        launch_gather_moments(moments, a->moments_dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s,
+                              moments_paired(K));
       launch_gather_moments(weights, 0, plan->tgt_inv, plan->nt, K, 1.0, W, s, false);
-      enqueue_far(plan, K, s, false);
+      if (!reuse) enqueue_far(plan, K, s, false);
+      plan->stats.backward_reused_forward = reuse ? 1 : 0;
       launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
                       plan->has_self ? plan->self_idx : nullptr, plan->depth, K, W, gpart, s);
       launch_l2p_grad(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, W, gpart, G, plan->n, plan->p, K,
@@ -990,7 +1068,9 @@ int cdfmm_b200_read_expansions(const cdfmm_b200_plan *plan, int32_t which, int32
   auto *mp = const_cast<cdfmm_b200_plan *>(plan);
   try {
     require(which == 0 || which == 1, "which must be 0 (multipoles) or 1 (locals)");
-    require(state >= 0 && state < std::max(plan->last_K, 1), "state out of range");
+    require(state >= plan->exp_state0 && state < plan->exp_state0 + std::max(plan->last_K, 1),
+            "state out of range (a host-memory evaluation of 128 or more states keeps the expansions of its last "
+            "64-state chunk only)");
     const size_t need = static_cast<size_t>(plan->n_nodes) * plan->n;
     require(out != nullptr && out_count >= need, "output buffer too small");
     check(cudaSetDevice(plan->device), "cudaSetDevice");
@@ -999,7 +1079,7 @@ int cdfmm_b200_read_expansions(const cdfmm_b200_plan *plan, int32_t which, int32
     std::vector<float> all(need * K);
     check(cudaMemcpy(all.data(), which == 0 ? plan->M : plan->L, all.size() * sizeof(float), cudaMemcpyDeviceToHost),
           "D2H expansions");
-    for (size_t q = 0; q < need; ++q) out[q] = all[q * K + state];
+    for (size_t q = 0; q < need; ++q) out[q] = all[q * K + (state - plan->exp_state0)];
     return CDFMM_B200_OK;
   } catch (const AbiError &e) {
     return fail(mp, e.code, e.what());

@@ -74,7 +74,7 @@ class BackwardArgs(ctypes.Structure):
         ("struct_size", ctypes.c_int32), ("n_states", ctypes.c_int32), ("grad_field", ctypes.c_void_p),
         ("moments", ctypes.c_void_p), ("moments_dtype", ctypes.c_int32), ("grad_moments", ctypes.c_void_p),
         ("grad_target_positions", ctypes.c_void_p), ("memory", ctypes.c_uint32), ("stream", ctypes.c_void_p),
-        ("synchronize", ctypes.c_int32),
+        ("synchronize", ctypes.c_int32), ("forward_evaluation", ctypes.c_uint64),
     ]
 
 
@@ -88,6 +88,7 @@ class Stats(ctypes.Structure):
         ("p2p_pairs", ctypes.c_uint64), ("kernel_launches_last", ctypes.c_uint64),
         ("m2l_mode_resolved", ctypes.c_int32), ("timing_enabled", ctypes.c_int32),
         ("m2l_tc_m_tiles", ctypes.c_int32), ("m2l_tc_stages", ctypes.c_int32),
+        ("backward_reused_forward", ctypes.c_int32), ("reserved0", ctypes.c_int32),
         ("ms_gather", ctypes.c_double), ("ms_p2m", ctypes.c_double), ("ms_m2m", ctypes.c_double),
         ("ms_m2l", ctypes.c_double), ("ms_l2l", ctypes.c_double), ("ms_l2p", ctypes.c_double),
         ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
@@ -334,7 +335,8 @@ class DevicePlan:
         _check(library().cdfmm_b200_evaluate_noalloc(self._h, ctypes.byref(a)), self._h)
 
     def backward(self, grad_field, moments=None, grad_moments=None, grad_target_positions=None,
-                 want_moments=True, want_positions=False, stream=None, synchronize=True, memory=None):
+                 want_moments=True, want_positions=False, stream=None, synchronize=True, memory=None,
+                 forward_evaluation=0):
         """Reverse mode of `evaluate` for L = sum w . H with w = grad_field
         (K, n_targets, 3) float32: returns {"moments": dL/dm (K, n_sources, 3),
         "positions": dL/dx_target (n_targets, 3), summed over states}.
@@ -370,6 +372,7 @@ class DevicePlan:
         a.memory = memory
         a.stream = stream
         a.synchronize = 1 if synchronize else 0
+        a.forward_evaluation = int(forward_evaluation)
         _check(library().cdfmm_b200_backward(self._h, ctypes.byref(a)), self._h)
         return {"moments": grad_moments if want_moments else None,
                 "positions": grad_target_positions if want_positions else None}
@@ -451,6 +454,9 @@ def dipole_field(plan: DevicePlan, moments, target_positions=None):
                           synchronize=False)
             ctx.save_for_backward(m3)
             ctx.squeeze = squeeze
+            # lets the backward reuse this evaluation's moments and locals if
+            # nothing else evaluates on the plan in between
+            ctx.evaluation = plan.stats()["evaluations"]
             return H.squeeze(0) if squeeze else H
 
         @staticmethod
@@ -464,7 +470,7 @@ def dipole_field(plan: DevicePlan, moments, target_positions=None):
             if want_m or want_x:
                 plan.backward(g3, moments=m3, grad_moments=gm, grad_target_positions=gx, want_moments=want_m,
                               want_positions=want_x, stream=torch.cuda.current_stream(m3.device).cuda_stream,
-                              synchronize=False)
+                              synchronize=False, forward_evaluation=ctx.evaluation)
             if gm is not None and ctx.squeeze:
                 gm = gm.squeeze(0)
             return gm, gx

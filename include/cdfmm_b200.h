@@ -121,6 +121,8 @@ typedef struct cdfmm_b200_stats {
   int32_t timing_enabled;
   int32_t m2l_tc_m_tiles;        /* tensor-core M2L shape last used: accumulators per CTA */
   int32_t m2l_tc_stages;         /*   and pipeline stages (chosen by the autotuner in AUTO mode) */
+  int32_t backward_reused_forward; /* last backward reused the forward's moments and locals */
+  int32_t reserved0;
   double ms_gather, ms_p2m, ms_m2m, ms_m2l, ms_l2l, ms_l2p, ms_p2p, ms_total;
 } cdfmm_b200_stats;
 
@@ -194,6 +196,11 @@ typedef struct cdfmm_b200_backward_args {
                                    RESULTS_ON_HOST: the outputs on the host */
   void *stream;                 /* cudaStream_t; NULL = the legacy default stream */
   int32_t synchronize;          /* nonzero: return only after the outputs are complete */
+  uint64_t forward_evaluation;  /* the plan's `evaluations` counter (cdfmm_b200_get_stats) read right
+                                   after the forward evaluate of these moments, or 0.  If no evaluate
+                                   on the plan happened since and that one kept all n_states (device
+                                   arrays, or fewer than 128 states), its sorted moments and leaf
+                                   locals are reused instead of recomputed (moments may then be NULL). */
 } cdfmm_b200_backward_args;
 int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *args);
 

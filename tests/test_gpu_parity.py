@@ -272,3 +272,35 @@ def test_large_uniform_accuracy_linearity_and_oracle():
                              target_source_indices=ids.tolist())["H"]
     comb = f.evaluate((2.0 * m1 - 0.5 * m2), output="field", target_source_indices=ids.tolist())["H"]
     assert oracle.rel_l2(comb, 2.0 * both[0] - 0.5 * both[1]) < 1e-5
+
+
+def test_host_io_chunk_pipeline_matches_device_path():
+    # Host-memory calls with >= 128 states run as a pipeline of 64-state
+    # chunks (copies overlapping the evaluation); results must equal the
+    # device path.
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(31)
+    n, K = 4096, 130
+    x = rng.uniform(0, 1, (n, 3))
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, 4, max_states=K)
+    plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+    m = rng.normal(size=(K, n, 3)).astype(np.float32)
+    host = plan.evaluate(m, output="both")
+    st = plan.stats()
+    assert st["evaluation_h2d_bytes"] == K * n * 3 * 4
+    assert st["evaluation_d2h_bytes"] == K * n * 4 * 4
+    dH = torch.zeros((K, n, 3), device="cuda")
+    dphi = torch.zeros((K, n), device="cuda")
+    plan.evaluate(torch.from_numpy(m).cuda(), output="both", field=dH, potential=dphi)
+    torch.cuda.synchronize()
+    # (the 130-state device call runs the FP32 SIMT M2L, the 64-state chunks
+    # the split-BF16 tensor cores: equal to the split's rounding)
+    assert oracle.rel_l2(host["H"], dH.cpu().numpy()) < 1e-5
+    assert oracle.rel_l2(host["phi"], dphi.cpu().numpy()) < 1e-5
+    for k in (37, 129):
+        ref = oracle.fmm(x, x, m[k].astype(np.float64), 4, 3, identities=np.arange(n))
+        assert oracle.rel_l2(host["H"][k], ref["H"]) < FP32_REL_L2
+    plan.close()

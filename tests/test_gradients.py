@@ -181,6 +181,8 @@ def test_autograd_function_matches_c_abi():
     H = cdfmm_b200.dipole_field(plan, m, xt)
     (w * H).sum().backward()
     torch.cuda.synchronize()
+    # the backward reused the forward's sorted moments and leaf locals
+    assert plan.stats()["backward_reused_forward"] == 1
     ref = plan.backward(w_np, moments=m_np, want_moments=True, want_positions=True)
     H_ref = plan.evaluate(m_np, output="field")["H"]
     np.testing.assert_allclose(H.detach().cpu().numpy(), H_ref, rtol=0, atol=1e-6 * np.abs(H_ref).max())
