@@ -256,72 +256,94 @@ __device__ inline void stage_pairs(const int *pair_off, const int *pairs, const 
   __syncthreads();
 }
 
-// One thread per parent output coefficient (parent, alpha, state); the loads
-// of the 8 children are independent of each other, so they overlap.
-__global__ void __launch_bounds__(256) m2m_kernel(float *__restrict__ M, const int *__restrict__ pair_off,
-                                                  const int *__restrict__ pairs, const float *__restrict__ coef,
-                                                  int n, int K, int parent_level, int n_pairs) {
+// M2M, one CTA per (parent, block of kShiftStates states): the 8 children's
+// multipoles of the block are staged in shared memory (contiguous runs of
+// states), then each thread forms parent coefficients from the staged pair
+// table and class coefficients; lanes sharing a coefficient share the pair
+// loads (broadcast) and read consecutive states (conflict-free).
+constexpr int kShiftStates = 16;
+constexpr int kShiftThreads = 256;
+
+__global__ void __launch_bounds__(kShiftThreads) m2m_kernel(float *__restrict__ M, const int *__restrict__ pair_off,
+                                                            const int *__restrict__ pairs,
+                                                            const float *__restrict__ coef, int n, int K,
+                                                            int parent_level, int n_pairs) {
   extern __shared__ int shp[];
   int *soff = shp;
   int *spair = soff + n + 1;
   float *scoef = reinterpret_cast<float *>(spair + n_pairs);
+  float *sM = scoef + 8 * n; // [8 children][n][kShiftStates]
   stage_pairs(pair_off, pairs, coef + static_cast<long long>(parent_level + 1) * 8 * n, n, n_pairs, soff, spair,
               scoef);
-  const int parent_base = level_offset_d(parent_level);
-  const int child_base = level_offset_d(parent_level + 1);
+  const long long parent = blockIdx.x;
+  const int kb = blockIdx.y * kShiftStates;
+  const int kc = min(kShiftStates, K - kb);
   const long long per = static_cast<long long>(n) * K;
-  const long long total = (static_cast<long long>(1) << (3 * parent_level)) * per;
-  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (q >= total) return;
-  const long long parent = q / per;
-  const int rem = static_cast<int>(q - parent * per);
-  const int a = rem / K;
-  const int k = rem - a * K;
-  const int e0 = soff[a], e1 = soff[a + 1];
-  const float *child0 = M + (child_base + parent * 8) * per + k;
-  float v = 0.0F;
-#pragma unroll 2
-  for (int c = 0; c < 8; ++c) {
-    const float *child = child0 + c * per;
-    const float *cc = scoef + c * n;
-    for (int e = e0; e < e1; ++e) {
-      const int pr = spair[e];
-      v = fmaf(cc[pr & 0xffff], __ldg(child + static_cast<long long>(pr >> 16) * K), v);
-    }
+  const float *child0 = M + (level_offset_d(parent_level + 1) + parent * 8) * per + kb;
+  for (int q = threadIdx.x; q < 8 * n * kc; q += kShiftThreads) {
+    const int cr = q / kc; // child * n + coefficient
+    const int k = q - cr * kc;
+    sM[cr * kShiftStates + k] = child0[(cr / n) * per + static_cast<long long>(cr % n) * K + k];
   }
-  M[(parent_base + parent) * per + rem] = v;
+  __syncthreads();
+  float *out = M + (level_offset_d(parent_level) + parent) * per + kb;
+  for (int q = threadIdx.x; q < n * kc; q += kShiftThreads) {
+    const int a = q / kc;
+    const int k = q - a * kc;
+    const int e0 = soff[a], e1 = soff[a + 1];
+    float v = 0.0F;
+    for (int c = 0; c < 8; ++c) {
+      const float *cc = scoef + c * n;
+      const float *mc = sM + c * n * kShiftStates + k;
+      for (int e = e0; e < e1; ++e) {
+        const int pr = spair[e];
+        v = fmaf(cc[pr & 0xffff], mc[(pr >> 16) * kShiftStates], v);
+      }
+    }
+    out[static_cast<long long>(a) * K + k] = v;
+  }
 }
 
 // ---------------------------------------------------------------------------
 // L2L for one child level (upstream src/far_field.cpp:533-581):
 //   L_child[beta] += sum_{|beta + g| <= p} B_class[g] L_parent[beta + g]
-__global__ void __launch_bounds__(256) l2l_kernel(float *__restrict__ L, const int *__restrict__ pair_off,
-                                                  const int *__restrict__ pairs, const float *__restrict__ coef,
-                                                  int n, int K, int child_level, int n_pairs) {
+// One CTA per (parent, block of states): the parent's locals are staged once
+// and shifted to its 8 children.
+__global__ void __launch_bounds__(kShiftThreads) l2l_kernel(float *__restrict__ L, const int *__restrict__ pair_off,
+                                                            const int *__restrict__ pairs,
+                                                            const float *__restrict__ coef, int n, int K,
+                                                            int child_level, int n_pairs) {
   extern __shared__ int shl[];
   int *soff = shl;
   int *spair = soff + n + 1;
   float *scoef = reinterpret_cast<float *>(spair + n_pairs);
+  float *sL = scoef + 8 * n; // [n][kShiftStates]
   stage_pairs(pair_off, pairs, coef + static_cast<long long>(child_level) * 8 * n, n, n_pairs, soff, spair, scoef);
-  const int child_base = level_offset_d(child_level);
-  const int parent_base = level_offset_d(child_level - 1);
+  const long long parent = blockIdx.x;
+  const int kb = blockIdx.y * kShiftStates;
+  const int kc = min(kShiftStates, K - kb);
   const long long per = static_cast<long long>(n) * K;
-  const long long total = (static_cast<long long>(1) << (3 * child_level)) * per;
-  const long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x;
-  if (q >= total) return;
-  const long long child = q / per;
-  const int rem = static_cast<int>(q - child * per);
-  const int b = rem / K;
-  const int k = rem - b * K;
-  const int cls = static_cast<int>(child & 7);
-  const float *parent = L + (parent_base + (child >> 3)) * per + k;
-  const float *cc = scoef + cls * n;
-  float v = 0.0F;
-  for (int e = soff[b]; e < soff[b + 1]; ++e) {
-    const int pr = spair[e];
-    v = fmaf(cc[pr & 0xffff], __ldg(parent + static_cast<long long>(pr >> 16) * K), v);
+  const float *src = L + (level_offset_d(child_level - 1) + parent) * per + kb;
+  for (int q = threadIdx.x; q < n * kc; q += kShiftThreads) {
+    const int b = q / kc;
+    const int k = q - b * kc;
+    sL[b * kShiftStates + k] = src[static_cast<long long>(b) * K + k];
   }
-  L[(child_base + child) * per + rem] += v;
+  __syncthreads();
+  float *child0 = L + (level_offset_d(child_level) + parent * 8) * per + kb;
+  for (int q = threadIdx.x; q < 8 * n * kc; q += kShiftThreads) {
+    const int cr = q / kc; // child * n + coefficient
+    const int k = q - cr * kc;
+    const int c = cr / n;
+    const int b = cr - c * n;
+    const float *cc = scoef + c * n;
+    float v = 0.0F;
+    for (int e = soff[b]; e < soff[b + 1]; ++e) {
+      const int pr = spair[e];
+      v = fmaf(cc[pr & 0xffff], sL[(pr >> 16) * kShiftStates + k], v);
+    }
+    child0[c * per + static_cast<long long>(b) * K + k] += v;
+  }
 }
 
 // ---------------------------------------------------------------------------
@@ -715,18 +737,16 @@ static size_t pair_smem(int n, int n_pairs) {
 
 void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *coef, int n, int K,
                 int parent_level, int n_pairs, cudaStream_t s) {
-  const long long total = (static_cast<long long>(1) << (3 * parent_level)) * n * K;
-  const long long blocks = (total + 255) / 256;
-  m2m_kernel<<<static_cast<unsigned>(blocks), 256, pair_smem(n, n_pairs), s>>>(M, pair_off, pairs, coef, n, K,
-                                                                              parent_level, n_pairs);
+  const dim3 grid(1u << (3 * parent_level), static_cast<unsigned>((K + kShiftStates - 1) / kShiftStates));
+  const size_t smem = pair_smem(n, n_pairs) + sizeof(float) * 8 * static_cast<size_t>(n) * kShiftStates;
+  m2m_kernel<<<grid, kShiftThreads, smem, s>>>(M, pair_off, pairs, coef, n, K, parent_level, n_pairs);
 }
 
 void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
                 int child_level, int n_pairs, cudaStream_t s) {
-  const long long total = (static_cast<long long>(1) << (3 * child_level)) * n * K;
-  const long long blocks = (total + 255) / 256;
-  l2l_kernel<<<static_cast<unsigned>(blocks), 256, pair_smem(n, n_pairs), s>>>(L, pair_off, pairs, coef, n, K,
-                                                                              child_level, n_pairs);
+  const dim3 grid(1u << (3 * (child_level - 1)), static_cast<unsigned>((K + kShiftStates - 1) / kShiftStates));
+  const size_t smem = pair_smem(n, n_pairs) + sizeof(float) * static_cast<size_t>(n) * kShiftStates;
+  l2l_kernel<<<grid, kShiftThreads, smem, s>>>(L, pair_off, pairs, coef, n, K, child_level, n_pairs);
 }
 
 size_t l2p_smem_bytes(int n, int p, int Kb) {
