@@ -256,51 +256,79 @@ __device__ inline void stage_pairs(const int *pair_off, const int *pairs, const 
   __syncthreads();
 }
 
-// M2M, one CTA per (parent, block of kShiftStates states): the 8 children's
-// multipoles of the block are staged in shared memory (contiguous runs of
-// states), then each thread forms parent coefficients from the staged pair
-// table and class coefficients; lanes sharing a coefficient share the pair
-// loads (broadcast) and read consecutive states (conflict-free).
-constexpr int kShiftStates = 16;
+// M2M, one CTA per (parent, block of Ks states): the 8 children's
+// multipoles of the block are staged in shared memory ([child][coef][state],
+// rows of Ks), then a thread forms one parent coefficient for 4
+// consecutive states: per (child, pair) one class coefficient, one pair entry
+// and one float4 of staged multipoles feed 4 FMAs.  Lanes of a warp take
+// consecutive state quads of the same coefficient (conflict-free float4
+// loads, broadcast pair/coefficient loads).
 constexpr int kShiftThreads = 256;
+
+__device__ __forceinline__ void store_quad(float *dst, const float4 &v, int valid, bool add) {
+  const float e[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+  for (int j = 0; j < 4; ++j)
+    if (j < valid) dst[j] = add ? dst[j] + e[j] : e[j];
+}
 
 __global__ void __launch_bounds__(kShiftThreads) m2m_kernel(float *__restrict__ M, const int *__restrict__ pair_off,
                                                             const int *__restrict__ pairs,
                                                             const float *__restrict__ coef, int n, int K,
-                                                            int parent_level, int n_pairs) {
-  extern __shared__ int shp[];
-  int *soff = shp;
+                                                            int parent_level, int n_pairs, int Ks) {
+  extern __shared__ float4 shp4[];
+  float *sM = reinterpret_cast<float *>(shp4);                  // [8 children][n][Ks]
+  float *scoef = sM + 8 * n * Ks;                     // [8][n]
+  int *soff = reinterpret_cast<int *>(scoef + 8 * n);
   int *spair = soff + n + 1;
-  float *scoef = reinterpret_cast<float *>(spair + n_pairs);
-  float *sM = scoef + 8 * n; // [8 children][n][kShiftStates]
   stage_pairs(pair_off, pairs, coef + static_cast<long long>(parent_level + 1) * 8 * n, n, n_pairs, soff, spair,
               scoef);
   const long long parent = blockIdx.x;
-  const int kb = blockIdx.y * kShiftStates;
-  const int kc = min(kShiftStates, K - kb);
+  const int kb = blockIdx.y * Ks;
+  const int kc = min(Ks, K - kb);
+  const int nq = (kc + 3) >> 2;
   const long long per = static_cast<long long>(n) * K;
   const float *child0 = M + (level_offset_d(parent_level + 1) + parent * 8) * per + kb;
-  for (int q = threadIdx.x; q < 8 * n * kc; q += kShiftThreads) {
-    const int cr = q / kc; // child * n + coefficient
-    const int k = q - cr * kc;
-    sM[cr * kShiftStates + k] = child0[(cr / n) * per + static_cast<long long>(cr % n) * K + k];
+  const int qpr = Ks >> 2; // float4 quads per staged row
+  if ((K & 3) == 0) {
+    // rows of 4-aligned states: one float4 load per quad, one division per quad
+    for (int q = threadIdx.x; q < 8 * n * qpr; q += kShiftThreads) {
+      const int cr = q / qpr; // child * n + coefficient
+      const int kq = q - cr * qpr;
+      const int c = cr / n;
+      float4 v = make_float4(0, 0, 0, 0);
+      if (4 * kq < kc)
+        v = *reinterpret_cast<const float4 *>(child0 + c * per + static_cast<long long>(cr - c * n) * K + 4 * kq);
+      reinterpret_cast<float4 *>(sM)[q] = v;
+    }
+  } else {
+    for (int q = threadIdx.x; q < 8 * n * Ks; q += kShiftThreads) {
+      const int cr = q / Ks;
+      const int k = q - cr * Ks;
+      sM[q] = k < kc ? child0[(cr / n) * per + static_cast<long long>(cr % n) * K + k] : 0.0F;
+    }
   }
   __syncthreads();
   float *out = M + (level_offset_d(parent_level) + parent) * per + kb;
-  for (int q = threadIdx.x; q < n * kc; q += kShiftThreads) {
-    const int a = q / kc;
-    const int k = q - a * kc;
+  for (int q = threadIdx.x; q < n * nq; q += kShiftThreads) {
+    const int a = q / nq;
+    const int kq = q - a * nq;
     const int e0 = soff[a], e1 = soff[a + 1];
-    float v = 0.0F;
+    float4 v = make_float4(0, 0, 0, 0);
     for (int c = 0; c < 8; ++c) {
       const float *cc = scoef + c * n;
-      const float *mc = sM + c * n * kShiftStates + k;
+      const float *mc = sM + c * n * Ks + 4 * kq;
       for (int e = e0; e < e1; ++e) {
         const int pr = spair[e];
-        v = fmaf(cc[pr & 0xffff], mc[(pr >> 16) * kShiftStates], v);
+        const float w = cc[pr & 0xffff];
+        const float4 m = *reinterpret_cast<const float4 *>(mc + (pr >> 16) * Ks);
+        v.x = fmaf(w, m.x, v.x);
+        v.y = fmaf(w, m.y, v.y);
+        v.z = fmaf(w, m.z, v.z);
+        v.w = fmaf(w, m.w, v.w);
       }
     }
-    out[static_cast<long long>(a) * K + k] = v;
+    store_quad(out + static_cast<long long>(a) * K + 4 * kq, v, kc - 4 * kq, false);
   }
 }
 
@@ -308,41 +336,59 @@ __global__ void __launch_bounds__(kShiftThreads) m2m_kernel(float *__restrict__ 
 // L2L for one child level (upstream src/far_field.cpp:533-581):
 //   L_child[beta] += sum_{|beta + g| <= p} B_class[g] L_parent[beta + g]
 // One CTA per (parent, block of states): the parent's locals are staged once
-// and shifted to its 8 children.
+// and shifted to its 8 children; a thread adds one child coefficient for 4
+// consecutive states.
 __global__ void __launch_bounds__(kShiftThreads) l2l_kernel(float *__restrict__ L, const int *__restrict__ pair_off,
                                                             const int *__restrict__ pairs,
                                                             const float *__restrict__ coef, int n, int K,
-                                                            int child_level, int n_pairs) {
-  extern __shared__ int shl[];
-  int *soff = shl;
+                                                            int child_level, int n_pairs, int Ks) {
+  extern __shared__ float4 shl4[];
+  float *sL = reinterpret_cast<float *>(shl4);                  // [n][Ks]
+  float *scoef = sL + n * Ks;                         // [8][n]
+  int *soff = reinterpret_cast<int *>(scoef + 8 * n);
   int *spair = soff + n + 1;
-  float *scoef = reinterpret_cast<float *>(spair + n_pairs);
-  float *sL = scoef + 8 * n; // [n][kShiftStates]
   stage_pairs(pair_off, pairs, coef + static_cast<long long>(child_level) * 8 * n, n, n_pairs, soff, spair, scoef);
   const long long parent = blockIdx.x;
-  const int kb = blockIdx.y * kShiftStates;
-  const int kc = min(kShiftStates, K - kb);
+  const int kb = blockIdx.y * Ks;
+  const int kc = min(Ks, K - kb);
+  const int nq = (kc + 3) >> 2;
   const long long per = static_cast<long long>(n) * K;
   const float *src = L + (level_offset_d(child_level - 1) + parent) * per + kb;
-  for (int q = threadIdx.x; q < n * kc; q += kShiftThreads) {
-    const int b = q / kc;
-    const int k = q - b * kc;
-    sL[b * kShiftStates + k] = src[static_cast<long long>(b) * K + k];
+  const int qpr = Ks >> 2;
+  if ((K & 3) == 0) {
+    for (int q = threadIdx.x; q < n * qpr; q += kShiftThreads) {
+      const int b = q / qpr;
+      const int kq = q - b * qpr;
+      float4 v = make_float4(0, 0, 0, 0);
+      if (4 * kq < kc) v = *reinterpret_cast<const float4 *>(src + static_cast<long long>(b) * K + 4 * kq);
+      reinterpret_cast<float4 *>(sL)[q] = v;
+    }
+  } else {
+    for (int q = threadIdx.x; q < n * Ks; q += kShiftThreads) {
+      const int b = q / Ks;
+      const int k = q - b * Ks;
+      sL[q] = k < kc ? src[static_cast<long long>(b) * K + k] : 0.0F;
+    }
   }
   __syncthreads();
   float *child0 = L + (level_offset_d(child_level) + parent * 8) * per + kb;
-  for (int q = threadIdx.x; q < 8 * n * kc; q += kShiftThreads) {
-    const int cr = q / kc; // child * n + coefficient
-    const int k = q - cr * kc;
+  for (int q = threadIdx.x; q < 8 * n * nq; q += kShiftThreads) {
+    const int cr = q / nq; // child * n + coefficient
+    const int kq = q - cr * nq;
     const int c = cr / n;
     const int b = cr - c * n;
     const float *cc = scoef + c * n;
-    float v = 0.0F;
+    float4 v = make_float4(0, 0, 0, 0);
     for (int e = soff[b]; e < soff[b + 1]; ++e) {
       const int pr = spair[e];
-      v = fmaf(cc[pr & 0xffff], sL[(pr >> 16) * kShiftStates + k], v);
+      const float w = cc[pr & 0xffff];
+      const float4 l = *reinterpret_cast<const float4 *>(sL + (pr >> 16) * Ks + 4 * kq);
+      v.x = fmaf(w, l.x, v.x);
+      v.y = fmaf(w, l.y, v.y);
+      v.z = fmaf(w, l.z, v.z);
+      v.w = fmaf(w, l.w, v.w);
     }
-    child0[c * per + static_cast<long long>(b) * K + k] += v;
+    store_quad(child0 + c * per + static_cast<long long>(b) * K + 4 * kq, v, kc - 4 * kq, true);
   }
 }
 
@@ -735,18 +781,28 @@ static size_t pair_smem(int n, int n_pairs) {
   return sizeof(int) * (static_cast<size_t>(n) + 1 + n_pairs) + sizeof(float) * 8 * static_cast<size_t>(n);
 }
 
+// State block of the shift kernels: the largest of 32, 16, 8, 4 whose staged
+// block (children for M2M) fits 200 KB of shared memory.
+static int shift_state_block(int n, int n_pairs, int K, int rows) {
+  int Ks = 32;
+  while (Ks > 4 && pair_smem(n, n_pairs) + sizeof(float) * rows * static_cast<size_t>(n) * Ks + 16 > 200 * 1024) Ks /= 2;
+  return std::min(Ks, (K + 3) & ~3);
+}
+
 void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *coef, int n, int K,
                 int parent_level, int n_pairs, cudaStream_t s) {
-  const dim3 grid(1u << (3 * parent_level), static_cast<unsigned>((K + kShiftStates - 1) / kShiftStates));
-  const size_t smem = pair_smem(n, n_pairs) + sizeof(float) * 8 * static_cast<size_t>(n) * kShiftStates;
-  m2m_kernel<<<grid, kShiftThreads, smem, s>>>(M, pair_off, pairs, coef, n, K, parent_level, n_pairs);
+  const int Ks = shift_state_block(n, n_pairs, K, 8);
+  const dim3 grid(1u << (3 * parent_level), static_cast<unsigned>((K + Ks - 1) / Ks));
+  const size_t smem = pair_smem(n, n_pairs) + sizeof(float) * 8 * static_cast<size_t>(n) * Ks + 16;
+  m2m_kernel<<<grid, kShiftThreads, smem, s>>>(M, pair_off, pairs, coef, n, K, parent_level, n_pairs, Ks);
 }
 
 void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
                 int child_level, int n_pairs, cudaStream_t s) {
-  const dim3 grid(1u << (3 * (child_level - 1)), static_cast<unsigned>((K + kShiftStates - 1) / kShiftStates));
-  const size_t smem = pair_smem(n, n_pairs) + sizeof(float) * static_cast<size_t>(n) * kShiftStates;
-  l2l_kernel<<<grid, kShiftThreads, smem, s>>>(L, pair_off, pairs, coef, n, K, child_level, n_pairs);
+  const int Ks = shift_state_block(n, n_pairs, K, 1);
+  const dim3 grid(1u << (3 * (child_level - 1)), static_cast<unsigned>((K + Ks - 1) / Ks));
+  const size_t smem = pair_smem(n, n_pairs) + sizeof(float) * static_cast<size_t>(n) * Ks + 16;
+  l2l_kernel<<<grid, kShiftThreads, smem, s>>>(L, pair_off, pairs, coef, n, K, child_level, n_pairs, Ks);
 }
 
 size_t l2p_smem_bytes(int n, int p, int Kb) {

@@ -56,6 +56,32 @@ std::vector<Vec3> parse_tree_points(const py::handle &input) {
   return out;
 }
 
+// A CUDA array (torch tensor, CuPy array, ...) through the CUDA Array
+// Interface: its device pointer after checking float32, C-contiguous layout
+// and the expected shape (zero-copy device I/O; the reference copies
+// element-wise through host memory, python/bindings.cpp:59-80,188-226).
+std::uintptr_t cuda_array_ptr(const py::object &a, const std::vector<long> &shape, const char *name) {
+  if (!py::hasattr(a, "__cuda_array_interface__"))
+    throw std::invalid_argument(std::string(name) + " must be a CUDA array (__cuda_array_interface__)");
+  const py::dict cai = a.attr("__cuda_array_interface__");
+  const std::string typestr = py::str(cai["typestr"]);
+  if (typestr != "<f4") throw std::invalid_argument(std::string(name) + " must be float32");
+  const py::tuple sh = cai["shape"];
+  if (sh.size() != shape.size()) throw std::invalid_argument(std::string(name) + " has the wrong number of dimensions");
+  for (size_t i = 0; i < shape.size(); ++i)
+    if (sh[i].cast<long>() != shape[i]) throw std::invalid_argument(std::string(name) + " has the wrong shape");
+  if (cai.contains("strides") && !cai["strides"].is_none()) {
+    const py::tuple st = cai["strides"];
+    long expect = 4;
+    for (size_t i = shape.size(); i-- > 0;) {
+      if (shape[i] > 1 && st[i].cast<long>() != expect) throw std::invalid_argument(std::string(name) + " must be C-contiguous");
+      expect *= shape[i];
+    }
+  }
+  const py::tuple data = cai["data"];
+  return data[0].cast<std::uintptr_t>();
+}
+
 OutputFlags parse_output(const std::string &output) {
   if (output == "field") return OutputFlags::Field;
   if (output == "potential") return OutputFlags::Potential;
@@ -372,6 +398,31 @@ PYBIND11_MODULE(cdfmm, m) {
           py::arg("moments_ptr"), py::arg("n_states"), py::arg("field_ptr"), py::arg("potential_ptr") = 0,
           py::arg("output") = "field", py::arg("stream") = 0,
           "Evaluate K states on device-resident float32 arrays (device pointers), stream-ordered.")
+      .def(
+          "evaluate_into",
+          [](UniformFmm &f, const py::object &moments, const py::object &field, const py::object &potential,
+             const std::string &output, std::uintptr_t stream) {
+            const OutputFlags flags = parse_output(output);
+            const py::dict cai = moments.attr("__cuda_array_interface__");
+            const py::tuple sh = cai["shape"];
+            const long K = sh.size() == 3 ? sh[0].cast<long>() : 1;
+            const long ns = static_cast<long>(f.tree().sorted_source_positions().size());
+            const long nt = static_cast<long>(f.tree().sorted_target_positions().size());
+            const std::uintptr_t m = cuda_array_ptr(moments, sh.size() == 3 ? std::vector<long>{K, ns, 3}
+                                                                             : std::vector<long>{ns, 3}, "moments");
+            std::uintptr_t h = 0, p = 0;
+            if (has_flag(flags, OutputFlags::Field))
+              h = cuda_array_ptr(field, sh.size() == 3 ? std::vector<long>{K, nt, 3} : std::vector<long>{nt, 3}, "field");
+            if (has_flag(flags, OutputFlags::Potential))
+              p = cuda_array_ptr(potential, sh.size() == 3 ? std::vector<long>{K, nt} : std::vector<long>{nt}, "potential");
+            py::gil_scoped_release release;
+            f.evaluate_device(reinterpret_cast<const float *>(m), static_cast<int>(K), reinterpret_cast<float *>(h),
+                              reinterpret_cast<float *>(p), flags, reinterpret_cast<void *>(stream));
+          },
+          py::arg("dipole_moments"), py::arg("field") = py::none(), py::arg("potential") = py::none(),
+          py::arg("output") = "field", py::arg("stream") = 0,
+          "Zero-copy evaluation on CUDA arrays (torch tensors, ...): moments (K, n_sources, 3) or (n_sources, 3) "
+          "float32 in user order; results written into `field` / `potential` in user order, stream-ordered.")
       .def_property_readonly("tree", &UniformFmm::tree, py::return_value_policy::reference_internal)
       .def_property_readonly("expansion_order", [](const UniformFmm &f) { return f.basis().order(); })
       .def_property_readonly("m2l_backend", &UniformFmm::m2l_backend)

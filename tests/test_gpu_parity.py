@@ -304,3 +304,26 @@ def test_host_io_chunk_pipeline_matches_device_path():
         ref = oracle.fmm(x, x, m[k].astype(np.float64), 4, 3, identities=np.arange(n))
         assert oracle.rel_l2(host["H"][k], ref["H"]) < FP32_REL_L2
     plan.close()
+
+
+def test_python_uniform_fmm_zero_copy_device_io():
+    # cdfmm.UniformFmm.evaluate_into takes CUDA arrays (torch tensors) in user
+    # order and writes the results in place: no host copies.
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(41)
+    n, K = 3000, 4
+    x = rng.uniform(0, 1, (n, 3))
+    f = make_fmm(x, x, 4, 3, max_states=K)
+    m = rng.normal(size=(K, n, 3)).astype(np.float32)
+    ref = f.evaluate_states(m, output="both", target_source_indices=list(range(n)))
+    dm = torch.from_numpy(m).cuda()
+    dH = torch.zeros((K, n, 3), device="cuda")
+    dphi = torch.zeros((K, n), device="cuda")
+    f.evaluate_into(dm, dH, dphi, output="both")
+    torch.cuda.synchronize()
+    np.testing.assert_allclose(dH.cpu().numpy(), ref["H"], rtol=1e-6, atol=1e-6 * np.abs(ref["H"]).max())
+    np.testing.assert_allclose(dphi.cpu().numpy(), ref["phi"], rtol=1e-6, atol=1e-6 * np.abs(ref["phi"]).max())
+    with pytest.raises(ValueError, match="wrong shape"):
+        f.evaluate_into(dm, dH[:, :10], dphi, output="both")
+    with pytest.raises(ValueError, match="float32"):
+        f.evaluate_into(dm.double(), dH, dphi, output="both")
