@@ -166,6 +166,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
   int *tgt_node = abort_flag + 1;            // [kTcMaxTargets]
   int *tgt_xyz = tgt_node + kTcMaxTargets;   // [kTcMaxTargets] packed coordinates
+  int *act = tgt_xyz + kTcMaxTargets;        // [216] offset positions that reach a source box in the grid
+  int *n_act = act + 216;                    // their count
 
   // Zero every stage once: A rows beyond a tile's targets are never written.
   for (uint32_t q = tid; q < S * stage_bytes / 16u; q += kTcThreads)
@@ -185,6 +187,30 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
+  __syncthreads();
+  // list2 offsets of class (cx, cy, cz): o in [c-3, c+2]^3 minus |o| <= 1, x
+  // fastest; an offset whose source box lies outside the grid for every
+  // target of the tile (zero multipoles) is dropped from the pipeline.
+  for (int i = tid; i < 216; i += kTcThreads) {
+    const int ox = cx - 3 + i % 6, oy = cy - 3 + (i / 6) % 6, oz = cz - 3 + i / 36;
+    bool use = !(ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1);
+    if (use) {
+      use = false;
+      for (int t = 0; t < count && !use; ++t) {
+        const int xyz = tgt_xyz[t];
+        const int sx = (xyz & 1023) - ox, sy = ((xyz >> 10) & 1023) - oy, sz = ((xyz >> 20) & 1023) - oz;
+        use = sx >= 0 && sy >= 0 && sz >= 0 && sx < side && sy < side && sz < side;
+      }
+    }
+    act[i] = use ? 1 : 0;
+  }
+  __syncthreads();
+  if (tid == 0) {
+    int c = 0;
+    for (int i = 0; i < 216; ++i)
+      if (act[i]) act[c++] = i;
+    *n_act = c;
+  }
   fence_proxy_async();
   if (tid < 32) {
     asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(tmem_slot)),
@@ -195,14 +221,13 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   __syncthreads();
   tc_fence_after();
   const uint32_t tmem = *tmem_slot;
-  const int units = 189 * nkc;
+  const int units = *n_act * nkc;
 
   if (tid >= 32 && tid < 64) {
     // Producer warp: bulk copies of (offset, chunk) operands into stage u % S.
     const size_t btile = static_cast<size_t>(args.Npad) * kKChunk * 2u; // stride of one B chunk tile
     int produced = 0;
     int slot = 0, ox = 0, oy = 0, oz = 0;
-    int o_next = 0; // position in the class's offset enumeration (x fastest)
     for (int u = 0; u < units; ++u) {
       const int s = u % S;
       int ok = 1;
@@ -217,14 +242,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
       if (!ok) break;
       const int kc = u % nkc;
       if (kc == 0) {
-        // Next list2 offset of class (cx, cy, cz): o in [c-3, c+2]^3 minus |o| <= 1.
-        for (;;) {
-          const int i = o_next++;
-          ox = cx - 3 + i % 6;
-          oy = cy - 3 + (i / 6) % 6;
-          oz = cz - 3 + i / 36;
-          if (!(ox >= -1 && ox <= 1 && oy >= -1 && oy <= 1 && oz >= -1 && oz <= 1)) break;
-        }
+        const int i = act[u / nkc];
+        ox = cx - 3 + i % 6;
+        oy = cy - 3 + (i / 6) % 6;
+        oz = cz - 3 + i / 36;
         slot = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
       }
       const int kcw = min(kKChunk, args.Kpad - kc * kKChunk);
@@ -335,6 +356,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
       for (int c0 = 0; c0 < args.Npad; c0 += 16) {
         float v[16];
         tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(m * args.acc_stride + c0), v);
+        if (units == 0) {
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] = 0.0F; // no source box in the grid: no MMA wrote the accumulator
+        }
         if (valid) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
@@ -396,7 +421,7 @@ size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages) {
   const size_t a = 128u * kKChunk * 2u * static_cast<size_t>(m_tiles);
   const size_t b = static_cast<size_t>(Npad) * kKChunk * 2u;
   return static_cast<size_t>(stages) * (2 * a + 2 * b) + 2 * stages * sizeof(uint64_t) + 8 +
-         2 * kTcMaxTargets * sizeof(int);
+         (2 * kTcMaxTargets + 216 + 1) * sizeof(int);
 }
 
 void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,

@@ -195,12 +195,16 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
 //
 // Staging: the neighbourhood positions (relative to this leaf's centre) and
 // sorted source indices are staged once; the moments of the round's state
-// window stream through a double-buffered cp.async pipeline in chunks of
-// kChunkB sources.  Within a moment row, state k sits at k + k/8 (one pad
+// window stream through a kBufs-buffered cp.async pipeline in chunks of
+// kChunkB sources, one barrier per chunk: the copy of chunk c + kBufs - 1 is
+// issued after the barrier that ends every thread's use of chunk c - 1,
+// whose buffer it overwrites.  (Three buffers of 24 sources, which fit two
+// CTAs per SM, measured slower than two of 32.)  Within a moment row, state k sits at k + k/8 (one pad
 // float4 per 8 states), so lanes of one warp that read the same source for
 // two state groups hit different banks; the row stride Kr is 1 mod 8 (in
 // float4) so the F lanes of one item, reading different sources, do too.
 constexpr int kChunkB = 32;         // sources per moment chunk
+constexpr int kBufs = 2;            // moment chunk buffers (copies run kBufs - 1 chunks ahead)
 constexpr int kNeighbourCap = 1024; // staged neighbourhood size per pass
 constexpr int kStateBlock = 64;     // states per state block (bounds shared memory)
 constexpr int kKbThreads = 256;
@@ -363,7 +367,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
   extern __shared__ float4 dynb[];
   float4 *sPos = dynb;                                            // [kNeighbourCap]
   int *sIdx = reinterpret_cast<int *>(sPos + kNeighbourCap);      // [kNeighbourCap]
-  float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [2][kChunkB][Kr <= kStateBlock + 9]
+  float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [kBufs][kChunkB][Kr <= kStateBlock + 9]
   __shared__ Neighbours nb;
   const int leaf = blockIdx.x;
   const int t0 = tgt_off[leaf];
@@ -437,7 +441,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
         auto issue = [&](int c) {
           const int q0 = c * kChunkB;
           const int sn = min(kChunkB, pn - q0);
-          float4 *dst = sMom + (c & 1) * kChunkB * Kr;
+          float4 *dst = sMom + (c % kBufs) * kChunkB * Kr;
           int q = cq0, k = ck0;
           while (q < sn) {
             cp_async16(dst + q * Kr + mrow_pos<KG>(k), mom + static_cast<long long>(sIdx[q0 + q]) * mrow + kblk + k_lo + k);
@@ -450,18 +454,23 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
           }
           cp_async_commit();
         };
-        issue(0);
-        for (int c = 0; c < chunks; ++c) {
-          if (c + 1 < chunks)
-            issue(c + 1);
+        for (int j = 0; j < kBufs - 1; ++j) {
+          if (j < chunks)
+            issue(j);
           else
-            cp_async_commit(); // one group per iteration keeps the wait count uniform
-          cp_async_wait<1>();
-          __syncthreads();
+            cp_async_commit(); // one group per step keeps the wait count uniform
+        }
+        for (int c = 0; c < chunks; ++c) {
+          cp_async_wait<kBufs - 2>(); // chunk c has landed (this thread's copies)
+          __syncthreads();            // ... and every thread's; all are done with chunk c - 1
+          if (c + kBufs - 1 < chunks)
+            issue(c + kBufs - 1); // into the buffer chunk c - 1 used
+          else
+            cp_async_commit();
           const int q0 = c * kChunkB;
           const int sn = min(kChunkB, pn - q0);
           if (valid) {
-            const float4 *m_row0 = sMom + (c & 1) * kChunkB * Kr + mrow_pos<KG>(kb - k_lo);
+            const float4 *m_row0 = sMom + (c % kBufs) * kChunkB * Kr + mrow_pos<KG>(kb - k_lo);
             if constexpr (GRAD) {
               if (kvalid == KG)
                 p2p_grad_chunk<KG, true, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
@@ -481,8 +490,8 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
                 p2p_kb_chunk<KG, PHI, false>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc);
             }
           }
-          __syncthreads();
         }
+        __syncthreads(); // the next pass or round refills the buffers
       }
       if constexpr (GRAD) {
         for (int o = 1; o < F; o <<= 1)
@@ -640,7 +649,7 @@ template <int KG> size_t p2p_kb_smem_bytes(int K) {
   const int Kc = (std::min(K, kStateBlock) + 1) & ~1; // widest window (paired rows round up)
   const int Kr = mrow_stride<KG>(Kc);
   return sizeof(float4) * kNeighbourCap + sizeof(int) * kNeighbourCap +
-         sizeof(float4) * 2 * kChunkB * static_cast<size_t>(Kr);
+         sizeof(float4) * kBufs * kChunkB * static_cast<size_t>(Kr);
 }
 
 template <int KG, bool PAIRED>

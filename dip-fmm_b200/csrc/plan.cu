@@ -467,14 +467,16 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
         while (st < 8 && m2l_tc_smem_bytes(Npad, mt, st + 1) <= budget) ++st;
         return st;
       };
-      const size_t one_cta = std::min<size_t>(smem, 224 * 1024), two_cta = 112 * 1024;
+      const size_t one_cta = std::min<size_t>(smem, 224 * 1024), two_cta = 112 * 1024, three_cta = 74 * 1024;
       plan->tc_candidates.clear();
       for (int mt : {2, 1, 4}) {
         if (mt * acc_stride > 512) continue;
         const int s1 = max_stages(mt, one_cta);
         if (s1 >= 2) plan->tc_candidates.emplace_back(mt, s1);
         const int s2 = max_stages(mt, two_cta);
-        if (s2 >= 2 && tmem_columns(mt, acc_stride) <= 256) plan->tc_candidates.emplace_back(mt, s2);
+        if (s2 >= 2 && s2 < s1 && tmem_columns(mt, acc_stride) <= 256) plan->tc_candidates.emplace_back(mt, s2);
+        const int s3 = max_stages(mt, three_cta);
+        if (s3 >= 2 && s3 < s2 && 3 * tmem_columns(mt, acc_stride) <= 512) plan->tc_candidates.emplace_back(mt, s3);
       }
       const int m_tiles = plan->tc_candidates.empty() ? 1 : plan->tc_candidates.front().first;
       const int stages = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().second;

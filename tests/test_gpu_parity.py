@@ -164,7 +164,7 @@ def test_upward_pass_root_matches_oracle():
     np.testing.assert_allclose(f.root_multipole, root_ref, rtol=1e-5, atol=1e-5 * np.abs(root_ref).max())
 
 
-@pytest.mark.parametrize("K", [2, 5, 8, 16, 64])
+@pytest.mark.parametrize("K", [2, 5, 8, 13, 16, 64])
 def test_batched_states_match_single_state_calls(K):
     """K states in one call equal K single-state calls.  K >= 8 takes the
     split-BF16 tensor-core M2L (three products), so the bar there is the
