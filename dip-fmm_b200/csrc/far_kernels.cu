@@ -171,16 +171,16 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
     const int Kc = min(Kb, K - kblk);
     const int Kq = (Kc + 3) >> 2;
     const int tiles = (nm1p >> 2) * Kq;
-    for (int q = tid; q < 3 * nm1p * Kc; q += kP2mThreads) P[q] = 0.0F;
+    for (int q = tid; q < 3 * nm1p * Kc; q += blockDim.x) P[q] = 0.0F;
     for (int c0 = s0; c0 < s1; c0 += kP2mChunk) {
       const int cn = min(kP2mChunk, s1 - c0);
       __syncthreads();
-      for (int j = tid; j < cn; j += kP2mThreads) {
+      for (int j = tid; j < cn; j += blockDim.x) {
         const float4 d = src_rel[c0 + j];
         if (nm1 > 0) monomials(d.x, d.y, d.z, p - 1, mono + j * nm1p);
         for (int q = nm1; q < nm1p; ++q) mono[j * nm1p + q] = 0.0F;
       }
-      for (int q = tid; q < cn * Kc; q += kP2mThreads) {
+      for (int q = tid; q < cn * Kc; q += blockDim.x) {
         const int j = q / Kc;
         const int k = kblk + q - j * Kc;
         // paired layout (K >= 4): state k is component k & 1 of its pair
@@ -190,7 +190,7 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
         smom[q] = make_float4(odd ? a.y : a.x, odd ? a.w : a.z, odd ? b.y : b.x, 0.0F);
       }
       __syncthreads();
-      for (int t = tid; t < tiles; t += kP2mThreads) {
+      for (int t = tid; t < tiles; t += blockDim.x) {
         const int mb = t / Kq;
         const int kb = t - mb * Kq;
         const int mu0 = mb * 4;
@@ -229,7 +229,7 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
       }
     }
     __syncthreads();
-    for (int q = tid; q < n * Kc; q += kP2mThreads) {
+    for (int q = tid; q < n * Kc; q += blockDim.x) {
       const int a = q / Kc;
       const int k = q - a * Kc;
       const int ax = basis[4 * a], ay = basis[4 * a + 1], az = basis[4 * a + 2];
@@ -751,8 +751,8 @@ void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, 
 // State block of the P2M kernel for K states: the largest of 64, 32, ...
 // (<= K) whose shared memory stays within 100 KB (two CTAs per SM).
 static int p2m_state_block(int p, int K) {
-  int Kb = std::min(K, 64);
-  while (Kb > 4 && p2m_smem_bytes(0, p, Kb, 0) > 100 * 1024) Kb = (Kb + 1) / 2;
+  int Kb = std::min(K, 32);
+  while (Kb > 4 && p2m_smem_bytes(0, p, Kb, 0) > 64 * 1024) Kb = (Kb + 1) / 2;
   return Kb;
 }
 
@@ -760,7 +760,7 @@ size_t p2m_smem_bytes(int n, int p, int K, int chunk) {
   (void)n;
   (void)chunk;
   const int nm1p = (basis_size_d(p - 1) + 3) & ~3;
-  const size_t Kb = static_cast<size_t>(std::min(K, 64));
+  const size_t Kb = static_cast<size_t>(std::min(K, 32));
   return sizeof(float4) * kP2mChunk * Kb + sizeof(float) * (3 * nm1p * Kb + static_cast<size_t>(kP2mChunk) * nm1p);
 }
 
@@ -772,9 +772,13 @@ void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, co
     p2m_small_kernel<<<leaves, 128, 0, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth));
     return;
   }
+  // State blocks of <= 32 keep a CTA within 64 KB (several CTAs per SM hide
+  // the staging latency); 128 threads cover the 4 x 4 tiles of p <= 6.
   const int Kb = p2m_state_block(p, K);
   const size_t smem = p2m_smem_bytes(n, p, Kb, 0);
-  p2m_kernel<<<leaves, kP2mThreads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb);
+  const int nm1p = (basis_size_d(p - 1) + 3) & ~3;
+  const int threads = (nm1p / 4) * ((Kb + 3) / 4) <= 128 ? 128 : kP2mThreads;
+  p2m_kernel<<<leaves, threads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb);
 }
 
 static size_t pair_smem(int n, int n_pairs) {

@@ -86,6 +86,8 @@ struct cdfmm_b200_plan {
 
   cudaStream_t stream = nullptr;   // far-field / main stream
   cudaStream_t near_stream = nullptr;
+  cudaStream_t far_stream = nullptr;                // far field, high priority (overlaps the near field)
+  cudaEvent_t ev_far = nullptr;
   cudaStream_t io_in = nullptr, io_out = nullptr;  // host-memory copies overlapping the evaluation
   std::vector<cudaEvent_t> io_events;               // chunk pipeline events
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;

@@ -109,6 +109,8 @@ void free_plan(cdfmm_b200_plan *p) {
   if (p->io_in) cudaStreamDestroy(p->io_in);
   if (p->io_out) cudaStreamDestroy(p->io_out);
   if (p->near_stream) cudaStreamDestroy(p->near_stream);
+  if (p->far_stream) cudaStreamDestroy(p->far_stream);
+  if (p->ev_far) cudaEventDestroy(p->ev_far);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
 }
@@ -266,6 +268,15 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
 
     check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaStreamCreateWithFlags(&plan->near_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    {
+      // The far field runs on a high-priority stream so its CTAs are
+      // dispatched into SM slots as they free up while the (FP32-bound) near
+      // field runs at the default priority: tensor-core M2L and P2P overlap.
+      int least = 0, greatest = 0;
+      check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+      check(cudaStreamCreateWithPriority(&plan->far_stream, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+      check(cudaEventCreateWithFlags(&plan->ev_far, cudaEventDisableTiming), "cudaEventCreate");
+    }
     check(cudaStreamCreateWithFlags(&plan->io_in, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaStreamCreateWithFlags(&plan->io_out, cudaStreamNonBlocking), "cudaStreamCreate");
     check(cudaEventCreateWithFlags(&plan->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
@@ -716,9 +727,11 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   // stage timing enabled it runs first on the main stream instead, so that
   // each stage's events measure that stage alone.
   cudaStream_t ns = timing ? s : plan->near_stream;
+  cudaStream_t fs = timing ? s : plan->far_stream;
   if (!timing) {
     check(cudaEventRecord(plan->ev_fork, s), "event");
     check(cudaStreamWaitEvent(ns, plan->ev_fork, 0), "wait");
+    check(cudaStreamWaitEvent(fs, plan->ev_fork, 0), "wait");
   }
   if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
   launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
@@ -729,9 +742,13 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   if (!timing) check(cudaEventRecord(plan->ev_join, ns), "event");
 
   // far field
-  launches += enqueue_far(plan, K, s, timing);
+  launches += enqueue_far(plan, K, fs, timing);
   if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
-  if (!timing) check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
+  if (!timing) {
+    check(cudaEventRecord(plan->ev_far, fs), "event");
+    check(cudaStreamWaitEvent(s, plan->ev_far, 0), "wait");
+    check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
+  }
   if (timing) check(cudaEventRecord(plan->ev_t[6], s), "event");
   launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis, plan->n,
              plan->p, K, plan->nt, plan->depth, output, layout, plan->phi_scale, field, potential, s);
