@@ -56,9 +56,9 @@ __device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
 }
 
 // Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity) {
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = kWaitLimit) {
   const uint32_t addr = smem_u32(bar);
-  for (uint32_t i = 0; i < kWaitLimit; ++i) {
+  for (uint32_t i = 0; i < limit; ++i) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -445,6 +445,22 @@ void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s) {
     m2l_tc_kernel<2><<<n_tiles, kTcThreads, smem, s>>>(args);
   else
     m2l_tc_kernel<1><<<n_tiles, kTcThreads, smem, s>>>(args);
+}
+
+// Self-test of the bounded-wait path: one thread waits on an mbarrier whose
+// phase nothing completes, with a short limit; the wait must give up and the
+// kernel record the same error code the M2L pipeline records and return.
+__global__ void bounded_wait_selftest_kernel(int *error_flag, uint32_t limit) {
+  __shared__ uint64_t bar;
+  if (threadIdx.x == 0) {
+    mbar_init(&bar, 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (!mbar_wait(&bar, 0, limit)) atomicExch(error_flag, 2);
+  }
+}
+
+void launch_bounded_wait_selftest(int *error_flag, cudaStream_t s) {
+  bounded_wait_selftest_kernel<<<1, 32, 0, s>>>(error_flag, 1u << 12);
 }
 
 bool configure_m2l_tc(size_t max_smem) {

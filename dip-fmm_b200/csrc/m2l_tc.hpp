@@ -36,6 +36,9 @@ void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, 
                      int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s);
 void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s);
 bool configure_m2l_tc(size_t max_smem);
+// Runs a kernel whose bounded mbarrier wait must expire (nothing arrives)
+// and set *error_flag = 2, exactly as an expired wait of the M2L pipeline.
+void launch_bounded_wait_selftest(int *error_flag, cudaStream_t s);
 std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, int Npad, int Kpad);
 
 } // namespace cdfmm_b200

@@ -1118,6 +1118,35 @@ int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out) {
   return CDFMM_B200_OK;
 }
 
+int cdfmm_b200_selftest_bounded_wait(int32_t device) {
+  int *flag = nullptr;
+  try {
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+      cudaGetLastError();
+      throw AbiError(CDFMM_B200_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    require(device >= 0 && device < devices, "device ordinal out of range");
+    check(cudaSetDevice(device), "cudaSetDevice");
+    check(cudaMalloc(&flag, sizeof(int)), "cudaMalloc");
+    check(cudaMemset(flag, 0, sizeof(int)), "cudaMemset");
+    launch_bounded_wait_selftest(flag, nullptr);
+    check(cudaGetLastError(), "self-test launch");
+    check(cudaDeviceSynchronize(), "self-test");
+    int v = 0;
+    check(cudaMemcpy(&v, flag, sizeof(int), cudaMemcpyDeviceToHost), "D2H");
+    cudaFree(flag);
+    flag = nullptr;
+    if (v != 0)
+      throw AbiError(CDFMM_B200_ERR_TIMEOUT, "bounded wait expired as intended (code " + std::to_string(v) +
+                                                 "); the device context remains usable");
+    throw AbiError(CDFMM_B200_ERR_LOGIC, "bounded-wait self-test: the wait did not expire");
+  } catch (const AbiError &e) {
+    if (flag) cudaFree(flag);
+    return fail(nullptr, e.code, e.what());
+  }
+}
+
 int cdfmm_b200_direct_grad_fp64(int32_t device, int32_t ns, const double *src, const double *mom, int32_t nt,
                                 const double *tgt, const int32_t *self, const double *weights, double *grad) {
   void *buf[6] = {};

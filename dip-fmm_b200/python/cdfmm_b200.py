@@ -42,6 +42,7 @@ EXPORTED = (
     "cdfmm_b200_direct_fp64", "cdfmm_b200_m2l_matrix", "cdfmm_b200_last_error",
     "cdfmm_b200_evaluate_noalloc", "cdfmm_b200_backward", "cdfmm_b200_batch_create",
     "cdfmm_b200_batch_launch", "cdfmm_b200_batch_destroy", "cdfmm_b200_direct_grad_fp64",
+    "cdfmm_b200_selftest_bounded_wait",
 )
 
 # Scratch capacity of cdfmm_b200_evaluate_noalloc (bytes).
@@ -134,6 +135,7 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.cdfmm_b200_direct_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
     lib.cdfmm_b200_direct_grad_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
+    lib.cdfmm_b200_selftest_bounded_wait.argtypes = [i32]
     lib.cdfmm_b200_m2l_matrix.argtypes = [i32, vp, vp, u64]
     lib.cdfmm_b200_last_error.argtypes = [vp]
     lib.cdfmm_b200_last_error.restype = ctypes.c_char_p

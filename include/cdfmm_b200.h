@@ -244,6 +244,13 @@ int cdfmm_b200_direct_fp64(int32_t device, int32_t n_sources, const double *sour
                            const double *target_positions, const int32_t *self_indices,
                            double *phi, double *field);
 
+/* Failure-detection self-test (no counterpart in the reference): launches a
+ * kernel whose bounded mbarrier wait cannot complete (nothing arrives) with a
+ * short iteration limit -- the mechanism every wait of the tensor-core M2L
+ * uses -- and returns CDFMM_B200_ERR_TIMEOUT when the wait gave up, set the
+ * device error flag and returned; the device context stays usable.  Nothing
+ * faults, traps or hangs. */
+int cdfmm_b200_selftest_bounded_wait(int32_t device);
 /* FP64 O(N*M) direct position gradient: grad[i] = d/dx_i (weights_i . H_i) with
  * explicit self exclusion (no counterpart in the reference; the validation
  * reference of cdfmm_b200_backward's grad_target_positions).  Host arrays in
