@@ -450,6 +450,30 @@ def b200_arm(args):
     roofline.update({"achieved": achieved, "peak": peak, "frac": achieved / peak if peak else None,
                      "kernel_ms": ms_dom, "traffic": traffic_from_profiles(dom)})
 
+    # HBM-bound stages: compulsory DRAM bytes per evaluation (FP32) / stage time
+    # -- P2M and L2P 12N + 12NK + 4 n L_leaf K (+ 4NK potential for L2P), M2M
+    # 4nK (nodes - 1) read + 4nK non-leaf written, L2L reads the locals of
+    # levels 2..d-1 and reads + writes those of levels 3..d, gather 12NK read +
+    # 16NK written.
+    n_leaves = 8 ** d
+    nodes = (8 ** (d + 1) - 1) // 7
+    nonleaf = nodes - n_leaves
+    hbm_peak = peaks.get("hbm_gbs", FALLBACK_PEAKS["hbm_gbs"])
+    hbm_bytes = {
+        "gather": 12.0 * N * K + 16.0 * N * K,
+        "p2m": 12.0 * N + 12.0 * N * K + 4.0 * n * n_leaves * K,
+        "m2m": 4.0 * n * K * (nodes - 1) + 4.0 * n * K * nonleaf,
+        "l2l": 4.0 * n * K * (nonleaf - 9) + 8.0 * n * K * (nodes - 73),  # parents at levels 2..d-1, children 3..d
+        "l2p": 12.0 * N + 12.0 * N * K + 4.0 * N * K + 4.0 * n * n_leaves * K,
+    }
+    hbm = {}
+    for k, b in hbm_bytes.items():
+        ms_k = stages.get(k, 0.0)
+        if ms_k > 0:
+            gbs = b / (ms_k * 1e-3) / 1e9
+            hbm[k] = {"bytes": b, "ms": ms_k, "GB/s": gbs, "frac": gbs / hbm_peak}
+    hbm["_peak"] = {"GB/s": hbm_peak, "source": f"{peak_kind} hbm_gbs"}
+
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
         v, info = run_reference_cpu(args.seed, 1, 3)
@@ -468,7 +492,7 @@ def b200_arm(args):
                    "parallelism": "replicas (independent states per GPU)" if world > 1 else "single GPU"},
         "rel_l2_H": rel_h, "rel_l2_phi": rel_phi,
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info, "roofline": roofline,
-        "cpu_baseline": cpu, "stages_ms": stages,
+        "cpu_baseline": cpu, "stages_ms": stages, "hbm_stages": hbm,
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_state": ms_state_plain, "states_timed": ks,
                   "m2l": "fp32"},
         "batched_over_plain": value / plain_value,

@@ -194,26 +194,28 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
         const int mb = t / Kq;
         const int kb = t - mb * Kq;
         const int mu0 = mb * 4;
-        float acc[3][4][4];
+        // acc[c][u pair][kk]: packed FP32x2 FMAs over pairs of monomials
+        float2 acc[3][2][4];
 #pragma unroll
         for (int c = 0; c < 3; ++c)
 #pragma unroll
-          for (int u = 0; u < 4; ++u)
+          for (int u = 0; u < 2; ++u)
 #pragma unroll
-            for (int kk = 0; kk < 4; ++kk) acc[c][u][kk] = 0.0F;
+            for (int kk = 0; kk < 4; ++kk) acc[c][u][kk] = make_float2(0.0F, 0.0F);
         for (int j = 0; j < cn; ++j) {
           const float4 mo = *reinterpret_cast<const float4 *>(mono + j * nm1p + mu0);
-          const float mv[4] = {mo.x, mo.y, mo.z, mo.w};
+          const float2 m01 = make_float2(mo.x, mo.y), m23 = make_float2(mo.z, mo.w);
 #pragma unroll
           for (int kk = 0; kk < 4; ++kk) {
             const int k = kb + kk * Kq;
             const float4 m = k < Kc ? smom[j * Kc + k] : make_float4(0, 0, 0, 0);
-#pragma unroll
-            for (int u = 0; u < 4; ++u) {
-              acc[0][u][kk] = fmaf(m.x, mv[u], acc[0][u][kk]);
-              acc[1][u][kk] = fmaf(m.y, mv[u], acc[1][u][kk]);
-              acc[2][u][kk] = fmaf(m.z, mv[u], acc[2][u][kk]);
-            }
+            const float2 X = make_float2(m.x, m.x), Y = make_float2(m.y, m.y), Z = make_float2(m.z, m.z);
+            acc[0][0][kk] = __ffma2_rn(m01, X, acc[0][0][kk]);
+            acc[0][1][kk] = __ffma2_rn(m23, X, acc[0][1][kk]);
+            acc[1][0][kk] = __ffma2_rn(m01, Y, acc[1][0][kk]);
+            acc[1][1][kk] = __ffma2_rn(m23, Y, acc[1][1][kk]);
+            acc[2][0][kk] = __ffma2_rn(m01, Z, acc[2][0][kk]);
+            acc[2][1][kk] = __ffma2_rn(m23, Z, acc[2][1][kk]);
           }
         }
 #pragma unroll
@@ -223,7 +225,8 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
 #pragma unroll
             for (int c = 0; c < 3; ++c)
 #pragma unroll
-              for (int u = 0; u < 4; ++u) P[(c * nm1p + mu0 + u) * Kc + k] += acc[c][u][kk];
+              for (int u = 0; u < 4; ++u)
+                P[(c * nm1p + mu0 + u) * Kc + k] += (u & 1) ? acc[c][u >> 1][kk].y : acc[c][u >> 1][kk].x;
           }
         }
       }
@@ -786,10 +789,11 @@ static size_t pair_smem(int n, int n_pairs) {
 }
 
 // State block of the shift kernels: the largest of 32, 16, 8, 4 whose staged
-// block (children for M2M) fits 200 KB of shared memory.
+// block (children for M2M) fits 48 KB of shared memory, so that several CTAs
+// per SM overlap one CTA's staging with another's arithmetic.
 static int shift_state_block(int n, int n_pairs, int K, int rows) {
   int Ks = 32;
-  while (Ks > 4 && pair_smem(n, n_pairs) + sizeof(float) * rows * static_cast<size_t>(n) * Ks + 16 > 200 * 1024) Ks /= 2;
+  while (Ks > 4 && pair_smem(n, n_pairs) + sizeof(float) * rows * static_cast<size_t>(n) * Ks + 16 > 48 * 1024) Ks /= 2;
   return std::min(Ks, (K + 3) & ~3);
 }
 
