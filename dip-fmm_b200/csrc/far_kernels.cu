@@ -25,7 +25,8 @@ namespace {
 template <typename T>
 __global__ void __launch_bounds__(256) gather_moments_kernel(const T *__restrict__ user, const int *__restrict__ inv,
                                                              int ns, int K, double inv_scale, float inv_scale3_f,
-                                                             bool paired, float4 *__restrict__ mom) {
+                                                             bool paired, float4 *__restrict__ mom, int k0,
+                                                             int krow) {
   __shared__ float tile[32][32 * 3 + 1]; // [user][state * 3 + component]
   const int u0 = blockIdx.x * 32;
   const int nu = min(32, ns - u0);
@@ -48,12 +49,12 @@ __global__ void __launch_bounds__(256) gather_moments_kernel(const T *__restrict
       // state pairs (k, k+1) as (x_k, x_k1, y_k, y_k1), (z_k, z_k1, 0, 0); a
       // missing partner (K odd) is zero
       const int kp = (kn + 1) >> 1;
-      const int row = (K + 1) & ~1;
+      const int row = krow;
       for (int e = threadIdx.x; e < nu * kp; e += blockDim.x) {
         const int t = e / kp;
         const int k = 2 * (e - t * kp);
         const bool b = k + 1 < kn;
-        float4 *dst = mom + static_cast<long long>(inv[u0 + t]) * row + kc + k;
+        float4 *dst = mom + static_cast<long long>(inv[u0 + t]) * row + k0 + kc + k;
         dst[0] = make_float4(tile[t][3 * k], b ? tile[t][3 * k + 3] : 0.0F, tile[t][3 * k + 1],
                              b ? tile[t][3 * k + 4] : 0.0F);
         dst[1] = make_float4(tile[t][3 * k + 2], b ? tile[t][3 * k + 5] : 0.0F, 0.0F, 0.0F);
@@ -62,7 +63,7 @@ __global__ void __launch_bounds__(256) gather_moments_kernel(const T *__restrict
       for (int e = threadIdx.x; e < nu * kn; e += blockDim.x) {
         const int t = e / kn;
         const int k = e - t * kn;
-        mom[static_cast<long long>(inv[u0 + t]) * K + kc + k] =
+        mom[static_cast<long long>(inv[u0 + t]) * krow + k0 + kc + k] =
             make_float4(tile[t][3 * k], tile[t][3 * k + 1], tile[t][3 * k + 2], 0.0F);
       }
     }
@@ -84,6 +85,31 @@ __device__ inline void monomials(float dx, float dy, float dz, int q, float *out
       xb = xb * dy * kInvInt[b + 1];
     }
     xa = xa * dx * kInvInt[a + 1];
+  }
+}
+
+// The monomials of monomials() whose x-degree a belongs to part r of 4:
+// a = r, 7 - r, 8 + r, 15 - r, ... (part 0 takes a = 0, the largest group;
+// for q = 6 the parts hold 28, 22, 18 and 16 of the 84 monomials).  Four
+// threads per point share the work; each runs the serial recurrences, so the
+// values are bit-identical to monomials().  zero: store zeros instead.
+__device__ inline void monomials_part(float dx, float dy, float dz, int q, float *out, int stride, int r, bool zero) {
+  for (int a0 = 0; a0 <= q; a0 += 8) {
+    for (int h = 0; h < 2; ++h) {
+      const int a = a0 + (h == 0 ? r : 7 - r);
+      if (a > q) continue;
+      float xa = 1.0F;
+      for (int i = 0; i < a; ++i) xa = xa * dx * kInvInt[i + 1];
+      float xb = xa;
+      for (int b = 0; a + b <= q; ++b) {
+        float xc = xb;
+        for (int c = 0; a + b + c <= q; ++c) {
+          out[rank3(a, b, c) * stride] = zero ? 0.0F : xc;
+          xc = xc * dz * kInvInt[c + 1];
+        }
+        xb = xb * dy * kInvInt[b + 1];
+      }
+    }
   }
 }
 
@@ -175,10 +201,14 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
     for (int c0 = s0; c0 < s1; c0 += kP2mChunk) {
       const int cn = min(kP2mChunk, s1 - c0);
       __syncthreads();
-      for (int j = tid; j < cn; j += blockDim.x) {
+      // four threads per source (consecutive lanes: consecutive sources, one part)
+      for (int w = tid; w < 4 * cn; w += blockDim.x) {
+        const int r = w / cn;
+        const int j = w - r * cn;
         const float4 d = src_rel[c0 + j];
-        if (nm1 > 0) monomials(d.x, d.y, d.z, p - 1, mono + j * nm1p);
-        for (int q = nm1; q < nm1p; ++q) mono[j * nm1p + q] = 0.0F;
+        if (nm1 > 0) monomials_part(d.x, d.y, d.z, p - 1, mono + j * nm1p, 1, r, false);
+        if (r == 0)
+          for (int q = nm1; q < nm1p; ++q) mono[j * nm1p + q] = 0.0F;
       }
       for (int q = tid; q < cn * Kc; q += blockDim.x) {
         const int j = q / Kc;
@@ -410,20 +440,89 @@ __global__ void __launch_bounds__(kShiftThreads) l2l_kernel(float *__restrict__ 
 // conflict-free L loads, broadcast monomial loads).
 constexpr int kL2pThreads = 128;
 constexpr int kL2pTargets = 32;
+static_assert(kL2pThreads == 4 * kL2pTargets, "L2P monomials: four threads per target");
 
-__device__ inline void monomials_strided(float dx, float dy, float dz, int q, float *out, int stride) {
-  float xa = 1.0F;
-  for (int a = 0; a <= q; ++a) {
-    float xb = xa;
-    for (int b = 0; a + b <= q; ++b) {
-      float xc = xb;
-      for (int c = 0; a + b + c <= q; ++c) {
-        out[rank3(a, b, c) * stride] = xc;
-        xc = xc * dz * kInvInt[c + 1];
+// One pass of L2P register tiles over a staged target chunk: tile =
+// (TU consecutive targets, 4 consecutive states).
+template <int TU>
+__device__ __forceinline__ void l2p_tiles(int tid, int tn, int Kq, int Kcp, int Kc, int n, int nm1,
+                                          const float *mono, const float *sL, const short *sidx, bool want_phi,
+                                          bool want_h, float4 *__restrict__ near, int tc, int kblk, int K,
+                                          float phi_scale) {
+  const int tiles = ((tn + TU - 1) / TU) * Kq;
+  for (int tile = tid; tile < tiles; tile += kL2pThreads) {
+    const int tq = tile / Kq;
+    const int kq = tile - tq * Kq;
+    float ph[TU][4], hx[TU][4], hy[TU][4], hz[TU][4];
+#pragma unroll
+    for (int u = 0; u < TU; ++u)
+#pragma unroll
+      for (int v = 0; v < 4; ++v) ph[u][v] = hx[u][v] = hy[u][v] = hz[u][v] = 0.0F;
+    const float *mq = mono + TU * tq;
+    const float *lq = sL + 4 * kq;
+    auto load_mono = [&](int b, float (&mv)[TU]) {
+      if constexpr (TU == 4) {
+        const float4 mo = *reinterpret_cast<const float4 *>(mq + b * kL2pTargets);
+        mv[0] = mo.x;
+        mv[1] = mo.y;
+        mv[2] = mo.z;
+        mv[3] = mo.w;
+      } else if constexpr (TU == 2) {
+        const float2 mo = *reinterpret_cast<const float2 *>(mq + b * kL2pTargets);
+        mv[0] = mo.x;
+        mv[1] = mo.y;
+      } else {
+        mv[0] = mq[b * kL2pTargets];
       }
-      xb = xb * dy * kInvInt[b + 1];
+    };
+    if (want_phi) {
+      for (int b = 0; b < n; ++b) {
+        float mv[TU];
+        load_mono(b, mv);
+        const float4 l = *reinterpret_cast<const float4 *>(lq + b * Kcp);
+        const float lv[4] = {l.x, l.y, l.z, l.w};
+#pragma unroll
+        for (int u = 0; u < TU; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) ph[u][v] = fmaf(mv[u], lv[v], ph[u][v]);
+      }
     }
-    xa = xa * dx * kInvInt[a + 1];
+    if (want_h) {
+      for (int mu = 0; mu < nm1; ++mu) {
+        float mv[TU];
+        load_mono(mu, mv);
+        const float4 lx = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu] * Kcp);
+        const float4 ly = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu + 1] * Kcp);
+        const float4 lz = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu + 2] * Kcp);
+        const float xv[4] = {lx.x, lx.y, lx.z, lx.w};
+        const float yv[4] = {ly.x, ly.y, ly.z, ly.w};
+        const float zv[4] = {lz.x, lz.y, lz.z, lz.w};
+#pragma unroll
+        for (int u = 0; u < TU; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            hx[u][v] = fmaf(mv[u], xv[v], hx[u][v]);
+            hy[u][v] = fmaf(mv[u], yv[v], hy[u][v]);
+            hz[u][v] = fmaf(mv[u], zv[v], hz[u][v]);
+          }
+      }
+    }
+#pragma unroll
+    for (int u = 0; u < TU; ++u) {
+      const int t = TU * tq + u;
+      if (t >= tn) break;
+      const int i = tc + t;
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int kl = 4 * kq + v;
+        if (kl >= Kc) break;
+        const int k = kblk + kl;
+        float4 *nr = near + static_cast<long long>(i) * K + k;
+        const float4 nv = *nr;
+        *nr = make_float4(want_phi ? (ph[u][v] + nv.x) * phi_scale : 0.0F, want_h ? nv.y - hx[u][v] : 0.0F,
+                          want_h ? nv.z - hy[u][v] : 0.0F, want_h ? nv.w - hz[u][v] : 0.0F);
+      }
+    }
   }
 }
 
@@ -431,7 +530,7 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
                                                           const int *__restrict__ tgt_off, float4 *__restrict__ near,
                                                           const int8_t *__restrict__ basis, int n, int p, int K,
                                                           int leaf_node_base, unsigned output, float phi_scale,
-                                                          int Kb) {
+                                                          int Kb, int k_begin, int k_end) {
   extern __shared__ float4 l2p_smem[];
   const int Kbp = (Kb + 3) & ~3;
   float *sL = reinterpret_cast<float *>(l2p_smem);                 // [n][Kcp]
@@ -452,8 +551,8 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
   const bool want_phi = (output & 1u) != 0u;
   const bool want_h = (output & 2u) != 0u;
   const float *src = L + static_cast<long long>(leaf_node_base + leaf) * n * K;
-  for (int kblk = 0; kblk < K; kblk += Kb) {
-    const int Kc = min(Kb, K - kblk);
+  for (int kblk = k_begin; kblk < k_end; kblk += Kb) {
+    const int Kc = min(Kb, k_end - kblk);
     const int Kcp = (Kc + 3) & ~3;
     const int Kq = Kcp >> 2;
     __syncthreads();
@@ -465,75 +564,22 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
     for (int tc = t0; tc < t1; tc += kL2pTargets) {
       const int tn = min(kL2pTargets, t1 - tc);
       __syncthreads();
-      for (int t = tid; t < kL2pTargets; t += kL2pThreads) {
-        if (t < tn) {
-          const float4 d = tgt_rel[tc + t];
-          monomials_strided(d.x, d.y, d.z, p, mono + t, kL2pTargets);
-        } else {
-          for (int b = 0; b < n; ++b) mono[b * kL2pTargets + t] = 0.0F;
-        }
+      {
+        // four threads per target: warp r computes part r of every target's monomials
+        const int t = tid & (kL2pTargets - 1);
+        const float4 d = t < tn ? tgt_rel[tc + t] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+        monomials_part(d.x, d.y, d.z, p, mono + t, kL2pTargets, tid / kL2pTargets, t >= tn);
       }
       __syncthreads();
-      const int tiles = ((tn + 3) >> 2) * Kq;
-      for (int tile = tid; tile < tiles; tile += kL2pThreads) {
-        const int tq = tile / Kq;
-        const int kq = tile - tq * Kq;
-        float ph[4][4], hx[4][4], hy[4][4], hz[4][4];
-#pragma unroll
-        for (int u = 0; u < 4; ++u)
-#pragma unroll
-          for (int v = 0; v < 4; ++v) ph[u][v] = hx[u][v] = hy[u][v] = hz[u][v] = 0.0F;
-        const float *mq = mono + 4 * tq;
-        const float *lq = sL + 4 * kq;
-        if (want_phi) {
-          for (int b = 0; b < n; ++b) {
-            const float4 mo = *reinterpret_cast<const float4 *>(mq + b * kL2pTargets);
-            const float4 l = *reinterpret_cast<const float4 *>(lq + b * Kcp);
-            const float mv[4] = {mo.x, mo.y, mo.z, mo.w};
-            const float lv[4] = {l.x, l.y, l.z, l.w};
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-              for (int v = 0; v < 4; ++v) ph[u][v] = fmaf(mv[u], lv[v], ph[u][v]);
-          }
-        }
-        if (want_h) {
-          for (int mu = 0; mu < nm1; ++mu) {
-            const float4 mo = *reinterpret_cast<const float4 *>(mq + mu * kL2pTargets);
-            const float4 lx = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu] * Kcp);
-            const float4 ly = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu + 1] * Kcp);
-            const float4 lz = *reinterpret_cast<const float4 *>(lq + sidx[3 * mu + 2] * Kcp);
-            const float mv[4] = {mo.x, mo.y, mo.z, mo.w};
-            const float xv[4] = {lx.x, lx.y, lx.z, lx.w};
-            const float yv[4] = {ly.x, ly.y, ly.z, ly.w};
-            const float zv[4] = {lz.x, lz.y, lz.z, lz.w};
-#pragma unroll
-            for (int u = 0; u < 4; ++u)
-#pragma unroll
-              for (int v = 0; v < 4; ++v) {
-                hx[u][v] = fmaf(mv[u], xv[v], hx[u][v]);
-                hy[u][v] = fmaf(mv[u], yv[v], hy[u][v]);
-                hz[u][v] = fmaf(mv[u], zv[v], hz[u][v]);
-              }
-          }
-        }
-#pragma unroll
-        for (int u = 0; u < 4; ++u) {
-          const int t = 4 * tq + u;
-          if (t >= tn) break;
-          const int i = tc + t;
-#pragma unroll
-          for (int v = 0; v < 4; ++v) {
-            const int kl = 4 * kq + v;
-            if (kl >= Kc) break;
-            const int k = kblk + kl;
-            float4 *nr = near + static_cast<long long>(i) * K + k;
-            const float4 nv = *nr;
-            *nr = make_float4(want_phi ? (ph[u][v] + nv.x) * phi_scale : 0.0F, want_h ? nv.y - hx[u][v] : 0.0F,
-                              want_h ? nv.z - hy[u][v] : 0.0F, want_h ? nv.w - hz[u][v] : 0.0F);
-          }
-        }
-      }
+      // register tiles of TU targets x 4 states: TU = 4 for wide state
+      // blocks, fewer targets per thread for narrow ones so that the 128
+      // threads stay busy
+      if (Kq >= 16)
+        l2p_tiles<4>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale);
+      else if (Kq >= 8)
+        l2p_tiles<2>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale);
+      else
+        l2p_tiles<1>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale);
     }
   }
 }
@@ -606,14 +652,15 @@ __global__ void __launch_bounds__(128) l2p_small_kernel(const float *__restrict_
 // contiguous runs of each state's user array.
 __global__ void __launch_bounds__(256) unsort_results_kernel(const float4 *__restrict__ res, const int *__restrict__ inv,
                                                              int nt, int K, unsigned output, int layout,
-                                                             float *__restrict__ field, float *__restrict__ potential) {
+                                                             float *__restrict__ field, float *__restrict__ potential,
+                                                             int k_begin, int k_end) {
   __shared__ float4 tile[32][33];
   const int u0 = blockIdx.x * 32;
   const int nu = min(32, nt - u0);
   const bool want_phi = (output & 1u) != 0u;
   const bool want_h = (output & 2u) != 0u;
-  for (int kc = 0; kc < K; kc += 32) {
-    const int kn = min(32, K - kc);
+  for (int kc = k_begin; kc < k_end; kc += 32) {
+    const int kn = min(32, k_end - kc);
     for (int e = threadIdx.x; e < nu * kn; e += blockDim.x) {
       const int t = e / kn;
       const int k = e - t * kn;
@@ -738,17 +785,19 @@ __global__ void __launch_bounds__(128) l2p_grad_kernel(const float *__restrict__
 // ---------------------------------------------------------------------------
 
 void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, int K,
-                           double scale, float4 *mom, cudaStream_t s, bool paired) {
+                           double scale, float4 *mom, cudaStream_t s, bool paired, int k0, int k_total) {
   if (ns == 0) return;
+  if (k_total < 0) k_total = K;
+  const int krow = paired ? (k_total + 1) & ~1 : k_total;
   const int blocks = (ns + 31) / 32;
   const double invs = 1.0 / scale;
   const float inv3f = static_cast<float>(invs * invs * invs);
   if (dtype == 1)
     gather_moments_kernel<double><<<blocks, 256, 0, s>>>(static_cast<const double *>(user), inv, ns, K, invs, inv3f,
-                                                         paired, mom);
+                                                         paired, mom, k0, krow);
   else
     gather_moments_kernel<float><<<blocks, 256, 0, s>>>(static_cast<const float *>(user), inv, ns, K, invs, inv3f,
-                                                        paired, mom);
+                                                        paired, mom, k0, krow);
 }
 
 // State block of the P2M kernel for K states: the largest of 64, 32, ...
@@ -821,8 +870,10 @@ size_t l2p_smem_bytes(int n, int p, int Kb) {
 
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm, const int *tgt_inv,
                 float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
-                int layout, float phi_scale, float *field, float *potential, cudaStream_t s) {
+                int layout, float phi_scale, float *field, float *potential, cudaStream_t s, int k_begin,
+                int k_end) {
   if (nt == 0) return;
+  if (k_end < 0) k_end = K;
   const int leaves = 1 << (3 * depth);
   if (K < 4) {
     l2p_small_kernel<<<leaves, 128, 0, s>>>(L, tgt_rel, tgt_off, tgt_perm, near, n, p, K, nt, level_offset_d(depth),
@@ -833,8 +884,9 @@ void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const
   while (Kb > 4 && l2p_smem_bytes(n, p, Kb) > 60 * 1024) Kb = (Kb + 1) / 2;
   const size_t smem = l2p_smem_bytes(n, p, Kb);
   l2p_kernel<<<leaves, kL2pThreads, smem, s>>>(L, tgt_rel, tgt_off, near, basis, n, p, K, level_offset_d(depth), output,
-                                               phi_scale, Kb);
-  unsort_results_kernel<<<(nt + 31) / 32, 256, 0, s>>>(near, tgt_inv, nt, K, output, layout, field, potential);
+                                               phi_scale, Kb, k_begin, k_end);
+  unsort_results_kernel<<<(nt + 31) / 32, 256, 0, s>>>(near, tgt_inv, nt, K, output, layout, field, potential, k_begin,
+                                                       k_end);
 }
 
 void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,

@@ -18,8 +18,11 @@ inline int moment_row(int K) { return moments_paired(K) ? (K + 1) & ~1 : K; }
 
 // inv: user index -> sorted index; paired: write the paired layout (used for
 // the moments of K >= 4 states; gradient weights are always plain).
+// K states of user moments (user points at the first) into states
+// [k0, k0 + K) of sorted rows laid out for k_total states (default K); k0 is
+// even in the paired layout.
 void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, int K,
-                           double scale, float4 *mom, cudaStream_t s, bool paired);
+                           double scale, float4 *mom, cudaStream_t s, bool paired, int k0 = 0, int k_total = -1);
 size_t p2m_smem_bytes(int n, int p, int K, int chunk);
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
                 float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s);
@@ -29,10 +32,13 @@ void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *co
                 int child_level, int n_pairs, cudaStream_t s);
 size_t l2p_smem_bytes(int n, int p, int Kb);
 // L2P + combine; K >= 4 writes the sorted results over `near` and then unsorts
-// them to user order (2 launches), K < 4 writes user order directly.
+// them to user order (2 launches), K < 4 writes user order directly.  A state
+// range [k_begin, k_end) (K >= 4 only; default all K) processes those states
+// of the K-state rows.
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm, const int *tgt_inv,
                 float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
-                int layout, float phi_scale, float *field, float *potential, cudaStream_t s);
+                int layout, float phi_scale, float *field, float *potential, cudaStream_t s, int k_begin = 0,
+                int k_end = -1);
 void configure_far_kernels(size_t max_smem);
 
 // M2L, FP32 SIMT, all levels 2..depth in one launch (overwrites L there).
@@ -42,10 +48,11 @@ void launch_m2l_simt(const float *M, float *L, const float *T, const float *scal
 void configure_m2l_simt(size_t max_smem);
 int m2l_simt_beta_per_thread(int n);
 
-// list1 P2P near field.
+// list1 P2P near field; states [k_begin, k_end) of the K-state rows (default
+// all; k_begin a multiple of 8 when K >= 8).
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
-                bool want_phi, float4 *near, cudaStream_t s);
+                bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1);
 void configure_p2p(size_t max_smem);
 // Position gradient of sum_k W_k . H_k, near part: partial sums per state
 // group, gpart[nt][p2p_grad_groups(K)] (normalised units, 1/(4 pi) applied).

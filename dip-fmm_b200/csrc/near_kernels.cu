@@ -34,31 +34,42 @@ struct Neighbours {
 
 // Builds the clipped 3x3x3 leaf neighbourhood of `leaf` (list1, upstream
 // src/uniform_tree.cpp:455-480) with each neighbour's source range and the
-// offset (neighbour centre - this centre) in normalised units.
-__device__ void build_neighbours(Neighbours &nb, int leaf, int depth, const int *src_off) {
+// offset (neighbour centre - this centre) in normalised units.  Run by one
+// full warp: lane l < 27 looks up neighbour (dx, dy, dz) = (l % 3, l / 3 % 3,
+// l / 9) - 1 (z outermost, x fastest), and the non-empty ones are compacted
+// in that order with a ballot and a shuffle scan of their source counts.
+__device__ void build_neighbours(Neighbours &nb, int leaf, int depth, const int *src_off, int lane) {
   int ix, iy, iz;
   demorton3(static_cast<uint32_t>(leaf), ix, iy, iz);
   const int side = 1 << depth;
   const float w = 1.0F / static_cast<float>(side);
-  int c = 0;
-  nb.prefix[0] = 0;
-  for (int dz = -1; dz <= 1; ++dz)
-    for (int dy = -1; dy <= 1; ++dy)
-      for (int dx = -1; dx <= 1; ++dx) {
-        const int x = ix + dx, y = iy + dy, z = iz + dz;
-        if (x < 0 || y < 0 || z < 0 || x >= side || y >= side || z >= side) continue;
-        const uint32_t m = morton3(x, y, z);
-        const int b = src_off[m];
-        const int e = src_off[m + 1];
-        if (e <= b) continue;
-        nb.begin[c] = b;
-        nb.sx[c] = static_cast<float>(dx) * w;
-        nb.sy[c] = static_cast<float>(dy) * w;
-        nb.sz[c] = static_cast<float>(dz) * w;
-        nb.prefix[c + 1] = nb.prefix[c] + (e - b);
-        ++c;
-      }
-  nb.count = c;
+  const int dx = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+  const int x = ix + dx, y = iy + dy, z = iz + dz;
+  int b = 0, e = 0;
+  if (lane < 27 && x >= 0 && y >= 0 && z >= 0 && x < side && y < side && z < side) {
+    const uint32_t m = morton3(x, y, z);
+    b = src_off[m];
+    e = src_off[m + 1];
+  }
+  const bool use = e > b;
+  const unsigned mask = __ballot_sync(0xffffffffu, use);
+  const int slot = __popc(mask & ((1u << lane) - 1u));
+  int incl = use ? e - b : 0;
+  for (int o = 1; o < 32; o <<= 1) {
+    const int v = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += v;
+  }
+  if (use) {
+    nb.begin[slot] = b;
+    nb.sx[slot] = static_cast<float>(dx) * w;
+    nb.sy[slot] = static_cast<float>(dy) * w;
+    nb.sz[slot] = static_cast<float>(dz) * w;
+    nb.prefix[slot + 1] = incl;
+  }
+  if (lane == 0) {
+    nb.prefix[0] = 0;
+    nb.count = __popc(mask);
+  }
 }
 
 // Stages sources [g0, g0 + cnt) of the flattened neighbourhood: position
@@ -113,7 +124,7 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
   const int t0 = tgt_off[leaf];
   const int t1 = tgt_off[leaf + 1];
   if (t0 == t1) return;
-  if (threadIdx.x == 0) build_neighbours(nb, leaf, depth, src_off);
+  if (threadIdx.x < 32) build_neighbours(nb, leaf, depth, src_off, threadIdx.x);
   __syncthreads();
   const int total = nb.prefix[nb.count];
   const int warp = threadIdx.x >> 5;
@@ -361,7 +372,8 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
                                                               const int *__restrict__ tgt_off,
                                                               const int *__restrict__ self_idx, int depth, int K,
                                                               float4 *__restrict__ near,
-                                                              const float4 *__restrict__ W) {
+                                                              const float4 *__restrict__ W, int k_begin,
+                                                              int k_end) {
   constexpr bool PHI = MODE == 1;
   constexpr bool GRAD = MODE == 2;
   extern __shared__ float4 dynb[];
@@ -373,13 +385,13 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
   const int t0 = tgt_off[leaf];
   const int nt = tgt_off[leaf + 1] - t0;
   if (nt == 0) return;
-  if (threadIdx.x == 0) build_neighbours(nb, leaf, depth, src_off);
+  if (threadIdx.x < 32) build_neighbours(nb, leaf, depth, src_off, threadIdx.x);
   __syncthreads();
   const int total = nb.prefix[nb.count];
   const int tid = threadIdx.x;
   bool staged = false; // positions of the single pass already in shared memory
-  for (int kblk = 0; kblk < K; kblk += kStateBlock) {
-    const int Kc = min(kStateBlock, K - kblk);
+  for (int kblk = k_begin; kblk < k_end; kblk += kStateBlock) {
+    const int Kc = min(kStateBlock, k_end - kblk);
     const int G = (Kc + KG - 1) / KG;
     const int items = nt * G;
     for (int ib = 0; ib < items; ib += kKbThreads) {
@@ -398,6 +410,10 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
       const int k_hi = min(Kc, ((ib + r - 1) / nt + 1) * KG);
       const int Kw = PAIRED ? (k_hi - k_lo + 1) & ~1 : k_hi - k_lo; // staged float4 units per source
       const int Kr = mrow_stride<KG>(Kw);
+      // sources per chunk: kChunkB at the widest window, more for narrower
+      // windows (a chunk buffer holds kChunkB rows of the widest stride), so
+      // each chunk carries about the same work between barriers
+      const int chunkB = kChunkB * (mrow_stride<KG>((min(K, kStateBlock) + 1) & ~1) / Kr);
       const int mrow = PAIRED ? (K + 1) & ~1 : K;                   // global row length (float4)
       const int i = t0 + t;
       const float4 ti = tgt_rel[i];
@@ -433,15 +449,15 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
           __syncthreads();
           staged = true;
         }
-        const int chunks = (pn + kChunkB - 1) / kChunkB;
+        const int chunks = (pn + chunkB - 1) / chunkB;
         // Copy element e = q * Kw + k of a chunk; each thread walks e = tid,
         // tid + 256, ... incrementally (no division in the loop).
         const int cq0 = tid / Kw, ck0 = tid - cq0 * Kw;
         const int cqs = kKbThreads / Kw, cks = kKbThreads - cqs * Kw;
         auto issue = [&](int c) {
-          const int q0 = c * kChunkB;
-          const int sn = min(kChunkB, pn - q0);
-          float4 *dst = sMom + (c % kBufs) * kChunkB * Kr;
+          const int q0 = c * chunkB;
+          const int sn = min(chunkB, pn - q0);
+          float4 *dst = sMom + (c % kBufs) * chunkB * Kr;
           int q = cq0, k = ck0;
           while (q < sn) {
             cp_async16(dst + q * Kr + mrow_pos<KG>(k), mom + static_cast<long long>(sIdx[q0 + q]) * mrow + kblk + k_lo + k);
@@ -467,10 +483,10 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
             issue(c + kBufs - 1); // into the buffer chunk c - 1 used
           else
             cp_async_commit();
-          const int q0 = c * kChunkB;
-          const int sn = min(kChunkB, pn - q0);
+          const int q0 = c * chunkB;
+          const int sn = min(chunkB, pn - q0);
           if (valid) {
-            const float4 *m_row0 = sMom + (c % kBufs) * kChunkB * Kr + mrow_pos<KG>(kb - k_lo);
+            const float4 *m_row0 = sMom + (c % kBufs) * chunkB * Kr + mrow_pos<KG>(kb - k_lo);
             if constexpr (GRAD) {
               if (kvalid == KG)
                 p2p_grad_chunk<KG, true, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
@@ -655,18 +671,18 @@ template <int KG> size_t p2p_kb_smem_bytes(int K) {
 template <int KG, bool PAIRED>
 void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-               cudaStream_t s) {
+               cudaStream_t s, int k_begin, int k_end) {
   const int leaves = 1 << (3 * depth);
   const size_t smem = p2p_kb_smem_bytes<KG>(K);
   if (mode == 1)
     p2p_kb_kernel<KG, 1, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
-                                                                  depth, K, near, W);
+                                                                  depth, K, near, W, k_begin, k_end);
   else if (mode == 2)
     p2p_kb_kernel<KG, 2, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
-                                                                  depth, K, near, W);
+                                                                  depth, K, near, W, k_begin, k_end);
   else
     p2p_kb_kernel<KG, 0, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
-                                                                  depth, K, near, W);
+                                                                  depth, K, near, W, k_begin, k_end);
 }
 
 // K >= 8: groups of 8 states, paired layout; 4 <= K < 8: groups of 4,
@@ -674,20 +690,21 @@ void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, con
 // slower at K = 64: the accumulators no longer fit the register budget.)
 void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                    const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-                   cudaStream_t s) {
+                   cudaStream_t s, int k_begin = 0, int k_end = -1) {
+  if (k_end < 0) k_end = K;
   if (K >= 8)
-    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s);
+    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end);
   else if (K >= 4)
-    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s);
+    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end);
   else
-    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s);
+    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end);
 }
 
 } // namespace
 
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
-                bool want_phi, float4 *near, cudaStream_t s) {
+                bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end) {
   const int leaves = 1 << (3 * depth);
   if (K == 1) {
     if (want_phi)
@@ -695,7 +712,8 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
     else
       p2p_k1_kernel<false><<<leaves, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, near);
   } else {
-    launch_kb_any(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s);
+    launch_kb_any(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
+                  k_begin, k_end);
   }
 }
 

@@ -306,6 +306,48 @@ def test_host_io_chunk_pipeline_matches_device_path():
     plan.close()
 
 
+@pytest.mark.parametrize("K,dtype,output", [(33, np.float32, "both"), (64, np.float32, "both"),
+                                             (48, np.float64, "field"), (40, np.float32, "potential")])
+def test_host_io_state_parts_match_device_path(K, dtype, output):
+    # Host-memory calls with 32 <= K < 128 states run as one evaluation whose
+    # copies overlap it in parts of up to a quarter of the states (a multiple
+    # of 8); results must equal the device-resident call's.
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(53 + K)
+    n = 5000
+    x = rng.uniform(0, 1, (n, 3))
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, 4, max_states=K)
+    plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+    m = rng.normal(size=(K, n, 3)).astype(dtype)
+    before = plan.stats()
+    host = plan.evaluate(m, output=output)
+    st = plan.stats()
+    part = ((K + 3) // 4 + 7) // 8 * 8
+    n_parts = -(-K // part)
+    assert st["evaluation_h2d_calls"] - before["evaluation_h2d_calls"] == n_parts
+    assert st["evaluation_h2d_bytes"] - before["evaluation_h2d_bytes"] == K * n * 3 * np.dtype(dtype).itemsize
+    per_target = {"both": 4, "field": 3, "potential": 1}[output]
+    assert st["evaluation_d2h_bytes"] - before["evaluation_d2h_bytes"] == K * n * per_target * 4
+    dH = torch.zeros((K, n, 3), device="cuda")
+    dphi = torch.zeros((K, n), device="cuda")
+    plan.evaluate(torch.from_numpy(m).cuda(), output=output, field=dH, potential=dphi)
+    torch.cuda.synchronize()
+    if output != "potential":
+        assert oracle.rel_l2(host["H"], dH.cpu().numpy()) < 1e-6
+    if output != "field":
+        assert oracle.rel_l2(host["phi"], dphi.cpu().numpy()) < 1e-6
+    for k in (0, K - 1):
+        ref = oracle.fmm(x, x, m[k].astype(np.float64), 4, 3, identities=np.arange(n))
+        if output != "potential":
+            assert oracle.rel_l2(host["H"][k], ref["H"]) < FP32_REL_L2
+        else:
+            assert oracle.rel_l2(host["phi"][k], ref["phi"]) < FP32_REL_L2
+    plan.close()
+
+
 def test_python_uniform_fmm_zero_copy_device_io():
     # cdfmm.UniformFmm.evaluate_into takes CUDA arrays (torch tensors) in user
     # order and writes the results in place: no host copies.
