@@ -816,85 +816,89 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     // Host arrays and 32 <= K < 128 states: one evaluation of all K states
     // (the far field keeps its full batch) whose host copies overlap it part
     // by part.  The states are cut into up to four parts of a multiple of 8
-    // states: part j's moments are copied in (io_in stream) and gathered, and
-    // its list-1 P2P starts, while later parts are still being copied; the
-    // far field runs once all parts are gathered; each part's L2P + unsort
-    // follows its P2P and the far field, and its results are copied out
-    // (io_out stream) while later parts' P2P runs.
+    // states; the copies run on their own streams and the kernels in one
+    // explicit order on the caller's stream (stream priorities alone let the
+    // later near-field parts delay the far field):
+    //   gather 0, P2P 0, gather 1, P2P 1, ..., far field,
+    //   L2P 0, L2P 1, P2P 2, L2P 2, P2P 3, L2P 3
+    // (the first half of the P2P parts before the far field, while the later
+    // moments are still being copied in; part j's results are copied out as
+    // soon as its L2P + unsort is done, while later parts are computed).
     const bool parts = (host_in || host_out) && !timing && K >= 32 && n_chunks == 1 && plan->ns > 0 && plan->nt > 0;
     int launches = 0;
     if (parts) {
       const int part = round_up((K + 3) / 4, 8);
       const int n_parts = (K + part - 1) / part;
-      while (static_cast<int>(plan->io_events.size()) < 4 * n_parts + 3) {
+      const int early = (n_parts + 1) / 2; // P2P parts before the far field
+      while (static_cast<int>(plan->io_events.size()) < 2 * n_parts + 2) {
         cudaEvent_t e;
         check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
         plan->io_events.push_back(e);
       }
       const bool want_phi_p = (a->output & CDFMM_B200_OUTPUT_POTENTIAL) != 0u;
-      cudaEvent_t ev_start = plan->io_events[0], ev_gathered = plan->io_events[1], ev_end = plan->io_events[2];
+      cudaEvent_t ev_start = plan->io_events[0], ev_end = plan->io_events[1];
       check(cudaEventRecord(ev_start, s), "event");
-      for (cudaStream_t t : {plan->io_in, plan->io_out, plan->near_stream, plan->far_stream})
-        check(cudaStreamWaitEvent(t, ev_start, 0), "wait");
+      check(cudaStreamWaitEvent(plan->io_in, ev_start, 0), "wait");
+      check(cudaStreamWaitEvent(plan->io_out, ev_start, 0), "wait");
+      auto near_part = [&](int j) {
+        const int k0 = j * part, kc = std::min(part, K - k0);
+        launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
+                   plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc);
+        ++launches;
+      };
+      auto finish_part = [&](int j) {
+        const int k0 = j * part, kc = std::min(part, K - k0);
+        launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis,
+                   plan->n, plan->p, K, plan->nt, plan->depth, a->output, a->layout, plan->phi_scale,
+                   reinterpret_cast<float *>(field), reinterpret_cast<float *>(potential), s, k0, k0 + kc);
+        launches += 2;
+        if (host_out) check(cudaEventRecord(plan->io_events[3 + 2 * j], s), "event");
+      };
+      // Copies out are enqueued after every kernel: a copy into pageable host
+      // memory returns only when it is done and must not hold back the
+      // enqueueing of later parts' kernels.
+      auto copy_out = [&](int j) {
+        const int k0 = j * part, kc = std::min(part, K - k0);
+        check(cudaStreamWaitEvent(plan->io_out, plan->io_events[3 + 2 * j], 0), "wait");
+        if (field_out && field_state > 0) {
+          check(cudaMemcpyAsync(reinterpret_cast<char *>(a->field) + field_state * k0, field + field_state * k0,
+                                field_state * kc, cudaMemcpyDeviceToHost, plan->io_out), "D2H field");
+          plan->stats.evaluation_d2h_bytes += field_state * kc;
+          plan->stats.evaluation_d2h_calls += 1;
+        }
+        if (phi_state > 0) {
+          check(cudaMemcpyAsync(reinterpret_cast<char *>(a->potential) + phi_state * k0, potential + phi_state * k0,
+                                phi_state * kc, cudaMemcpyDeviceToHost, plan->io_out), "D2H potential");
+          plan->stats.evaluation_d2h_bytes += phi_state * kc;
+          plan->stats.evaluation_d2h_calls += 1;
+        }
+      };
       for (int j = 0; j < n_parts; ++j) {
         const int k0 = j * part, kc = std::min(part, K - k0);
-        cudaEvent_t ev_in = plan->io_events[3 + 4 * j], ev_g = plan->io_events[4 + 4 * j];
-        cudaEvent_t ev_p = plan->io_events[5 + 4 * j];
         if (host_in) {
+          // (a copy from pageable memory blocks here while earlier parts compute)
           check(cudaMemcpyAsync(const_cast<char *>(moments) + in_state * k0, static_cast<const char *>(a->moments) + in_state * k0,
                                 in_state * kc, cudaMemcpyHostToDevice, plan->io_in), "H2D moments");
           plan->stats.evaluation_h2d_bytes += in_state * kc;
           plan->stats.evaluation_h2d_calls += 1;
-          check(cudaEventRecord(ev_in, plan->io_in), "event");
-          check(cudaStreamWaitEvent(s, ev_in, 0), "wait");
+          check(cudaEventRecord(plan->io_events[2 + 2 * j], plan->io_in), "event");
+          check(cudaStreamWaitEvent(s, plan->io_events[2 + 2 * j], 0), "wait");
         }
         launch_gather_moments(moments + in_state * k0, a->moments_dtype, plan->src_inv, plan->ns, kc, plan->scale,
                               plan->mom, s, moments_paired(K), k0, K);
-        check(cudaEventRecord(ev_g, s), "event");
-        check(cudaStreamWaitEvent(plan->near_stream, ev_g, 0), "wait");
-        launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
-                   plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi_p, plan->near,
-                   plan->near_stream, k0, k0 + kc);
-        check(cudaEventRecord(ev_p, plan->near_stream), "event");
-        launches += 2;
+        ++launches;
+        if (j < early) near_part(j);
       }
-      check(cudaEventRecord(ev_gathered, s), "event");
-      check(cudaStreamWaitEvent(plan->far_stream, ev_gathered, 0), "wait");
-      launches += enqueue_far(plan, K, plan->far_stream, false);
-      check(cudaEventRecord(plan->ev_far, plan->far_stream), "event");
-      check(cudaStreamWaitEvent(s, plan->ev_far, 0), "wait");
-      // every part's L2P before any copy-out: a copy into pageable host
-      // memory returns only when done, and must not hold back later parts
-      for (int j = 0; j < n_parts; ++j) {
-        const int k0 = j * part, kc = std::min(part, K - k0);
-        check(cudaStreamWaitEvent(s, plan->io_events[5 + 4 * j], 0), "wait");
-        launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis,
-                   plan->n, plan->p, K, plan->nt, plan->depth, a->output, a->layout, plan->phi_scale,
-                   reinterpret_cast<float *>(field), reinterpret_cast<float *>(potential), s, k0, k0 + kc);
-        check(cudaEventRecord(plan->io_events[6 + 4 * j], s), "event");
-        launches += 2;
+      launches += enqueue_far(plan, K, s, false);
+      for (int j = 0; j < early; ++j) finish_part(j);
+      for (int j = early; j < n_parts; ++j) {
+        near_part(j);
+        finish_part(j);
       }
       check(cudaGetLastError(), "kernel launch");
       if (host_out) {
-        for (int j = 0; j < n_parts; ++j) {
-          const int k0 = j * part, kc = std::min(part, K - k0);
-          check(cudaStreamWaitEvent(plan->io_out, plan->io_events[6 + 4 * j], 0), "wait");
-          if (field_out && field_state > 0) {
-            check(cudaMemcpyAsync(reinterpret_cast<char *>(a->field) + field_state * k0, field + field_state * k0,
-                                  field_state * kc, cudaMemcpyDeviceToHost, plan->io_out), "D2H field");
-            plan->stats.evaluation_d2h_bytes += field_state * kc;
-            plan->stats.evaluation_d2h_calls += 1;
-          }
-          if (phi_state > 0) {
-            check(cudaMemcpyAsync(reinterpret_cast<char *>(a->potential) + phi_state * k0, potential + phi_state * k0,
-                                  phi_state * kc, cudaMemcpyDeviceToHost, plan->io_out), "D2H potential");
-            plan->stats.evaluation_d2h_bytes += phi_state * kc;
-            plan->stats.evaluation_d2h_calls += 1;
-          }
-        }
-      }
-      for (cudaStream_t t : {plan->io_in, plan->io_out, plan->near_stream}) {
-        check(cudaEventRecord(ev_end, t), "event");
+        for (int j = 0; j < n_parts; ++j) copy_out(j);
+        check(cudaEventRecord(ev_end, plan->io_out), "event");
         check(cudaStreamWaitEvent(s, ev_end, 0), "wait");
       }
       plan->exp_state0 = 0;
