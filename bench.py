@@ -487,6 +487,7 @@ def b200_arm(args):
                    "n_dipoles": N, "order": p, "depth": d, "states_per_step": K, "output": "field+potential",
                    "m2l": ["auto", "fp32", "bf16x3"][st["m2l_mode_resolved"]],
                    "m2l_shape": {"accumulators_per_cta": st["m2l_tc_m_tiles"], "stages": st["m2l_tc_stages"],
+                                 "fused_hi_lo_mma": bool(st["m2l_tc_fused"]),
                                  "chosen_by": "autotuner"},
                    "l2": f"inputs larger than L2 ({dm.numel() * 4 / 2**20:.0f} MiB of moments per step)",
                    "parallelism": "replicas (independent states per GPU)" if world > 1 else "single GPU"},
@@ -642,7 +643,8 @@ def lattice_leg(args, stream, local):
     return {"workload": "64^3 jittered lattice, N=262144, p=8, depth 5, K=64, field only", "ms_per_step": ms,
             "value": N * K / (ms * 1e-3), "unit": UNIT, "rel_l2_H": rel,
             "m2l": ["auto", "fp32", "bf16x3"][st["m2l_mode_resolved"]],
-            "m2l_shape": {"accumulators_per_cta": st["m2l_tc_m_tiles"], "stages": st["m2l_tc_stages"]}}
+            "m2l_shape": {"accumulators_per_cta": st["m2l_tc_m_tiles"], "stages": st["m2l_tc_stages"],
+                          "fused_hi_lo_mma": bool(st["m2l_tc_fused"])}}
 
 
 def differentiable_leg(args, stream, local):

@@ -122,7 +122,11 @@ struct cdfmm_b200_plan {
   bool tc_supported = false;
   int tc_Kpad = 0, tc_Npad = 0, tc_stages = 0, tc_Kp_max = 0;
   int tc_m_tiles = 1, tc_acc_stride = 0; // accumulators per CTA, TMEM columns apart
-  std::vector<std::pair<int, int>> tc_candidates; // (m_tiles, stages) shapes the autotuner tries
+  int tc_fuse = 0;                        // 1: A_hi x [B_hi | B_lo] as one N = 2 Npad MMA
+  struct TcShape {
+    int m_tiles, stages, fuse;
+  };
+  std::vector<TcShape> tc_candidates;     // pipeline shapes the autotuner tries
   uint32_t tc_tmem_cols = 0;
   void *tc_a_hi = nullptr, *tc_a_lo = nullptr; // [boxes + 1][Kp_max * Kpad] BF16
   void *tc_b = nullptr;                        // [343][Kpad/32][2][Npad * 32] BF16

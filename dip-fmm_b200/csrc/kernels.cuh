@@ -25,14 +25,27 @@ __host__ __device__ inline int rank3(int a, int b, int c) {
 
 __host__ __device__ inline int level_offset_d(int level) { return ((1 << (3 * level)) - 1) / 7; }
 
+// Bit dilation of a 10-bit coordinate: bit b moves to bit 3b (the
+// shift-and-mask "part 1 by 2" construction), and its inverse.
+__host__ __device__ inline uint32_t dilate3(uint32_t v) {
+  v &= 0x3ffu;
+  v = (v | (v << 16)) & 0x030000ffu;
+  v = (v | (v << 8)) & 0x0300f00fu;
+  v = (v | (v << 4)) & 0x030c30c3u;
+  v = (v | (v << 2)) & 0x09249249u;
+  return v;
+}
+__host__ __device__ inline uint32_t undilate3(uint32_t v) {
+  v &= 0x09249249u;
+  v = (v | (v >> 2)) & 0x030c30c3u;
+  v = (v | (v >> 4)) & 0x0300f00fu;
+  v = (v | (v >> 8)) & 0x030000ffu;
+  v = (v | (v >> 16)) & 0x000003ffu;
+  return v;
+}
+
 __host__ __device__ inline uint32_t morton3(uint32_t x, uint32_t y, uint32_t z) {
-  uint32_t m = 0;
-  for (int b = 0; b < 10; ++b) {
-    m |= ((x >> b) & 1u) << (3 * b);
-    m |= ((y >> b) & 1u) << (3 * b + 1);
-    m |= ((z >> b) & 1u) << (3 * b + 2);
-  }
-  return m;
+  return dilate3(x) | (dilate3(y) << 1) | (dilate3(z) << 2);
 }
 
 // Lets `kernel` use all opt-in shared memory left after its static shared
@@ -53,12 +66,9 @@ template <typename Kernel> inline bool allow_dynamic_smem(Kernel *kernel, size_t
 }
 
 __host__ __device__ inline void demorton3(uint32_t m, int &x, int &y, int &z) {
-  x = y = z = 0;
-  for (int b = 0; b < 10; ++b) {
-    x |= static_cast<int>((m >> (3 * b)) & 1u) << b;
-    y |= static_cast<int>((m >> (3 * b + 1)) & 1u) << b;
-    z |= static_cast<int>((m >> (3 * b + 2)) & 1u) << b;
-  }
+  x = static_cast<int>(undilate3(m));
+  y = static_cast<int>(undilate3(m >> 1));
+  z = static_cast<int>(undilate3(m >> 2));
 }
 
 } // namespace cdfmm_b200

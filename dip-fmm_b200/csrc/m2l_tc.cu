@@ -223,12 +223,20 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   const uint32_t tmem = *tmem_slot;
   const int units = *n_act * nkc;
 
-  if (tid >= 32 && tid < 64) {
-    // Producer warp: bulk copies of (offset, chunk) operands into stage u % S.
+  if (tid >= 32) {
+    // Producer warps 1..npw: warp 1 + w issues the bulk copies of units
+    // u = w, w + npw, ... (an (offset, chunk) pair each) into stage u % S.
+    // Several warps overlap the address arithmetic and copy issue of
+    // consecutive units.  npw <= S: a producer waiting for the previous use
+    // (u - S) of its stage knows that its own previous unit's stage wait
+    // (u - npw - S) completed, so every unit up to u - 2S has completed and
+    // the stage's empty barrier is at most one phase behind (a parity wait
+    // cannot alias an older phase).
+    const int npw = min(kTcThreads / 32 - 1, S);
+    const int pw = (tid >> 5) - 1;
     const size_t btile = static_cast<size_t>(args.Npad) * kKChunk * 2u; // stride of one B chunk tile
     int produced = 0;
-    int slot = 0, ox = 0, oy = 0, oz = 0;
-    for (int u = 0; u < units; ++u) {
+    for (int u = pw; pw < npw && u < units; u += npw) {
       const int s = u % S;
       int ok = 1;
       if (lane == 0) {
@@ -241,13 +249,9 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
       const int kc = u % nkc;
-      if (kc == 0) {
-        const int i = act[u / nkc];
-        ox = cx - 3 + i % 6;
-        oy = cy - 3 + (i / 6) % 6;
-        oz = cz - 3 + i / 36;
-        slot = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
-      }
+      const int i = act[u / nkc];
+      const int ox = cx - 3 + i % 6, oy = cy - 3 + (i / 6) % 6, oz = cz - 3 + i / 36;
+      const int slot = (ox + 3) * 49 + (oy + 3) * 7 + (oz + 3);
       const int kcw = min(kKChunk, args.Kpad - kc * kKChunk);
       const uint32_t box_chunk = static_cast<uint32_t>(args.Kp * kcw * 2); // one box's rows of this chunk
       uint8_t *st = stage0 + s * stage_bytes;
@@ -273,15 +277,19 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
         } else {
           const int h = c - n_a;
           const uint8_t *bsrc = args.b_tiles + (static_cast<size_t>(slot) * nkc + kc) * 2u * btile + h * btile;
-          bulk_g2s(st + 2 * a_bytes + h * b_bytes, bsrc, static_cast<uint32_t>(args.Npad) * kcw * 2u, &full[s]);
+          // B_lo right after B_hi (both kcw wide): the 2 Npad rows form one
+          // operand of uniform row-group stride for the fused-N MMA
+          const uint32_t bw = static_cast<uint32_t>(args.Npad) * kcw * 2u;
+          bulk_g2s(st + 2 * a_bytes + h * bw, bsrc, bw, &full[s]);
         }
       }
       __syncwarp();
       produced = u + 1;
     }
-    if (lane == 0 && *reinterpret_cast<volatile int *>(abort_flag)) {
+    if (lane == 0 && pw < npw && *reinterpret_cast<volatile int *>(abort_flag)) {
       // Abort: wait (bounded) for this warp's copies still in flight.
-      for (int u = max(0, produced - S); u < produced; ++u) mbar_wait(&full[u % S], (u / S) & 1);
+      for (int u = max(0, produced - S); u < produced; ++u)
+        if (u % npw == pw) mbar_wait(&full[u % S], (u / S) & 1);
     }
   } else if (tid == 0) {
     // MMA issuer: waits for each unit's operands, issues its MMAs, commits
@@ -289,9 +297,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     // shared-memory descriptors are built once: a byte offset o < 256 KB is
     // added to a descriptor as o >> 4 in its 14-bit start-address field.
     const uint32_t idesc = instr_desc_bf16(args.Npad);
+    const uint32_t idesc2 = instr_desc_bf16(2 * args.Npad); // fused: N = [B_hi | B_lo]
+    const bool fuse = args.fuse_n != 0;
     const uint64_t desc_full = smem_desc(smem_u32(stage0), 128u, kKChunk * 16u); // SBO = chunk width * 16 B
     const uint64_t desc_half = smem_desc(smem_u32(stage0), 128u, 16u * 16u);     // last chunk 16 wide
-    const uint64_t o_alo = a_bytes >> 4, o_bhi = (2u * a_bytes) >> 4, o_blo = (2u * a_bytes + b_bytes) >> 4;
+    const uint64_t o_alo = a_bytes >> 4, o_bhi = (2u * a_bytes) >> 4;
     uint32_t accumulate = 0;
     int issued = 0;
     int s = 0, kc = 0;
@@ -305,6 +315,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
       tc_fence_after();
       const int kcw = min(kKChunk, args.Kpad - kc * kKChunk);
       const uint64_t base = (kcw == kKChunk ? desc_full : desc_half) + ((static_cast<uint32_t>(s) * stage_bytes) >> 4);
+      const uint64_t o_blo = (2u * a_bytes + static_cast<uint32_t>(args.Npad) * kcw * 2u) >> 4;
 #pragma unroll
       for (int ks = 0; ks < kKChunk / 16; ++ks) {
         if (ks * 16 < kcw) {
@@ -314,9 +325,15 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
             if (m < m_active) {
               const uint32_t d = tmem + static_cast<uint32_t>(m * args.acc_stride);
               const uint64_t ah = o + ((static_cast<uint32_t>(m) * a_tile) >> 4);
-              mma_bf16(d, ah, o + o_bhi, idesc, accumulate);
-              mma_bf16(d, ah, o + o_blo, idesc, 1);
-              mma_bf16(d, ah + o_alo, o + o_bhi, idesc, 1);
+              if (fuse) {
+                // columns [0, Npad): hi*hi + lo*hi; [Npad, 2 Npad): hi*lo
+                mma_bf16(d, ah, o + o_bhi, idesc2, accumulate);
+                mma_bf16(d, ah + o_alo, o + o_bhi, idesc, 1);
+              } else {
+                mma_bf16(d, ah, o + o_bhi, idesc, accumulate);
+                mma_bf16(d, ah, o + o_blo, idesc, 1);
+                mma_bf16(d, ah + o_alo, o + o_bhi, idesc, 1);
+              }
             }
           }
           accumulate = 1;
@@ -355,7 +372,14 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
       const long long base = static_cast<long long>(node) * args.n * args.K + k;
       for (int c0 = 0; c0 < args.Npad; c0 += 16) {
         float v[16];
-        tmem_ld16(tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(m * args.acc_stride + c0), v);
+        const uint32_t tcol = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(m * args.acc_stride + c0);
+        tmem_ld16(tcol, v);
+        if (args.fuse_n) {
+          float w[16];
+          tmem_ld16(tcol + static_cast<uint32_t>(args.Npad), w);
+#pragma unroll
+          for (int j = 0; j < 16; ++j) v[j] += w[j];
+        }
         if (units == 0) {
 #pragma unroll
           for (int j = 0; j < 16; ++j) v[j] = 0.0F; // no source box in the grid: no MMA wrote the accumulator

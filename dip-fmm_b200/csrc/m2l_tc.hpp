@@ -24,6 +24,7 @@ struct TcArgs {
   int stages;
   int m_tiles;             // 128-row accumulators per CTA sharing each B tile
   int acc_stride;          // TMEM columns between accumulators (multiple of 32)
+  int fuse_n;              // 1: A_hi x [B_hi | B_lo] as one N = 2 Npad MMA (acc_stride >= 2 Npad)
   uint32_t tmem_cols;
   uint32_t box_bytes;      // Kp * Kpad * 2
 };

@@ -201,6 +201,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
     ta.stages = plan->tc_stages;
     ta.m_tiles = plan->tc_m_tiles;
     ta.acc_stride = plan->tc_acc_stride;
+    ta.fuse_n = plan->tc_fuse;
     ta.tmem_cols = plan->tc_tmem_cols;
     ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
     launch_m2l_tc(ta, n_tiles, s);

@@ -469,10 +469,15 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
       const int Kpad = round_up(n, 16);
       const int Npad = round_up(n, 16);
       // Pipeline shapes: 1, 2 or 4 128-row accumulators per CTA sharing each
-      // B tile, with as many stages as fit one CTA per SM, or half of that
-      // for two CTAs per SM.  Default: two accumulators, one CTA per SM; the
-      // AUTO mode times the candidates on first use for each K.
-      const int acc_stride = round_up(Npad, 32);
+      // B tile, with as many stages as fit one CTA per SM, or half / a third
+      // of that for two / three CTAs per SM; each with the three products as
+      // three MMAs of N = Npad, or (when 2 Npad <= 256) A_hi x [B_hi | B_lo]
+      // fused into one MMA of N = 2 Npad plus A_lo x B_hi (two larger MMAs
+      // instead of three: fewer instructions for the one issuing thread;
+      // twice the TMEM columns).  Default: two accumulators, two CTAs per SM,
+      // three MMAs; the autotuner times the candidates on first use for
+      // each K.
+      auto acc_stride_of = [&](int fuse) { return round_up(fuse ? 2 * Npad : Npad, 32); };
       auto max_stages = [&](int mt, size_t budget) {
         int st = 0;
         while (st < 8 && m2l_tc_smem_bytes(Npad, mt, st + 1) <= budget) ++st;
@@ -480,17 +485,23 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
       };
       const size_t one_cta = std::min<size_t>(smem, 224 * 1024), two_cta = 112 * 1024, three_cta = 74 * 1024;
       plan->tc_candidates.clear();
-      for (int mt : {2, 1, 4}) {
-        if (mt * acc_stride > 512) continue;
-        const int s1 = max_stages(mt, one_cta);
-        if (s1 >= 2) plan->tc_candidates.emplace_back(mt, s1);
-        const int s2 = max_stages(mt, two_cta);
-        if (s2 >= 2 && s2 < s1 && tmem_columns(mt, acc_stride) <= 256) plan->tc_candidates.emplace_back(mt, s2);
-        const int s3 = max_stages(mt, three_cta);
-        if (s3 >= 2 && s3 < s2 && 3 * tmem_columns(mt, acc_stride) <= 512) plan->tc_candidates.emplace_back(mt, s3);
+      for (int fuse : {0, 1}) {
+        if (fuse && 2 * Npad > 256) continue; // MMA N <= 256
+        const int acc = acc_stride_of(fuse);
+        for (int mt : {2, 1, 4}) {
+          if (mt * acc > 512) continue;
+          const int s1 = max_stages(mt, one_cta);
+          const int s2 = max_stages(mt, two_cta);
+          const int s3 = max_stages(mt, three_cta);
+          if (s2 >= 2 && s2 < s1 && tmem_columns(mt, acc) <= 256) plan->tc_candidates.push_back({mt, s2, fuse});
+          if (s1 >= 2) plan->tc_candidates.push_back({mt, s1, fuse});
+          if (s3 >= 2 && s3 < s2 && 3 * tmem_columns(mt, acc) <= 512) plan->tc_candidates.push_back({mt, s3, fuse});
+        }
       }
-      const int m_tiles = plan->tc_candidates.empty() ? 1 : plan->tc_candidates.front().first;
-      const int stages = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().second;
+      const int m_tiles = plan->tc_candidates.empty() ? 1 : plan->tc_candidates.front().m_tiles;
+      const int stages = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().stages;
+      const int fuse0 = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().fuse;
+      const int acc_stride = acc_stride_of(fuse0);
       // AUTO uses the tensor cores from K = 8 states on: a plan that never
       // evaluates 8 states at once does not allocate their operand buffers.
       const bool wanted = desc->m2l_mode == CDFMM_B200_M2L_BF16X3 ||
@@ -503,6 +514,7 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
         plan->tc_stages = stages;
         plan->tc_m_tiles = m_tiles;
         plan->tc_acc_stride = acc_stride;
+        plan->tc_fuse = fuse0;
         plan->tc_tmem_cols = tmem_columns(m_tiles, acc_stride);
         plan->tc_Kp_max = round_up(std::min(plan->max_states, 128), 8);
         const size_t boxes = static_cast<size_t>(plan->n_nodes - level_offset(2)) + 1;
@@ -589,10 +601,13 @@ static void upload_tc_tiles(cdfmm_b200_plan *plan, int Kp) {
 }
 
 // Autotuner of the tensor-core M2L pipeline shape (accumulators per CTA,
-// stages): times every candidate on this call's packed operands (device
-// events, second of two launches) and keeps the fastest.  Candidates trade B
-// reuse (more accumulators per CTA) against pipeline depth and two CTAs per
-// SM; all give bit-identical results (the per-row MMA sequence is the same).
+// stages, fused hi/lo B operand): times every candidate on this call's
+// packed operands (device events, second of two launches) and keeps the
+// fastest.  Candidates trade B reuse (more accumulators per CTA) against
+// pipeline depth, CTAs per SM and MMA size.  Shapes with the same fusion
+// give bit-identical results (the per-row MMA sequence is the same); the
+// fused form sums the hi*lo product in its own accumulator, a difference at
+// FP32 rounding level.
 static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
   const int Kp = round_up(K, 8);
   const int node_base = level_offset(2);
@@ -610,19 +625,20 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
   ta.Npad = plan->tc_Npad;
   ta.node_base = node_base;
   ta.zero_node = plan->n_nodes - node_base;
-  ta.acc_stride = plan->tc_acc_stride;
   ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
   float best = 0.0F;
   int best_i = -1;
   for (size_t c = 0; c < plan->tc_candidates.size(); ++c) {
-    const int mt = plan->tc_candidates[c].first;
+    const int mt = plan->tc_candidates[c].m_tiles;
     const std::vector<int4> tiles = build_tc_tiles(plan->depth, mt * (128 / Kp));
     grow(plan->tc_tiles, plan->tc_tiles_capacity, tiles.size(), "cudaMalloc tiles");
     check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
     ta.tiles = plan->tc_tiles;
     ta.m_tiles = mt;
-    ta.stages = plan->tc_candidates[c].second;
-    ta.tmem_cols = tmem_columns(mt, plan->tc_acc_stride);
+    ta.stages = plan->tc_candidates[c].stages;
+    ta.fuse_n = plan->tc_candidates[c].fuse;
+    ta.acc_stride = round_up(ta.fuse_n ? 2 * plan->tc_Npad : plan->tc_Npad, 32);
+    ta.tmem_cols = tmem_columns(mt, ta.acc_stride);
     float ms = 0.0F;
     for (int rep = 0; rep < 2; ++rep) {
       check(cudaEventRecord(plan->ev_t[10], s), "event");
@@ -636,8 +652,11 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
       best_i = static_cast<int>(c);
     }
   }
-  plan->tc_m_tiles = plan->tc_candidates[static_cast<size_t>(best_i)].first;
-  plan->tc_stages = plan->tc_candidates[static_cast<size_t>(best_i)].second;
+  const cdfmm_b200_plan::TcShape &best_shape = plan->tc_candidates[static_cast<size_t>(best_i)];
+  plan->tc_m_tiles = best_shape.m_tiles;
+  plan->tc_stages = best_shape.stages;
+  plan->tc_fuse = best_shape.fuse;
+  plan->tc_acc_stride = round_up(best_shape.fuse ? 2 * plan->tc_Npad : plan->tc_Npad, 32);
   plan->tc_tmem_cols = tmem_columns(plan->tc_m_tiles, plan->tc_acc_stride);
   plan->tc_tiles_Kp = 0; // rebuilt for the chosen shape by the caller
 }
@@ -668,7 +687,7 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
                       plan->depth, node_base, boxes, s);
       if (plan->tc_tiles_Kp != Kp) {
         check(cudaStreamSynchronize(s), "sync");
-        if (plan->m2l_mode == CDFMM_B200_M2L_AUTO && plan->tc_candidates.size() > 1) tune_m2l_tc(plan, K, s);
+        if (plan->tc_candidates.size() > 1) tune_m2l_tc(plan, K, s);
         upload_tc_tiles(plan, Kp);
       }
       TcArgs ta{};
@@ -689,12 +708,14 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
       ta.stages = plan->tc_stages;
       ta.m_tiles = plan->tc_m_tiles;
       ta.acc_stride = plan->tc_acc_stride;
+      ta.fuse_n = plan->tc_fuse;
       ta.tmem_cols = plan->tc_tmem_cols;
       ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
       launch_m2l_tc(ta, plan->tc_n_tiles, s);
       launches += 2;
       plan->stats.m2l_tc_m_tiles = plan->tc_m_tiles;
       plan->stats.m2l_tc_stages = plan->tc_stages;
+      plan->stats.m2l_tc_fused = plan->tc_fuse;
     } else if (plan->depth >= 2) {
       launch_m2l_simt(plan->M, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles,
                       plan->n_tiles, n, plan->ops.m2l_ld, K, s);

@@ -89,7 +89,7 @@ class Stats(ctypes.Structure):
         ("p2p_pairs", ctypes.c_uint64), ("kernel_launches_last", ctypes.c_uint64),
         ("m2l_mode_resolved", ctypes.c_int32), ("timing_enabled", ctypes.c_int32),
         ("m2l_tc_m_tiles", ctypes.c_int32), ("m2l_tc_stages", ctypes.c_int32),
-        ("backward_reused_forward", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+        ("backward_reused_forward", ctypes.c_int32), ("m2l_tc_fused", ctypes.c_int32),
         ("ms_gather", ctypes.c_double), ("ms_p2m", ctypes.c_double), ("ms_m2m", ctypes.c_double),
         ("ms_m2l", ctypes.c_double), ("ms_l2l", ctypes.c_double), ("ms_l2p", ctypes.c_double),
         ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),

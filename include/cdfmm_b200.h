@@ -122,7 +122,7 @@ typedef struct cdfmm_b200_stats {
   int32_t m2l_tc_m_tiles;        /* tensor-core M2L shape last used: accumulators per CTA */
   int32_t m2l_tc_stages;         /*   and pipeline stages (chosen by the autotuner in AUTO mode) */
   int32_t backward_reused_forward; /* last backward reused the forward's moments and locals */
-  int32_t reserved0;
+  int32_t m2l_tc_fused;          /*   1: hi and lo translation tiles side by side in one wider MMA */
   double ms_gather, ms_p2m, ms_m2m, ms_m2l, ms_l2l, ms_l2p, ms_p2p, ms_total;
 } cdfmm_b200_stats;
 
