@@ -1,11 +1,10 @@
 // Allocation-free evaluation: cdfmm_b200_evaluate_noalloc.
 //
 // Who needs it: code that must not call cudaMalloc/cudaFree at evaluation
-// time -- a host program capturing its evaluation loop into a CUDA graph
-// (an allocation inside a capture is not recorded into the graph and breaks
-// it), a framework whose caching pool already owns the device memory a
-// library would ask for, or a real-time loop that cannot afford the
-// allocator's implicit synchronisation.  Such callers create the plan once
+// time -- a framework whose caching pool already owns the device memory a
+// library would ask for, a program that reserves all its device memory up
+// front, or a real-time loop that cannot afford the allocator's implicit
+// synchronisation.  Such callers create the plan once
 // (plan creation allocates) and then evaluate with device-resident arrays
 // through this entry point, which allocates nothing.
 //
@@ -70,8 +69,8 @@ cudaError_t scratch_address(int device, void **out) {
 
 size_t align256(size_t v) { return (v + 255) / 256 * 256; }
 
-// Tensor-core M2L work tiles, written on the device (no host copy, so the
-// call stays capturable): per level from `depth` down to 2, runs of T
+// Tensor-core M2L work tiles, written on the device (no host copy, no host
+// synchronisation): per level from `depth` down to 2, runs of T
 // consecutive parents, the 8 parity classes of a run adjacent (the plan's order).
 __global__ void noalloc_tiles_kernel(int4 *tiles, int depth, int T, int n_tiles) {
   const int q = blockIdx.x * blockDim.x + threadIdx.x;

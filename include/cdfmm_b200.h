@@ -156,9 +156,9 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args)
 
 /* Allocation-free variant of cdfmm_b200_evaluate (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc/cudaFree while they
- * evaluate -- a host program capturing its evaluation loop into a CUDA graph,
- * a framework whose memory pool owns the device memory, a real-time loop
- * that cannot take the allocator's implicit synchronisation.  Same
+ * evaluate -- a framework whose memory pool owns the device memory, a program
+ * that reserves all its device memory up front, a real-time loop that cannot
+ * take the allocator's implicit synchronisation.  Same
  * arguments and results as cdfmm_b200_evaluate, with these limits:
  *  - moments and results must be device-resident (args->memory == 0);
  *  - all per-call scratch (sorted moments, expansions, near field, tensor-

@@ -1,10 +1,9 @@
 """The allocation-free entry point, cdfmm_b200_evaluate_noalloc.
 
-Some callers cannot allocate device memory while they evaluate: a program
-capturing its evaluation loop into a CUDA graph (an allocation made during a
-capture is not part of the graph), a framework whose memory pool already owns
-the GPU's memory, or a real-time loop that cannot afford the allocator's
-implicit synchronisation.  They create the plan once and then evaluate
+Some callers cannot allocate device memory while they evaluate: a framework
+whose memory pool already owns the GPU's memory, a program that reserves all
+its device memory up front, or a real-time loop that cannot afford the
+allocator's implicit synchronisation.  They create the plan once and then evaluate
 through this entry point, whose scratch lives in a fixed 64 MiB device array
 compiled into the library.
 
