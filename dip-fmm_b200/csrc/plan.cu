@@ -836,10 +836,11 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     const int n_chunks = (K + chunk - 1) / chunk;
     // Host arrays and 32 <= K < 128 states: one evaluation of all K states
     // (the far field keeps its full batch) whose host copies overlap it part
-    // by part.  The states are cut into up to four parts of a multiple of 8
-    // states; the copies run on their own streams and the kernels in one
-    // explicit order on the caller's stream (stream priorities alone let the
-    // later near-field parts delay the far field):
+    // by part.  The states are cut into parts of about a quarter of them (a
+    // multiple of 8; the first part half as long, as its copy-in is exposed,
+    // and the last the remainder); the copies run on their own streams and
+    // the kernels in one explicit order on the caller's stream (stream
+    // priorities alone let the later near-field parts delay the far field):
     //   gather 0, P2P 0, gather 1, P2P 1, ..., far field,
     //   L2P 0, L2P 1, P2P 2, L2P 2, P2P 3, L2P 3
     // (the first half of the P2P parts before the far field, while the later
@@ -848,8 +849,15 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     const bool parts = (host_in || host_out) && !timing && K >= 32 && n_chunks == 1 && plan->ns > 0 && plan->nt > 0;
     int launches = 0;
     if (parts) {
+      // Parts of `part` states, the first one half as long (the first copy in
+      // and the last copy out are the exposed ones): 8, 16, 16, 16, 8 for K = 64.
       const int part = round_up((K + 3) / 4, 8);
-      const int n_parts = (K + part - 1) / part;
+      std::vector<int> bounds = {0};
+      for (int k = std::min(K, round_up(part / 2, 8)); ; k = std::min(K, k + part)) {
+        bounds.push_back(k);
+        if (k == K) break;
+      }
+      const int n_parts = static_cast<int>(bounds.size()) - 1;
       const int early = (n_parts + 1) / 2; // P2P parts before the far field
       while (static_cast<int>(plan->io_events.size()) < 2 * n_parts + 2) {
         cudaEvent_t e;
@@ -862,13 +870,13 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       check(cudaStreamWaitEvent(plan->io_in, ev_start, 0), "wait");
       check(cudaStreamWaitEvent(plan->io_out, ev_start, 0), "wait");
       auto near_part = [&](int j) {
-        const int k0 = j * part, kc = std::min(part, K - k0);
+        const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
         launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
                    plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc);
         ++launches;
       };
       auto finish_part = [&](int j) {
-        const int k0 = j * part, kc = std::min(part, K - k0);
+        const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
         launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis,
                    plan->n, plan->p, K, plan->nt, plan->depth, a->output, a->layout, plan->phi_scale,
                    reinterpret_cast<float *>(field), reinterpret_cast<float *>(potential), s, k0, k0 + kc);
@@ -879,7 +887,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       // memory returns only when it is done and must not hold back the
       // enqueueing of later parts' kernels.
       auto copy_out = [&](int j) {
-        const int k0 = j * part, kc = std::min(part, K - k0);
+        const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
         check(cudaStreamWaitEvent(plan->io_out, plan->io_events[3 + 2 * j], 0), "wait");
         if (field_out && field_state > 0) {
           check(cudaMemcpyAsync(reinterpret_cast<char *>(a->field) + field_state * k0, field + field_state * k0,
@@ -895,7 +903,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
         }
       };
       for (int j = 0; j < n_parts; ++j) {
-        const int k0 = j * part, kc = std::min(part, K - k0);
+        const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
         if (host_in) {
           // (a copy from pageable memory blocks here while earlier parts compute)
           check(cudaMemcpyAsync(const_cast<char *>(moments) + in_state * k0, static_cast<const char *>(a->moments) + in_state * k0,
