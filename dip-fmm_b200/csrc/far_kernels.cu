@@ -697,73 +697,128 @@ __global__ void __launch_bounds__(256) unsort_results_kernel(const float4 *__res
 }
 
 // Position gradient of L = sum_k w_k . H_k (reverse mode; no counterpart in
-// the reference).  H_k = -grad phi_k, so dL/dx_m = -sum_k sum_l w_kl d_l d_m phi_k
-// and, from phi = sum_b L_b dx^b/b!,
-//   d_l d_m phi = sum_{|g| <= p-2} L_{g + e_l + e_m} dx^g/g!
-// (the exact derivative of the evaluated polynomial).  Four lanes share a
-// target and split its states (k = lane quarter mod 4); their sums are
-// combined with shuffles, then the near partial sums of the P2P gradient
-// kernel are added and the total is scaled to physical units.
-__global__ void __launch_bounds__(128) l2p_grad_kernel(const float *__restrict__ L, const float4 *__restrict__ tgt_rel,
-                                                       const int *__restrict__ tgt_off, const int *__restrict__ tgt_perm,
-                                                       const float4 *__restrict__ W, const float4 *__restrict__ gpart,
-                                                       int G, int n, int p, int K, int leaf_node_base,
-                                                       float inv_scale, float *__restrict__ out, int Kb) {
-  extern __shared__ float sLg[]; // [n][Kc], one state block
+// the reference), far part.  H_k = -grad phi_k, so dL/dx_j = -sum_k sum_c
+// w_kc d_c d_j phi_k, and from phi = sum_b L_b dx^b/b! (the exact derivative
+// of the evaluated polynomial) the Hessian at the target is
+//   S_cj[k] = sum_{|mu| <= p-2} x^mu/mu! L_{mu + e_c + e_j}[k]   (6 unique c <= j),
+// so g_j -= sum_k sum_c w_kc S_cj[k].  Per leaf
+// the leaf's locals (a state block) and the monomials of 32 targets are
+// staged in shared memory; a thread owns a register tile of 2 targets x 4
+// states x 6 Hessian components (a small GEMM over the monomials), contracts
+// it with the weights and adds its 2 targets' partial gradients into shared
+// memory; then the list-1 part (gpart, one partial per state group) is added
+// and the result written in user order.
+constexpr int kL2pGradThreads = 128;
+
+__global__ void __launch_bounds__(kL2pGradThreads) l2p_grad_kernel(
+    const float *__restrict__ L, const float4 *__restrict__ tgt_rel, const int *__restrict__ tgt_off,
+    const int *__restrict__ tgt_perm, const float4 *__restrict__ W, const float4 *__restrict__ gpart, int G, int n,
+    int p, int K, int leaf_node_base, float inv_scale, float *__restrict__ out, int Kb) {
+  extern __shared__ float4 l2pg_smem[];
+  const int Kbp = (Kb + 3) & ~3;
+  const int q = max(p - 2, 0);
+  const int nm2 = p >= 2 ? basis_size_d(p - 2) : 0;
+  float *sL = reinterpret_cast<float *>(l2pg_smem);               // [n][Kcp]
+  float *mono = sL + n * Kbp;                                      // [nm2][kL2pTargets]
+  float *gsum = mono + nm2 * kL2pTargets;                          // [kL2pTargets][3]
+  short *sidx = reinterpret_cast<short *>(gsum + 3 * kL2pTargets); // [nm2][6] ranks of mu + e_c + e_j
+  const int tid = threadIdx.x;
   const int leaf = blockIdx.x;
   const int t0 = tgt_off[leaf];
   const int t1 = tgt_off[leaf + 1];
   if (t0 == t1) return;
+  for (int m = tid; m < nm2; m += kL2pGradThreads) {
+    int a = 0, b = 0, c = 0;
+    for (int aa = 0; aa <= q; ++aa)
+      for (int bb = 0; aa + bb <= q; ++bb)
+        for (int cc = 0; aa + bb + cc <= q; ++cc)
+          if (rank3(aa, bb, cc) == m) {
+            a = aa;
+            b = bb;
+            c = cc;
+          }
+    sidx[6 * m + 0] = static_cast<short>(rank3(a + 2, b, c));         // xx
+    sidx[6 * m + 1] = static_cast<short>(rank3(a + 1, b + 1, c));     // xy
+    sidx[6 * m + 2] = static_cast<short>(rank3(a + 1, b, c + 1));     // xz
+    sidx[6 * m + 3] = static_cast<short>(rank3(a, b + 2, c));         // yy
+    sidx[6 * m + 4] = static_cast<short>(rank3(a, b + 1, c + 1));     // yz
+    sidx[6 * m + 5] = static_cast<short>(rank3(a, b, c + 2));         // zz
+  }
   const float *src = L + static_cast<long long>(leaf_node_base + leaf) * n * K;
-  const int items = (t1 - t0) * 4;
-  for (int base = 0; base < items; base += blockDim.x) {
-    const int it = base + threadIdx.x;
-    const bool valid = it < items;
-    const int i = t0 + (valid ? it >> 2 : 0);
-    const int q4 = it & 3;
-    const float4 d = tgt_rel[i];
-    float g0 = 0.0F, g1 = 0.0F, g2 = 0.0F;
+  for (int tc = t0; tc < t1; tc += kL2pTargets) {
+    const int tn = min(kL2pTargets, t1 - tc);
+    __syncthreads(); // previous chunk's gsum and mono reads are done
+    if (tid < 3 * kL2pTargets) gsum[tid] = 0.0F;
+    if (nm2 > 0) {
+      const int t = tid & (kL2pTargets - 1);
+      const float4 d = t < tn ? tgt_rel[tc + t] : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+      monomials_part(d.x, d.y, d.z, q, mono + t, kL2pTargets, tid / kL2pTargets, t >= tn);
+    }
     for (int kblk = 0; kblk < K; kblk += Kb) {
       const int Kc = min(Kb, K - kblk);
-      __syncthreads();
-      for (int q = threadIdx.x; q < n * Kc; q += blockDim.x) {
-        const int b = q / Kc;
-        sLg[q] = src[static_cast<long long>(b) * K + kblk + (q - b * Kc)];
+      const int Kcp = (Kc + 3) & ~3;
+      const int Kq = Kcp >> 2;
+      __syncthreads(); // previous block's sL reads are done
+      for (int e = tid; e < n * Kcp; e += kL2pGradThreads) {
+        const int b = e / Kcp;
+        const int k = e - b * Kcp;
+        sL[e] = k < Kc ? src[static_cast<long long>(b) * K + kblk + k] : 0.0F;
       }
       __syncthreads();
-      if (!valid || p < 2) continue;
-      for (int kl = q4; kl < Kc; kl += 4) {
-        const float4 w = W[static_cast<long long>(i) * K + kblk + kl];
-        float xa = 1.0F;
-        for (int a = 0; a <= p - 2; ++a) {
-          float xb = xa;
-          for (int b = 0; a + b <= p - 2; ++b) {
-            float xc = xb;
-            for (int c = 0; a + b + c <= p - 2; ++c) {
-              const float lxx = sLg[rank3(a + 2, b, c) * Kc + kl];
-              const float lxy = sLg[rank3(a + 1, b + 1, c) * Kc + kl];
-              const float lxz = sLg[rank3(a + 1, b, c + 1) * Kc + kl];
-              const float lyy = sLg[rank3(a, b + 2, c) * Kc + kl];
-              const float lyz = sLg[rank3(a, b + 1, c + 1) * Kc + kl];
-              const float lzz = sLg[rank3(a, b, c + 2) * Kc + kl];
-              g0 = fmaf(-xc, fmaf(w.x, lxx, fmaf(w.y, lxy, w.z * lxz)), g0);
-              g1 = fmaf(-xc, fmaf(w.x, lxy, fmaf(w.y, lyy, w.z * lyz)), g1);
-              g2 = fmaf(-xc, fmaf(w.x, lxz, fmaf(w.y, lyz, w.z * lzz)), g2);
-              xc = xc * d.z * kInvInt[c + 1];
-            }
-            xb = xb * d.y * kInvInt[b + 1];
+      if (nm2 == 0) continue;
+      const int tiles = ((tn + 1) >> 1) * Kq;
+      for (int tile = tid; tile < tiles; tile += kL2pGradThreads) {
+        const int tp = tile / Kq;
+        const int kq = tile - tp * Kq;
+        float hs[2][4][6];
+#pragma unroll
+        for (int u = 0; u < 2; ++u)
+#pragma unroll
+          for (int v = 0; v < 4; ++v)
+#pragma unroll
+            for (int h = 0; h < 6; ++h) hs[u][v][h] = 0.0F;
+        const float *mq = mono + 2 * tp;
+        const float *lq = sL + 4 * kq;
+        for (int m = 0; m < nm2; ++m) {
+          const float2 mo = *reinterpret_cast<const float2 *>(mq + m * kL2pTargets);
+#pragma unroll
+          for (int h = 0; h < 6; ++h) {
+            const float4 l = *reinterpret_cast<const float4 *>(lq + sidx[6 * m + h] * Kcp);
+            hs[0][0][h] = fmaf(mo.x, l.x, hs[0][0][h]);
+            hs[0][1][h] = fmaf(mo.x, l.y, hs[0][1][h]);
+            hs[0][2][h] = fmaf(mo.x, l.z, hs[0][2][h]);
+            hs[0][3][h] = fmaf(mo.x, l.w, hs[0][3][h]);
+            hs[1][0][h] = fmaf(mo.y, l.x, hs[1][0][h]);
+            hs[1][1][h] = fmaf(mo.y, l.y, hs[1][1][h]);
+            hs[1][2][h] = fmaf(mo.y, l.z, hs[1][2][h]);
+            hs[1][3][h] = fmaf(mo.y, l.w, hs[1][3][h]);
           }
-          xa = xa * d.x * kInvInt[a + 1];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+          const int t = 2 * tp + u;
+          float g0 = 0.0F, g1 = 0.0F, g2 = 0.0F;
+#pragma unroll
+          for (int v = 0; v < 4; ++v) {
+            const int kl = 4 * kq + v;
+            const float4 w = (t < tn && kl < Kc) ? W[static_cast<long long>(tc + t) * K + kblk + kl]
+                                                 : make_float4(0.0F, 0.0F, 0.0F, 0.0F);
+            g0 = fmaf(w.x, hs[u][v][0], fmaf(w.y, hs[u][v][1], fmaf(w.z, hs[u][v][2], g0)));
+            g1 = fmaf(w.x, hs[u][v][1], fmaf(w.y, hs[u][v][3], fmaf(w.z, hs[u][v][4], g1)));
+            g2 = fmaf(w.x, hs[u][v][2], fmaf(w.y, hs[u][v][4], fmaf(w.z, hs[u][v][5], g2)));
+          }
+          if (t < tn) {
+            atomicAdd(&gsum[3 * t], -g0);
+            atomicAdd(&gsum[3 * t + 1], -g1);
+            atomicAdd(&gsum[3 * t + 2], -g2);
+          }
         }
       }
     }
-#pragma unroll
-    for (int o = 1; o < 4; o <<= 1) {
-      g0 += __shfl_xor_sync(0xffffffffu, g0, o);
-      g1 += __shfl_xor_sync(0xffffffffu, g1, o);
-      g2 += __shfl_xor_sync(0xffffffffu, g2, o);
-    }
-    if (valid && q4 == 0) {
+    __syncthreads();
+    for (int t = tid; t < tn; t += kL2pGradThreads) {
+      const int i = tc + t;
+      float g0 = gsum[3 * t], g1 = gsum[3 * t + 1], g2 = gsum[3 * t + 2];
       for (int gi = 0; gi < G; ++gi) {
         const float4 v = gpart[static_cast<long long>(i) * G + gi];
         g0 += v.x;
@@ -894,11 +949,16 @@ void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, 
                      float inv_scale, float *out, cudaStream_t s) {
   if (nt == 0) return;
   const int leaves = 1 << (3 * depth);
+  const int nm2 = p >= 2 ? basis_size_d(p - 2) : 0;
+  auto smem_of = [&](int Kb) {
+    return sizeof(float) * (static_cast<size_t>(n) * ((Kb + 3) & ~3) + static_cast<size_t>(nm2) * kL2pTargets +
+                            3 * kL2pTargets) +
+           sizeof(short) * 6 * static_cast<size_t>(nm2) + 16;
+  };
   int Kb = std::min(K, 64);
-  while (Kb > 4 && sizeof(float) * static_cast<size_t>(n) * Kb > 48 * 1024) Kb = (Kb + 1) / 2;
-  const size_t smem = sizeof(float) * static_cast<size_t>(n) * Kb;
-  l2p_grad_kernel<<<leaves, 128, smem, s>>>(L, tgt_rel, tgt_off, tgt_perm, W, gpart, G, n, p, K, level_offset_d(depth),
-                                            inv_scale, out, Kb);
+  while (Kb > 4 && smem_of(Kb) > 48 * 1024) Kb = (Kb + 1) / 2;
+  l2p_grad_kernel<<<leaves, kL2pGradThreads, smem_of(Kb), s>>>(L, tgt_rel, tgt_off, tgt_perm, W, gpart, G, n, p, K,
+                                                              level_offset_d(depth), inv_scale, out, Kb);
 }
 
 void configure_far_kernels(size_t max_smem) {
