@@ -275,9 +275,12 @@ __device__ __forceinline__ void p2p_kb_chunk(const float4 &ti, int self, const f
 // Paired states (K >= 4): the staged row holds state pairs as
 // (x_a, x_b, y_a, y_b), (z_a, z_b, 0, 0) and the per-state arithmetic runs on
 // packed FP32x2 FMAs, one instruction for two states (same FP32 throughput,
-// half the issue slots).
+// half the issue slots).  The self source is recognised by its position in
+// the staged chunk (self_q, computed once per item; out of range when it is
+// not in this chunk), and the self pair needs no zeroed w: with 1/|r| = 0
+// the pair's s = m.u is 0.
 template <int KG, bool PHI, bool FULL>
-__device__ __forceinline__ void p2p_kb_chunk_x2(const float4 &ti, int self, const float4 *sPos, const int *sIdx,
+__device__ __forceinline__ void p2p_kb_chunk_x2(const float4 &ti, int self_q, const float4 *sPos,
                                                 const float4 *m_row0, int Kr, int qbeg, int sn, int F, int kvalid,
                                                 float2 (&acc)[KG / 2][4]) {
 #pragma unroll 2
@@ -285,11 +288,10 @@ __device__ __forceinline__ void p2p_kb_chunk_x2(const float4 &ti, int self, cons
     const float4 s = sPos[q];
     const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const bool is_self = sIdx[q] == self;
-    const float rinv = is_self ? 0.0F : rsqrtf(r2);
+    const float rinv = q == self_q ? 0.0F : rsqrtf(r2);
     const float v = rinv * rinv * rinv;
     const float f = 3.0F * v * rinv * rinv;
-    const float w = is_self ? 0.0F : r2 * (1.0F / 3.0F);
+    const float w = r2 * (1.0F / 3.0F);
     const float2 UX = make_float2(f * dx, f * dx), UY = make_float2(f * dy, f * dy), UZ = make_float2(f * dz, f * dz);
     const float2 DX = make_float2(dx, dx), DY = make_float2(dy, dy), DZ = make_float2(dz, dz);
     const float2 NV = make_float2(-v, -v), W2 = make_float2(w, w);
@@ -418,6 +420,13 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
       const int i = t0 + t;
       const float4 ti = tgt_rel[i];
       const int self = self_idx != nullptr ? self_idx[i] : -1;
+      // staged position of the self source in the neighbourhood (-1: none)
+      int self_g = -1;
+      if (self >= 0)
+        for (int c = 0; c < nb.count; ++c) {
+          const int off = self - nb.begin[c];
+          if (off >= 0 && off < nb.prefix[c + 1] - nb.prefix[c]) self_g = nb.prefix[c] + off;
+        }
       float acc[KG][4];
 #pragma unroll
       for (int st = 0; st < KG; ++st) acc[st][0] = acc[st][1] = acc[st][2] = acc[st][3] = 0.0F;
@@ -495,10 +504,11 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
                 p2p_grad_chunk<KG, false, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
                                                   gacc);
             } else if constexpr (PAIRED) {
+              const int self_q = self_g >= 0 ? self_g - pass - q0 : -1;
               if (kvalid == KG)
-                p2p_kb_chunk_x2<KG, PHI, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc2);
+                p2p_kb_chunk_x2<KG, PHI, true>(ti, self_q, sPos + q0, m_row0, Kr, f, sn, F, kvalid, acc2);
               else
-                p2p_kb_chunk_x2<KG, PHI, false>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc2);
+                p2p_kb_chunk_x2<KG, PHI, false>(ti, self_q, sPos + q0, m_row0, Kr, f, sn, F, kvalid, acc2);
             } else {
               if (kvalid == KG)
                 p2p_kb_chunk<KG, PHI, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc);
