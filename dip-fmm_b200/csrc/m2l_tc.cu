@@ -406,36 +406,58 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
 // Kp rows (states) x Kpad alphas stored chunk by chunk (32 alphas; the last
 // chunk may be 16), each chunk as [Kp/8 row groups][w/8 column blocks][8][8]
 // so one box's rows of one chunk are contiguous.  One extra all-zero box
-// (index n_boxes) stands for sources outside the grid.
-__global__ void m2l_pack_kernel(const float *__restrict__ M, const float *__restrict__ scale_m,
-                                __nv_bfloat16 *__restrict__ hi, __nv_bfloat16 *__restrict__ lo, int n, int K, int Kp,
-                                int Kpad, int depth, int node_base, int n_boxes) {
-  const long long per_box = static_cast<long long>(Kp) * Kpad;
-  const long long total = (static_cast<long long>(n_boxes) + 1) * per_box;
-  for (long long q = blockIdx.x * static_cast<long long>(blockDim.x) + threadIdx.x; q < total;
-       q += static_cast<long long>(gridDim.x) * blockDim.x) {
-    const long long box = q / per_box;
-    const int e = static_cast<int>(q - box * per_box);
-    const int kc = e / (Kp * kKChunk);
-    const int rem = e - kc * Kp * kKChunk;
-    const int ncj = min(kKChunk, Kpad - kc * kKChunk) / 8;
-    const int a8 = rem & 7;
-    const int r8 = (rem >> 3) & 7;
-    const int x = rem >> 6;
-    const int cjl = x % ncj;
-    const int rg = x / ncj;
-    const int k = rg * 8 + r8;
-    const int a = kc * kKChunk + cjl * 8 + a8;
-    float v = 0.0F;
-    if (box < n_boxes && k < K && a < n) {
-      const int node = node_base + static_cast<int>(box);
-      int level = 0;
-      while (level < depth && level_offset_d(level + 1) <= node) ++level;
-      v = M[static_cast<long long>(node) * n * K + static_cast<long long>(a) * K + k] * scale_m[level * n + a];
+// (index n_boxes) stands for sources outside the grid.  One CTA per box: a
+// chunk's 32 alphas x Kp states are read along the states (coalesced rows
+// of M[node][alpha][k]) into a shared tile, then written as 16-byte runs of
+// 8 alphas (one core-matrix row of hi and of lo).
+constexpr int kPackThreads = 256;
+constexpr int kPackMaxKp = 128;
+
+__global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__restrict__ M,
+                                                                const float *__restrict__ scale_m,
+                                                                uint4 *__restrict__ hi, uint4 *__restrict__ lo, int n,
+                                                                int K, int Kp, int Kpad, int depth, int node_base,
+                                                                int n_boxes) {
+  __shared__ float tile[kKChunk][kPackMaxKp + 1]; // [alpha in chunk][state]
+  const int box = blockIdx.x;
+  const int tid = threadIdx.x;
+  const int node = node_base + box;
+  int level = 0;
+  while (level < depth && level_offset_d(level + 1) <= node) ++level;
+  const float *src = M + static_cast<long long>(node) * n * K;
+  const long long box_vec = static_cast<long long>(box) * Kp * Kpad / 8; // 16-byte vectors before this box
+  const int nkc = (Kpad + kKChunk - 1) / kKChunk;
+  for (int kc = 0; kc < nkc; ++kc) {
+    const int w = min(kKChunk, Kpad - kc * kKChunk);
+    const int ncj = w / 8;
+    __syncthreads();
+    for (int e = tid; e < w * Kp; e += kPackThreads) {
+      const int al = e / Kp;
+      const int k = e - al * Kp;
+      const int a = kc * kKChunk + al;
+      tile[al][k] = (box < n_boxes && a < n && k < K) ? src[static_cast<long long>(a) * K + k] * scale_m[level * n + a]
+                                                     : 0.0F;
     }
-    const __nv_bfloat16 h = __float2bfloat16_rn(v);
-    hi[q] = h;
-    lo[q] = __float2bfloat16_rn(v - __bfloat162float(h));
+    __syncthreads();
+    const long long chunk_vec = box_vec + static_cast<long long>(kc) * Kp * kKChunk / 8;
+    for (int v = tid; v < Kp * w / 8; v += kPackThreads) {
+      const int x = v >> 3;
+      const int r8 = v & 7;
+      const int cjl = x % ncj;
+      const int k = (x / ncj) * 8 + r8;
+      uint32_t h[4], l[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+        const float v0 = tile[cjl * 8 + 2 * j][k], v1 = tile[cjl * 8 + 2 * j + 1][k];
+        const __nv_bfloat16 h0 = __float2bfloat16_rn(v0), h1 = __float2bfloat16_rn(v1);
+        const __nv_bfloat16 l0 = __float2bfloat16_rn(v0 - __bfloat162float(h0));
+        const __nv_bfloat16 l1 = __float2bfloat16_rn(v1 - __bfloat162float(h1));
+        h[j] = static_cast<uint32_t>(__bfloat16_as_ushort(h0)) | (static_cast<uint32_t>(__bfloat16_as_ushort(h1)) << 16);
+        l[j] = static_cast<uint32_t>(__bfloat16_as_ushort(l0)) | (static_cast<uint32_t>(__bfloat16_as_ushort(l1)) << 16);
+      }
+      hi[chunk_vec + v] = make_uint4(h[0], h[1], h[2], h[3]);
+      lo[chunk_vec + v] = make_uint4(l[0], l[1], l[2], l[3]);
+    }
   }
 }
 
@@ -451,10 +473,9 @@ size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages) {
 void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,
                      int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s) {
   (void)basis;
-  const long long total = (static_cast<long long>(n_boxes) + 1) * Kp * Kpad;
-  const int blocks = static_cast<int>(std::min<long long>((total + 255) / 256, 148LL * 64));
-  m2l_pack_kernel<<<blocks, 256, 0, s>>>(M, scale_m, static_cast<__nv_bfloat16 *>(hi),
-                                          static_cast<__nv_bfloat16 *>(lo), n, K, Kp, Kpad, depth, node_base, n_boxes);
+  if (Kp > kPackMaxKp || Kp % 8 != 0 || Kpad % 16 != 0) return; // the plan keeps Kp <= 128, multiples of 8
+  m2l_pack_kernel<<<n_boxes + 1, kPackThreads, 0, s>>>(M, scale_m, static_cast<uint4 *>(hi), static_cast<uint4 *>(lo),
+                                                        n, K, Kp, Kpad, depth, node_base, n_boxes);
 }
 
 void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s) {
