@@ -96,27 +96,77 @@ def load_peaks():
 
 # ------------------------------------------------------------------ clocks
 class ClockSampler:
-    """nvidia-smi clock/throttle samples during the timed region."""
+    """SM clock and clock-event (throttle) reasons sampled DURING the timed
+    region: NVML read every 20 ms from a background thread (the timed region
+    of a short run lasts only a few hundred ms), or `nvidia-smi -lms 100`
+    when NVML is not importable.  Reads only; changes no GPU setting."""
 
     FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
               "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
               "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+    REASON_BITS = (("hw_slowdown", 0x8), ("hw_thermal_slowdown", 0x40), ("sw_thermal_slowdown", 0x20),
+                   ("sw_power_cap", 0x4))
 
-    def __init__(self, gpu_index):
+    def __init__(self, gpu_index, pci_bus_id=None):
         self.gpu = gpu_index
+        self.pci = pci_bus_id
         self.proc = None
         self.file = None
+        self.thread = None
+        self.samples = []
+        self.kind = None
+
+    def _nvml_loop(self, nvml, handle, stop):
+        while not stop.is_set():
+            try:
+                sm = nvml.nvmlDeviceGetClockInfo(handle, nvml.NVML_CLOCK_SM)
+                reasons = nvml.nvmlDeviceGetCurrentClocksEventReasons(handle)
+                self.samples.append((float(sm), int(reasons)))
+            except Exception:  # noqa: BLE001 - a failed read is a missing sample
+                pass
+            stop.wait(0.02)
 
     def start(self):
+        try:
+            import threading
+
+            import pynvml as nvml
+
+            nvml.nvmlInit()
+            handle = None
+            if self.pci:
+                try:
+                    handle = nvml.nvmlDeviceGetHandleByPciBusId(self.pci)
+                except Exception:  # noqa: BLE001
+                    handle = None
+            if handle is None:
+                handle = nvml.nvmlDeviceGetHandleByIndex(self.gpu)
+            self.smax = float(nvml.nvmlDeviceGetMaxClockInfo(handle, nvml.NVML_CLOCK_SM))
+            self.stop_event = threading.Event()
+            self.thread = threading.Thread(target=self._nvml_loop, args=(nvml, handle, self.stop_event), daemon=True)
+            self.kind = "nvml, 20 ms"
+            self.thread.start()
+            return
+        except Exception:  # noqa: BLE001 - fall back to nvidia-smi
+            self.thread = None
         try:
             self.file = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
-                 "-lms", "200"], stdout=self.file, stderr=subprocess.DEVNULL)
+                 "-lms", "100"], stdout=self.file, stderr=subprocess.DEVNULL)
+            self.kind = "nvidia-smi, 100 ms"
         except (OSError, ValueError):
             self.proc = None
 
     def stop(self):
+        if self.thread is not None:
+            self.stop_event.set()
+            self.thread.join(timeout=5)
+            if not self.samples:
+                return None
+            reasons = {name for name, bit in self.REASON_BITS for _, r in self.samples if r & bit}
+            return {"sm_mhz": statistics.median(s for s, _ in self.samples), "sm_max_mhz": self.smax,
+                    "reasons": sorted(reasons), "samples": len(self.samples), "sampler": self.kind}
         if self.proc is None:
             return None
         self.proc.send_signal(signal.SIGTERM)
@@ -141,7 +191,8 @@ class ClockSampler:
                 continue
         if not sm:
             return None
-        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm)}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": smax, "reasons": sorted(reasons), "samples": len(sm),
+                "sampler": self.kind}
 
 
 # --------------------------------------------------------------- reference
@@ -286,7 +337,11 @@ def b200_arm(args):
     for _ in range(max(args.warmup, 0)):
         step()
     torch.cuda.synchronize()
-    clocks = ClockSampler(local)
+    props = torch.cuda.get_device_properties(local)
+    pci = None
+    if all(hasattr(props, f) for f in ("pci_domain_id", "pci_bus_id", "pci_device_id")):
+        pci = f"{props.pci_domain_id:08x}:{props.pci_bus_id:02x}:{props.pci_device_id:02x}.0"
+    clocks = ClockSampler(local, pci)
     clocks.start()
     barrier()
     torch.cuda.synchronize()
