@@ -324,16 +324,19 @@ __global__ void __launch_bounds__(kShiftThreads) m2m_kernel(float *__restrict__ 
   const float *child0 = M + (level_offset_d(parent_level + 1) + parent * 8) * per + kb;
   const int qpr = Ks >> 2; // float4 quads per staged row
   if ((K & 3) == 0) {
-    // rows of 4-aligned states: one float4 load per quad, one division per quad
+    // rows of 4-aligned states: one asynchronous 16-byte copy per quad (all
+    // of a thread's copies in flight at once), one division per quad
     for (int q = threadIdx.x; q < 8 * n * qpr; q += kShiftThreads) {
       const int cr = q / qpr; // child * n + coefficient
       const int kq = q - cr * qpr;
       const int c = cr / n;
-      float4 v = make_float4(0, 0, 0, 0);
       if (4 * kq < kc)
-        v = *reinterpret_cast<const float4 *>(child0 + c * per + static_cast<long long>(cr - c * n) * K + 4 * kq);
-      reinterpret_cast<float4 *>(sM)[q] = v;
+        cp_async16(reinterpret_cast<float4 *>(sM) + q, child0 + c * per + static_cast<long long>(cr - c * n) * K + 4 * kq);
+      else
+        reinterpret_cast<float4 *>(sM)[q] = make_float4(0, 0, 0, 0);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
   } else {
     for (int q = threadIdx.x; q < 8 * n * Ks; q += kShiftThreads) {
       const int cr = q / Ks;
@@ -392,10 +395,13 @@ __global__ void __launch_bounds__(kShiftThreads) l2l_kernel(float *__restrict__ 
     for (int q = threadIdx.x; q < n * qpr; q += kShiftThreads) {
       const int b = q / qpr;
       const int kq = q - b * qpr;
-      float4 v = make_float4(0, 0, 0, 0);
-      if (4 * kq < kc) v = *reinterpret_cast<const float4 *>(src + static_cast<long long>(b) * K + 4 * kq);
-      reinterpret_cast<float4 *>(sL)[q] = v;
+      if (4 * kq < kc)
+        cp_async16(reinterpret_cast<float4 *>(sL) + q, src + static_cast<long long>(b) * K + 4 * kq);
+      else
+        reinterpret_cast<float4 *>(sL)[q] = make_float4(0, 0, 0, 0);
     }
+    cp_async_commit();
+    cp_async_wait<0>();
   } else {
     for (int q = threadIdx.x; q < n * Ks; q += kShiftThreads) {
       const int b = q / Ks;
@@ -507,20 +513,26 @@ __device__ __forceinline__ void l2p_tiles(int tid, int tn, int Kq, int Kcp, int 
           }
       }
     }
+    // Combine with the near field: each target's 4 near values are loaded
+    // together (one batch of independent loads per target, not one
+    // load-store round trip per value), then written back.
 #pragma unroll
     for (int u = 0; u < TU; ++u) {
       const int t = TU * tq + u;
-      if (t >= tn) break;
       const int i = tc + t;
+      float4 nv[4];
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const int kl = 4 * kq + v;
-        if (kl >= Kc) break;
-        const int k = kblk + kl;
-        float4 *nr = near + static_cast<long long>(i) * K + k;
-        const float4 nv = *nr;
-        *nr = make_float4(want_phi ? (ph[u][v] + nv.x) * phi_scale : 0.0F, want_h ? nv.y - hx[u][v] : 0.0F,
-                          want_h ? nv.z - hy[u][v] : 0.0F, want_h ? nv.w - hz[u][v] : 0.0F);
+        nv[v] = (t < tn && kl < Kc) ? near[static_cast<long long>(i) * K + kblk + kl] : make_float4(0, 0, 0, 0);
+      }
+#pragma unroll
+      for (int v = 0; v < 4; ++v) {
+        const int kl = 4 * kq + v;
+        if (t < tn && kl < Kc)
+          near[static_cast<long long>(i) * K + kblk + kl] =
+              make_float4(want_phi ? (ph[u][v] + nv[v].x) * phi_scale : 0.0F, want_h ? nv[v].y - hx[u][v] : 0.0F,
+                          want_h ? nv[v].z - hy[u][v] : 0.0F, want_h ? nv[v].w - hz[u][v] : 0.0F);
       }
     }
   }
@@ -556,10 +568,21 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
     const int Kcp = (Kc + 3) & ~3;
     const int Kq = Kcp >> 2;
     __syncthreads();
-    for (int q = tid; q < n * Kcp; q += kL2pThreads) {
-      const int b = q / Kcp;
-      const int k = q - b * Kcp;
-      sL[q] = k < Kc ? src[static_cast<long long>(b) * K + kblk + k] : 0.0F;
+    if ((K & 3) == 0 && (kblk & 3) == 0 && (Kc & 3) == 0) {
+      // 4-aligned rows: asynchronous 16-byte copies, all in flight at once
+      const int nq = Kcp >> 2;
+      for (int q = tid; q < n * nq; q += kL2pThreads) {
+        const int b = q / nq;
+        cp_async16(reinterpret_cast<float4 *>(sL) + q, src + static_cast<long long>(b) * K + kblk + 4 * (q - b * nq));
+      }
+      cp_async_commit();
+      cp_async_wait<0>();
+    } else {
+      for (int q = tid; q < n * Kcp; q += kL2pThreads) {
+        const int b = q / Kcp;
+        const int k = q - b * Kcp;
+        sL[q] = k < Kc ? src[static_cast<long long>(b) * K + kblk + k] : 0.0F;
+      }
     }
     for (int tc = t0; tc < t1; tc += kL2pTargets) {
       const int tn = min(kL2pTargets, t1 - tc);
@@ -759,10 +782,20 @@ __global__ void __launch_bounds__(kL2pGradThreads) l2p_grad_kernel(
       const int Kcp = (Kc + 3) & ~3;
       const int Kq = Kcp >> 2;
       __syncthreads(); // previous block's sL reads are done
-      for (int e = tid; e < n * Kcp; e += kL2pGradThreads) {
-        const int b = e / Kcp;
-        const int k = e - b * Kcp;
-        sL[e] = k < Kc ? src[static_cast<long long>(b) * K + kblk + k] : 0.0F;
+      if ((K & 3) == 0 && (kblk & 3) == 0 && (Kc & 3) == 0) {
+        const int nq = Kcp >> 2;
+        for (int e = tid; e < n * nq; e += kL2pGradThreads) {
+          const int b = e / nq;
+          cp_async16(reinterpret_cast<float4 *>(sL) + e, src + static_cast<long long>(b) * K + kblk + 4 * (e - b * nq));
+        }
+        cp_async_commit();
+        cp_async_wait<0>();
+      } else {
+        for (int e = tid; e < n * Kcp; e += kL2pGradThreads) {
+          const int b = e / Kcp;
+          const int k = e - b * Kcp;
+          sL[e] = k < Kc ? src[static_cast<long long>(b) * K + kblk + k] : 0.0F;
+        }
       }
       __syncthreads();
       if (nm2 == 0) continue;

@@ -71,4 +71,18 @@ __host__ __device__ inline void demorton3(uint32_t m, int &x, int &y, int &z) {
   z = static_cast<int>(undilate3(m >> 2));
 }
 
+#ifdef __CUDACC__
+// 16-byte asynchronous global -> shared copy (bypasses registers, so many
+// copies of one thread are in flight at once), its commit and wait.
+__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
+               "l"(gmem)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+template <int N> __device__ __forceinline__ void cp_async_wait() {
+  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
+}
+#endif
+
 } // namespace cdfmm_b200

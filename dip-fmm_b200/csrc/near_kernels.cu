@@ -220,16 +220,6 @@ constexpr int kNeighbourCap = 1024; // staged neighbourhood size per pass
 constexpr int kStateBlock = 64;     // states per state block (bounds shared memory)
 constexpr int kKbThreads = 256;
 
-__device__ __forceinline__ void cp_async16(void *smem, const void *gmem) {
-  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(smem))),
-               "l"(gmem)
-               : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-template <int N> __device__ __forceinline__ void cp_async_wait() {
-  asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
-}
-
 // Shared-memory position of state k within a staged moment row (one pad
 // float4 after every group of KG states), and the row stride for a window of
 // Kw states (1 mod 8 float4).
