@@ -210,14 +210,38 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
         if (r == 0)
           for (int q = nm1; q < nm1p; ++q) mono[j * nm1p + q] = 0.0F;
       }
-      for (int q = tid; q < cn * Kc; q += blockDim.x) {
-        const int j = q / Kc;
-        const int k = kblk + q - j * Kc;
-        // paired layout (K >= 4): state k is component k & 1 of its pair
-        const float4 *row = mom + static_cast<long long>(c0 + j) * ((K + 1) & ~1);
-        const float4 a = row[k & ~1], b = row[k | 1];
-        const bool odd = (k & 1) != 0;
-        smom[q] = make_float4(odd ? a.y : a.x, odd ? a.w : a.z, odd ? b.y : b.x, 0.0F);
+      {
+        // paired layout (K >= 4): states (2i, 2i+1) share two float4
+        // (x, x', y, y'), (z, z', 0, 0).  A thread loads whole pairs (each
+        // pair read once) in batches of 4 pairs whose loads are all issued
+        // before the shared-memory stores that consume them.
+        const int pp0 = kblk >> 1;
+        const int npair = ((kblk + Kc - 1) >> 1) - pp0 + 1;
+        const int np = cn * npair;
+        const long long row_len = (K + 1) & ~1;
+        for (int q0 = tid; q0 < np; q0 += 4 * blockDim.x) {
+          float4 A[4], B[4];
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int q = q0 + u * blockDim.x;
+            if (q < np) {
+              const int j = q / npair;
+              const float4 *pr = mom + (c0 + j) * row_len + 2 * (pp0 + q - j * npair);
+              A[u] = pr[0];
+              B[u] = pr[1];
+            }
+          }
+#pragma unroll
+          for (int u = 0; u < 4; ++u) {
+            const int q = q0 + u * blockDim.x;
+            if (q < np) {
+              const int j = q / npair;
+              const int s0 = 2 * (pp0 + q - j * npair) - kblk; // state of the pair's first half, block-relative
+              if (s0 >= 0) smom[j * Kc + s0] = make_float4(A[u].x, A[u].z, B[u].x, 0.0F);
+              if (s0 + 1 < Kc) smom[j * Kc + s0 + 1] = make_float4(A[u].y, A[u].w, B[u].y, 0.0F);
+            }
+          }
+        }
       }
       __syncthreads();
       for (int t = tid; t < tiles; t += blockDim.x) {
