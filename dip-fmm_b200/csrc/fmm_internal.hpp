@@ -123,6 +123,7 @@ struct cdfmm_b200_plan {
   int tc_Kpad = 0, tc_Npad = 0, tc_stages = 0, tc_Kp_max = 0;
   int tc_m_tiles = 1, tc_acc_stride = 0; // accumulators per CTA, TMEM columns apart
   int tc_fuse = 0;                        // 1: A_hi x [B_hi | B_lo] as one N = 2 Npad MMA
+  bool tc_pinned = false;                 // shape set by cdfmm_b200_set_m2l_shape: no autotuning
   struct TcShape {
     int m_tiles, stages, fuse;
   };

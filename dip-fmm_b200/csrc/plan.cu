@@ -687,7 +687,7 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
                       plan->depth, node_base, boxes, s);
       if (plan->tc_tiles_Kp != Kp) {
         check(cudaStreamSynchronize(s), "sync");
-        if (plan->tc_candidates.size() > 1) tune_m2l_tc(plan, K, s);
+        if (plan->tc_candidates.size() > 1 && !plan->tc_pinned) tune_m2l_tc(plan, K, s);
         upload_tc_tiles(plan, Kp);
       }
       TcArgs ta{};
@@ -1234,6 +1234,45 @@ int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out) {
   if (plan == nullptr || out == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan and out must not be NULL");
   *out = plan->stats;
   return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_m2l_shapes(const cdfmm_b200_plan *plan, int32_t *out, int32_t capacity) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (capacity < 0 || (capacity > 0 && out == nullptr))
+    return fail(const_cast<cdfmm_b200_plan *>(plan), CDFMM_B200_ERR_INVALID_ARGUMENT, "out is NULL");
+  if (!plan->tc_supported) return 0;
+  const int n = static_cast<int>(plan->tc_candidates.size());
+  for (int i = 0; i < n && i < capacity; ++i) {
+    out[3 * i] = plan->tc_candidates[static_cast<size_t>(i)].m_tiles;
+    out[3 * i + 1] = plan->tc_candidates[static_cast<size_t>(i)].stages;
+    out[3 * i + 2] = plan->tc_candidates[static_cast<size_t>(i)].fuse;
+  }
+  return n;
+}
+
+int cdfmm_b200_set_m2l_shape(cdfmm_b200_plan *plan, int32_t m_tiles, int32_t stages, int32_t fused) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (m_tiles == 0) {
+    plan->tc_pinned = false;
+    plan->tc_tiles_Kp = 0; // re-tune on the next tensor-core evaluate
+    return CDFMM_B200_OK;
+  }
+  if (!plan->tc_supported)
+    return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT, "this plan has no tensor-core M2L (m2l_mode, order or device)");
+  for (const cdfmm_b200_plan::TcShape &c : plan->tc_candidates) {
+    if (c.m_tiles == m_tiles && c.stages == stages && c.fuse == (fused != 0 ? 1 : 0)) {
+      plan->tc_m_tiles = c.m_tiles;
+      plan->tc_stages = c.stages;
+      plan->tc_fuse = c.fuse;
+      plan->tc_acc_stride = round_up(c.fuse ? 2 * plan->tc_Npad : plan->tc_Npad, 32);
+      plan->tc_tmem_cols = tmem_columns(plan->tc_m_tiles, plan->tc_acc_stride);
+      plan->tc_pinned = true;
+      plan->tc_tiles_Kp = 0; // work tiles rebuilt for this shape on the next evaluate
+      return CDFMM_B200_OK;
+    }
+  }
+  return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT,
+              "not a pipeline shape of this plan (cdfmm_b200_m2l_shapes lists them)");
 }
 
 int cdfmm_b200_selftest_bounded_wait(int32_t device) {

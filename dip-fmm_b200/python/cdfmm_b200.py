@@ -42,7 +42,7 @@ EXPORTED = (
     "cdfmm_b200_direct_fp64", "cdfmm_b200_m2l_matrix", "cdfmm_b200_last_error",
     "cdfmm_b200_evaluate_noalloc", "cdfmm_b200_backward", "cdfmm_b200_batch_create",
     "cdfmm_b200_batch_launch", "cdfmm_b200_batch_destroy", "cdfmm_b200_direct_grad_fp64",
-    "cdfmm_b200_selftest_bounded_wait",
+    "cdfmm_b200_selftest_bounded_wait", "cdfmm_b200_m2l_shapes", "cdfmm_b200_set_m2l_shape",
 )
 
 # Scratch capacity of cdfmm_b200_evaluate_noalloc (bytes).
@@ -132,6 +132,8 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_batch_destroy.restype = None
     lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
     lib.cdfmm_b200_set_timing.argtypes = [vp, i32]
+    lib.cdfmm_b200_m2l_shapes.argtypes = [vp, ctypes.POINTER(i32), i32]
+    lib.cdfmm_b200_set_m2l_shape.argtypes = [vp, i32, i32, i32]
     lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.cdfmm_b200_direct_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
     lib.cdfmm_b200_direct_grad_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
@@ -268,6 +270,22 @@ class DevicePlan:
 
     def set_timing(self, enabled=True):
         _check(library().cdfmm_b200_set_timing(self._h, 1 if enabled else 0), self._h)
+
+    def m2l_shapes(self) -> list:
+        """Tensor-core M2L pipeline shapes of this plan as (accumulators per
+        CTA, stages, fused) tuples (empty without the tensor-core M2L)."""
+        lib = library()
+        n = lib.cdfmm_b200_m2l_shapes(self._h, None, 0)
+        if n < 0:
+            _check(n, self._h)
+        buf = (ctypes.c_int32 * (3 * max(n, 1)))()
+        lib.cdfmm_b200_m2l_shapes(self._h, buf, n)
+        return [(buf[3 * i], buf[3 * i + 1], bool(buf[3 * i + 2])) for i in range(n)]
+
+    def set_m2l_shape(self, m_tiles, stages=0, fused=False):
+        """Pins one of m2l_shapes() (no autotuning, run-to-run identical
+        results); m_tiles = 0 returns to autotuning."""
+        _check(library().cdfmm_b200_set_m2l_shape(self._h, int(m_tiles), int(stages), 1 if fused else 0), self._h)
 
     def stats(self) -> dict:
         s = Stats()

@@ -235,6 +235,20 @@ int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled);
 
 int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out);
 
+/* Tensor-core M2L pipeline shapes (no counterpart in the reference, whose
+ * CudaFull M2L has one fixed shape).  cdfmm_b200_m2l_shapes writes up to
+ * `capacity` shapes as (accumulators per CTA, stages, fused) triples into
+ * `out` ([capacity][3], may be NULL with capacity 0) and returns how many the
+ * plan supports (negative: an error code).  By default the first
+ * tensor-core evaluate of each K times them all and keeps the fastest; shapes
+ * that differ only in accumulators or stages give bit-identical results,
+ * the fused form (A_hi x [B_hi | B_lo] in one MMA) differs at FP32 rounding,
+ * so timing noise can switch results at that level between runs.
+ * cdfmm_b200_set_m2l_shape pins one of the listed shapes (no timing, the
+ * same results on every run); m_tiles = 0 returns to autotuning. */
+int cdfmm_b200_m2l_shapes(const cdfmm_b200_plan *plan, int32_t *out, int32_t capacity);
+int cdfmm_b200_set_m2l_shape(cdfmm_b200_plan *plan, int32_t m_tiles, int32_t stages, int32_t fused);
+
 /* FP64 O(N*M) direct sum on the device with explicit self exclusion: the
  * oracle-grade reference field (upstream validation.cpp:71-111 on the CPU and
  * dipole_field_kernel, src/cuda_fmm.cu:518-569).  Host arrays in user order;

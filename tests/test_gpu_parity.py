@@ -371,3 +371,43 @@ def test_python_uniform_fmm_zero_copy_device_io():
         f.evaluate_into(dm, dH[:, :10], dphi, output="both")
     with pytest.raises(ValueError, match="float32"):
         f.evaluate_into(dm.double(), dH, dphi, output="both")
+
+
+@pytest.mark.parametrize("order,K", [(5, 16), (6, 64)])
+def test_every_m2l_pipeline_shape_gives_the_same_field(order, K):
+    # Each tensor-core M2L pipeline shape the autotuner may pick, pinned in
+    # turn: shapes with the same hi/lo fusion are bit-identical, fused and
+    # unfused agree to FP32 rounding, and all meet the FP32 bar against the
+    # FP64 oracle FMM.
+    rng = np.random.default_rng(71 + order)
+    n = 6000
+    x = rng.uniform(0, 1, (n, 3))
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, order, max_states=K, m2l_mode=cdfmm_b200.M2L_BF16X3)
+    plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+    m = rng.normal(size=(K, n, 3)).astype(np.float32)
+    shapes = plan.m2l_shapes()
+    assert len(shapes) >= 2 and any(f for _, _, f in shapes) and any(not f for _, _, f in shapes)
+    results = {}
+    for mt, st, fused in shapes:
+        plan.set_m2l_shape(mt, st, fused)
+        H = plan.evaluate(m, output="field")["H"].copy()
+        s = plan.stats()
+        assert (s["m2l_tc_m_tiles"], s["m2l_tc_stages"], bool(s["m2l_tc_fused"])) == (mt, st, fused)
+        results[(mt, st, fused)] = H
+    for fused in (False, True):
+        group = [H for (mt, st, f), H in results.items() if f == fused]
+        for H in group[1:]:
+            np.testing.assert_array_equal(H, group[0])
+    unfused = next(H for (mt, st, f), H in results.items() if not f)
+    fused_h = next(H for (mt, st, f), H in results.items() if f)
+    assert oracle.rel_l2(fused_h, unfused) < 1e-6
+    ref = oracle.fmm(x, x, m[K - 1].astype(np.float64), order, 3, identities=np.arange(n), flags=2)["H"]
+    assert oracle.rel_l2(unfused[K - 1], ref) < FP32_REL_L2
+    with pytest.raises(ValueError, match="not a pipeline shape"):
+        plan.set_m2l_shape(3, 99, False)
+    plan.set_m2l_shape(0)  # back to autotuning
+    plan.evaluate(m, output="field")
+    plan.close()
