@@ -198,11 +198,13 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
 // A self pair gets u = v = w = 0; a coincident non-self pair gives u = NaN
 // (0 * inf), hence NaN results, as in the reference.
 //
-// Load balance: the items of a leaf are processed in rounds of 256; a round
-// with r < 256 items gives each item F = 2^j <= min(8, 256 / r) lanes that
-// split the sources (lane f takes sources f, f + F, ...) and are summed with
-// warp shuffles at the end of the round, so a leaf whose target count is not
-// a multiple of 32 does not leave most lanes idle in its last round.
+// Load balance: the items of a leaf are processed in rounds of 256 lanes; a
+// round gives each of its r items F = 2^j <= 8 lanes that split the sources
+// (lane f takes sources f, f + F, ...) and are summed with warp shuffles at
+// the end of the round.  Each round takes the F (and r = min(remaining,
+// 256 / F)) that keeps the most lanes busy, so a leaf whose item count is
+// not a multiple of 256 -- fewer than 32 targets, or a narrow state window
+// -- does not leave lanes idle.
 //
 // Staging: the neighbourhood positions (relative to this leaf's centre) and
 // sorted source indices are staged once; the moments of the round's state
@@ -386,10 +388,20 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
     const int Kc = min(kStateBlock, k_end - kblk);
     const int G = (Kc + KG - 1) / KG;
     const int items = nt * G;
-    for (int ib = 0; ib < items; ib += kKbThreads) {
-      const int r = min(kKbThreads, items - ib);
-      int F = 1;
-      while (F < 8 && 2 * F * r <= kKbThreads) F <<= 1;
+    for (int ib = 0, r = 0; ib < items; ib += r) {
+      // This round's items r and lanes per item F (a power of two <= 8):
+      // the F that keeps the most of the 256 lanes busy (the fewest lanes
+      // per item among equals), e.g. 72 items -> 64 items x 4 lanes, then
+      // 8 x 8, instead of 72 x 2 with 112 lanes idle.
+      int F = 1, busy = 0;
+      for (int fc = 1; fc <= 8; fc <<= 1) {
+        const int lanes = min(items - ib, kKbThreads / fc) * fc;
+        if (lanes > busy) {
+          busy = lanes;
+          F = fc;
+        }
+      }
+      r = min(items - ib, kKbThreads / F);
       const int li = tid / F;
       const int f = tid - li * F;
       const bool valid = li < r;
