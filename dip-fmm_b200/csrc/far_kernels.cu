@@ -478,7 +478,7 @@ template <int TU>
 __device__ __forceinline__ void l2p_tiles(int tid, int tn, int Kq, int Kcp, int Kc, int n, int nm1,
                                           const float *mono, const float *sL, const short *sidx, bool want_phi,
                                           bool want_h, float4 *__restrict__ near, int tc, int kblk, int K,
-                                          float phi_scale) {
+                                          float phi_scale, int k_near_end) {
   const int tiles = ((tn + TU - 1) / TU) * Kq;
   for (int tile = tid; tile < tiles; tile += kL2pThreads) {
     const int tq = tile / Kq;
@@ -548,7 +548,9 @@ __device__ __forceinline__ void l2p_tiles(int tid, int tn, int Kq, int Kcp, int 
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
         const int kl = 4 * kq + v;
-        nv[v] = (t < tn && kl < Kc) ? near[static_cast<long long>(i) * K + kblk + kl] : make_float4(0, 0, 0, 0);
+        // states from k_near_end on have no near field yet (it is added later)
+        nv[v] = (t < tn && kl < Kc && kblk + kl < k_near_end) ? near[static_cast<long long>(i) * K + kblk + kl]
+                                                              : make_float4(0, 0, 0, 0);
       }
 #pragma unroll
       for (int v = 0; v < 4; ++v) {
@@ -566,7 +568,7 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
                                                           const int *__restrict__ tgt_off, float4 *__restrict__ near,
                                                           const int8_t *__restrict__ basis, int n, int p, int K,
                                                           int leaf_node_base, unsigned output, float phi_scale,
-                                                          int Kb, int k_begin, int k_end) {
+                                                          int Kb, int k_begin, int k_end, int k_near_end) {
   extern __shared__ float4 l2p_smem[];
   const int Kbp = (Kb + 3) & ~3;
   float *sL = reinterpret_cast<float *>(l2p_smem);                 // [n][Kcp]
@@ -622,11 +624,14 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
       // blocks, fewer targets per thread for narrow ones so that the 128
       // threads stay busy
       if (Kq >= 16)
-        l2p_tiles<4>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale);
+        l2p_tiles<4>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale,
+                     k_near_end);
       else if (Kq >= 8)
-        l2p_tiles<2>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale);
+        l2p_tiles<2>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale,
+                     k_near_end);
       else
-        l2p_tiles<1>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale);
+        l2p_tiles<1>(tid, tn, Kq, Kcp, Kc, n, nm1, mono, sL, sidx, want_phi, want_h, near, tc, kblk, K, phi_scale,
+                     k_near_end);
     }
   }
 }
@@ -983,9 +988,10 @@ size_t l2p_smem_bytes(int n, int p, int Kb) {
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm, const int *tgt_inv,
                 float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
                 int layout, float phi_scale, float *field, float *potential, cudaStream_t s, int k_begin,
-                int k_end) {
+                int k_end, int k_near_end, bool unsort) {
   if (nt == 0) return;
   if (k_end < 0) k_end = K;
+  if (k_near_end < 0) k_near_end = K;
   const int leaves = 1 << (3 * depth);
   if (K < 4) {
     l2p_small_kernel<<<leaves, 128, 0, s>>>(L, tgt_rel, tgt_off, tgt_perm, near, n, p, K, nt, level_offset_d(depth),
@@ -996,8 +1002,14 @@ void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const
   while (Kb > 4 && l2p_smem_bytes(n, p, Kb) > 60 * 1024) Kb = (Kb + 1) / 2;
   const size_t smem = l2p_smem_bytes(n, p, Kb);
   l2p_kernel<<<leaves, kL2pThreads, smem, s>>>(L, tgt_rel, tgt_off, near, basis, n, p, K, level_offset_d(depth), output,
-                                               phi_scale, Kb, k_begin, k_end);
-  unsort_results_kernel<<<(nt + 31) / 32, 256, 0, s>>>(near, tgt_inv, nt, K, output, layout, field, potential, k_begin,
+                                               phi_scale, Kb, k_begin, k_end, k_near_end);
+  if (unsort) launch_unsort(near, tgt_inv, nt, K, output, layout, field, potential, s, k_begin, k_end);
+}
+
+void launch_unsort(const float4 *res, const int *tgt_inv, int nt, int K, unsigned output, int layout, float *field,
+                   float *potential, cudaStream_t s, int k_begin, int k_end) {
+  if (nt == 0 || k_end <= k_begin) return;
+  unsort_results_kernel<<<(nt + 31) / 32, 256, 0, s>>>(res, tgt_inv, nt, K, output, layout, field, potential, k_begin,
                                                        k_end);
 }
 

@@ -34,11 +34,18 @@ size_t l2p_smem_bytes(int n, int p, int Kb);
 // L2P + combine; K >= 4 writes the sorted results over `near` and then unsorts
 // them to user order (2 launches), K < 4 writes user order directly.  A state
 // range [k_begin, k_end) (K >= 4 only; default all K) processes those states
-// of the K-state rows.
+// of the K-state rows.  States from k_near_end on (default K) have no near
+// field yet: L2P writes the far field alone there, and a later P2P in
+// accumulate mode adds the near field; unsort = false leaves the results
+// sorted (launch_unsort does that part).
 void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm, const int *tgt_inv,
                 float4 *near, const int8_t *basis, int n, int p, int K, int nt, int depth, unsigned output,
                 int layout, float phi_scale, float *field, float *potential, cudaStream_t s, int k_begin = 0,
-                int k_end = -1);
+                int k_end = -1, int k_near_end = -1, bool unsort = true);
+// Sorted combined results (near, K states per target) of states
+// [k_begin, k_end) -> user order (the second launch of launch_l2p).
+void launch_unsort(const float4 *res, const int *tgt_inv, int nt, int K, unsigned output, int layout, float *field,
+                   float *potential, cudaStream_t s, int k_begin, int k_end);
 void configure_far_kernels(size_t max_smem);
 
 // M2L, FP32 SIMT, all levels 2..depth in one launch (overwrites L there).
@@ -49,10 +56,13 @@ void configure_m2l_simt(size_t max_smem);
 int m2l_simt_beta_per_thread(int n);
 
 // list1 P2P near field; states [k_begin, k_end) of the K-state rows (default
-// all; k_begin a multiple of 8 when K >= 8).
+// all; k_begin a multiple of 8 when K >= 8).  accumulate (K > 1): add the
+// near field (phi times phi_scale) to the combined far-field results already
+// in `near` instead of writing it (1: phi and H, 2: phi only).
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
-                bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1);
+                bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1,
+                int accumulate = 0, float phi_scale = 1.0F);
 void configure_p2p(size_t max_smem);
 // Position gradient of sum_k W_k . H_k, near part: partial sums per state
 // group, gpart[nt][p2p_grad_groups(K)] (normalised units, 1/(4 pi) applied).

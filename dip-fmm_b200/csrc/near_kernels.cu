@@ -367,7 +367,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
                                                               const int *__restrict__ self_idx, int depth, int K,
                                                               float4 *__restrict__ near,
                                                               const float4 *__restrict__ W, int k_begin,
-                                                              int k_end) {
+                                                              int k_end, int accumulate, float acc_phi_scale) {
   constexpr bool PHI = MODE == 1;
   constexpr bool GRAD = MODE == 2;
   extern __shared__ float4 dynb[];
@@ -547,9 +547,19 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
         float4 *out = near + static_cast<long long>(i) * K + kblk + kb;
 #pragma unroll
         for (int st = 0; st < KG; ++st)
-          if (st < kvalid)
-            out[st] = make_float4(acc[st][0] * kInvFourPiF, acc[st][1] * kInvFourPiF, acc[st][2] * kInvFourPiF,
-                                  acc[st][3] * kInvFourPiF);
+          if (st < kvalid) {
+            const float4 v = make_float4(acc[st][0] * kInvFourPiF, acc[st][1] * kInvFourPiF, acc[st][2] * kInvFourPiF,
+                                         acc[st][3] * kInvFourPiF);
+            if (accumulate) {
+              // onto the far-field results: phi = (far + near) * phi_scale,
+              // H = near - grad far (accumulate == 2: potential only, H stays 0)
+              const float4 o = out[st];
+              out[st] = accumulate == 1 ? make_float4(fmaf(v.x, acc_phi_scale, o.x), o.y + v.y, o.z + v.z, o.w + v.w)
+                                        : make_float4(fmaf(v.x, acc_phi_scale, o.x), o.y, o.z, o.w);
+            } else {
+              out[st] = v;
+            }
+          }
       }
     }
   }
@@ -683,18 +693,18 @@ template <int KG> size_t p2p_kb_smem_bytes(int K) {
 template <int KG, bool PAIRED>
 void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-               cudaStream_t s, int k_begin, int k_end) {
+               cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale) {
   const int leaves = 1 << (3 * depth);
   const size_t smem = p2p_kb_smem_bytes<KG>(K);
   if (mode == 1)
     p2p_kb_kernel<KG, 1, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
-                                                                  depth, K, near, W, k_begin, k_end);
+                                                                  depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
   else if (mode == 2)
     p2p_kb_kernel<KG, 2, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
-                                                                  depth, K, near, W, k_begin, k_end);
+                                                                  depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
   else
     p2p_kb_kernel<KG, 0, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
-                                                                  depth, K, near, W, k_begin, k_end);
+                                                                  depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
 }
 
 // K >= 8: groups of 8 states, paired layout; 4 <= K < 8: groups of 4,
@@ -702,21 +712,22 @@ void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, con
 // slower at K = 64: the accumulators no longer fit the register budget.)
 void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                    const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-                   cudaStream_t s, int k_begin = 0, int k_end = -1) {
+                   cudaStream_t s, int k_begin = 0, int k_end = -1, int accumulate = 0, float acc_phi_scale = 1.0F) {
   if (k_end < 0) k_end = K;
   if (K >= 8)
-    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end);
+    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
   else if (K >= 4)
-    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end);
+    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
   else
-    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end);
+    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
 }
 
 } // namespace
 
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
-                bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end) {
+                bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end, int accumulate,
+                float phi_scale) {
   const int leaves = 1 << (3 * depth);
   if (K == 1) {
     if (want_phi)
@@ -725,7 +736,7 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
       p2p_k1_kernel<false><<<leaves, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, near);
   } else {
     launch_kb_any(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
-                  k_begin, k_end);
+                  k_begin, k_end, accumulate, phi_scale);
   }
 }
 

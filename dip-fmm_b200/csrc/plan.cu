@@ -841,11 +841,11 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     // and the last the remainder); the copies run on their own streams and
     // the kernels in one explicit order on the caller's stream (stream
     // priorities alone let the later near-field parts delay the far field):
-    //   gather 0, P2P 0, gather 1, P2P 1, ..., far field,
-    //   L2P 0, L2P 1, P2P 2, L2P 2, P2P 3, L2P 3
+    //   gather 0, P2P 0, gather 1, P2P 1, ..., far field, L2P (all states),
+    //   unsort 0, unsort 1, P2P 2 (adding to L2P's far field), unsort 2, ...
     // (the first half of the P2P parts before the far field, while the later
     // moments are still being copied in; part j's results are copied out as
-    // soon as its L2P + unsort is done, while later parts are computed).
+    // soon as its unsort is done, while later parts are computed).
     const bool parts = (host_in || host_out) && !timing && K >= 32 && n_chunks == 1 && plan->ns > 0 && plan->nt > 0;
     int launches = 0;
     if (parts) {
@@ -869,18 +869,20 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       check(cudaEventRecord(ev_start, s), "event");
       check(cudaStreamWaitEvent(plan->io_in, ev_start, 0), "wait");
       check(cudaStreamWaitEvent(plan->io_out, ev_start, 0), "wait");
-      auto near_part = [&](int j) {
+      // P2P of part j: the early parts write the near field; the later
+      // ones run after the (single) L2P and add theirs onto its far field.
+      auto near_part = [&](int j, bool accumulate) {
         const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
         launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
-                   plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc);
+                   plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc,
+                   accumulate ? ((a->output & CDFMM_B200_OUTPUT_FIELD) != 0u ? 1 : 2) : 0, plan->phi_scale);
         ++launches;
       };
       auto finish_part = [&](int j) {
         const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
-        launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis,
-                   plan->n, plan->p, K, plan->nt, plan->depth, a->output, a->layout, plan->phi_scale,
-                   reinterpret_cast<float *>(field), reinterpret_cast<float *>(potential), s, k0, k0 + kc);
-        launches += 2;
+        launch_unsort(plan->near, plan->tgt_inv, plan->nt, K, a->output, a->layout, reinterpret_cast<float *>(field),
+                      reinterpret_cast<float *>(potential), s, k0, k0 + kc);
+        ++launches;
         if (host_out) check(cudaEventRecord(plan->io_events[3 + 2 * j], s), "event");
       };
       // Copies out are enqueued after every kernel: a copy into pageable host
@@ -916,12 +918,18 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
         launch_gather_moments(moments + in_state * k0, a->moments_dtype, plan->src_inv, plan->ns, kc, plan->scale,
                               plan->mom, s, moments_paired(K), k0, K);
         ++launches;
-        if (j < early) near_part(j);
+        if (j < early) near_part(j, false);
       }
       launches += enqueue_far(plan, K, s, false);
+      // one L2P for all K states: combined with the near field of the early
+      // parts, far field alone for the later ones
+      launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis,
+                 plan->n, plan->p, K, plan->nt, plan->depth, a->output, a->layout, plan->phi_scale,
+                 reinterpret_cast<float *>(field), reinterpret_cast<float *>(potential), s, 0, K, bounds[early], false);
+      ++launches;
       for (int j = 0; j < early; ++j) finish_part(j);
       for (int j = early; j < n_parts; ++j) {
-        near_part(j);
+        near_part(j, true);
         finish_part(j);
       }
       check(cudaGetLastError(), "kernel launch");

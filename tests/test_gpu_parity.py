@@ -350,6 +350,37 @@ def test_host_io_state_parts_match_device_path(K, dtype, output):
     plan.close()
 
 
+@pytest.mark.parametrize("output", ["both", "potential", "field"])
+def test_host_io_state_parts_interleaved_layout(output):
+    # The same pipeline writing (phi, Hx, Hy, Hz) per target: the later
+    # parts add their near field onto the far field of one L2P; components
+    # that were not requested stay 0 as in the device-resident call.
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(91)
+    n, K = 4000, 64
+    x = rng.uniform(0, 1, (n, 3))
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, 4, max_states=K)
+    plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+    m = rng.normal(size=(K, n, 3)).astype(np.float32)
+    host = plan.evaluate(m, output=output, layout=cdfmm_b200.LAYOUT_INTERLEAVED)["H"]
+    dF = torch.zeros((K, n, 4), device="cuda")
+    plan.evaluate(torch.from_numpy(m).cuda(), output=output, layout=cdfmm_b200.LAYOUT_INTERLEAVED, field=dF)
+    torch.cuda.synchronize()
+    dev = dF.cpu().numpy()
+    assert host.shape == (K, n, 4)
+    for c in range(4):
+        wanted = (c == 0 and output != "field") or (c > 0 and output != "potential")
+        if wanted:
+            assert oracle.rel_l2(host[..., c], dev[..., c]) < 1e-6
+        else:
+            np.testing.assert_array_equal(host[..., c], 0.0)
+            np.testing.assert_array_equal(dev[..., c], 0.0)
+    plan.close()
+
+
 def test_python_uniform_fmm_zero_copy_device_io():
     # cdfmm.UniformFmm.evaluate_into takes CUDA arrays (torch tensors) in user
     # order and writes the results in place: no host copies.
