@@ -843,7 +843,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     // priorities alone let the later near-field parts delay the far field):
     //   gather 0, P2P 0, gather 1, P2P 1, ..., far field, L2P (all states),
     //   unsort 0, unsort 1, P2P 2 (adding to L2P's far field), unsort 2, ...
-    // (the first half of the P2P parts before the far field, while the later
+    // (the first n_parts / 2 P2P parts before the far field, while the later
     // moments are still being copied in; part j's results are copied out as
     // soon as its unsort is done, while later parts are computed).
     const bool parts = (host_in || host_out) && !timing && K >= 32 && n_chunks == 1 && plan->ns > 0 && plan->nt > 0;
@@ -858,7 +858,10 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
         if (k == K) break;
       }
       const int n_parts = static_cast<int>(bounds.size()) - 1;
-      const int early = (n_parts + 1) / 2; // P2P parts before the far field
+      // P2P parts before the far field: as many as run while the later
+      // moments are still being copied in (the far field, which needs them
+      // all, then starts as early as possible, and so do the copies out)
+      const int early = std::max(1, n_parts / 2);
       while (static_cast<int>(plan->io_events.size()) < 2 * n_parts + 2) {
         cudaEvent_t e;
         check(cudaEventCreateWithFlags(&e, cudaEventDisableTiming), "cudaEventCreate");
