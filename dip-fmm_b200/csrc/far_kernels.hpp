@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstddef>
 #include <cstdint>
+#include <vector>
 
 namespace cdfmm_b200 {
 
@@ -55,12 +56,23 @@ void launch_m2l_simt(const float *M, float *L, const float *T, const float *scal
 void configure_m2l_simt(size_t max_smem);
 int m2l_simt_beta_per_thread(int n);
 
-// list1 P2P near field; states [k_begin, k_end) of the K-state rows (default
-// all; k_begin a multiple of 8 when K >= 8).  accumulate (K > 1): add the
-// near field (phi times phi_scale) to the combined far-field results already
-// in `near` instead of writing it (1: phi and H, 2: phi only).
+// list1 P2P work units, one CTA each: (leaf, first sorted target, targets,
+// 0), at most kP2pUnitTargets targets per unit, so the targets of a dense
+// leaf spread over many SMs.  Units costing at least 4x the mean (targets x
+// neighbourhood sources) come first, heaviest first, so they start before
+// the light ones fill the machine; the rest keep the Morton order, in which
+// CTAs that run together share neighbourhood sources in L2.  Built once per
+// geometry from the host leaf offsets (n_leaves + 1 prefix sums each).
+constexpr int kP2pUnitTargets = 128;
+std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int depth);
+
+// list1 P2P near field over the work units; states [k_begin, k_end) of the
+// K-state rows (default all; k_begin a multiple of 8 when K >= 8).
+// accumulate (K > 1): add the near field (phi times phi_scale) to the
+// combined far-field results already in `near` instead of writing it (1: phi
+// and H, 2: phi only).
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
-                const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
+                const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1,
                 int accumulate = 0, float phi_scale = 1.0F);
 void configure_p2p(size_t max_smem);
@@ -68,8 +80,8 @@ void configure_p2p(size_t max_smem);
 // group, gpart[nt][p2p_grad_groups(K)] (normalised units, 1/(4 pi) applied).
 int p2p_grad_groups(int K);
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
-                     const int *tgt_off, const int *self_idx, int depth, int K, const float4 *W, float4 *gpart,
-                     cudaStream_t s);
+                     const int4 *work, int n_work, const int *self_idx, int depth, int K, const float4 *W,
+                     float4 *gpart, cudaStream_t s);
 // Far part (second derivatives of the leaf local expansions) plus the near
 // partial sums, scaled by inv_scale, written as out[user target][3].
 void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,

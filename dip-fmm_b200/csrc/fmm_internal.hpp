@@ -103,6 +103,8 @@ struct cdfmm_b200_plan {
   int *src_inv = nullptr;      // [ns] user -> sorted
   int *tgt_inv = nullptr;      // [nt]
   int *self_idx = nullptr;     // [nt] sorted target -> sorted source, -1 none
+  int4 *p2p_work = nullptr;    // [n_p2p_work] list1 work units (leaf, first target, targets, 0)
+  int n_p2p_work = 0;
 
   // operators (device)
   int *m2m_off = nullptr, *m2m_pair = nullptr; // pair = g | (in << 16)

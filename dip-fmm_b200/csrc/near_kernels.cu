@@ -17,6 +17,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <vector>
 
 #include "far_kernels.hpp"
 #include "kernels.cuh"
@@ -103,27 +104,28 @@ __device__ __forceinline__ void pair_k1(const float4 &ti, int self, const float4
 }
 
 constexpr int kK1Chunk = 1024;
-constexpr int kK1TargetChunk = 128;
+constexpr int kK1TargetChunk = kP2pUnitTargets;
 
-// K = 1: one CTA per target leaf, all neighbour sources staged in shared
-// memory; each warp owns 4 targets at a time, lanes stride over the staged
-// sources and the partial sums are combined with warp shuffles.
+// K = 1: one CTA per work unit (up to 128 targets of one leaf), the
+// neighbourhood sources staged in shared memory kK1Chunk at a time; each warp
+// owns 4 targets at a time, lanes stride over the staged sources and the
+// partial sums are combined with warp shuffles.
 template <bool PHI>
 __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ src_rel,
                                                      const float4 *__restrict__ mom,
                                                      const int *__restrict__ src_off,
                                                      const float4 *__restrict__ tgt_rel,
-                                                     const int *__restrict__ tgt_off,
+                                                     const int4 *__restrict__ work,
                                                      const int *__restrict__ self_idx, int depth,
                                                      float4 *__restrict__ near) {
   __shared__ float4 sPos[kK1Chunk];
   __shared__ float4 sMom[kK1Chunk];
   __shared__ float4 sAcc[kK1TargetChunk];
   __shared__ Neighbours nb;
-  const int leaf = blockIdx.x;
-  const int t0 = tgt_off[leaf];
-  const int t1 = tgt_off[leaf + 1];
-  if (t0 == t1) return;
+  const int4 unit = work[blockIdx.x];
+  const int leaf = unit.x;
+  const int t0 = unit.y;
+  const int t1 = unit.y + unit.z;
   if (threadIdx.x < 32) build_neighbours(nb, leaf, depth, src_off, threadIdx.x);
   __syncthreads();
   const int total = nb.prefix[nb.count];
@@ -190,19 +192,20 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
   }
 }
 
-// K > 1.  One CTA per target leaf.  Work items are (target, group of KG
-// states); a lane owns one item and computes a pair's geometry once --
+// K > 1.  One CTA per work unit (up to 128 targets of one leaf).  Work
+// items are (target, group of KG states); a lane owns one item and computes
+// a pair's geometry once --
 // r, v = 1/|r|^3, u = 3 r / |r|^5, w = |r|^2 / 3 -- applying it to its KG
 // states:
 //   s = m.u,  phi += s w,  H += s r - v m          (10 FP ops per pair-state)
 // A self pair gets u = v = w = 0; a coincident non-self pair gives u = NaN
 // (0 * inf), hence NaN results, as in the reference.
 //
-// Load balance: the items of a leaf are processed in rounds of 256 lanes; a
+// Load balance: the items of a unit are processed in rounds of 256 lanes; a
 // round gives each of its r items F = 2^j <= 8 lanes that split the sources
 // (lane f takes sources f, f + F, ...) and are summed with warp shuffles at
 // the end of the round.  Each round takes the F (and r = min(remaining,
-// 256 / F)) that keeps the most lanes busy, so a leaf whose item count is
+// 256 / F)) that keeps the most lanes busy, so a unit whose item count is
 // not a multiple of 256 -- fewer than 32 targets, or a narrow state window
 // -- does not leave lanes idle.
 //
@@ -363,7 +366,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
                                                               const float4 *__restrict__ mom,
                                                               const int *__restrict__ src_off,
                                                               const float4 *__restrict__ tgt_rel,
-                                                              const int *__restrict__ tgt_off,
+                                                              const int4 *__restrict__ work,
                                                               const int *__restrict__ self_idx, int depth, int K,
                                                               float4 *__restrict__ near,
                                                               const float4 *__restrict__ W, int k_begin,
@@ -375,10 +378,10 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
   int *sIdx = reinterpret_cast<int *>(sPos + kNeighbourCap);      // [kNeighbourCap]
   float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [kBufs][kChunkB][Kr <= kStateBlock + 9]
   __shared__ Neighbours nb;
-  const int leaf = blockIdx.x;
-  const int t0 = tgt_off[leaf];
-  const int nt = tgt_off[leaf + 1] - t0;
-  if (nt == 0) return;
+  const int4 unit = work[blockIdx.x];
+  const int leaf = unit.x;
+  const int t0 = unit.y;
+  const int nt = unit.z;
   if (threadIdx.x < 32) build_neighbours(nb, leaf, depth, src_off, threadIdx.x);
   __syncthreads();
   const int total = nb.prefix[nb.count];
@@ -692,18 +695,18 @@ template <int KG> size_t p2p_kb_smem_bytes(int K) {
 
 template <int KG, bool PAIRED>
 void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
-               const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
+               const int4 *work, int n_work, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
                cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale) {
-  const int leaves = 1 << (3 * depth);
+  if (n_work == 0) return;
   const size_t smem = p2p_kb_smem_bytes<KG>(K);
   if (mode == 1)
-    p2p_kb_kernel<KG, 1, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
+    p2p_kb_kernel<KG, 1, PAIRED><<<n_work, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx,
                                                                   depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
   else if (mode == 2)
-    p2p_kb_kernel<KG, 2, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
+    p2p_kb_kernel<KG, 2, PAIRED><<<n_work, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx,
                                                                   depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
   else
-    p2p_kb_kernel<KG, 0, PAIRED><<<leaves, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx,
+    p2p_kb_kernel<KG, 0, PAIRED><<<n_work, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx,
                                                                   depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
 }
 
@@ -711,31 +714,69 @@ void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, con
 // paired; K = 2, 3: groups of 4, plain layout.  (Groups of 16 were measured
 // slower at K = 64: the accumulators no longer fit the register budget.)
 void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
-                   const int *tgt_off, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
+                   const int4 *work, int n_work, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
                    cudaStream_t s, int k_begin = 0, int k_end = -1, int accumulate = 0, float acc_phi_scale = 1.0F) {
   if (k_end < 0) k_end = K;
   if (K >= 8)
-    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
   else if (K >= 4)
-    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
   else
-    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
 }
 
 } // namespace
 
+std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int depth) {
+  const int side = 1 << depth;
+  const int leaves = 1 << (3 * depth);
+  std::vector<int4> units;
+  std::vector<long long> cost;
+  long long total = 0;
+  for (int m = 0; m < leaves; ++m) {
+    const int nt = tgt_off[m + 1] - tgt_off[m];
+    if (nt == 0) continue;
+    int ix, iy, iz;
+    demorton3(static_cast<uint32_t>(m), ix, iy, iz);
+    long long sources = 0;
+    for (int z = std::max(iz - 1, 0); z <= std::min(iz + 1, side - 1); ++z)
+      for (int y = std::max(iy - 1, 0); y <= std::min(iy + 1, side - 1); ++y)
+        for (int x = std::max(ix - 1, 0); x <= std::min(ix + 1, side - 1); ++x) {
+          const uint32_t b = morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y), static_cast<uint32_t>(z));
+          sources += src_off[b + 1] - src_off[b];
+        }
+    for (int t = 0; t < nt; t += kP2pUnitTargets) {
+      const int tn = std::min(kP2pUnitTargets, nt - t);
+      units.push_back(make_int4(m, tgt_off[m] + t, tn, 0));
+      cost.push_back(static_cast<long long>(tn) * sources);
+      total += cost.back();
+    }
+  }
+  const long long n = static_cast<long long>(units.size());
+  std::vector<int> order(units.size());
+  for (size_t u = 0; u < order.size(); ++u) order[u] = static_cast<int>(u);
+  // heavy: cost >= 4 x mean
+  const auto heavy_end = std::stable_partition(order.begin(), order.end(),
+                                               [&](int u) { return cost[static_cast<size_t>(u)] * n >= 4 * total; });
+  std::stable_sort(order.begin(), heavy_end,
+                   [&](int a, int b) { return cost[static_cast<size_t>(a)] > cost[static_cast<size_t>(b)]; });
+  std::vector<int4> out(units.size());
+  for (size_t u = 0; u < order.size(); ++u) out[u] = units[static_cast<size_t>(order[u])];
+  return out;
+}
+
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
-                const float4 *tgt_rel, const int *tgt_off, const int *self_idx, int depth, int K,
+                const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end, int accumulate,
                 float phi_scale) {
-  const int leaves = 1 << (3 * depth);
+  if (n_work == 0) return;
   if (K == 1) {
     if (want_phi)
-      p2p_k1_kernel<true><<<leaves, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, near);
+      p2p_k1_kernel<true><<<n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, near);
     else
-      p2p_k1_kernel<false><<<leaves, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, near);
+      p2p_k1_kernel<false><<<n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, near);
   } else {
-    launch_kb_any(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
+    launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
                   k_begin, k_end, accumulate, phi_scale);
   }
 }
@@ -743,9 +784,9 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
 int p2p_grad_groups(int K) { return K >= 8 ? (K + 7) / 8 : (K + 3) / 4; }
 
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
-                     const int *tgt_off, const int *self_idx, int depth, int K, const float4 *W, float4 *gpart,
+                     const int4 *work, int n_work, const int *self_idx, int depth, int K, const float4 *W, float4 *gpart,
                      cudaStream_t s) {
-  launch_kb_any(src_rel, mom, src_off, tgt_rel, tgt_off, self_idx, depth, K, 2, gpart, W, s);
+  launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, 2, gpart, W, s);
 }
 
 void configure_p2p(size_t max_smem) {

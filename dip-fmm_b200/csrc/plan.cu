@@ -93,7 +93,7 @@ template <typename T> T *grow(T *&buf, size_t &have, size_t need, const char *wh
 void free_plan(cdfmm_b200_plan *p) {
   if (p == nullptr) return;
   void *ptrs[] = {p->src_rel, p->tgt_rel, p->src_off, p->tgt_off, p->src_perm, p->tgt_perm, p->src_inv, p->tgt_inv,
-                  p->self_idx, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
+                  p->self_idx, p->p2p_work, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
                   p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad};
@@ -307,6 +307,14 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     upload(plan->tgt_off, desc->leaf_target_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
     upload(plan->src_perm, desc->source_permutation, static_cast<size_t>(plan->ns), h2d);
     upload(plan->tgt_perm, desc->target_permutation, static_cast<size_t>(plan->nt), h2d);
+    {
+      const std::vector<int4> work = p2p_work_units(desc->leaf_source_offsets, desc->leaf_target_offsets, plan->depth);
+      plan->n_p2p_work = static_cast<int>(work.size());
+      if (!work.empty()) {
+        plan->p2p_work = dalloc<int4>(work.size(), bytes);
+        upload(plan->p2p_work, work.data(), work.size(), h2d);
+      }
+    }
     {
       std::vector<int> inv(static_cast<size_t>(std::max(plan->ns, plan->nt)), -1);
       for (int j = 0; j < plan->ns; ++j) {
@@ -755,7 +763,7 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
     check(cudaStreamWaitEvent(fs, plan->ev_fork, 0), "wait");
   }
   if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
-  launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
+  launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
              plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi, plan->near, ns);
   ++launches;
   if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
@@ -876,7 +884,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       // ones run after the (single) L2P and add theirs onto its far field.
       auto near_part = [&](int j, bool accumulate) {
         const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
-        launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
+        launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
                    plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc,
                    accumulate ? ((a->output & CDFMM_B200_OUTPUT_FIELD) != 0u ? 1 : 2) : 0, plan->phi_scale);
         ++launches;
@@ -1178,7 +1186,7 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
       launch_gather_moments(weights, 0, plan->tgt_inv, plan->nt, K, 1.0, W, s, false);
       if (!reuse) enqueue_far(plan, K, s, false);
       plan->stats.backward_reused_forward = reuse ? 1 : 0;
-      launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->tgt_off,
+      launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
                       plan->has_self ? plan->self_idx : nullptr, plan->depth, K, W, gpart, s);
       launch_l2p_grad(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, W, gpart, G, plan->n, plan->p, K,
                       plan->nt, plan->depth, static_cast<float>(1.0 / plan->scale), out, s);
