@@ -84,14 +84,16 @@ __device__ inline void stage_source(const Neighbours &nb, int g, const float4 *s
   pos = make_float4(d.x + nb.sx[b], d.y + nb.sy[b], d.z + nb.sz[b], __int_as_float(j));
 }
 
-template <bool PHI>
+// SELF: the source may be a target's self source (compared by sorted index;
+// the self pair gets r2 = inf, hence no contribution).
+template <bool PHI, bool SELF>
 __device__ __forceinline__ void pair_k1(const float4 &ti, int self, const float4 &s, const float4 &m,
                                         float &phi, float &hx, float &hy, float &hz) {
   const float dx = ti.x - s.x;
   const float dy = ti.y - s.y;
   const float dz = ti.z - s.z;
   float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  r2 = (__float_as_int(s.w) == self) ? __int_as_float(0x7f800000) : r2;
+  if (SELF) r2 = (__float_as_int(s.w) == self) ? __int_as_float(0x7f800000) : r2;
   const float rinv = rsqrtf(r2);
   const float rinv2 = rinv * rinv;
   const float rinv3 = rinv2 * rinv;
@@ -106,10 +108,27 @@ __device__ __forceinline__ void pair_k1(const float4 &ti, int self, const float4
 constexpr int kK1Chunk = 1024;
 constexpr int kK1TargetChunk = kP2pUnitTargets;
 
+// Staged sources [qa, qb) against a warp's 4 targets, lane l taking qa + l,
+// qa + l + 32, ...
+template <bool PHI, bool SELF>
+__device__ __forceinline__ void k1_segment(const float4 (&ti)[4], const int (&self)[4], const float4 *sPos,
+                                           const float4 *sMom, int qa, int qb, int lane, float (&acc)[4][4]) {
+  for (int q = qa + lane; q < qb; q += 32) {
+    const float4 s = sPos[q];
+    const float4 m = sMom[q];
+#pragma unroll
+    for (int u = 0; u < 4; ++u)
+      pair_k1<PHI, SELF>(ti[u], self[u], s, m, acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+  }
+}
+
 // K = 1: one CTA per work unit (up to 128 targets of one leaf), the
 // neighbourhood sources staged in shared memory kK1Chunk at a time; each warp
 // owns 4 targets at a time, lanes stride over the staged sources and the
-// partial sums are combined with warp shuffles.
+// partial sums are combined with warp shuffles.  Only the staged positions
+// between the lowest and highest self source of the unit's targets are
+// compared against the self indices (the unit's own leaf, when sources and
+// targets are the same points).
 template <bool PHI>
 __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ src_rel,
                                                      const float4 *__restrict__ mom,
@@ -122,11 +141,28 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
   __shared__ float4 sMom[kK1Chunk];
   __shared__ float4 sAcc[kK1TargetChunk];
   __shared__ Neighbours nb;
+  __shared__ int sSelf[2]; // staged positions [lo, hi] of the unit's self sources
   const int4 unit = work[blockIdx.x];
   const int leaf = unit.x;
   const int t0 = unit.y;
   const int t1 = unit.y + unit.z;
   if (threadIdx.x < 32) build_neighbours(nb, leaf, depth, src_off, threadIdx.x);
+  if (threadIdx.x == 32) {
+    sSelf[0] = 0x7fffffff;
+    sSelf[1] = -1;
+  }
+  __syncthreads();
+  if (self_idx != nullptr)
+    for (int i = t0 + static_cast<int>(threadIdx.x); i < t1; i += blockDim.x) {
+      const int j = self_idx[i];
+      for (int c = 0; j >= 0 && c < nb.count; ++c) {
+        const int off = j - nb.begin[c];
+        if (off >= 0 && off < nb.prefix[c + 1] - nb.prefix[c]) {
+          atomicMin(&sSelf[0], nb.prefix[c] + off);
+          atomicMax(&sSelf[1], nb.prefix[c] + off);
+        }
+      }
+    }
   __syncthreads();
   const int total = nb.prefix[nb.count];
   const int warp = threadIdx.x >> 5;
@@ -156,12 +192,12 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
           self[u] = self_idx != nullptr ? self_idx[i] : -1;
           acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0F;
         }
-        for (int q = lane; q < sn; q += 32) {
-          const float4 s = sPos[q];
-          const float4 m = sMom[q];
-#pragma unroll
-          for (int u = 0; u < 4; ++u) pair_k1<PHI>(ti[u], self[u], s, m, acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
-        }
+        // [0, qa) and [qb, sn) hold no self source of these targets
+        const int qa = min(max(sSelf[0] - sc, 0), sn);
+        const int qb = max(min(sSelf[1] + 1 - sc, sn), qa);
+        k1_segment<PHI, false>(ti, self, sPos, sMom, 0, qa, lane, acc);
+        k1_segment<PHI, true>(ti, self, sPos, sMom, qa, qb, lane, acc);
+        k1_segment<PHI, false>(ti, self, sPos, sMom, qb, sn, lane, acc);
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
