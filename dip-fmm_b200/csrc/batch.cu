@@ -100,7 +100,9 @@ int cdfmm_b200_batch_create(cdfmm_b200_plan *const *plans, const cdfmm_b200_eval
     cdfmm_b200_eval_args a = args[i];
     a.stream = p->stream;
     a.synchronize = 0;
+    p->in_batch = true; // the wide P2P units: other geometries run beside a long unit
     const int rc = cdfmm_b200_evaluate(p, &a);
+    p->in_batch = false;
     if (rc != CDFMM_B200_OK) {
       failed_rc = rc;
       failed_msg = std::string("capture of plan ") + std::to_string(i) + ": " + cdfmm_b200_last_error(p);

@@ -57,22 +57,33 @@ void configure_m2l_simt(size_t max_smem);
 int m2l_simt_beta_per_thread(int n);
 
 // list1 P2P work units, one CTA each: (leaf, first sorted target, targets,
-// 0), at most kP2pUnitTargets targets per unit, so the targets of a dense
-// leaf spread over many SMs.  Units costing at least 4x the mean (targets x
-// neighbourhood sources) come first, heaviest first, so they start before
-// the light ones fill the machine; the rest keep the Morton order, in which
-// CTAs that run together share neighbourhood sources in L2.  Built once per
-// geometry from the host leaf offsets (n_leaves + 1 prefix sums each).
+// 0), so the targets of a dense leaf spread over many SMs.  A unit holds at
+// most kP2pUnitTargets targets, and fewer (a multiple of kP2pUnitMinTargets,
+// at least that) where its cost -- targets x neighbourhood sources -- would
+// exceed the total over kP2pUnitsPerSm x sm_count units: one CTA shares its
+// SM with several others, so a unit above that cap would outlast the rest
+// of the launch.  Units costing at least 4x the mean come first, heaviest
+// first, so they start before the light ones fill the machine; the rest
+// keep the Morton order, in which CTAs that run together share
+// neighbourhood sources in L2 (a uniform geometry's units are its leaves, in
+// Morton order).  Built once per geometry from the host leaf offsets
+// (n_leaves + 1 prefix sums each); cap_cost = false keeps every unit at
+// kP2pUnitTargets targets.
 constexpr int kP2pUnitTargets = 128;
-std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int depth);
+constexpr int kP2pUnitMinTargets = 16;
+constexpr int kP2pUnitsPerSm = 20;
+std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int depth, int sm_count, bool cap_cost);
 
 // list1 P2P near field over the work units; states [k_begin, k_end) of the
 // K-state rows (default all; k_begin a multiple of 8 when K >= 8).
 // accumulate (K > 1): add the near field (phi times phi_scale) to the
 // combined far-field results already in `near` instead of writing it (1: phi
 // and H, 2: phi only).
+// leaf_self: per leaf, the lowest and highest self source of its targets
+// (read when self_idx is given).
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
-                const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx, int depth, int K,
+                const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
+                const int2 *leaf_self, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1,
                 int accumulate = 0, float phi_scale = 1.0F);
 void configure_p2p(size_t max_smem);

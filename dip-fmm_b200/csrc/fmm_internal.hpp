@@ -103,8 +103,16 @@ struct cdfmm_b200_plan {
   int *src_inv = nullptr;      // [ns] user -> sorted
   int *tgt_inv = nullptr;      // [nt]
   int *self_idx = nullptr;     // [nt] sorted target -> sorted source, -1 none
+  int2 *leaf_self = nullptr;   // [n_leaves] lowest, highest self source of each leaf's targets ((INT_MAX, -1): none)
   int4 *p2p_work = nullptr;    // [n_p2p_work] list1 work units (leaf, first target, targets, 0)
   int n_p2p_work = 0;
+  // Units of up to 128 targets without the per-unit cost cap (the same array
+  // as p2p_work when no unit was capped): used while the plan is captured
+  // into a batch graph, where the other geometries' work runs beside a long
+  // unit and the cap's extra staging only costs time.
+  int4 *p2p_work_wide = nullptr;
+  int n_p2p_work_wide = 0;
+  bool in_batch = false;
 
   // operators (device)
   int *m2m_off = nullptr, *m2m_pair = nullptr; // pair = g | (in << 16)

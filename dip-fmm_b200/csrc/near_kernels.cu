@@ -84,85 +84,110 @@ __device__ inline void stage_source(const Neighbours &nb, int g, const float4 *s
   pos = make_float4(d.x + nb.sx[b], d.y + nb.sy[b], d.z + nb.sz[b], __int_as_float(j));
 }
 
-// SELF: the source may be a target's self source (compared by sorted index;
-// the self pair gets r2 = inf, hence no contribution).
+// One staged source pair (components .x, .y: two sources) against one
+// target in packed FP32x2 arithmetic.  With d = source - target (= -r) and
+// v = 1/|r|^3 the pair adds
+//   P += (m.d) v                          (phi = -P)
+//   G += v (m - 3 (m.d) / |d|^2 d)        (H = -G)
+// so the target's coordinates enter negated and no operand needs a sign
+// flip inside the loop.  SELF: the sources' sorted indices are compared with
+// the target's self index; the self pair gets 1/|r| = 0 (no contribution).
+// A coincident non-self pair gives 1/|r| = inf and NaN, as in the reference.
 template <bool PHI, bool SELF>
-__device__ __forceinline__ void pair_k1(const float4 &ti, int self, const float4 &s, const float4 &m,
-                                        float &phi, float &hx, float &hy, float &hz) {
-  const float dx = ti.x - s.x;
-  const float dy = ti.y - s.y;
-  const float dz = ti.z - s.z;
-  float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-  if (SELF) r2 = (__float_as_int(s.w) == self) ? __int_as_float(0x7f800000) : r2;
-  const float rinv = rsqrtf(r2);
-  const float rinv2 = rinv * rinv;
-  const float rinv3 = rinv2 * rinv;
-  const float mr = fmaf(m.x, dx, fmaf(m.y, dy, m.z * dz));
-  if (PHI) phi = fmaf(mr, rinv3, phi);
-  const float a = 3.0F * mr * rinv2;
-  hx = fmaf(rinv3, fmaf(a, dx, -m.x), hx);
-  hy = fmaf(rinv3, fmaf(a, dy, -m.y), hy);
-  hz = fmaf(rinv3, fmaf(a, dz, -m.z), hz);
+__device__ __forceinline__ void pair_k1_x2(const float2 &ntx, const float2 &nty, const float2 &ntz, int self,
+                                           const float4 &pxy, const float4 &pzj, const float4 &mxy,
+                                           const float2 &mz, float2 (&acc)[4]) {
+  const float2 dx = __fadd2_rn(make_float2(pxy.x, pxy.y), ntx);
+  const float2 dy = __fadd2_rn(make_float2(pxy.z, pxy.w), nty);
+  const float2 dz = __fadd2_rn(make_float2(pzj.x, pzj.y), ntz);
+  const float2 r2 = __ffma2_rn(dx, dx, __ffma2_rn(dy, dy, __fmul2_rn(dz, dz)));
+  float2 rinv = make_float2(rsqrtf(r2.x), rsqrtf(r2.y));
+  if (SELF) {
+    rinv.x = __float_as_int(pzj.z) == self ? 0.0F : rinv.x;
+    rinv.y = __float_as_int(pzj.w) == self ? 0.0F : rinv.y;
+  }
+  const float2 rinv2 = __fmul2_rn(rinv, rinv);
+  const float2 rinv3 = __fmul2_rn(rinv2, rinv);
+  const float2 mx = make_float2(mxy.x, mxy.y), my = make_float2(mxy.z, mxy.w);
+  const float2 md = __ffma2_rn(mx, dx, __ffma2_rn(my, dy, __fmul2_rn(mz, dz)));
+  if (PHI) acc[0] = __ffma2_rn(md, rinv3, acc[0]);
+  const float2 nb = __fmul2_rn(__fmul2_rn(md, make_float2(-3.0F, -3.0F)), rinv2);
+  acc[1] = __ffma2_rn(rinv3, __ffma2_rn(nb, dx, mx), acc[1]);
+  acc[2] = __ffma2_rn(rinv3, __ffma2_rn(nb, dy, my), acc[2]);
+  acc[3] = __ffma2_rn(rinv3, __ffma2_rn(nb, dz, mz), acc[3]);
 }
 
-constexpr int kK1Chunk = 1024;
+constexpr int kK1Chunk = 1024;               // staged sources per pass
+constexpr int kK1Pairs = kK1Chunk / 2;
 constexpr int kK1TargetChunk = kP2pUnitTargets;
 
-// Staged sources [qa, qb) against a warp's 4 targets, lane l taking qa + l,
-// qa + l + 32, ...
+// Staged source pairs [pa, pb) against a warp's 4 targets, lane l taking
+// pa + l, pa + l + 32, ...
 template <bool PHI, bool SELF>
-__device__ __forceinline__ void k1_segment(const float4 (&ti)[4], const int (&self)[4], const float4 *sPos,
-                                           const float4 *sMom, int qa, int qb, int lane, float (&acc)[4][4]) {
-  for (int q = qa + lane; q < qb; q += 32) {
-    const float4 s = sPos[q];
-    const float4 m = sMom[q];
+__device__ __forceinline__ void k1_segment(const float2 (&nt)[4][3], const int (&self)[4], const float4 *sPxy,
+                                           const float4 *sPzj, const float4 *sMxy, const float2 *sMz, int pa,
+                                           int pb, int lane, float2 (&acc)[4][4]) {
+  for (int q = pa + lane; q < pb; q += 32) {
+    const float4 pxy = sPxy[q];
+    const float4 pzj = sPzj[q];
+    const float4 mxy = sMxy[q];
+    const float2 mz = sMz[q];
 #pragma unroll
     for (int u = 0; u < 4; ++u)
-      pair_k1<PHI, SELF>(ti[u], self[u], s, m, acc[u][0], acc[u][1], acc[u][2], acc[u][3]);
+      pair_k1_x2<PHI, SELF>(nt[u][0], nt[u][1], nt[u][2], self[u], pxy, pzj, mxy, mz, acc[u]);
   }
 }
 
 // K = 1: one CTA per work unit (up to 128 targets of one leaf), the
-// neighbourhood sources staged in shared memory kK1Chunk at a time; each warp
-// owns 4 targets at a time, lanes stride over the staged sources and the
-// partial sums are combined with warp shuffles.  Only the staged positions
-// between the lowest and highest self source of the unit's targets are
-// compared against the self indices (the unit's own leaf, when sources and
-// targets are the same points).
+// neighbourhood sources staged in shared memory kK1Chunk at a time as pairs
+// of consecutive sources in structure-of-arrays form (x0 x1 y0 y1 | z0 z1 j0
+// j1 | mx0 mx1 my0 my1 | mz0 mz1; an odd chunk is padded with a zero moment
+// 1e18 away), so each lane reads two sources' operands ready for packed
+// FP32x2 arithmetic; each warp owns 4 targets at a time, lanes stride over
+// the staged pairs and the partial sums are combined with warp shuffles.
+// Only the staged positions of the sources between the lowest and highest
+// self source of the leaf's targets are compared against the self indices
+// (the own leaf's, when sources and targets are the same points).
 template <bool PHI>
 __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ src_rel,
                                                      const float4 *__restrict__ mom,
                                                      const int *__restrict__ src_off,
                                                      const float4 *__restrict__ tgt_rel,
                                                      const int4 *__restrict__ work,
-                                                     const int *__restrict__ self_idx, int depth,
+                                                     const int *__restrict__ self_idx,
+                                                     const int2 *__restrict__ leaf_self, int depth,
                                                      float4 *__restrict__ near) {
-  __shared__ float4 sPos[kK1Chunk];
-  __shared__ float4 sMom[kK1Chunk];
+  __shared__ float4 sPxy[kK1Pairs];
+  __shared__ float4 sPzj[kK1Pairs];
+  __shared__ float4 sMxy[kK1Pairs];
+  __shared__ float2 sMz[kK1Pairs];
   __shared__ float4 sAcc[kK1TargetChunk];
   __shared__ Neighbours nb;
-  __shared__ int sSelf[2]; // staged positions [lo, hi] of the unit's self sources
+  __shared__ int sSelf[2]; // staged positions [lo, hi] of the leaf's self-source range
   const int4 unit = work[blockIdx.x];
   const int leaf = unit.x;
   const int t0 = unit.y;
   const int t1 = unit.y + unit.z;
   if (threadIdx.x < 32) build_neighbours(nb, leaf, depth, src_off, threadIdx.x);
-  if (threadIdx.x == 32) {
-    sSelf[0] = 0x7fffffff;
-    sSelf[1] = -1;
-  }
   __syncthreads();
-  if (self_idx != nullptr)
-    for (int i = t0 + static_cast<int>(threadIdx.x); i < t1; i += blockDim.x) {
-      const int j = self_idx[i];
-      for (int c = 0; j >= 0 && c < nb.count; ++c) {
-        const int off = j - nb.begin[c];
-        if (off >= 0 && off < nb.prefix[c + 1] - nb.prefix[c]) {
-          atomicMin(&sSelf[0], nb.prefix[c] + off);
-          atomicMax(&sSelf[1], nb.prefix[c] + off);
+  if (threadIdx.x == 0) {
+    // staged positions of the leaf's self-source range (the whole leaf's, so
+    // a target's sum does not depend on how its leaf is cut into units)
+    int lo = 0x7fffffff, hi = -1;
+    if (self_idx != nullptr) {
+      const int2 r = leaf_self[leaf];
+      for (int c = 0; c < nb.count; ++c) {
+        const int b = nb.begin[c], len = nb.prefix[c + 1] - nb.prefix[c];
+        const int a0 = max(r.x, b), a1 = min(r.y, b + len - 1);
+        if (a0 <= a1) {
+          lo = min(lo, nb.prefix[c] + a0 - b);
+          hi = max(hi, nb.prefix[c] + a1 - b);
         }
       }
     }
+    sSelf[0] = lo;
+    sSelf[1] = hi;
+  }
   __syncthreads();
   const int total = nb.prefix[nb.count];
   const int warp = threadIdx.x >> 5;
@@ -172,38 +197,54 @@ __global__ void __launch_bounds__(128) p2p_k1_kernel(const float4 *__restrict__ 
     for (int q = threadIdx.x; q < tn; q += blockDim.x) sAcc[q] = make_float4(0, 0, 0, 0);
     for (int sc = 0; sc < total; sc += kK1Chunk) {
       const int sn = min(kK1Chunk, total - sc);
+      const int np = (sn + 1) / 2;
       __syncthreads();
-      for (int q = threadIdx.x; q < sn; q += blockDim.x) {
-        float4 pos;
+      for (int q = threadIdx.x; q < np; q += blockDim.x) {
+        float4 p0, p1 = make_float4(1.0e18F, 1.0e18F, 1.0e18F, __int_as_float(-1));
+        float4 m0, m1 = make_float4(0.0F, 0.0F, 0.0F, 0.0F);
         int j;
-        stage_source(nb, sc + q, src_rel, pos, j);
-        sPos[q] = pos;
-        sMom[q] = mom[j];
+        stage_source(nb, sc + 2 * q, src_rel, p0, j);
+        m0 = mom[j];
+        if (2 * q + 1 < sn) {
+          stage_source(nb, sc + 2 * q + 1, src_rel, p1, j);
+          m1 = mom[j];
+        }
+        sPxy[q] = make_float4(p0.x, p1.x, p0.y, p1.y);
+        sPzj[q] = make_float4(p0.z, p1.z, p0.w, p1.w);
+        sMxy[q] = make_float4(m0.x, m1.x, m0.y, m1.y);
+        sMz[q] = make_float2(m0.z, m1.z);
       }
       __syncthreads();
+      // pairs [0, pa) and [pb, np) hold no self source of the leaf's targets
+      const int qa = min(max(sSelf[0] - sc, 0), sn);
+      const int qb = max(min(sSelf[1] + 1 - sc, sn), qa);
+      const int pa = qa / 2, pb = max((qb + 1) / 2, pa);
       for (int tb = warp * 4; tb < tn; tb += 16) {
-        float4 ti[4];
+        float2 nt[4][3];
         int self[4];
-        float acc[4][4];
+        float2 acc2[4][4];
 #pragma unroll
         for (int u = 0; u < 4; ++u) {
           const int i = tc + min(tb + u, tn - 1);
-          ti[u] = tgt_rel[i];
+          const float4 t = tgt_rel[i];
+          nt[u][0] = make_float2(-t.x, -t.x);
+          nt[u][1] = make_float2(-t.y, -t.y);
+          nt[u][2] = make_float2(-t.z, -t.z);
           self[u] = self_idx != nullptr ? self_idx[i] : -1;
-          acc[u][0] = acc[u][1] = acc[u][2] = acc[u][3] = 0.0F;
+          acc2[u][0] = acc2[u][1] = acc2[u][2] = acc2[u][3] = make_float2(0.0F, 0.0F);
         }
-        // [0, qa) and [qb, sn) hold no self source of these targets
-        const int qa = min(max(sSelf[0] - sc, 0), sn);
-        const int qb = max(min(sSelf[1] + 1 - sc, sn), qa);
-        k1_segment<PHI, false>(ti, self, sPos, sMom, 0, qa, lane, acc);
-        k1_segment<PHI, true>(ti, self, sPos, sMom, qa, qb, lane, acc);
-        k1_segment<PHI, false>(ti, self, sPos, sMom, qb, sn, lane, acc);
+        k1_segment<PHI, false>(nt, self, sPxy, sPzj, sMxy, sMz, 0, pa, lane, acc2);
+        k1_segment<PHI, true>(nt, self, sPxy, sPzj, sMxy, sMz, pa, pb, lane, acc2);
+        k1_segment<PHI, false>(nt, self, sPxy, sPzj, sMxy, sMz, pb, np, lane, acc2);
+        float acc[4][4];
 #pragma unroll
         for (int u = 0; u < 4; ++u)
 #pragma unroll
-          for (int c = 0; c < 4; ++c)
+          for (int c = 0; c < 4; ++c) {
+            acc[u][c] = -(acc2[u][c].x + acc2[u][c].y); // phi = -P, H = -G
 #pragma unroll
             for (int o = 16; o > 0; o >>= 1) acc[u][c] += __shfl_xor_sync(0xffffffffu, acc[u][c], o);
+          }
         if (lane == 0) {
 #pragma unroll
           for (int u = 0; u < 4; ++u) {
@@ -763,29 +804,41 @@ void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off,
 
 } // namespace
 
-std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int depth) {
+std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int depth, int sm_count, bool cap_cost) {
   const int side = 1 << depth;
   const int leaves = 1 << (3 * depth);
-  std::vector<int4> units;
-  std::vector<long long> cost;
+  std::vector<long long> sources(static_cast<size_t>(leaves), 0);
   long long total = 0;
   for (int m = 0; m < leaves; ++m) {
     const int nt = tgt_off[m + 1] - tgt_off[m];
     if (nt == 0) continue;
     int ix, iy, iz;
     demorton3(static_cast<uint32_t>(m), ix, iy, iz);
-    long long sources = 0;
+    long long sn = 0;
     for (int z = std::max(iz - 1, 0); z <= std::min(iz + 1, side - 1); ++z)
       for (int y = std::max(iy - 1, 0); y <= std::min(iy + 1, side - 1); ++y)
         for (int x = std::max(ix - 1, 0); x <= std::min(ix + 1, side - 1); ++x) {
           const uint32_t b = morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y), static_cast<uint32_t>(z));
-          sources += src_off[b + 1] - src_off[b];
+          sn += src_off[b + 1] - src_off[b];
         }
-    for (int t = 0; t < nt; t += kP2pUnitTargets) {
-      const int tn = std::min(kP2pUnitTargets, nt - t);
+    sources[static_cast<size_t>(m)] = sn;
+    total += nt * sn;
+  }
+  // unit cost cap: total / (kP2pUnitsPerSm x SMs) pairs
+  const long long cap = std::max(1LL, total / (static_cast<long long>(kP2pUnitsPerSm) * std::max(sm_count, 1)));
+  std::vector<int4> units;
+  std::vector<long long> cost;
+  for (int m = 0; m < leaves; ++m) {
+    const int nt = tgt_off[m + 1] - tgt_off[m];
+    if (nt == 0) continue;
+    const long long sn = sources[static_cast<size_t>(m)];
+    int width = kP2pUnitTargets;
+    if (cap_cost && sn > 0 && width * sn > cap)
+      width = static_cast<int>(std::max<long long>(kP2pUnitMinTargets, cap / sn / kP2pUnitMinTargets * kP2pUnitMinTargets));
+    for (int t = 0; t < nt; t += width) {
+      const int tn = std::min(width, nt - t);
       units.push_back(make_int4(m, tgt_off[m] + t, tn, 0));
-      cost.push_back(static_cast<long long>(tn) * sources);
-      total += cost.back();
+      cost.push_back(static_cast<long long>(tn) * sn);
     }
   }
   const long long n = static_cast<long long>(units.size());
@@ -802,15 +855,18 @@ std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int dep
 }
 
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
-                const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx, int depth, int K,
+                const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
+                const int2 *leaf_self, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end, int accumulate,
                 float phi_scale) {
   if (n_work == 0) return;
   if (K == 1) {
     if (want_phi)
-      p2p_k1_kernel<true><<<n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, near);
+      p2p_k1_kernel<true><<<n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx, leaf_self, depth,
+                                                 near);
     else
-      p2p_k1_kernel<false><<<n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, near);
+      p2p_k1_kernel<false><<<n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx, leaf_self, depth,
+                                                  near);
   } else {
     launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
                   k_begin, k_end, accumulate, phi_scale);

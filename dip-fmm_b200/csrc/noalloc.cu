@@ -174,7 +174,8 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
                         moments_paired(K));
   cudaEventRecord(plan->ev_fork, s);
   cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0);
-  launch_p2p(plan->src_rel, mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work, plan->has_self ? plan->self_idx : nullptr,
+  launch_p2p(plan->src_rel, mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
+             plan->has_self ? plan->self_idx : nullptr, plan->leaf_self,
              plan->depth, K, want_phi, near, plan->near_stream);
   cudaEventRecord(plan->ev_join, plan->near_stream);
   launch_p2m(plan->src_rel, mom, plan->src_off, plan->basis, M, n, plan->p, K, plan->depth, plan->p2m_chunk, s);

@@ -93,12 +93,13 @@ template <typename T> T *grow(T *&buf, size_t &have, size_t need, const char *wh
 void free_plan(cdfmm_b200_plan *p) {
   if (p == nullptr) return;
   void *ptrs[] = {p->src_rel, p->tgt_rel, p->src_off, p->tgt_off, p->src_perm, p->tgt_perm, p->src_inv, p->tgt_inv,
-                  p->self_idx, p->p2p_work, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
+                  p->self_idx, p->leaf_self, p->p2p_work, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
                   p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
+  if (p->p2p_work_wide != nullptr && p->p2p_work_wide != p->p2p_work) cudaFree(p->p2p_work_wide);
   if (p->adjoint != nullptr) free_plan(p->adjoint);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   if (p->ev_join) cudaEventDestroy(p->ev_join);
@@ -301,6 +302,7 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     plan->src_perm = dalloc<int>(plan->ns, bytes);
     plan->tgt_perm = dalloc<int>(plan->nt, bytes);
     plan->self_idx = dalloc<int>(plan->nt, bytes);
+    plan->leaf_self = dalloc<int2>(n_leaves, bytes);
     upload(plan->src_rel, srel.data(), srel.size(), h2d);
     upload(plan->tgt_rel, trel.data(), trel.size(), h2d);
     upload(plan->src_off, desc->leaf_source_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
@@ -308,11 +310,23 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     upload(plan->src_perm, desc->source_permutation, static_cast<size_t>(plan->ns), h2d);
     upload(plan->tgt_perm, desc->target_permutation, static_cast<size_t>(plan->nt), h2d);
     {
-      const std::vector<int4> work = p2p_work_units(desc->leaf_source_offsets, desc->leaf_target_offsets, plan->depth);
+      int sms = 0;
+      check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device), "device attribute");
+      const std::vector<int4> work =
+          p2p_work_units(desc->leaf_source_offsets, desc->leaf_target_offsets, plan->depth, sms, true);
+      const std::vector<int4> wide =
+          p2p_work_units(desc->leaf_source_offsets, desc->leaf_target_offsets, plan->depth, sms, false);
       plan->n_p2p_work = static_cast<int>(work.size());
+      plan->n_p2p_work_wide = static_cast<int>(wide.size());
       if (!work.empty()) {
         plan->p2p_work = dalloc<int4>(work.size(), bytes);
         upload(plan->p2p_work, work.data(), work.size(), h2d);
+      }
+      if (wide.size() == work.size()) {
+        plan->p2p_work_wide = plan->p2p_work; // no unit was capped: the same units
+      } else {
+        plan->p2p_work_wide = dalloc<int4>(wide.size(), bytes);
+        upload(plan->p2p_work_wide, wide.data(), wide.size(), h2d);
       }
     }
     {
@@ -578,6 +592,19 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
     check(cudaDeviceSynchronize(), "sync");
     if (plan->nt > 0)
       check(cudaMemcpy(plan->self_idx, sorted_self, sizeof(int) * plan->nt, cudaMemcpyHostToDevice), "cudaMemcpy");
+    {
+      // per leaf: the lowest and highest self source of its targets
+      std::vector<int2> range(static_cast<size_t>(plan->n_leaves), make_int2(0x7fffffff, -1));
+      for (int m = 0; m < plan->n_leaves; ++m)
+        for (int i = plan->h_tgt_off[static_cast<size_t>(m)]; i < plan->h_tgt_off[static_cast<size_t>(m) + 1]; ++i)
+          if (sorted_self[i] >= 0) {
+            int2 &r = range[static_cast<size_t>(m)];
+            r.x = std::min(r.x, sorted_self[i]);
+            r.y = std::max(r.y, sorted_self[i]);
+          }
+      check(cudaMemcpy(plan->leaf_self, range.data(), sizeof(int2) * range.size(), cudaMemcpyHostToDevice),
+            "cudaMemcpy");
+    }
     plan->h_self.assign(sorted_self, sorted_self + plan->nt);
     plan->has_self = true;
     return CDFMM_B200_OK;
@@ -763,8 +790,13 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
     check(cudaStreamWaitEvent(fs, plan->ev_fork, 0), "wait");
   }
   if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
-  launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
-             plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi, plan->near, ns);
+  // Inside a batch graph the K = 1 near field takes the uncapped units
+  // (same results bit for bit: a K = 1 target's sum does not depend on how
+  // its leaf is cut into units).
+  const bool wide = plan->in_batch && K == 1;
+  launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, wide ? plan->p2p_work_wide : plan->p2p_work,
+             wide ? plan->n_p2p_work_wide : plan->n_p2p_work, plan->has_self ? plan->self_idx : nullptr,
+             plan->leaf_self, plan->depth, K, want_phi, plan->near, ns);
   ++launches;
   if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
   if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
@@ -885,7 +917,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       auto near_part = [&](int j, bool accumulate) {
         const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
         launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
-                   plan->has_self ? plan->self_idx : nullptr, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc,
+                   plan->has_self ? plan->self_idx : nullptr, plan->leaf_self, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc,
                    accumulate ? ((a->output & CDFMM_B200_OUTPUT_FIELD) != 0u ? 1 : 2) : 0, plan->phi_scale);
         ++launches;
       };
