@@ -65,8 +65,8 @@ int m2l_simt_beta_per_thread(int n);
 // of the launch.  Units costing at least 4x the mean come first, heaviest
 // first, so they start before the light ones fill the machine; the rest
 // keep the Morton order, in which CTAs that run together share
-// neighbourhood sources in L2 (a uniform geometry's units are its leaves, in
-// Morton order).  Built once per geometry from the host leaf offsets
+// neighbourhood sources in L2 (a uniform geometry large enough that no leaf
+// reaches the cap has its leaves as units, in Morton order).  Built once per geometry from the host leaf offsets
 // (n_leaves + 1 prefix sums each); cap_cost = false keeps every unit at
 // kP2pUnitTargets targets.
 constexpr int kP2pUnitTargets = 128;
