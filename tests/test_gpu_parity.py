@@ -460,8 +460,9 @@ def test_dense_leaves_split_over_work_units(K):
     still meets the FP32 bar against the FP64 oracle FMM, for the K = 1
     kernel, the plain K < 4 layout and the paired K >= 4 layout.  The bar is
     1e-4 rather than 3e-5: a target here sums up to ~7,500 near sources with
-    strong cancellation in FP32 (K = 1 measures 3.5e-5, and its per-target
-    summation order does not depend on the split)."""
+    strong cancellation in FP32, which puts the rounding error itself near
+    3.5e-5 (measured for K = 1, whose per-target summation order does not
+    depend on how a leaf is split)."""
     rng, x = clustered_6000(5)
     n = len(x)
     leaf = np.floor(x * 4).astype(int) @ np.array([16, 4, 1])
