@@ -365,6 +365,10 @@ def b200_arm(args):
     rel_h = float(np.sqrt(np.sum((H0 - H_ref) ** 2) / np.sum(H_ref ** 2)))
     rel_phi = float(np.sqrt(np.sum((phi0 - phi_ref) ** 2) / np.sum(phi_ref ** 2)))
 
+    # near/far schedules: device time per step of each, and one concurrent
+    # trace each (per-stream events: when the near field and the M2L ran)
+    schedules = schedule_leg(plan, step, stream, args.steps, max_over_ranks)
+
     # per-stage device times (separate, instrumented evaluations)
     plan.set_timing(True)
     stage_runs = []
@@ -548,7 +552,7 @@ def b200_arm(args):
                    "parallelism": "replicas (independent states per GPU)" if world > 1 else "single GPU"},
         "rel_l2_H": rel_h, "rel_l2_phi": rel_phi,
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info, "roofline": roofline,
-        "cpu_baseline": cpu, "stages_ms": stages, "hbm_stages": hbm,
+        "cpu_baseline": cpu, "stages_ms": stages, "hbm_stages": hbm, "schedules": schedules,
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_state": ms_state_plain, "states_timed": ks,
                   "m2l": "fp32"},
         "batched_over_plain": value / plain_value,
@@ -561,6 +565,44 @@ def b200_arm(args):
     if dist is not None:
         dist.barrier()
         dist.destroy_process_group()
+
+
+SCHEDULE_NAMES = {1: "separate", 2: "corun", 3: "corun_upward_first"}
+
+
+def schedule_leg(plan, step, stream, steps, max_over_ranks):
+    """Each near/far schedule of the K-state evaluation: device time per step
+    (CUDA events around `steps` steps after a warm-up) and a trace of one
+    evaluation (device events on the near and far streams, ms from its
+    start).  The plan returns to its automatic schedule afterwards."""
+    import cdfmm_b200
+    import torch
+
+    out = {}
+    for sched, name in SCHEDULE_NAMES.items():
+        plan.set_schedule(sched)
+        step()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(max(1, steps)):
+            step()
+        b.record(stream)
+        torch.cuda.synchronize()
+        ms = max_over_ranks(a.elapsed_time(b) / max(1, steps))
+        plan.set_timing(2)
+        step()
+        torch.cuda.synchronize()
+        st = plan.stats()
+        plan.set_timing(0)
+        trace = {k[6:]: st[k] for k in st if k.startswith("trace_")}
+        overlap = max(0.0, min(trace["p2p_end"], trace["far_end"]) - max(trace["p2p_begin"], trace["m2l_begin"]))
+        out[name] = {"ms_per_step": ms, "trace_ms": trace, "p2p_m2l_overlap_ms": overlap}
+    plan.set_schedule(cdfmm_b200.SCHEDULE_AUTO)
+    step()
+    torch.cuda.synchronize()
+    out["auto"] = SCHEDULE_NAMES.get(plan.stats()["schedule_last"])
+    return out
 
 
 def clustered_points(rng, n, clusters=8, sigma=0.05):

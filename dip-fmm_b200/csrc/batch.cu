@@ -136,17 +136,26 @@ int cdfmm_b200_batch_launch(cdfmm_b200_batch *batch, void *stream, int32_t synch
   if (e == cudaSuccess) e = cudaGraphLaunch(batch->exec, s);
   if (e == cudaSuccess && synchronize) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return batch_fail(CDFMM_B200_ERR_RUNTIME, std::string("batch launch: ") + cudaGetErrorString(e));
+  // The launch rewrote every plan's moments and expansions: a backward call
+  // holding an older evaluation number must not reuse them.
+  for (cdfmm_b200_plan *p : batch->plans) p->stats.evaluations += 1;
   if (synchronize) {
+    // Each plan's captured work ends with its status kernel, which moved an
+    // expired wait's error code into the plan's host record.
+    int failed = 0, code = 0;
     for (cdfmm_b200_plan *p : batch->plans) {
-      int flag = 0;
-      if (cudaMemcpy(&flag, p->error_flag, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
-        return batch_fail(CDFMM_B200_ERR_RUNTIME, "batch: error flag read failed");
-      if (flag != 0) {
-        cudaMemset(p->error_flag, 0, sizeof(int));
-        return batch_fail(CDFMM_B200_ERR_TIMEOUT, "tensor-core M2L: a bounded wait expired (code " +
-                                                     std::to_string(flag) + "); results are invalid");
+      const volatile cdfmm_b200_plan::StatusRecord *r = p->status;
+      const int count = r->count;
+      if (count != p->status_seen) {
+        failed += 1;
+        code = r->code;
+        p->status_seen = count;
       }
     }
+    if (failed > 0)
+      return batch_fail(CDFMM_B200_ERR_TIMEOUT, "tensor-core M2L: a bounded wait expired (code " + std::to_string(code) +
+                                                   ") in " + std::to_string(failed) +
+                                                   " plan(s) of the batch; their results are invalid (NaN)");
   }
   return CDFMM_B200_OK;
 }

@@ -80,12 +80,14 @@ std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int dep
 // combined far-field results already in `near` instead of writing it (1: phi
 // and H, 2: phi only).
 // leaf_self: per leaf, the lowest and highest self source of its targets
-// (read when self_idx is given).
+// (read when self_idx is given).  corun (K > 1): the co-resident form, whose
+// two CTAs per SM leave room for one far-field CTA beside them (same
+// results up to the summation order of the state blocks).
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
                 const int2 *leaf_self, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1,
-                int accumulate = 0, float phi_scale = 1.0F);
+                int accumulate = 0, float phi_scale = 1.0F, bool corun = false);
 void configure_p2p(size_t max_smem);
 // Position gradient of sum_k W_k . H_k, near part: partial sums per state
 // group, gpart[nt][p2p_grad_groups(K)] (normalised units, 1/(4 pi) applied).

@@ -67,6 +67,15 @@ struct Plan;
 // as reported by cdfmm_b200_last_error.
 void cdfmm_b200_record_error(cdfmm_b200_plan *plan, const std::string &msg);
 
+// Enqueues on `s` the move of the plan's device error flag into its host
+// status record, tagged with call number `call` (the last work of a call).
+cudaError_t cdfmm_b200_collect_status(cdfmm_b200_plan *plan, cudaStream_t s, unsigned long long call);
+// After the stream of call number `call` was synchronised: an empty string if
+// that call's work recorded no expired wait, else the error message (and the
+// record counts as reported).  Failures of earlier calls are left for
+// cdfmm_b200_poll_status.
+std::string cdfmm_b200_own_status(cdfmm_b200_plan *plan, unsigned long long call);
+
 // The opaque ABI handle.
 struct cdfmm_b200_plan {
   int device = 0;
@@ -91,7 +100,10 @@ struct cdfmm_b200_plan {
   cudaStream_t io_in = nullptr, io_out = nullptr;  // host-memory copies overlapping the evaluation
   std::vector<cudaEvent_t> io_events;               // chunk pipeline events
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
-  cudaEvent_t ev_t[16] = {};
+  cudaEvent_t ev_t[20] = {};
+  bool trace = false;                               // concurrent trace events (timing mode 2)
+  int schedule = CDFMM_B200_SCHEDULE_AUTO;          // near/far schedule of K > 1 evaluations
+  int last_schedule = CDFMM_B200_SCHEDULE_SEPARATE;
 
   // geometry (device)
   float4 *src_rel = nullptr;   // [ns] (x - leaf centre) normalised, .w unused
@@ -146,6 +158,22 @@ struct cdfmm_b200_plan {
   int tc_tiles_Kp = 0, tc_n_tiles = 0;
   int *error_flag = nullptr;                   // device: nonzero after an expired bounded wait
   bool last_m2l_tc = false;
+  uint32_t tc_wait_limit = 0;                  // iterations of each M2L pipeline progress wait
+
+  // Expired bounded waits, as seen by the host: every call ends with a
+  // one-thread kernel on its stream that moves a nonzero device error flag
+  // into this record (pinned host memory mapped into the device address
+  // space) and clears the flag, so a failure is attributed to the call whose
+  // work raised it even when that call did not wait for its results.
+  struct StatusRecord {
+    int code;                  // error code of the last expired wait
+    int count;                 // calls whose GPU work recorded an expired wait
+    unsigned long long call;   // call number (call_seq) of the last such call
+  };
+  StatusRecord *status = nullptr;              // host address
+  StatusRecord *status_dev = nullptr;          // device address of the same record
+  int status_seen = 0;                         // `count` already reported to the caller
+  unsigned long long call_seq = 0;             // evaluate / backward / noalloc calls so far
 
   // state (device), sized for max_states
   float4 *mom = nullptr;       // [ns][K] sorted scaled moments

@@ -23,7 +23,10 @@
 // A pipeline unit is one offset and one 32-wide alpha chunk, so 4-8 stages
 // fit in shared memory and copies run several units ahead of the MMAs.
 // Every wait is bounded: on expiry the kernel records an error code, stops
-// issuing, drains what it issued, frees its TMEM and returns.
+// issuing, drains what it issued (those waits always keep the full limit, so
+// no copy or MMA is still in flight when the CTA exits), writes NaN into its
+// targets' locals (stale values of an earlier call never pass for results),
+// frees its TMEM and returns.
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
@@ -39,7 +42,7 @@ namespace cdfmm_b200 {
 namespace {
 
 constexpr int kTcThreads = 128;
-constexpr uint32_t kWaitLimit = 1u << 26; // ~2 s with the back-off below
+constexpr uint32_t kWaitLimit = kTcWaitLimit; // ~2 s with the back-off below
 constexpr int kKChunk = 32;               // alphas per pipeline unit
 
 __device__ __forceinline__ uint32_t smem_u32(const void *p) {
@@ -168,6 +171,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   int *tgt_xyz = tgt_node + kTcMaxTargets;   // [kTcMaxTargets] packed coordinates
   int *act = tgt_xyz + kTcMaxTargets;        // [216] offset positions that reach a source box in the grid
   int *n_act = act + 216;                    // their count
+  int *last_unit = n_act + 1;                // [8] per stage: the last pipeline unit issued into it
 
   // Zero every stage once: A rows beyond a tile's targets are never written.
   for (uint32_t q = tid; q < S * stage_bytes / 16u; q += kTcThreads)
@@ -179,6 +183,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     tgt_node[tid] = level_offset_d(level) + static_cast<int>(morton3(tx, ty, tz));
     tgt_xyz[tid] = tx | (ty << 10) | (tz << 20);
   }
+  if (tid < 8) last_unit[tid] = -1;
   if (tid == 0) {
     for (int s = 0; s < S; ++s) {
       mbar_init(&full[s], 1);
@@ -235,12 +240,11 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     const int npw = min(kTcThreads / 32 - 1, S);
     const int pw = (tid >> 5) - 1;
     const size_t btile = static_cast<size_t>(args.Npad) * kKChunk * 2u; // stride of one B chunk tile
-    int produced = 0;
     for (int u = pw; pw < npw && u < units; u += npw) {
       const int s = u % S;
       int ok = 1;
       if (lane == 0) {
-        if (u >= S && !mbar_wait(&empty[s], ((u / S) - 1) & 1)) {
+        if (u >= S && !mbar_wait(&empty[s], ((u / S) - 1) & 1, args.wait_limit)) {
           *abort_flag = 1;
           atomicExch(args.error_flag, 1);
         }
@@ -284,12 +288,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
         }
       }
       __syncwarp();
-      produced = u + 1;
-    }
-    if (lane == 0 && pw < npw && *reinterpret_cast<volatile int *>(abort_flag)) {
-      // Abort: wait (bounded) for this warp's copies still in flight.
-      for (int u = max(0, produced - S); u < produced; ++u)
-        if (u % npw == pw) mbar_wait(&full[u % S], (u / S) & 1);
+      if (lane == 0) atomicMax(&last_unit[s], u);
     }
   } else if (tid == 0) {
     // MMA issuer: waits for each unit's operands, issues its MMAs, commits
@@ -307,7 +306,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     int s = 0, kc = 0;
     uint32_t phase = 0;
     for (int u = 0; u < units; ++u) {
-      if (!mbar_wait(&full[s], phase)) {
+      if (!mbar_wait(&full[s], phase, args.wait_limit)) {
         *abort_flag = 1;
         atomicExch(args.error_flag, 2);
         break;
@@ -356,10 +355,29 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   tc_fence_before();
   __syncthreads();
   tc_fence_after();
+  if (*abort_flag != 0 && tid < S) {
+    // Abort: the copies of the last unit issued into each stage may still be
+    // in flight (earlier units of a stage completed before it was reused).
+    // Wait for them with the full limit before the CTA's shared memory is
+    // released.
+    const int u = last_unit[tid];
+    if (u >= 0) mbar_wait(&full[tid], static_cast<uint32_t>(u / S) & 1u);
+  }
 
   // Epilogue: warp w owns TMEM lanes 32w..32w+31 (rows of every M tile);
-  // scale by D_L and store.
-  if (*abort_flag == 0) {
+  // scale by D_L and store.  After an expired wait the accumulators are
+  // incomplete: the tile's locals are written as NaN instead.
+  if (*abort_flag != 0) {
+    const int tr = tid / args.Kp;
+    const int k = tid - tr * args.Kp;
+    for (int m = 0; m < m_active; ++m) {
+      const int tt = m * T + tr;
+      if (tr < T && tt < count && k < args.K) {
+        const long long base = static_cast<long long>(tgt_node[tt]) * args.n * args.K + k;
+        for (int b = 0; b < args.n; ++b) args.L[base + static_cast<long long>(b) * args.K] = __int_as_float(0x7fc00000);
+      }
+    }
+  } else {
     const int warp = tid >> 5;
     const int row = tid;
     const int tr = row / args.Kp;
@@ -467,7 +485,7 @@ size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages) {
   const size_t a = 128u * kKChunk * 2u * static_cast<size_t>(m_tiles);
   const size_t b = static_cast<size_t>(Npad) * kKChunk * 2u;
   return static_cast<size_t>(stages) * (2 * a + 2 * b) + 2 * stages * sizeof(uint64_t) + 8 +
-         (2 * kTcMaxTargets + 216 + 1) * sizeof(int);
+         (2 * kTcMaxTargets + 216 + 1 + 8) * sizeof(int);
 }
 
 void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,

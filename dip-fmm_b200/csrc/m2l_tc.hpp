@@ -27,7 +27,11 @@ struct TcArgs {
   int fuse_n;              // 1: A_hi x [B_hi | B_lo] as one N = 2 Npad MMA (acc_stride >= 2 Npad)
   uint32_t tmem_cols;
   uint32_t box_bytes;      // Kp * Kpad * 2
+  uint32_t wait_limit;     // iterations of each pipeline progress wait (kTcWaitLimit; 0 = expire at once)
 };
+
+// Default iterations of a bounded mbarrier wait (about 2 s with the back-off).
+constexpr uint32_t kTcWaitLimit = 1u << 26;
 
 // Largest target count of one CTA: m_tiles (<= 4) x 128 / Kp with Kp >= 8.
 constexpr int kTcMaxTargets = 64;

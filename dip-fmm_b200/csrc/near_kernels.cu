@@ -301,6 +301,14 @@ constexpr int kBufs = 2;            // moment chunk buffers (copies run kBufs - 
 constexpr int kNeighbourCap = 1024; // staged neighbourhood size per pass
 constexpr int kStateBlock = 64;     // states per state block (bounds shared memory)
 constexpr int kKbThreads = 256;
+// Co-resident form: two CTAs of this kernel leave room on every SM for one
+// CTA of a far-field kernel (the tensor-core M2L: 128 threads, <= 56
+// registers, <= 100 KB of shared memory), so the near field and the far
+// field run side by side instead of taking SMs from each other: state blocks
+// of 32 (61 KB of shared memory per CTA) and at most 112 registers per thread
+// (2 x 256 x 112 + 128 x 56 <= 65,536).
+constexpr int kStateBlockCorun = 32;
+constexpr int kKbRegsCorun = 112;
 
 // Shared-memory position of state k within a staged moment row (one pad
 // float4 after every group of KG states), and the row stride for a window of
@@ -438,22 +446,21 @@ __device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const
 //    gpart[nt][G] (G = ceil(K / KG)) from the weights W[nt][K] (plain layout).
 // PAIRED: the sorted moments use the paired layout (rows of round_up(K, 2)
 // float4), K >= 4.
-template <int KG, int MODE, bool PAIRED>
-__global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__restrict__ src_rel,
-                                                              const float4 *__restrict__ mom,
-                                                              const int *__restrict__ src_off,
-                                                              const float4 *__restrict__ tgt_rel,
-                                                              const int4 *__restrict__ work,
-                                                              const int *__restrict__ self_idx, int depth, int K,
-                                                              float4 *__restrict__ near,
-                                                              const float4 *__restrict__ W, int k_begin,
-                                                              int k_end, int accumulate, float acc_phi_scale) {
+// SB: states per state block (kStateBlock, or kStateBlockCorun for the
+// co-resident form).
+template <int KG, int MODE, bool PAIRED, int SB>
+__device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, const float4 *__restrict__ mom,
+                                            const int *__restrict__ src_off, const float4 *__restrict__ tgt_rel,
+                                            const int4 *__restrict__ work, const int *__restrict__ self_idx,
+                                            int depth, int K, float4 *__restrict__ near,
+                                            const float4 *__restrict__ W, int k_begin, int k_end, int accumulate,
+                                            float acc_phi_scale) {
   constexpr bool PHI = MODE == 1;
   constexpr bool GRAD = MODE == 2;
   extern __shared__ float4 dynb[];
   float4 *sPos = dynb;                                            // [kNeighbourCap]
   int *sIdx = reinterpret_cast<int *>(sPos + kNeighbourCap);      // [kNeighbourCap]
-  float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [kBufs][kChunkB][Kr <= kStateBlock + 9]
+  float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [kBufs][kChunkB][Kr <= SB + 9]
   __shared__ Neighbours nb;
   const int4 unit = work[blockIdx.x];
   const int leaf = unit.x;
@@ -464,8 +471,8 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
   const int total = nb.prefix[nb.count];
   const int tid = threadIdx.x;
   bool staged = false; // positions of the single pass already in shared memory
-  for (int kblk = k_begin; kblk < k_end; kblk += kStateBlock) {
-    const int Kc = min(kStateBlock, k_end - kblk);
+  for (int kblk = k_begin; kblk < k_end; kblk += SB) {
+    const int Kc = min(SB, k_end - kblk);
     const int G = (Kc + KG - 1) / KG;
     const int items = nt * G;
     for (int ib = 0, r = 0; ib < items; ib += r) {
@@ -497,7 +504,7 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
       // sources per chunk: kChunkB at the widest window, more for narrower
       // windows (a chunk buffer holds kChunkB rows of the widest stride), so
       // each chunk carries about the same work between barriers
-      const int chunkB = kChunkB * (mrow_stride<KG>((min(K, kStateBlock) + 1) & ~1) / Kr);
+      const int chunkB = kChunkB * (mrow_stride<KG>((min(K, SB) + 1) & ~1) / Kr);
       const int mrow = PAIRED ? (K + 1) & ~1 : K;                   // global row length (float4)
       const int i = t0 + t;
       const float4 ti = tgt_rel[i];
@@ -645,6 +652,29 @@ __global__ void __launch_bounds__(kKbThreads, 2) p2p_kb_kernel(const float4 *__r
   }
 }
 
+template <int KG, int MODE, bool PAIRED>
+__global__ void __launch_bounds__(kKbThreads, 2)
+    p2p_kb_kernel(const float4 *__restrict__ src_rel, const float4 *__restrict__ mom,
+                  const int *__restrict__ src_off, const float4 *__restrict__ tgt_rel,
+                  const int4 *__restrict__ work, const int *__restrict__ self_idx, int depth, int K,
+                  float4 *__restrict__ near, const float4 *__restrict__ W, int k_begin, int k_end, int accumulate,
+                  float acc_phi_scale) {
+  p2p_kb_body<KG, MODE, PAIRED, kStateBlock>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W,
+                                             k_begin, k_end, accumulate, acc_phi_scale);
+}
+
+// The co-resident form (see kStateBlockCorun).
+template <int KG, int MODE, bool PAIRED>
+__global__ void __maxnreg__(kKbRegsCorun)
+    p2p_kb_corun_kernel(const float4 *__restrict__ src_rel, const float4 *__restrict__ mom,
+                        const int *__restrict__ src_off, const float4 *__restrict__ tgt_rel,
+                        const int4 *__restrict__ work, const int *__restrict__ self_idx, int depth, int K,
+                        float4 *__restrict__ near, const float4 *__restrict__ W, int k_begin, int k_end,
+                        int accumulate, float acc_phi_scale) {
+  p2p_kb_body<KG, MODE, PAIRED, kStateBlockCorun>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W,
+                                                  k_begin, k_end, accumulate, acc_phi_scale);
+}
+
 // FP64 O(N*M) direct sum, one thread per target, sources tiled through
 // shared memory (upstream validation.cpp:71-111; cuda_fmm.cu:518-569).
 __global__ void __launch_bounds__(256) direct_fp64_kernel(const double *__restrict__ src,
@@ -763,28 +793,40 @@ __global__ void __launch_bounds__(256) direct_grad_fp64_kernel(const double *__r
   }
 }
 
-template <int KG> size_t p2p_kb_smem_bytes(int K) {
-  const int Kc = (std::min(K, kStateBlock) + 1) & ~1; // widest window (paired rows round up)
+template <int KG> size_t p2p_kb_smem_bytes(int K, int state_block) {
+  const int Kc = (std::min(K, state_block) + 1) & ~1; // widest window (paired rows round up)
   const int Kr = mrow_stride<KG>(Kc);
   return sizeof(float4) * kNeighbourCap + sizeof(int) * kNeighbourCap +
          sizeof(float4) * kBufs * kChunkB * static_cast<size_t>(Kr);
 }
 
+template <int KG, bool PAIRED, int MODE>
+void launch_kb_mode(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
+                    const int4 *work, int n_work, const int *self_idx, int depth, int K, float4 *near,
+                    const float4 *W, cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale,
+                    bool corun) {
+  if (corun)
+    p2p_kb_corun_kernel<KG, MODE, PAIRED><<<n_work, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlockCorun), s>>>(
+        src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
+  else
+    p2p_kb_kernel<KG, MODE, PAIRED><<<n_work, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlock), s>>>(
+        src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
+}
+
 template <int KG, bool PAIRED>
 void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                const int4 *work, int n_work, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-               cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale) {
+               cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale, bool corun) {
   if (n_work == 0) return;
-  const size_t smem = p2p_kb_smem_bytes<KG>(K);
   if (mode == 1)
-    p2p_kb_kernel<KG, 1, PAIRED><<<n_work, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx,
-                                                                  depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb_mode<KG, PAIRED, 1>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, near, W, s, k_begin,
+                                  k_end, accumulate, acc_phi_scale, corun);
   else if (mode == 2)
-    p2p_kb_kernel<KG, 2, PAIRED><<<n_work, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx,
-                                                                  depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb_mode<KG, PAIRED, 2>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, near, W, s, k_begin,
+                                  k_end, accumulate, acc_phi_scale, corun);
   else
-    p2p_kb_kernel<KG, 0, PAIRED><<<n_work, kKbThreads, smem, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx,
-                                                                  depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb_mode<KG, PAIRED, 0>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, near, W, s, k_begin,
+                                  k_end, accumulate, acc_phi_scale, corun);
 }
 
 // K >= 8: groups of 8 states, paired layout; 4 <= K < 8: groups of 4,
@@ -792,14 +834,15 @@ void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, con
 // slower at K = 64: the accumulators no longer fit the register budget.)
 void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                    const int4 *work, int n_work, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-                   cudaStream_t s, int k_begin = 0, int k_end = -1, int accumulate = 0, float acc_phi_scale = 1.0F) {
+                   cudaStream_t s, int k_begin = 0, int k_end = -1, int accumulate = 0, float acc_phi_scale = 1.0F,
+                   bool corun = false) {
   if (k_end < 0) k_end = K;
   if (K >= 8)
-    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale, corun);
   else if (K >= 4)
-    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb<4, true>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale, corun);
   else
-    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale);
+    launch_kb<4, false>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale, corun);
 }
 
 } // namespace
@@ -858,7 +901,7 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
                 const int2 *leaf_self, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end, int accumulate,
-                float phi_scale) {
+                float phi_scale, bool corun) {
   if (n_work == 0) return;
   if (K == 1) {
     if (want_phi)
@@ -869,7 +912,7 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                                                   near);
   } else {
     launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
-                  k_begin, k_end, accumulate, phi_scale);
+                  k_begin, k_end, accumulate, phi_scale, corun);
   }
 }
 
@@ -881,16 +924,19 @@ void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_of
   launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, 2, gpart, W, s);
 }
 
+template <int KG, bool PAIRED> void configure_p2p_kb(size_t max_smem) {
+  allow_dynamic_smem(p2p_kb_kernel<KG, 0, PAIRED>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<KG, 1, PAIRED>, max_smem);
+  allow_dynamic_smem(p2p_kb_kernel<KG, 2, PAIRED>, max_smem);
+  allow_dynamic_smem(p2p_kb_corun_kernel<KG, 0, PAIRED>, max_smem);
+  allow_dynamic_smem(p2p_kb_corun_kernel<KG, 1, PAIRED>, max_smem);
+  allow_dynamic_smem(p2p_kb_corun_kernel<KG, 2, PAIRED>, max_smem);
+}
+
 void configure_p2p(size_t max_smem) {
-  allow_dynamic_smem(p2p_kb_kernel<8, 0, true>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<8, 1, true>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<8, 2, true>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 0, true>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 1, true>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 2, true>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 0, false>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 1, false>, max_smem);
-  allow_dynamic_smem(p2p_kb_kernel<4, 2, false>, max_smem);
+  configure_p2p_kb<8, true>(max_smem);
+  configure_p2p_kb<4, true>(max_smem);
+  configure_p2p_kb<4, false>(max_smem);
 }
 
 void launch_direct_grad_fp64(const double *src, const double *mom, int ns, const double *tgt, int nt,

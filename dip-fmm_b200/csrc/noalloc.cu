@@ -164,6 +164,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   int4 *dtiles = reinterpret_cast<int4 *>(take(tile_bytes));
 
   cudaStream_t s = static_cast<cudaStream_t>(a->stream);
+  const unsigned long long call = ++plan->call_seq;
   // Locals of levels 0 and 1 are never written (no M2L there) and must read
   // as zero; the array still holds the previous call's values.
   e = cudaMemsetAsync(L, 0, exp_bytes, s);
@@ -204,6 +205,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
     ta.fuse_n = plan->tc_fuse;
     ta.tmem_cols = plan->tc_tmem_cols;
     ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
+    ta.wait_limit = plan->tc_wait_limit;
     launch_m2l_tc(ta, n_tiles, s);
   } else if (plan->depth >= 2) {
     launch_m2l_simt(M, L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles, plan->n_tiles, n,
@@ -215,15 +217,14 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   launch_l2p(L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, near, plan->basis, n, plan->p, K, plan->nt, plan->depth, a->output,
              a->layout, plan->phi_scale, a->field, a->potential, s);
   e = cudaGetLastError();
+  // The plan's error flag (set by an expired wait of the tensor-core M2L)
+  // goes to the plan's host status record, tagged with this call.
+  if (e == cudaSuccess) e = cdfmm_b200_collect_status(plan, s, call);
   if (e == cudaSuccess && a->synchronize) e = cudaStreamSynchronize(s);
   if (e != cudaSuccess) return noalloc_fail(plan, CDFMM_B200_ERR_RUNTIME, std::string("evaluate_noalloc: ") + cudaGetErrorString(e));
-  if (a->synchronize && use_tc) {
-    int flag = 0;
-    e = cudaMemcpy(&flag, plan->error_flag, sizeof(int), cudaMemcpyDeviceToHost);
-    if (e != cudaSuccess || flag != 0) {
-      cudaMemset(plan->error_flag, 0, sizeof(int));
-      return noalloc_fail(plan, CDFMM_B200_ERR_TIMEOUT, "tensor-core M2L: a bounded wait expired; results are invalid");
-    }
+  if (a->synchronize) {
+    const std::string own = cdfmm_b200_own_status(plan, call);
+    if (!own.empty()) return noalloc_fail(plan, CDFMM_B200_ERR_TIMEOUT, own);
   }
   return CDFMM_B200_OK;
 }

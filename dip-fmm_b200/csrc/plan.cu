@@ -59,6 +59,10 @@ template <typename T> void upload(T *dst, const T *src, size_t count, uint64_t &
   bytes += count * sizeof(T);
 }
 
+// Events of the concurrent trace (cdfmm_b200_set_timing mode 2).
+constexpr int kTraceBegin = 12, kTraceP2pBegin = 13, kTraceP2pEnd = 14, kTraceFarBegin = 15, kTraceM2lBegin = 16,
+              kTraceFarEnd = 17, kTraceEnd = 18;
+
 // Grows a device buffer to at least `need` bytes (contents not kept).
 template <typename T> T *grow_bytes(T *&buf, size_t &have, size_t need, const char *what) {
   if (have < need) {
@@ -100,6 +104,7 @@ void free_plan(cdfmm_b200_plan *p) {
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
   if (p->p2p_work_wide != nullptr && p->p2p_work_wide != p->p2p_work) cudaFree(p->p2p_work_wide);
+  if (p->status != nullptr) cudaFreeHost(p->status);
   if (p->adjoint != nullptr) free_plan(p->adjoint);
   if (p->ev_fork) cudaEventDestroy(p->ev_fork);
   if (p->ev_join) cudaEventDestroy(p->ev_join);
@@ -157,7 +162,46 @@ size_t device_smem_optin(int device) {
   return static_cast<size_t>(v);
 }
 
+// Moves a nonzero device error flag into the host status record (one thread).
+__global__ void collect_status_kernel(int *flag, cdfmm_b200_plan::StatusRecord *rec, unsigned long long call) {
+  const int f = *reinterpret_cast<volatile int *>(flag);
+  if (f != 0) {
+    *flag = 0;
+    volatile cdfmm_b200_plan::StatusRecord *r = rec;
+    r->code = f;
+    r->call = call;
+    r->count = r->count + 1;
+    __threadfence_system();
+  }
+}
+
+std::string timeout_message(int code, int calls, bool own) {
+  std::string m = "tensor-core M2L: a bounded wait expired (code " + std::to_string(code) + ")";
+  if (own) {
+    m += "; the results of this call are invalid (the affected local expansions were set to NaN)";
+    if (calls > 1) m += "; " + std::to_string(calls - 1) + " earlier call(s) on this plan failed the same way";
+  } else {
+    m += " in " + std::to_string(calls) + " call(s) on this plan since the last report; their results are invalid "
+         "(the affected local expansions were set to NaN)";
+  }
+  return m;
+}
+
 } // namespace
+
+cudaError_t cdfmm_b200_collect_status(cdfmm_b200_plan *plan, cudaStream_t s, unsigned long long call) {
+  collect_status_kernel<<<1, 1, 0, s>>>(plan->error_flag, plan->status_dev, call);
+  return cudaGetLastError();
+}
+
+std::string cdfmm_b200_own_status(cdfmm_b200_plan *plan, unsigned long long call) {
+  const volatile cdfmm_b200_plan::StatusRecord *r = plan->status;
+  const int count = r->count;
+  if (count == plan->status_seen || r->call != call) return std::string();
+  const int calls = count - plan->status_seen;
+  plan->status_seen = count;
+  return timeout_message(r->code, calls, true);
+}
 
 void cdfmm_b200_record_error(cdfmm_b200_plan *plan, const std::string &msg) {
   if (plan != nullptr) plan->last_error = msg;
@@ -482,6 +526,12 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     check(cudaDeviceSynchronize(), "plan upload");
     plan->error_flag = dalloc<int>(1, bytes);
     check(cudaMemset(plan->error_flag, 0, sizeof(int)), "cudaMemset");
+    check(cudaHostAlloc(reinterpret_cast<void **>(&plan->status), sizeof(cdfmm_b200_plan::StatusRecord),
+                        cudaHostAllocMapped), "cudaHostAlloc");
+    std::memset(plan->status, 0, sizeof(cdfmm_b200_plan::StatusRecord));
+    check(cudaHostGetDevicePointer(reinterpret_cast<void **>(&plan->status_dev), plan->status, 0),
+          "cudaHostGetDevicePointer");
+    plan->tc_wait_limit = kTcWaitLimit;
 
     // Tensor-core M2L: sm_100 devices, order <= 9 (N = 16 * ceil(n/16) <= 256
     // accumulator columns) and at least one pipeline stage in shared memory.
@@ -661,6 +711,7 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
   ta.node_base = node_base;
   ta.zero_node = plan->n_nodes - node_base;
   ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
+  ta.wait_limit = plan->tc_wait_limit;
   float best = 0.0F;
   int best_i = -1;
   for (size_t c = 0; c < plan->tc_candidates.size(); ++c) {
@@ -696,22 +747,29 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
   plan->tc_tiles_Kp = 0; // rebuilt for the chosen shape by the caller
 }
 
-// Upward and downward far-field passes for K states whose sorted, scaled
-// moments are in plan->mom: P2M, M2M, M2L (tensor cores or FP32 SIMT), L2L,
-// leaving the leaf local expansions in plan->L.  Returns the launch count.
-static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing) {
+// Upward pass for K states whose sorted, scaled moments are in plan->mom:
+// P2M and M2M, leaving the multipoles in plan->M.  Returns the launch count.
+static int enqueue_upward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing) {
   const int n = plan->n;
   int launches = 0;
-    launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
-               plan->p2m_chunk, s);
+  launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
+             plan->p2m_chunk, s);
+  ++launches;
+  if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
+  for (int level = plan->depth - 1; level >= 0; --level) {
+    launch_m2m(plan->M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level,
+               static_cast<int>(plan->ops.m2m_pair_g.size()), s);
     ++launches;
-    if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
-    for (int level = plan->depth - 1; level >= 0; --level) {
-      launch_m2m(plan->M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level,
-                 static_cast<int>(plan->ops.m2m_pair_g.size()), s);
-      ++launches;
-    }
-    if (timing) check(cudaEventRecord(plan->ev_t[3], s), "event");
+  }
+  if (timing) check(cudaEventRecord(plan->ev_t[3], s), "event");
+  return launches;
+}
+
+// Downward pass: M2L (tensor cores or FP32 SIMT) and L2L, leaving the leaf
+// local expansions in plan->L.  Returns the launch count.
+static int enqueue_downward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing) {
+  const int n = plan->n;
+  int launches = 0;
     const bool use_tc = plan->depth >= 2 && plan->tc_supported && K <= 128 &&
                         (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || (plan->m2l_mode == CDFMM_B200_M2L_AUTO && K >= 8));
     if (use_tc) {
@@ -746,6 +804,7 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
       ta.fuse_n = plan->tc_fuse;
       ta.tmem_cols = plan->tc_tmem_cols;
       ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
+      ta.wait_limit = plan->tc_wait_limit;
       launch_m2l_tc(ta, plan->tc_n_tiles, s);
       launches += 2;
       plan->stats.m2l_tc_m_tiles = plan->tc_m_tiles;
@@ -766,6 +825,18 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
   return launches;
 }
 
+// Upward and downward far-field passes (P2M, M2M, M2L, L2L).
+static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing) {
+  const int launches = enqueue_upward(plan, K, s, timing);
+  return launches + enqueue_downward(plan, K, s, timing);
+}
+
+// Near/far schedule of one evaluation of K > 1 states (cdfmm_b200_set_schedule).
+static int resolved_schedule(const cdfmm_b200_plan *plan, int K) {
+  if (K <= 1) return CDFMM_B200_SCHEDULE_SEPARATE;
+  return plan->schedule == CDFMM_B200_SCHEDULE_AUTO ? CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST : plan->schedule;
+}
+
 // Enqueues one evaluation of K states on stream s: device-resident moments
 // ([K][ns][3], dtype) -> gather -> (list-1 P2P on the near stream || P2M, M2M,
 // M2L, L2L) -> L2P + combine + unsort into device results.  Returns the
@@ -775,6 +846,7 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   const bool want_phi = (output & CDFMM_B200_OUTPUT_POTENTIAL) != 0u;
   int launches = 0;
   if (timing) check(cudaEventRecord(plan->ev_t[0], s), "event");
+  if (plan->trace && !timing) check(cudaEventRecord(plan->ev_t[kTraceBegin], s), "event");
   launch_gather_moments(moments, dtype, plan->src_inv, plan->ns, K, plan->scale, plan->mom, s, moments_paired(K));
   launches += plan->ns > 0 ? 1 : 0;
   if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
@@ -782,28 +854,54 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   // Near field on its own stream, concurrent with the far field.  With
   // stage timing enabled it runs first on the main stream instead, so that
   // each stage's events measure that stage alone.
+  //   SEPARATE: the full-size near-field kernel (two CTAs fill an SM) beside
+  //     the far field on a high-priority stream;
+  //   CORUN: the co-resident near-field form, two CTAs of which leave room
+  //     on every SM for one tensor-core M2L CTA, so the FP32 near field and
+  //     the tensor-core far field run side by side;
+  //   CORUN_UPWARD_FIRST: as CORUN, with P2M and M2M (short, HBM-bound, and
+  //     too large to sit beside the near field) run on all SMs first.
+  const int schedule = timing ? CDFMM_B200_SCHEDULE_SEPARATE : resolved_schedule(plan, K);
+  const bool corun = schedule != CDFMM_B200_SCHEDULE_SEPARATE;
+  const bool trace = plan->trace && !timing;
   cudaStream_t ns = timing ? s : plan->near_stream;
   cudaStream_t fs = timing ? s : plan->far_stream;
+  if (schedule == CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST) {
+    if (trace) check(cudaEventRecord(plan->ev_t[kTraceFarBegin], s), "event");
+    launches += enqueue_upward(plan, K, s, false);
+  }
   if (!timing) {
     check(cudaEventRecord(plan->ev_fork, s), "event");
     check(cudaStreamWaitEvent(ns, plan->ev_fork, 0), "wait");
     check(cudaStreamWaitEvent(fs, plan->ev_fork, 0), "wait");
   }
   if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
+  if (trace) check(cudaEventRecord(plan->ev_t[kTraceP2pBegin], ns), "event");
   // Inside a batch graph the K = 1 near field takes the uncapped units
   // (same results bit for bit: a K = 1 target's sum does not depend on how
   // its leaf is cut into units).
   const bool wide = plan->in_batch && K == 1;
   launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, wide ? plan->p2p_work_wide : plan->p2p_work,
              wide ? plan->n_p2p_work_wide : plan->n_p2p_work, plan->has_self ? plan->self_idx : nullptr,
-             plan->leaf_self, plan->depth, K, want_phi, plan->near, ns);
+             plan->leaf_self, plan->depth, K, want_phi, plan->near, ns, 0, -1, 0, 1.0F, corun);
   ++launches;
   if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
+  if (trace) check(cudaEventRecord(plan->ev_t[kTraceP2pEnd], ns), "event");
   if (timing) check(cudaEventRecord(plan->ev_t[1], s), "event");
   if (!timing) check(cudaEventRecord(plan->ev_join, ns), "event");
 
   // far field
-  launches += enqueue_far(plan, K, fs, timing);
+  if (schedule == CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST) {
+    if (trace) check(cudaEventRecord(plan->ev_t[kTraceM2lBegin], fs), "event");
+    launches += enqueue_downward(plan, K, fs, false);
+  } else {
+    if (trace) check(cudaEventRecord(plan->ev_t[kTraceFarBegin], fs), "event");
+    launches += enqueue_upward(plan, K, fs, timing);
+    if (trace) check(cudaEventRecord(plan->ev_t[kTraceM2lBegin], fs), "event");
+    launches += enqueue_downward(plan, K, fs, timing);
+  }
+  if (trace) check(cudaEventRecord(plan->ev_t[kTraceFarEnd], fs), "event");
+  plan->last_schedule = schedule;
   if (timing) check(cudaEventRecord(plan->ev_t[5], s), "event");
   if (!timing) {
     check(cudaEventRecord(plan->ev_far, fs), "event");
@@ -816,6 +914,7 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   launches += (K >= 4 && plan->nt > 0) ? 2 : 1;
   check(cudaGetLastError(), "kernel launch");
   if (timing) check(cudaEventRecord(plan->ev_t[7], s), "event");
+  if (trace) check(cudaEventRecord(plan->ev_t[kTraceEnd], s), "event");
   return launches;
 }
 
@@ -842,6 +941,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     (void)cudaGetLastError();
 
     const int K = a->n_states;
+    const unsigned long long call = ++plan->call_seq;
     // NULL is the legacy default stream, as everywhere in CUDA (a torch tensor
     // on the default stream and our kernels are then ordered).
     cudaStream_t s = static_cast<cudaStream_t>(a->stream);
@@ -853,6 +953,8 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
     const bool field_out = want_h || a->layout == CDFMM_B200_LAYOUT_INTERLEAVED;
     const size_t phi_state = (a->layout == CDFMM_B200_LAYOUT_SEPARATE && want_phi) ? static_cast<size_t>(plan->nt) * sizeof(float) : 0;
     const bool timing = plan->timing;
+    // a concurrent trace is read back once the call's work is done
+    bool traced = false;
 
     // Device staging of host arrays: [K][ns][3] moments; results field then potential.
     const char *moments = static_cast<const char *>(a->moments);
@@ -1036,6 +1138,7 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       }
       launches += enqueue_evaluation(plan, moments, a->moments_dtype, K, a->output, a->layout,
                                      reinterpret_cast<float *>(field), reinterpret_cast<float *>(potential), s, timing);
+      traced = plan->trace && !timing;
       if (host_out) {
         if (field_out && field_state > 0) {
           check(cudaMemcpyAsync(a->field, field, field_state * K, cudaMemcpyDeviceToHost, s), "D2H field");
@@ -1051,18 +1154,27 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       plan->exp_state0 = 0;
       plan->last_K = K;
     }
-    if (a->synchronize || host_out || timing) {
+    check(cdfmm_b200_collect_status(plan, s, call), "status kernel launch");
+    ++launches;
+    if (a->synchronize || host_out || timing || traced) {
       check(cudaStreamSynchronize(s), "evaluate");
-      if (plan->last_m2l_tc) {
-        int flag = 0;
-        check(cudaMemcpy(&flag, plan->error_flag, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
-        if (flag != 0) {
-          cudaMemset(plan->error_flag, 0, sizeof(int));
-          throw AbiError(CDFMM_B200_ERR_TIMEOUT, "tensor-core M2L: a bounded wait expired (code " +
-                                                     std::to_string(flag) + "); results are invalid");
-        }
-      }
+      const std::string own = cdfmm_b200_own_status(plan, call);
+      if (!own.empty()) throw AbiError(CDFMM_B200_ERR_TIMEOUT, own);
     }
+    if (traced) {
+      auto at = [&](int i) {
+        float v = 0.0F;
+        cudaEventElapsedTime(&v, plan->ev_t[kTraceBegin], plan->ev_t[i]);
+        return static_cast<double>(v);
+      };
+      plan->stats.trace_p2p_begin = at(kTraceP2pBegin);
+      plan->stats.trace_p2p_end = at(kTraceP2pEnd);
+      plan->stats.trace_far_begin = at(kTraceFarBegin);
+      plan->stats.trace_m2l_begin = at(kTraceM2lBegin);
+      plan->stats.trace_far_end = at(kTraceFarEnd);
+      plan->stats.trace_end = at(kTraceEnd);
+    }
+    plan->stats.schedule_last = plan->last_schedule;
     plan->stats.m2l_mode_resolved = plan->last_m2l_tc ? CDFMM_B200_M2L_BF16X3 : CDFMM_B200_M2L_FP32;
     if (timing) {
       auto ms = [&](int i, int j) {
@@ -1162,9 +1274,11 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
     check(cudaSetDevice(plan->device), "cudaSetDevice");
     (void)cudaGetLastError();
     const int K = a->n_states;
+    const unsigned long long call = ++plan->call_seq;
     cudaStream_t s = static_cast<cudaStream_t>(a->stream);
     const bool host_in = (a->memory & CDFMM_B200_MOMENTS_ON_HOST) != 0u;
     const bool host_out = (a->memory & CDFMM_B200_RESULTS_ON_HOST) != 0u;
+    unsigned long long adjoint_call = 0;
 
     if (a->grad_moments != nullptr) {
       // dL/dm = A^t dL/dH: the transposed plan evaluated on the weights.
@@ -1181,6 +1295,7 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
       e.synchronize = 0;
       const int rc = cdfmm_b200_evaluate(plan->adjoint, &e);
       if (rc != CDFMM_B200_OK) throw AbiError(rc, std::string("transposed evaluate: ") + cdfmm_b200_last_error(plan->adjoint));
+      adjoint_call = plan->adjoint->call_seq;
     }
 
     if (want_x && plan->nt > 0) {
@@ -1229,18 +1344,12 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
         plan->stats.evaluation_d2h_calls += 1;
       }
     }
+    check(cdfmm_b200_collect_status(plan, s, call), "status kernel launch");
     if (a->synchronize || host_in || host_out) {
       check(cudaStreamSynchronize(s), "backward");
-      int flag = 0;
-      check(cudaMemcpy(&flag, plan->error_flag, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
-      if (flag == 0 && plan->adjoint != nullptr)
-        check(cudaMemcpy(&flag, plan->adjoint->error_flag, sizeof(int), cudaMemcpyDeviceToHost), "error flag");
-      if (flag != 0) {
-        cudaMemset(plan->error_flag, 0, sizeof(int));
-        if (plan->adjoint != nullptr) cudaMemset(plan->adjoint->error_flag, 0, sizeof(int));
-        throw AbiError(CDFMM_B200_ERR_TIMEOUT, "tensor-core M2L: a bounded wait expired (code " + std::to_string(flag) +
-                                                   "); results are invalid");
-      }
+      std::string own = cdfmm_b200_own_status(plan, call);
+      if (own.empty() && adjoint_call != 0) own = cdfmm_b200_own_status(plan->adjoint, adjoint_call);
+      if (!own.empty()) throw AbiError(CDFMM_B200_ERR_TIMEOUT, own);
     }
     return CDFMM_B200_OK;
   } catch (const AbiError &e) {
@@ -1276,8 +1385,18 @@ int cdfmm_b200_read_expansions(const cdfmm_b200_plan *plan, int32_t which, int32
 
 int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled) {
   if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
-  plan->timing = enabled != 0;
-  plan->stats.timing_enabled = plan->timing ? 1 : 0;
+  if (enabled < 0 || enabled > 2) return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT, "timing mode must be 0, 1 or 2");
+  plan->timing = enabled == 1;
+  plan->trace = enabled == 2;
+  plan->stats.timing_enabled = enabled;
+  return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_set_schedule(cdfmm_b200_plan *plan, int32_t schedule) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (schedule < CDFMM_B200_SCHEDULE_AUTO || schedule > CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST)
+    return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT, "unknown schedule");
+  plan->schedule = schedule;
   return CDFMM_B200_OK;
 }
 
@@ -1324,6 +1443,33 @@ int cdfmm_b200_set_m2l_shape(cdfmm_b200_plan *plan, int32_t m_tiles, int32_t sta
   }
   return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT,
               "not a pipeline shape of this plan (cdfmm_b200_m2l_shapes lists them)");
+}
+
+int cdfmm_b200_poll_status(cdfmm_b200_plan *plan) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  int code = 0, calls = 0;
+  for (cdfmm_b200_plan *q : {plan, plan->adjoint}) {
+    if (q == nullptr || q->status == nullptr) continue;
+    const volatile cdfmm_b200_plan::StatusRecord *r = q->status;
+    const int count = r->count;
+    if (count != q->status_seen) {
+      calls += count - q->status_seen;
+      code = r->code;
+      q->status_seen = count;
+    }
+  }
+  if (calls == 0) return CDFMM_B200_OK;
+  return fail(plan, CDFMM_B200_ERR_TIMEOUT, timeout_message(code, calls, false));
+}
+
+int cdfmm_b200_set_wait_limit(cdfmm_b200_plan *plan, int64_t iterations) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (iterations > static_cast<int64_t>(0xffffffffu))
+    return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT, "iterations must be below 2^32");
+  const uint32_t limit = iterations < 0 ? kTcWaitLimit : static_cast<uint32_t>(iterations);
+  plan->tc_wait_limit = limit;
+  if (plan->adjoint != nullptr) plan->adjoint->tc_wait_limit = limit;
+  return CDFMM_B200_OK;
 }
 
 int cdfmm_b200_selftest_bounded_wait(int32_t device) {

@@ -34,6 +34,7 @@ MOMENTS_ON_HOST = 1
 RESULTS_ON_HOST = 2
 LAYOUT_SEPARATE = 0
 LAYOUT_INTERLEAVED = 1
+SCHEDULE_AUTO, SCHEDULE_SEPARATE, SCHEDULE_CORUN, SCHEDULE_CORUN_UPWARD_FIRST = 0, 1, 2, 3
 
 EXPORTED = (
     "cdfmm_b200_device_count", "cdfmm_b200_device_info", "cdfmm_b200_plan_create",
@@ -43,6 +44,7 @@ EXPORTED = (
     "cdfmm_b200_evaluate_noalloc", "cdfmm_b200_backward", "cdfmm_b200_batch_create",
     "cdfmm_b200_batch_launch", "cdfmm_b200_batch_destroy", "cdfmm_b200_direct_grad_fp64",
     "cdfmm_b200_selftest_bounded_wait", "cdfmm_b200_m2l_shapes", "cdfmm_b200_set_m2l_shape",
+    "cdfmm_b200_poll_status", "cdfmm_b200_set_wait_limit", "cdfmm_b200_set_schedule",
 )
 
 # Scratch capacity of cdfmm_b200_evaluate_noalloc (bytes).
@@ -93,6 +95,10 @@ class Stats(ctypes.Structure):
         ("ms_gather", ctypes.c_double), ("ms_p2m", ctypes.c_double), ("ms_m2m", ctypes.c_double),
         ("ms_m2l", ctypes.c_double), ("ms_l2l", ctypes.c_double), ("ms_l2p", ctypes.c_double),
         ("ms_p2p", ctypes.c_double), ("ms_total", ctypes.c_double),
+        ("trace_p2p_begin", ctypes.c_double), ("trace_p2p_end", ctypes.c_double),
+        ("trace_far_begin", ctypes.c_double), ("trace_m2l_begin", ctypes.c_double),
+        ("trace_far_end", ctypes.c_double), ("trace_end", ctypes.c_double),
+        ("schedule_last", ctypes.c_int32), ("reserved0", ctypes.c_int32),
     ]
 
     def as_dict(self):
@@ -132,12 +138,15 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_batch_destroy.restype = None
     lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
     lib.cdfmm_b200_set_timing.argtypes = [vp, i32]
+    lib.cdfmm_b200_set_schedule.argtypes = [vp, i32]
     lib.cdfmm_b200_m2l_shapes.argtypes = [vp, ctypes.POINTER(i32), i32]
     lib.cdfmm_b200_set_m2l_shape.argtypes = [vp, i32, i32, i32]
     lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
     lib.cdfmm_b200_direct_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
     lib.cdfmm_b200_direct_grad_fp64.argtypes = [i32, i32, vp, vp, i32, vp, vp, vp, vp]
     lib.cdfmm_b200_selftest_bounded_wait.argtypes = [i32]
+    lib.cdfmm_b200_poll_status.argtypes = [vp]
+    lib.cdfmm_b200_set_wait_limit.argtypes = [vp, ctypes.c_int64]
     lib.cdfmm_b200_m2l_matrix.argtypes = [i32, vp, vp, u64]
     lib.cdfmm_b200_last_error.argtypes = [vp]
     lib.cdfmm_b200_last_error.restype = ctypes.c_char_p
@@ -269,7 +278,13 @@ class DevicePlan:
         _check(library().cdfmm_b200_set_self_indices(self._h, _ptr(a)), self._h)
 
     def set_timing(self, enabled=True):
-        _check(library().cdfmm_b200_set_timing(self._h, 1 if enabled else 0), self._h)
+        """True / 1: per-stage times (stages serialised); 2: trace of the
+        concurrent schedule; False / 0: off."""
+        _check(library().cdfmm_b200_set_timing(self._h, int(enabled)), self._h)
+
+    def set_schedule(self, schedule):
+        """Near/far schedule of K > 1 evaluations (SCHEDULE_*)."""
+        _check(library().cdfmm_b200_set_schedule(self._h, int(schedule)), self._h)
 
     def m2l_shapes(self) -> list:
         """Tensor-core M2L pipeline shapes of this plan as (accumulators per
@@ -286,6 +301,17 @@ class DevicePlan:
         """Pins one of m2l_shapes() (no autotuning, run-to-run identical
         results); m_tiles = 0 returns to autotuning."""
         _check(library().cdfmm_b200_set_m2l_shape(self._h, int(m_tiles), int(stages), 1 if fused else 0), self._h)
+
+    def poll_status(self):
+        """Raises CdfmmError (ERR_TIMEOUT) if the completed work of an earlier
+        call on this plan recorded an expired bounded wait not yet reported
+        (cdfmm_b200_poll_status); does not wait for work in flight."""
+        _check(library().cdfmm_b200_poll_status(self._h), self._h)
+
+    def set_wait_limit(self, iterations):
+        """Failure injection for tests: polls per tensor-core M2L progress
+        wait before it expires (0: at once; negative: the default)."""
+        _check(library().cdfmm_b200_set_wait_limit(self._h, int(iterations)), self._h)
 
     def stats(self) -> dict:
         s = Stats()

@@ -57,6 +57,12 @@ extern "C" {
 #define CDFMM_B200_MOMENTS_ON_HOST 1u
 #define CDFMM_B200_RESULTS_ON_HOST 2u
 
+/* Near/far schedule of an evaluation of K > 1 states (cdfmm_b200_set_schedule). */
+#define CDFMM_B200_SCHEDULE_AUTO 0                 /* CORUN_UPWARD_FIRST */
+#define CDFMM_B200_SCHEDULE_SEPARATE 1             /* full-size near-field CTAs beside a high-priority far field */
+#define CDFMM_B200_SCHEDULE_CORUN 2                /* near-field CTAs sized to leave one far-field CTA per SM */
+#define CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST 3   /* CORUN, with P2M and M2M on all SMs before the near field */
+
 /* Result layout (cdfmm_b200_eval_args.layout). */
 #define CDFMM_B200_LAYOUT_SEPARATE 0    /* field[K][Nt][3] and potential[K][Nt] */
 #define CDFMM_B200_LAYOUT_INTERLEAVED 1 /* field[K][Nt][4] = {phi, Hx, Hy, Hz}: cdfmm::FloatPotentialField */
@@ -124,6 +130,12 @@ typedef struct cdfmm_b200_stats {
   int32_t backward_reused_forward; /* last backward reused the forward's moments and locals */
   int32_t m2l_tc_fused;          /*   1: hi and lo translation tiles side by side in one wider MMA */
   double ms_gather, ms_p2m, ms_m2m, ms_m2l, ms_l2l, ms_l2p, ms_p2p, ms_total;
+  /* Concurrent trace of the last evaluate (timing mode 2; ms from its start,
+   * device events on the streams the stages ran on): near field begin / end,
+   * far field begin (P2M), M2L begin, far field end (after L2L), end. */
+  double trace_p2p_begin, trace_p2p_end, trace_far_begin, trace_m2l_begin, trace_far_end, trace_end;
+  int32_t schedule_last;         /* CDFMM_B200_SCHEDULE_* the last evaluate ran */
+  int32_t reserved0;
 } cdfmm_b200_stats;
 
 /* Library / device probing.  Returns OK and *count = 0 when no device. */
@@ -151,8 +163,31 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
 /* Runs P2M -> M2M -> M2L -> L2L -> L2P plus list1 P2P for K states and writes
  * the results in user target order (the reference's UniformFmm::evaluate_into_float32
  * with CudaFull, src/uniform_fmm.cpp:1281-1349 upstream, generalised to K states,
- * potential output and device-resident arrays). */
+ * potential output and device-resident arrays).
+ * Expired bounded waits: the tensor-core M2L gives up a wait after about 2 s
+ * (nothing faults or hangs); the locals it could not finish are set to NaN,
+ * so the affected results are NaN, never stale values.  A call that waits for
+ * its results (synchronize, host arrays or stage timing) returns
+ * CDFMM_B200_ERR_TIMEOUT when its own work expired; for a call that returns
+ * before its work is done, cdfmm_b200_poll_status reports it later. */
 int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args);
+
+/* Non-blocking report of expired bounded waits (no counterpart in the
+ * reference, whose evaluate always blocks): CDFMM_B200_ERR_TIMEOUT if the
+ * completed GPU work of any evaluate, backward or noalloc call on this plan
+ * (or on its transposed plan) recorded an expired wait that no synchronous
+ * call has reported yet, else CDFMM_B200_OK.  Work still in flight is not
+ * seen: synchronise the call's stream first to include it.  Each failure is
+ * reported once. */
+int cdfmm_b200_poll_status(cdfmm_b200_plan *plan);
+
+/* Failure injection for tests (no counterpart in the reference): sets how
+ * many times each pipeline progress wait of the tensor-core M2L polls its
+ * mbarrier before it gives up (0: every such wait expires at once; negative:
+ * the default, about 2 s).  The waits that drain copies and MMAs already in
+ * flight after an expiry always keep the default, so an injected expiry ends
+ * the kernel cleanly.  Applies to the plan and its transposed plan. */
+int cdfmm_b200_set_wait_limit(cdfmm_b200_plan *plan, int64_t iterations);
 
 /* Allocation-free variant of cdfmm_b200_evaluate (no counterpart in the
  * reference).  For callers that cannot call cudaMalloc/cudaFree while they
@@ -168,7 +203,14 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args)
  *  - the first call on a device looks up that array's device address
  *    (cudaGetSymbolAddress): make it before any stream capture starts;
  *  - every call shares the array: calls whose GPU work overlaps race, so
- *    order them on one stream.
+ *    order them on one stream;
+ *  - the device address is looked up once per device for the life of the
+ *    process: do not use this entry point after cudaDeviceReset (or any
+ *    other reset of the device's primary context) in the same process;
+ *  - its expansions stay in the scratch array: cdfmm_b200_read_expansions
+ *    keeps returning those of the last cdfmm_b200_evaluate.
+ * Expired waits are reported as for cdfmm_b200_evaluate (this call when it
+ * synchronises, else cdfmm_b200_poll_status).
  * The plan itself is created (and allocated) by cdfmm_b200_plan_create. */
 int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *args);
 
@@ -218,20 +260,36 @@ typedef struct cdfmm_b200_batch cdfmm_b200_batch;
 int cdfmm_b200_batch_create(cdfmm_b200_plan *const *plans, const cdfmm_b200_eval_args *args, int32_t count,
                             cdfmm_b200_batch **out_batch);
 /* One graph launch on `stream` (NULL = legacy default stream); with
- * synchronize nonzero, waits and checks the plans' device error flags. */
+ * synchronize nonzero, waits and returns CDFMM_B200_ERR_TIMEOUT if a plan's
+ * work recorded an expired bounded wait.  Each launch counts as one
+ * evaluation of every plan of the batch (the `evaluations` counter), so a
+ * backward call cannot reuse expansions from before the launch. */
 int cdfmm_b200_batch_launch(cdfmm_b200_batch *batch, void *stream, int32_t synchronize);
 void cdfmm_b200_batch_destroy(cdfmm_b200_batch *batch);
 
 /* Copies the FP32 multipole (which = 0) or local (which = 1) expansions of one
- * state of the last evaluate to host memory as out[node][coefficient], node in
+ * state of the last cdfmm_b200_evaluate (cdfmm_b200_evaluate_noalloc keeps its
+ * expansions in its scratch array and does not update these) to host memory
+ * as out[node][coefficient], node in
  * flat level-wise Morton order and coefficients in the total-degree basis
  * order; the values are in the normalised units of the reference FP32 plan
  * (UniformFmm::multipole_float32 / local_float32, include/cdfmm/uniform_fmm.hpp:262-269 upstream). */
 int cdfmm_b200_read_expansions(const cdfmm_b200_plan *plan, int32_t which, int32_t state,
                                float *out, size_t out_count);
 
-/* Enables (nonzero) or disables per-stage CUDA-event timing of evaluate. */
+/* Timing of evaluate: 0 off; 1 per-stage CUDA-event times (the stages run
+ * one after another on the caller's stream, ms_* fields); 2 a trace of the
+ * concurrent schedule as it normally runs (trace_* fields; the call then
+ * waits for its work). */
 int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled);
+
+/* Near/far schedule for evaluations of K > 1 states (no counterpart in the
+ * reference, which overlaps a cuSPARSE near field with its M2L on two
+ * streams, src/cuda_fmm.cu:3295-3300, 3386-3391 upstream):
+ * CDFMM_B200_SCHEDULE_*.  All schedules compute the same sums; the near
+ * field's summation order differs between SEPARATE and the CORUN forms
+ * (state blocks of 64 vs 32), at FP32 rounding level. */
+int cdfmm_b200_set_schedule(cdfmm_b200_plan *plan, int32_t schedule);
 
 int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out);
 

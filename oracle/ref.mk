@@ -4,7 +4,8 @@
 # with every output written under oracle/_ref/.  This is test and baseline
 # infrastructure: nothing in the product links or loads these files.
 #
-#   make -f oracle/ref.mk REF=/path/to/dip-fmm        (from the repo root)
+#   make -f oracle/ref.mk REF=/path/to/dip-fmm        (from the repo root; the default
+#                                                      is a `reference` checkout beside the repo)
 #
 # Outputs
 #   oracle/_ref/libcdfmm_ref.so   reference core (CpuStatic/CpuReference) + cuda_fmm.cu
@@ -16,7 +17,7 @@
 # but -march=x86-64-v3 instead of -march=native because the binaries are built
 # here and run on another host's CPU.
 
-REF      ?= /root/reference
+REF      ?= $(abspath ../reference)
 OUT      := oracle/_ref
 CUDA     ?= /usr/local/cuda
 HOSTCXX  ?= /usr/bin/g++

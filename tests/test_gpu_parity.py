@@ -476,3 +476,50 @@ def test_dense_leaves_split_over_work_units(K):
                          root_half_width=0.5)
         assert oracle.rel_l2(r["H"][k], ref["H"]) < 1e-4
         assert oracle.rel_l2(r["phi"][k], ref["phi"]) < 1e-4
+
+
+@pytest.mark.parametrize("K", [8, 64])
+def test_near_far_schedules_give_the_same_field(K):
+    """Every near/far schedule of a K-state evaluation (the full-size near
+    field beside the far field, the co-resident near-field form, and that
+    form after an upward pass on all SMs) computes the same sums: results
+    agree to FP32 rounding (the co-resident form sums each target's state
+    blocks of 32 in another order) and meet the FP32 bar against the FP64
+    oracle FMM.  The concurrent trace reports each stream's interval."""
+    torch = pytest.importorskip("torch")
+    rng = np.random.default_rng(400 + K)
+    n = 6000
+    x = rng.uniform(0, 1, (n, 3))
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, x, o)
+    plan = cdfmm_b200.DevicePlan.from_tree(tree, 5, max_states=K)
+    plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+    m = torch.from_numpy(rng.normal(size=(K, n, 3)).astype(np.float32)).cuda()
+    out = {}
+    for sched in (cdfmm_b200.SCHEDULE_SEPARATE, cdfmm_b200.SCHEDULE_CORUN, cdfmm_b200.SCHEDULE_CORUN_UPWARD_FIRST,
+                  cdfmm_b200.SCHEDULE_AUTO):
+        plan.set_schedule(sched)
+        H = torch.empty((K, n, 3), device="cuda")
+        phi = torch.empty((K, n), device="cuda")
+        plan.set_timing(2)
+        plan.evaluate(m, output="both", field=H, potential=phi, synchronize=True)
+        plan.set_timing(0)
+        st = plan.stats()
+        expect = cdfmm_b200.SCHEDULE_CORUN_UPWARD_FIRST if sched == cdfmm_b200.SCHEDULE_AUTO else sched
+        assert st["schedule_last"] == expect
+        assert 0.0 <= st["trace_p2p_begin"] <= st["trace_p2p_end"] <= st["trace_end"]
+        assert st["trace_far_begin"] <= st["trace_m2l_begin"] <= st["trace_far_end"] <= st["trace_end"]
+        out[sched] = (H.cpu().numpy(), phi.cpu().numpy())
+    base_h, base_phi = out[cdfmm_b200.SCHEDULE_SEPARATE]
+    for sched, (h, p) in out.items():
+        assert oracle.rel_l2(h, base_h) < 1e-6
+        assert oracle.rel_l2(p, base_phi) < 1e-6
+    np.testing.assert_array_equal(out[cdfmm_b200.SCHEDULE_CORUN][0], out[cdfmm_b200.SCHEDULE_CORUN_UPWARD_FIRST][0])
+    ref = oracle.fmm(x, x, m[K - 1].cpu().numpy().astype(np.float64), 5, 3, identities=np.arange(n))
+    h, p = out[cdfmm_b200.SCHEDULE_AUTO]
+    assert oracle.rel_l2(h[K - 1], ref["H"]) < FP32_REL_L2
+    assert oracle.rel_l2(p[K - 1], ref["phi"]) < FP32_REL_L2
+    with pytest.raises(ValueError, match="unknown schedule"):
+        plan.set_schedule(7)
+    plan.close()
