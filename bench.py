@@ -75,6 +75,9 @@ def parse_args():
     ap.add_argument("--no-backward", action="store_true")
     ap.add_argument("--no-multi", action="store_true")
     ap.add_argument("--no-lattice", action="store_true")
+    ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--corun-shape-sweep", action="store_true",
+                    help="time every M2L pipeline shape under the co-resident schedule")
     ap.add_argument("--multi-problems", type=int, default=48)
     return ap.parse_args()
 
@@ -196,9 +199,9 @@ class ClockSampler:
 
 
 # --------------------------------------------------------------- reference
-def write_ref_input(path, x, moments, order, depth, warmup, steps):
+def write_ref_input(path, x, moments, order, depth, warmup, steps, output=3, backend=0):
     n = len(x)
-    hdr = np.array([n, n, order, depth, 0, 3, len(moments), warmup, steps, 1, 0, 0], dtype=np.int32)
+    hdr = np.array([n, n, order, depth, 0, output, len(moments), warmup, steps, 1, 0, backend], dtype=np.int32)
     with open(path, "wb") as f:
         f.write(b"CDFMMIN1")
         f.write(hdr.tobytes())
@@ -209,38 +212,56 @@ def write_ref_input(path, x, moments, order, depth, warmup, steps):
         f.write(np.arange(n, dtype=np.int32).tobytes())
 
 
-def run_reference_cpu(seed, warmup, steps):
-    """Reference CpuStatic (FP32, field+potential) on the host cores; returns
-    (target-states/s, detail).  Falls back to the oracle port if the reference
-    build is absent."""
+def ref_sample_inputs(seed, states):
+    """The bounded sample the reference is timed on: N = 131,072 uniform
+    dipoles (seeded) and `states` unit-direction x U[0.5, 1.5] moment states."""
     s = REF_SAMPLE
     rng = np.random.default_rng(seed)
     x = rng.uniform(0.0, 1.0, size=(s["n"], 3))
-    m = unit_moments(rng, 1, s["n"])
+    return x, unit_moments(rng, states, s["n"])
+
+
+def run_reference_binary(x, m, warmup, steps, output, backend, threads):
+    """Runs oracle/_ref/ref_bench (the reference built from its own sources)
+    on inputs x, m (m: states x N x 3); a timed step evaluates every state
+    once.  Returns its JSON summary."""
+    s = REF_SAMPLE
+    exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
+    with tempfile.TemporaryDirectory() as tmp:
+        inp, out = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
+        write_ref_input(inp, x, m, s["order"], s["depth"], warmup, steps, output=output, backend=backend)
+        env = dict(os.environ, OMP_NUM_THREADS=str(threads), OMP_PROC_BIND="close", OMP_PLACES="cores")
+        r = subprocess.run([exe, inp, out], capture_output=True, text=True, env=env, timeout=1800)
+        if r.returncode != 0:
+            raise RuntimeError(f"reference run failed: {r.stderr[-400:]}")
+        return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def run_reference_cpu(seed, warmup, steps, per_step=1):
+    """Reference CpuStatic (FP32, field+potential) on the host cores: `warmup`
+    untimed evaluations, then the median of `steps` samples of `per_step`
+    evaluations each.  Returns (target-states/s, detail).  Falls back to the
+    oracle port if the reference build is absent."""
+    s = REF_SAMPLE
+    x, m = ref_sample_inputs(seed, per_step)
     cores = os.cpu_count() or 1
     exe = os.path.join(ROOT, "oracle", "_ref", "ref_bench")
     sample = (f"N={s['n']} uniform dipoles, p={s['order']}, depth {s['depth']} (~32/leaf), one state per "
-              f"evaluation, field+potential, FP32 CpuStatic; {steps} timed evaluations after {warmup} warm-up")
+              f"evaluation, field+potential, FP32 CpuStatic; median of {steps} samples of {per_step} evaluations "
+              f"after {warmup} warm-up evaluations")
     if os.path.exists(exe):
-        with tempfile.TemporaryDirectory() as tmp:
-            inp, out = os.path.join(tmp, "in.bin"), os.path.join(tmp, "out.bin")
-            write_ref_input(inp, x, m, s["order"], s["depth"], warmup, steps)
-            env = dict(os.environ, OMP_NUM_THREADS=str(cores), OMP_PROC_BIND="close", OMP_PLACES="cores")
-            r = subprocess.run([exe, inp, out], capture_output=True, text=True, env=env, timeout=1800)
-            if r.returncode != 0:
-                raise RuntimeError(f"reference run failed: {r.stderr[-400:]}")
-            info = json.loads(r.stdout.strip().splitlines()[-1])
-        per_step = info["median_step_s"]
-        return s["n"] / per_step, {"kind": "reference", "cores": info["threads"], "sample": sample,
-                                   "setup_s": info["setup_s"], "ms_per_state": per_step * 1e3}
+        info = run_reference_binary(x, m, warmup, steps, 3, 0, cores)
+        per_eval = info["median_step_s"] / per_step
+        return s["n"] / per_eval, {"kind": "reference", "cores": info["threads"], "sample": sample,
+                                   "setup_s": info["setup_s"], "ms_per_state": per_eval * 1e3}
     import oracle
 
     t0 = time.perf_counter()
     oracle.fmm(x, x, m[0], s["order"], s["depth"], identities=np.arange(s["n"]))
-    per_step = time.perf_counter() - t0
-    return s["n"] / per_step, {"kind": "port", "cores": cores, "sample": sample.replace("FP32 CpuStatic",
+    per_eval = time.perf_counter() - t0
+    return s["n"] / per_eval, {"kind": "port", "cores": cores, "sample": sample.replace("FP32 CpuStatic",
                                                                                          "FP64 oracle port"),
-                               "ms_per_state": per_step * 1e3}
+                               "ms_per_state": per_eval * 1e3}
 
 
 def reference_arm(args):
@@ -367,7 +388,7 @@ def b200_arm(args):
 
     # near/far schedules: device time per step of each, and one concurrent
     # trace each (per-stream events: when the near field and the M2L ran)
-    schedules = schedule_leg(plan, step, stream, args.steps, max_over_ranks)
+    schedules = schedule_leg(plan, step, stream, args.steps, max_over_ranks, args.corun_shape_sweep)
 
     # per-stage device times (separate, instrumented evaluations)
     plan.set_timing(True)
@@ -535,8 +556,13 @@ def b200_arm(args):
 
     cpu = None
     if world == 1 and not args.no_cpu_baseline:
-        v, info = run_reference_cpu(args.seed, 1, 3)
-        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"]}
+        # the reference's own protocol: 2 warm-ups, median of 5 samples x 10 evaluations
+        v, info = run_reference_cpu(args.seed, 2, 5, 10)
+        cpu = {"value": v, "unit": UNIT, "cores": info["cores"], "kind": info["kind"], "sample": info["sample"],
+               "ms_per_state": info["ms_per_state"]}
+    reference_gpu = None
+    if world == 1 and not args.no_reference_gpu:
+        reference_gpu = reference_gpu_leg(args, stream, local)
 
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
@@ -552,7 +578,8 @@ def b200_arm(args):
                    "parallelism": "replicas (independent states per GPU)" if world > 1 else "single GPU"},
         "rel_l2_H": rel_h, "rel_l2_phi": rel_phi,
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info, "roofline": roofline,
-        "cpu_baseline": cpu, "stages_ms": stages, "hbm_stages": hbm, "schedules": schedules,
+        "cpu_baseline": cpu, "reference_gpu": reference_gpu, "stages_ms": stages, "hbm_stages": hbm,
+        "schedules": schedules,
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_state": ms_state_plain, "states_timed": ks,
                   "m2l": "fp32"},
         "batched_over_plain": value / plain_value,
@@ -567,10 +594,102 @@ def b200_arm(args):
         dist.destroy_process_group()
 
 
-SCHEDULE_NAMES = {1: "separate", 2: "corun", 3: "corun_upward_first"}
+def reference_gpu_leg(args, stream, local):
+    """The reference's own GPU path (CudaFull: cuSPARSE near field, cuBLAS
+    M2L; FP32, field only, one state per call, host arrays in and out) on
+    this GPU, on the bounded sample N = 131,072, p = 6, depth 4 where its
+    host plan fits, timed by the reference itself (median per evaluation of
+    its device-kernel and whole-call seconds, 2 warm-ups then 5 x 10
+    evaluations), beside this library on the same inputs: one state per
+    call (the plain path, host arrays, as the reference's API) and K = 64
+    states per call (device-resident and through host arrays)."""
+    import cdfmm
+    import cdfmm_b200
+    import torch
+
+    s = REF_SAMPLE
+    if not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "ref_bench")):
+        return {"unavailable": "reference build (oracle/_ref) absent"}
+    x, m = ref_sample_inputs(args.seed + 5, 10)
+    try:
+        info = run_reference_binary(x, m, 2, 5, 2, 2, os.cpu_count() or 1)
+    except (RuntimeError, subprocess.TimeoutExpired, ValueError) as e:
+        return {"unavailable": f"reference CudaFull run failed: {str(e)[-300:]}"}
+    per_call = info["median_step_s"] / len(m)
+    ref = {"ms_kernel": info["median_kernel_s"] * 1e3, "ms_h2d": info["median_h2d_s"] * 1e3,
+           "ms_d2h": info["median_d2h_s"] * 1e3, "ms_call": per_call * 1e3, "setup_s": info["setup_s"],
+           "value_call": s["n"] / per_call, "value_kernel": s["n"] / info["median_kernel_s"]}
+
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = s["depth"]
+    tree = cdfmm.UniformTree(x, x, o)
+    sorted_self = np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)]
+
+    def timed_ms(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for _ in range(reps):
+            fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / reps
+
+    plain = cdfmm_b200.DevicePlan.from_tree(tree, s["order"], max_states=1, m2l_mode=cdfmm_b200.M2L_FP32,
+                                            device=local)
+    plain.set_self_indices(sorted_self)
+    hm1 = torch.from_numpy(m[:1]).pin_memory()
+    hH1 = torch.empty((1, s["n"], 3), dtype=torch.float32).pin_memory()
+
+    def plain_host():
+        plain.evaluate(hm1, output="field", field=hH1, stream=stream.cuda_stream, synchronize=True,
+                       memory=cdfmm_b200.MOMENTS_ON_HOST | cdfmm_b200.RESULTS_ON_HOST)
+
+    dm1 = hm1.cuda()
+    dH1 = torch.empty((1, s["n"], 3), dtype=torch.float32, device="cuda")
+
+    def plain_dev():
+        plain.evaluate(dm1, output="field", field=dH1, stream=stream.cuda_stream, synchronize=False)
+
+    ms_plain_call = timed_ms(plain_host, 10)
+    ms_plain_dev = timed_ms(plain_dev, 10)
+    plain.close()
+    K = 64
+    batched = cdfmm_b200.DevicePlan.from_tree(tree, s["order"], max_states=K, device=local)
+    batched.set_self_indices(sorted_self)
+    mk = unit_moments(np.random.default_rng(args.seed + 6), K, s["n"])
+    dmk = torch.from_numpy(mk).cuda()
+    dHk = torch.empty((K, s["n"], 3), dtype=torch.float32, device="cuda")
+    hmk = torch.from_numpy(mk).pin_memory()
+    hHk = torch.empty((K, s["n"], 3), dtype=torch.float32).pin_memory()
+
+    def batched_dev():
+        batched.evaluate(dmk, output="field", field=dHk, stream=stream.cuda_stream, synchronize=False)
+
+    def batched_host():
+        batched.evaluate(hmk, output="field", field=hHk, stream=stream.cuda_stream, synchronize=True,
+                         memory=cdfmm_b200.MOMENTS_ON_HOST | cdfmm_b200.RESULTS_ON_HOST)
+
+    ms_k_dev = timed_ms(batched_dev, 5)
+    ms_k_call = timed_ms(batched_host, 5)
+    batched.close()
+    n = s["n"]
+    ours = {"plain_ms_call": ms_plain_call, "plain_ms_device": ms_plain_dev,
+            "plain_value_call": n / (ms_plain_call * 1e-3),
+            "batched_ms_device": ms_k_dev, "batched_ms_call": ms_k_call,
+            "batched_value_device": n * K / (ms_k_dev * 1e-3), "batched_value_call": n * K / (ms_k_call * 1e-3)}
+    return {"workload": f"uniform N={n}, p={s['order']}, depth {s['depth']}, field only, FP32",
+            "reference_cudafull": ref, "b200": ours, "unit": UNIT,
+            "plain_over_reference_call": ours["plain_value_call"] / ref["value_call"],
+            "batched_over_reference_call": ours["batched_value_call"] / ref["value_call"],
+            "batched_device_over_reference_kernel": ours["batched_value_device"] / ref["value_kernel"]}
 
 
-def schedule_leg(plan, step, stream, steps, max_over_ranks):
+SCHEDULE_NAMES = {1: "separate", 2: "corun"}
+
+
+def schedule_leg(plan, step, stream, steps, max_over_ranks, shape_sweep=False):
     """Each near/far schedule of the K-state evaluation: device time per step
     (CUDA events around `steps` steps after a warm-up) and a trace of one
     evaluation (device events on the near and far streams, ms from its
@@ -598,6 +717,30 @@ def schedule_leg(plan, step, stream, steps, max_over_ranks):
         trace = {k[6:]: st[k] for k in st if k.startswith("trace_")}
         overlap = max(0.0, min(trace["p2p_end"], trace["far_end"]) - max(trace["p2p_begin"], trace["m2l_begin"]))
         out[name] = {"ms_per_step": ms, "trace_ms": trace, "p2p_m2l_overlap_ms": overlap}
+    if shape_sweep:
+        # every M2L pipeline shape pinned in turn under the co-resident schedule
+        plan.set_schedule(cdfmm_b200.SCHEDULE_CORUN)
+        sweep = []
+        for mt, st, fused in plan.m2l_shapes():
+            plan.set_m2l_shape(mt, st, fused)
+            step()
+            torch.cuda.synchronize()
+            a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            a.record(stream)
+            for _ in range(max(1, steps)):
+                step()
+            b.record(stream)
+            torch.cuda.synchronize()
+            plan.set_timing(2)
+            step()
+            torch.cuda.synchronize()
+            tr = plan.stats()
+            plan.set_timing(0)
+            sweep.append({"shape": [mt, st, bool(fused)], "ms_per_step": a.elapsed_time(b) / max(1, steps),
+                          "p2p_ms": tr["trace_p2p_end"] - tr["trace_p2p_begin"],
+                          "m2l_ms": tr["trace_far_end"] - tr["trace_m2l_begin"]})
+        plan.set_m2l_shape(0)
+        out["corun_shape_sweep"] = sweep
     plan.set_schedule(cdfmm_b200.SCHEDULE_AUTO)
     step()
     torch.cuda.synchronize()

@@ -1036,6 +1036,7 @@ void configure_far_kernels(size_t max_smem) {
   allow_dynamic_smem(l2p_kernel, max_smem);
   allow_dynamic_smem(m2m_kernel, max_smem);
   allow_dynamic_smem(l2l_kernel, max_smem);
+  prefer_max_shared_carveout(l2l_kernel); // runs beside the co-resident near field
 }
 
 } // namespace cdfmm_b200

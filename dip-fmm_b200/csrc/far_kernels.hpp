@@ -80,21 +80,53 @@ std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int dep
 // combined far-field results already in `near` instead of writing it (1: phi
 // and H, 2: phi only).
 // leaf_self: per leaf, the lowest and highest self source of its targets
-// (read when self_idx is given).  corun (K > 1): the co-resident form, whose
-// two CTAs per SM leave room for one far-field CTA beside them (same
-// results up to the summation order of the state blocks).
+// (read when self_idx is given).  corun (K > 1, NULL otherwise): the
+// co-resident form -- persistent, `ctas` CTAs (two per SM) taking work units
+// from the device counter `next_unit`, each CTA leaving room on its SM for
+// one far-field CTA (same results up to the summation order of the state
+// blocks).
+struct CorunLaunch {
+  int ctas;        // grid size: two per SM
+  int *next_unit;  // device counter (reset on the launch stream)
+};
+// Close pairs: the plan's list of (target, source) pairs closer than a leaf
+// width / 2^k, with the FP32 r the near-field kernels form (.w: source
+// index) and r from the FP64 positions; a correction pass after every
+// near-field launch swaps each pair's field at the FP32 r for its field at
+// the exact r.  targets: (sorted target, first pair, pairs, 0).
+struct CloseGeometry {
+  const int4 *targets;
+  int n_targets;
+  const float4 *r_fp32;
+  const float4 *r_exact;
+};
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
-                const int2 *leaf_self, int depth, int K,
+                const int2 *leaf_self, const CloseGeometry &cg, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1,
-                int accumulate = 0, float phi_scale = 1.0F, bool corun = false);
+                int accumulate = 0, float phi_scale = 1.0F, const CorunLaunch *corun = nullptr);
+// Close-pair search (once per plan), over work units covering every
+// target, with r formed as the near-field kernels form it.  Count pass:
+// counts[i][l] = pairs of target i with 0 < r^2 < thresholds[l]; write pass:
+// the pairs with r^2 < r2_max of target i from out_first[i] on (FP32 r with
+// the source index in .w; r from the FP64 root-normalised positions [n][3]).
+constexpr int kCloseLevels = 4;
+void launch_p2p_close_count(const float4 *src_rel, const int *src_off, const float4 *tgt_rel, const int4 *work,
+                            int n_work, int depth, const float (&thresholds)[kCloseLevels], int *counts,
+                            cudaStream_t s);
+void launch_p2p_close_write(const float4 *src_rel, const int *src_off, const float4 *tgt_rel, const int4 *work,
+                            int n_work, int depth, float r2_max, const int *out_first, const double *src_abs,
+                            const double *tgt_abs, float4 *r_fp32, float4 *r_exact, cudaStream_t s);
 void configure_p2p(size_t max_smem);
+// Shared memory (dynamic + static bytes) of one CTA of the co-resident
+// near-field form for K states.
+size_t p2p_corun_cta_smem(int K);
 // Position gradient of sum_k W_k . H_k, near part: partial sums per state
 // group, gpart[nt][p2p_grad_groups(K)] (normalised units, 1/(4 pi) applied).
 int p2p_grad_groups(int K);
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
-                     const int4 *work, int n_work, const int *self_idx, int depth, int K, const float4 *W,
-                     float4 *gpart, cudaStream_t s);
+                     const int4 *work, int n_work, const int *self_idx, const CloseGeometry &cg, int depth, int K,
+                     const float4 *W, float4 *gpart, cudaStream_t s);
 // Far part (second derivatives of the leaf local expansions) plus the near
 // partial sums, scaled by inv_scale, written as out[user target][3].
 void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,

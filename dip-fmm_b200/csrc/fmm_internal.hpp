@@ -15,6 +15,12 @@ namespace cdfmm_b200 {
 constexpr int kMaxOrder = 10;
 constexpr int kMaxDepth = 8;
 constexpr int kMaxCoef = (kMaxOrder + 1) * (kMaxOrder + 2) * (kMaxOrder + 3) / 6; // 286
+// Pairs closer than a leaf width / 2^kCloseShift (or a smaller threshold in
+// dense clusters) have their near field corrected with r from the FP64
+// positions: FP32 coordinates relative to a leaf centre carry an absolute
+// error of about 2^-25 leaf widths, which for such pairs is no longer small
+// against their distance.
+constexpr int kCloseShift = 4;
 
 inline int basis_size(int p) { return p < 0 ? 0 : (p + 1) * (p + 2) * (p + 3) / 6; }
 inline int level_offset(int level) {
@@ -108,6 +114,13 @@ struct cdfmm_b200_plan {
   // geometry (device)
   float4 *src_rel = nullptr;   // [ns] (x - leaf centre) normalised, .w unused
   float4 *tgt_rel = nullptr;   // [nt]
+  // close pairs (closer than a leaf width / 2^close_shift; see CloseGeometry)
+  int4 *close_targets = nullptr;  // [n_close_targets] (sorted target, first pair, pairs, 0)
+  int n_close_targets = 0;
+  float4 *close_r_fp32 = nullptr; // [pairs] r as the near-field kernels form it, .w = source index
+  float4 *close_r_exact = nullptr; // [pairs] r from the FP64 positions
+  uint64_t close_pairs = 0;
+  int close_shift = 0;
   int *src_off = nullptr;      // [n_leaves + 1]
   int *tgt_off = nullptr;      // [n_leaves + 1]
   int *src_perm = nullptr;     // [ns] sorted -> user
@@ -118,6 +131,8 @@ struct cdfmm_b200_plan {
   int2 *leaf_self = nullptr;   // [n_leaves] lowest, highest self source of each leaf's targets ((INT_MAX, -1): none)
   int4 *p2p_work = nullptr;    // [n_p2p_work] list1 work units (leaf, first target, targets, 0)
   int n_p2p_work = 0;
+  int *p2p_next_unit = nullptr; // work-unit counter of the persistent co-resident near field
+  int sm_count = 0;
   // Units of up to 128 targets without the per-unit cost cap (the same array
   // as p2p_work when no unit was capped): used while the plan is captured
   // into a batch graph, where the other geometries' work runs beside a long
@@ -146,6 +161,7 @@ struct cdfmm_b200_plan {
   int tc_m_tiles = 1, tc_acc_stride = 0; // accumulators per CTA, TMEM columns apart
   int tc_fuse = 0;                        // 1: A_hi x [B_hi | B_lo] as one N = 2 Npad MMA
   bool tc_pinned = false;                 // shape set by cdfmm_b200_set_m2l_shape: no autotuning
+  size_t tc_tuned_budget = 0;             // shared-memory budget the current shape was chosen for
   struct TcShape {
     int m_tiles, stages, fuse;
   };

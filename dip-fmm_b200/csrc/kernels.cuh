@@ -65,6 +65,16 @@ template <typename Kernel> inline bool allow_dynamic_smem(Kernel *kernel, size_t
   return true;
 }
 
+// Asks for the largest shared-memory carve-out of the unified L1 / shared
+// memory whenever `kernel` runs: kernels that share an SM must run under one
+// carve-out, and one sized for a smaller footprint would leave no room for
+// the other kernel's CTA.
+template <typename Kernel> inline void prefer_max_shared_carveout(Kernel *kernel) {
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributePreferredSharedMemoryCarveout,
+                           static_cast<int>(cudaSharedmemCarveoutMaxShared)) != cudaSuccess)
+    cudaGetLastError();
+}
+
 __host__ __device__ inline void demorton3(uint32_t m, int &x, int &y, int &z) {
   x = static_cast<int>(undilate3(m));
   y = static_cast<int>(undilate3(m >> 1));

@@ -1,5 +1,6 @@
 // M2L on the 5th-generation tensor cores (tcgen05), split BF16 with FP32
-// accumulation in tensor memory -- the batched (K >= 8 states) path.
+// accumulation in tensor memory (K states per call; fewer than 8 fill an
+// 8-row group of each MMA tile with zero rows).
 //
 // For one level, parity class c and a tile of T targets (rows = target x
 // state, 128 rows = one MMA M tile), the kernel accumulates over the 189 list2
@@ -527,6 +528,9 @@ void launch_bounded_wait_selftest(int *error_flag, cudaStream_t s) {
 }
 
 bool configure_m2l_tc(size_t max_smem) {
+  prefer_max_shared_carveout(m2l_tc_kernel<1>);
+  prefer_max_shared_carveout(m2l_tc_kernel<2>);
+  prefer_max_shared_carveout(m2l_tc_kernel<4>);
   return allow_dynamic_smem(m2l_tc_kernel<1>, max_smem) && allow_dynamic_smem(m2l_tc_kernel<2>, max_smem) &&
          allow_dynamic_smem(m2l_tc_kernel<4>, max_smem);
 }

@@ -84,6 +84,17 @@ __device__ inline void stage_source(const Neighbours &nb, int g, const float4 *s
   pos = make_float4(d.x + nb.sx[b], d.y + nb.sy[b], d.z + nb.sz[b], __int_as_float(j));
 }
 
+// Close pairs.  Positions are kept in FP32 relative to their leaf centre,
+// an absolute error of about 2^-25 leaf widths; for a pair much closer than
+// a leaf that error is no longer small against |r| (the reference builds its
+// pair tensors from FP64 positions).  The near-field kernels treat every
+// pair alike; the plan lists the pairs closer than a leaf width / 2^k (k >= 4,
+// chosen so the list stays within a few entries per target) with both the
+// FP32 r the kernels form and r from the FP64 positions, and a correction
+// pass after each near-field launch adds, per listed pair, its field at the
+// exact r minus its field at the FP32 r.  An exact zero r^2 in FP32 (the
+// self pair, or coincident points) is never listed.
+
 // One staged source pair (components .x, .y: two sources) against one
 // target in packed FP32x2 arithmetic.  With d = source - target (= -r) and
 // v = 1/|r|^3 the pair adds
@@ -454,7 +465,7 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
                                             const int4 *__restrict__ work, const int *__restrict__ self_idx,
                                             int depth, int K, float4 *__restrict__ near,
                                             const float4 *__restrict__ W, int k_begin, int k_end, int accumulate,
-                                            float acc_phi_scale) {
+                                            float acc_phi_scale, int unit_index) {
   constexpr bool PHI = MODE == 1;
   constexpr bool GRAD = MODE == 2;
   extern __shared__ float4 dynb[];
@@ -462,7 +473,7 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
   int *sIdx = reinterpret_cast<int *>(sPos + kNeighbourCap);      // [kNeighbourCap]
   float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [kBufs][kChunkB][Kr <= SB + 9]
   __shared__ Neighbours nb;
-  const int4 unit = work[blockIdx.x];
+  const int4 unit = work[unit_index];
   const int leaf = unit.x;
   const int t0 = unit.y;
   const int nt = unit.z;
@@ -660,19 +671,32 @@ __global__ void __launch_bounds__(kKbThreads, 2)
                   float4 *__restrict__ near, const float4 *__restrict__ W, int k_begin, int k_end, int accumulate,
                   float acc_phi_scale) {
   p2p_kb_body<KG, MODE, PAIRED, kStateBlock>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W,
-                                             k_begin, k_end, accumulate, acc_phi_scale);
+                                             k_begin, k_end, accumulate, acc_phi_scale, blockIdx.x);
 }
 
-// The co-resident form (see kStateBlockCorun).
+// The co-resident form (see kStateBlockCorun), persistent: the grid is two
+// CTAs per SM, each taking work units from `next_unit` (zero at launch) until
+// none are left.  A kernel with CTAs still waiting to be placed keeps a
+// lower-priority kernel's CTAs off the SMs even where they would fit, so the
+// near field leaves nothing waiting: every CTA is placed at launch and the
+// far field's CTAs take the room left beside them.
 template <int KG, int MODE, bool PAIRED>
 __global__ void __maxnreg__(kKbRegsCorun)
     p2p_kb_corun_kernel(const float4 *__restrict__ src_rel, const float4 *__restrict__ mom,
                         const int *__restrict__ src_off, const float4 *__restrict__ tgt_rel,
-                        const int4 *__restrict__ work, const int *__restrict__ self_idx, int depth, int K,
-                        float4 *__restrict__ near, const float4 *__restrict__ W, int k_begin, int k_end,
-                        int accumulate, float acc_phi_scale) {
-  p2p_kb_body<KG, MODE, PAIRED, kStateBlockCorun>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W,
-                                                  k_begin, k_end, accumulate, acc_phi_scale);
+                        const int4 *__restrict__ work, int n_work, int *__restrict__ next_unit,
+                        const int *__restrict__ self_idx, int depth, int K, float4 *__restrict__ near,
+                        const float4 *__restrict__ W, int k_begin, int k_end, int accumulate, float acc_phi_scale) {
+  __shared__ int s_unit;
+  for (;;) {
+    __syncthreads(); // the previous unit is done with shared memory (and s_unit)
+    if (threadIdx.x == 0) s_unit = atomicAdd(next_unit, 1);
+    __syncthreads();
+    const int u = s_unit;
+    if (u >= n_work) break;
+    p2p_kb_body<KG, MODE, PAIRED, kStateBlockCorun>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near,
+                                                    W, k_begin, k_end, accumulate, acc_phi_scale, u);
+  }
 }
 
 // FP64 O(N*M) direct sum, one thread per target, sources tiled through
@@ -804,11 +828,14 @@ template <int KG, bool PAIRED, int MODE>
 void launch_kb_mode(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                     const int4 *work, int n_work, const int *self_idx, int depth, int K, float4 *near,
                     const float4 *W, cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale,
-                    bool corun) {
-  if (corun)
-    p2p_kb_corun_kernel<KG, MODE, PAIRED><<<n_work, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlockCorun), s>>>(
-        src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
-  else
+                    const CorunLaunch *corun) {
+  if (corun != nullptr) {
+    cudaMemsetAsync(corun->next_unit, 0, sizeof(int), s);
+    const int grid = std::min(n_work, corun->ctas);
+    p2p_kb_corun_kernel<KG, MODE, PAIRED><<<grid, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlockCorun), s>>>(
+        src_rel, mom, src_off, tgt_rel, work, n_work, corun->next_unit, self_idx, depth, K, near, W, k_begin, k_end,
+        accumulate, acc_phi_scale);
+  } else
     p2p_kb_kernel<KG, MODE, PAIRED><<<n_work, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlock), s>>>(
         src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
 }
@@ -816,7 +843,7 @@ void launch_kb_mode(const float4 *src_rel, const float4 *mom, const int *src_off
 template <int KG, bool PAIRED>
 void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                const int4 *work, int n_work, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-               cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale, bool corun) {
+               cudaStream_t s, int k_begin, int k_end, int accumulate, float acc_phi_scale, const CorunLaunch *corun) {
   if (n_work == 0) return;
   if (mode == 1)
     launch_kb_mode<KG, PAIRED, 1>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, near, W, s, k_begin,
@@ -834,8 +861,8 @@ void launch_kb(const float4 *src_rel, const float4 *mom, const int *src_off, con
 // slower at K = 64: the accumulators no longer fit the register budget.)
 void launch_kb_any(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                    const int4 *work, int n_work, const int *self_idx, int depth, int K, int mode, float4 *near, const float4 *W,
-                   cudaStream_t s, int k_begin = 0, int k_end = -1, int accumulate = 0, float acc_phi_scale = 1.0F,
-                   bool corun = false) {
+                   cudaStream_t s, int k_begin = 0, int k_end = -1, int accumulate = 0,
+                   float acc_phi_scale = 1.0F, const CorunLaunch *corun = nullptr) {
   if (k_end < 0) k_end = K;
   if (K >= 8)
     launch_kb<8, true>(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, mode, near, W, s, k_begin, k_end, accumulate, acc_phi_scale, corun);
@@ -897,11 +924,143 @@ std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int dep
   return out;
 }
 
+namespace {
+
+// Moment of state k of sorted source j (paired rows for K >= 4, else plain).
+template <bool PAIRED>
+__device__ __forceinline__ float3 moment_of(const float4 *mom, int j, int K, int k) {
+  if constexpr (PAIRED) {
+    const float4 *row = mom + static_cast<long long>(j) * ((K + 1) & ~1) + (k & ~1);
+    const float4 a = row[0], b = row[1];
+    return (k & 1) ? make_float3(a.y, a.w, b.y) : make_float3(a.x, a.z, b.x);
+  } else {
+    const float4 m = mom[static_cast<long long>(j) * K + k];
+    return make_float3(m.x, m.y, m.z);
+  }
+}
+
+// Pair field at r (= target - source) for moment m: (phi, H) times 4 pi.
+__device__ __forceinline__ float4 pair_field(float rx, float ry, float rz, float3 m) {
+  const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+  const float rinv = rsqrtf(r2);
+  const float v = rinv * rinv * rinv;
+  const float mr = fmaf(m.x, rx, fmaf(m.y, ry, m.z * rz));
+  const float f = 3.0F * mr * v * rinv * rinv;
+  return make_float4(mr * v, fmaf(f, rx, -v * m.x), fmaf(f, ry, -v * m.y), fmaf(f, rz, -v * m.z));
+}
+// Position gradient of w . H (times 4 pi) at r for moment m.
+__device__ __forceinline__ float3 pair_grad(float rx, float ry, float rz, float3 m, float3 w) {
+  const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+  const float rinv = rsqrtf(r2);
+  const float r2inv = rinv * rinv;
+  const float f5 = 3.0F * r2inv * r2inv * rinv, f7 = 5.0F * f5 * r2inv;
+  const float a = fmaf(m.x, rx, fmaf(m.y, ry, m.z * rz)), b = fmaf(w.x, rx, fmaf(w.y, ry, w.z * rz));
+  const float c = fmaf(w.x, m.x, fmaf(w.y, m.y, w.z * m.z));
+  const float coef = fmaf(f5, c, -f7 * a * b);
+  return make_float3(fmaf(f5, fmaf(b, m.x, a * w.x), coef * rx), fmaf(f5, fmaf(b, m.y, a * w.y), coef * ry),
+                     fmaf(f5, fmaf(b, m.z, a * w.z), coef * rz));
+}
+
+// Close-pair correction (see above): one warp per listed target, which walks
+// its pairs (skipping its current self source); the lanes take the states
+// k_begin + lane, + 32, ... and add (field at the exact r) - (field at the
+// FP32 r), times 1 / (4 pi), to the near-field result in the form the
+// kernel wrote it:
+//   MODE 0 / 1: field / field and potential, near[i][K] (accumulate 1: onto
+//     the far field, potential times phi_scale; accumulate 2: potential only);
+//   MODE 2: the position gradient summed over the states, added to the
+//     partial sum of state group 0, gpart[i][G].
+// Both fields are formed in FP32 at their own r; at a close pair's r the
+// exact one is as accurate as FP32 arithmetic allows.
+template <int MODE, bool PAIRED>
+__global__ void __launch_bounds__(256) p2p_close_correction_kernel(const float4 *__restrict__ mom, CloseGeometry cg,
+                                                                   const int *__restrict__ self_idx, int K,
+                                                                   float4 *__restrict__ near,
+                                                                   const float4 *__restrict__ W, int G, int k_begin,
+                                                                   int k_end, int accumulate, float acc_phi_scale) {
+  const int lane = threadIdx.x & 31;
+  const int entry = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (entry >= cg.n_targets) return;
+  const int4 ct = cg.targets[entry]; // (target, first pair, pairs, 0)
+  const int i = ct.x;
+  const int self = self_idx != nullptr ? self_idx[i] : -1;
+  float3 gsum = make_float3(0.0F, 0.0F, 0.0F);
+  for (int q = ct.y; q < ct.y + ct.z; ++q) {
+    const float4 rf = cg.r_fp32[q]; // .w: sorted source index
+    const float4 re = cg.r_exact[q];
+    const int j = __float_as_int(rf.w);
+    if (j == self) continue;
+    for (int k = k_begin + lane; k < k_end; k += 32) {
+      const float3 mk = moment_of<PAIRED>(mom, j, K, k);
+      if constexpr (MODE == 2) {
+        const float4 wv = W[static_cast<long long>(i) * K + k];
+        const float3 wk = make_float3(wv.x, wv.y, wv.z);
+        const float3 ge = pair_grad(re.x, re.y, re.z, mk, wk);
+        const float3 gf = pair_grad(rf.x, rf.y, rf.z, mk, wk);
+        gsum.x += ge.x - gf.x;
+        gsum.y += ge.y - gf.y;
+        gsum.z += ge.z - gf.z;
+      } else {
+        const float4 fe = pair_field(re.x, re.y, re.z, mk);
+        const float4 ff = pair_field(rf.x, rf.y, rf.z, mk);
+        const float dphi = (fe.x - ff.x) * kInvFourPiF;
+        const float dhx = (fe.y - ff.y) * kInvFourPiF, dhy = (fe.z - ff.z) * kInvFourPiF;
+        const float dhz = (fe.w - ff.w) * kInvFourPiF;
+        float4 &o = near[static_cast<long long>(i) * K + k];
+        float4 v = o;
+        if (accumulate != 0) {
+          if (MODE == 1) v.x = fmaf(dphi, acc_phi_scale, v.x);
+          if (accumulate == 1) {
+            v.y += dhx;
+            v.z += dhy;
+            v.w += dhz;
+          }
+        } else {
+          if (MODE == 1) v.x += dphi;
+          v.y += dhx;
+          v.z += dhy;
+          v.w += dhz;
+        }
+        o = v;
+      }
+    }
+  }
+  if constexpr (MODE == 2) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      gsum.x += __shfl_xor_sync(0xffffffffu, gsum.x, o);
+      gsum.y += __shfl_xor_sync(0xffffffffu, gsum.y, o);
+      gsum.z += __shfl_xor_sync(0xffffffffu, gsum.z, o);
+    }
+    if (lane == 0) {
+      float4 &g = near[static_cast<long long>(i) * G];
+      g = make_float4(fmaf(gsum.x, kInvFourPiF, g.x), fmaf(gsum.y, kInvFourPiF, g.y), fmaf(gsum.z, kInvFourPiF, g.z),
+                      g.w);
+    }
+  }
+}
+
+template <int MODE>
+void launch_close_correction(const float4 *mom, const CloseGeometry &cg, const int *self_idx, int K, float4 *near,
+                             const float4 *W, int G, int k_begin, int k_end, int accumulate, float acc_phi_scale,
+                             cudaStream_t s) {
+  if (cg.n_targets == 0) return;
+  const int grid = (cg.n_targets + 7) / 8;
+  if (K >= 4)
+    p2p_close_correction_kernel<MODE, true><<<grid, 256, 0, s>>>(mom, cg, self_idx, K, near, W, G, k_begin, k_end,
+                                                                 accumulate, acc_phi_scale);
+  else
+    p2p_close_correction_kernel<MODE, false><<<grid, 256, 0, s>>>(mom, cg, self_idx, K, near, W, G, k_begin, k_end,
+                                                                  accumulate, acc_phi_scale);
+}
+
+} // namespace
+
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
-                const int2 *leaf_self, int depth, int K,
+                const int2 *leaf_self, const CloseGeometry &cg, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end, int accumulate,
-                float phi_scale, bool corun) {
+                float phi_scale, const CorunLaunch *corun) {
   if (n_work == 0) return;
   if (K == 1) {
     if (want_phi)
@@ -914,14 +1073,108 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
     launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
                   k_begin, k_end, accumulate, phi_scale, corun);
   }
+  const int kb = k_begin, ke = k_end < 0 ? K : k_end;
+  if (want_phi)
+    launch_close_correction<1>(mom, cg, self_idx, K, near, nullptr, 0, kb, ke, accumulate, phi_scale, s);
+  else
+    launch_close_correction<0>(mom, cg, self_idx, K, near, nullptr, 0, kb, ke, accumulate, phi_scale, s);
 }
 
 int p2p_grad_groups(int K) { return K >= 8 ? (K + 7) / 8 : (K + 3) / 4; }
 
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
-                     const int4 *work, int n_work, const int *self_idx, int depth, int K, const float4 *W, float4 *gpart,
-                     cudaStream_t s) {
+                     const int4 *work, int n_work, const int *self_idx, const CloseGeometry &cg, int depth, int K,
+                     const float4 *W, float4 *gpart, cudaStream_t s) {
   launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, 2, gpart, W, s);
+  launch_close_correction<2>(mom, cg, self_idx, K, gpart, W, p2p_grad_groups(K), 0, K, 0, 1.0F, s);
+}
+
+namespace {
+
+// Close-pair search over every target's list 1, with r formed in FP32
+// exactly as the near-field kernels form it (staged source = leaf-relative
+// position + neighbour offset; exactly coincident points excluded).  COUNT:
+// counts[i][l] = pairs with r^2 below thresholds[l] (l < kCloseLevels);
+// else: writes the pairs of threshold r2_max from out_first[i] on, as
+// (FP32 r, source index in .w) and r from the FP64 root-normalised positions.
+// One CTA per work unit (at most 128 targets, one thread each), the
+// neighbourhood staged in chunks of kSearchChunk.
+constexpr int kSearchChunk = 512;
+
+template <bool COUNT>
+__global__ void __launch_bounds__(128) p2p_close_search_kernel(
+    const float4 *__restrict__ src_rel, const int *__restrict__ src_off, const float4 *__restrict__ tgt_rel,
+    const int4 *__restrict__ work, int depth, float4 thresholds, int *__restrict__ counts, float r2_max,
+    const int *__restrict__ out_first, const double *__restrict__ src_abs, const double *__restrict__ tgt_abs,
+    float4 *__restrict__ r_fp32, float4 *__restrict__ r_exact) {
+  __shared__ Neighbours nb;
+  __shared__ float4 sPos[kSearchChunk];
+  const int4 unit = work[blockIdx.x];
+  if (threadIdx.x < 32) build_neighbours(nb, unit.x, depth, src_off, threadIdx.x);
+  __syncthreads();
+  const int total = nb.prefix[nb.count];
+  const bool mine = static_cast<int>(threadIdx.x) < unit.z;
+  const int i = unit.y + (mine ? static_cast<int>(threadIdx.x) : 0);
+  const float4 t = tgt_rel[i];
+  int c0 = 0, c1 = 0, c2 = 0, c3 = 0;
+  int out = (!COUNT && mine) ? out_first[i] : 0;
+  for (int sc = 0; sc < total; sc += kSearchChunk) {
+    const int sn = min(kSearchChunk, total - sc);
+    __syncthreads();
+    for (int q = threadIdx.x; q < sn; q += blockDim.x) {
+      float4 p;
+      int j;
+      stage_source(nb, sc + q, src_rel, p, j);
+      sPos[q] = p;
+    }
+    __syncthreads();
+    if (!mine) continue;
+    for (int q = 0; q < sn; ++q) {
+      const float4 p = sPos[q];
+      const float rx = t.x - p.x, ry = t.y - p.y, rz = t.z - p.z;
+      const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+      if (!(r2 > 0.0F)) continue;
+      if constexpr (COUNT) {
+        c0 += r2 < thresholds.x;
+        c1 += r2 < thresholds.y;
+        c2 += r2 < thresholds.z;
+        c3 += r2 < thresholds.w;
+      } else if (r2 < r2_max) {
+        const int j = __float_as_int(p.w);
+        r_fp32[out] = make_float4(rx, ry, rz, p.w);
+        r_exact[out] = make_float4(static_cast<float>(tgt_abs[3LL * i] - src_abs[3LL * j]),
+                                   static_cast<float>(tgt_abs[3LL * i + 1] - src_abs[3LL * j + 1]),
+                                   static_cast<float>(tgt_abs[3LL * i + 2] - src_abs[3LL * j + 2]), 0.0F);
+        ++out;
+      }
+    }
+  }
+  if (COUNT && mine) {
+    counts[4 * i] = c0;
+    counts[4 * i + 1] = c1;
+    counts[4 * i + 2] = c2;
+    counts[4 * i + 3] = c3;
+  }
+}
+
+} // namespace
+
+void launch_p2p_close_count(const float4 *src_rel, const int *src_off, const float4 *tgt_rel, const int4 *work,
+                            int n_work, int depth, const float (&thresholds)[kCloseLevels], int *counts,
+                            cudaStream_t s) {
+  if (n_work == 0) return;
+  p2p_close_search_kernel<true><<<n_work, 128, 0, s>>>(
+      src_rel, src_off, tgt_rel, work, depth, make_float4(thresholds[0], thresholds[1], thresholds[2], thresholds[3]),
+      counts, 0.0F, nullptr, nullptr, nullptr, nullptr, nullptr);
+}
+
+void launch_p2p_close_write(const float4 *src_rel, const int *src_off, const float4 *tgt_rel, const int4 *work,
+                            int n_work, int depth, float r2_max, const int *out_first, const double *src_abs,
+                            const double *tgt_abs, float4 *r_fp32, float4 *r_exact, cudaStream_t s) {
+  if (n_work == 0) return;
+  p2p_close_search_kernel<false><<<n_work, 128, 0, s>>>(src_rel, src_off, tgt_rel, work, depth,
+                                                        make_float4(0.0F, 0.0F, 0.0F, 0.0F), nullptr, r2_max,
+                                                        out_first, src_abs, tgt_abs, r_fp32, r_exact);
 }
 
 template <int KG, bool PAIRED> void configure_p2p_kb(size_t max_smem) {
@@ -931,6 +1184,20 @@ template <int KG, bool PAIRED> void configure_p2p_kb(size_t max_smem) {
   allow_dynamic_smem(p2p_kb_corun_kernel<KG, 0, PAIRED>, max_smem);
   allow_dynamic_smem(p2p_kb_corun_kernel<KG, 1, PAIRED>, max_smem);
   allow_dynamic_smem(p2p_kb_corun_kernel<KG, 2, PAIRED>, max_smem);
+  // the co-resident form shares its SMs with a far-field CTA
+  prefer_max_shared_carveout(p2p_kb_corun_kernel<KG, 0, PAIRED>);
+  prefer_max_shared_carveout(p2p_kb_corun_kernel<KG, 1, PAIRED>);
+  prefer_max_shared_carveout(p2p_kb_corun_kernel<KG, 2, PAIRED>);
+}
+
+size_t p2p_corun_cta_smem(int K) {
+  cudaFuncAttributes attr{};
+  if (K >= 8) {
+    cudaFuncGetAttributes(&attr, p2p_kb_corun_kernel<8, 1, true>);
+    return p2p_kb_smem_bytes<8>(K, kStateBlockCorun) + attr.sharedSizeBytes;
+  }
+  cudaFuncGetAttributes(&attr, p2p_kb_corun_kernel<4, 1, true>);
+  return p2p_kb_smem_bytes<4>(K, kStateBlockCorun) + attr.sharedSizeBytes;
 }
 
 void configure_p2p(size_t max_smem) {

@@ -122,7 +122,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   const int K = a->n_states;
   const int n = plan->n;
   const bool use_tc = plan->depth >= 2 && plan->tc_supported && K <= 128 &&
-                      (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || (plan->m2l_mode == CDFMM_B200_M2L_AUTO && K >= 8));
+                      (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || plan->m2l_mode == CDFMM_B200_M2L_AUTO);
   const int Kp = round_up(K, 8);
   const int node_base = level_offset(2);
   const int boxes = plan->n_nodes - node_base;
@@ -177,7 +177,9 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0);
   launch_p2p(plan->src_rel, mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
              plan->has_self ? plan->self_idx : nullptr, plan->leaf_self,
-             plan->depth, K, want_phi, near, plan->near_stream);
+             CloseGeometry{plan->close_targets, plan->n_close_targets, plan->close_r_fp32, plan->close_r_exact},
+             plan->depth, K, want_phi, near,
+             plan->near_stream);
   cudaEventRecord(plan->ev_join, plan->near_stream);
   launch_p2m(plan->src_rel, mom, plan->src_off, plan->basis, M, n, plan->p, K, plan->depth, plan->p2m_chunk, s);
   for (int level = plan->depth - 1; level >= 0; --level)

@@ -100,7 +100,8 @@ void free_plan(cdfmm_b200_plan *p) {
                   p->self_idx, p->leaf_self, p->p2p_work, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
-                  p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad};
+                  p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
+                  p->close_targets, p->close_r_fp32, p->close_r_exact};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
   if (p->p2p_work_wide != nullptr && p->p2p_work_wide != p->p2p_work) cudaFree(p->p2p_work_wide);
@@ -147,6 +148,16 @@ std::vector<float4> relative_positions(const double *pos, const int32_t *leaf_of
                                                 static_cast<float>(np[2] - nc[2]), 0.0F);
     }
   }
+  return out;
+}
+
+// Root-normalised FP64 positions ((x - centre) / scale), [n][3]: the exact
+// geometry of pairs much closer than a leaf (see p2p_close_r2).
+std::vector<double> normalised_positions(const double *pos, size_t n, const double centre[3], double scale) {
+  std::vector<double> out(3 * n);
+  const double inv = 1.0 / scale;
+  for (size_t j = 0; j < n; ++j)
+    for (int a = 0; a < 3; ++a) out[3 * j + a] = (pos[3 * j + a] - centre[a]) * inv;
   return out;
 }
 
@@ -201,6 +212,77 @@ std::string cdfmm_b200_own_status(cdfmm_b200_plan *plan, unsigned long long call
   const int calls = count - plan->status_seen;
   plan->status_seen = count;
   return timeout_message(r->code, calls, true);
+}
+
+// The plan's close-pair list (see CloseGeometry): counts every target's
+// pairs below four thresholds (leaf width / 2^k, k = kCloseShift .. + 3),
+// takes the largest threshold whose list holds at most 4 pairs per target
+// on average (dense clusters get a smaller one; the closest pairs, which
+// need the exact r most, are always inside it), and writes the list.  A
+// geometry with more than 64 pairs per target even at the smallest
+// threshold keeps no list (close_shift = -1).
+static void build_close_pairs(cdfmm_b200_plan *plan, const cdfmm_b200_plan_desc *desc, uint64_t &bytes,
+                              uint64_t &h2d) {
+  plan->n_close_targets = 0;
+  plan->close_pairs = 0;
+  plan->close_shift = -1;
+  if (plan->nt == 0 || plan->ns == 0 || plan->n_p2p_work_wide == 0) return;
+  float thr[kCloseLevels];
+  for (int l = 0; l < kCloseLevels; ++l)
+    thr[l] = static_cast<float>(std::ldexp(1.0, -2 * (plan->depth + kCloseShift + l)));
+  uint64_t tmp = 0;
+  int *counts = dalloc<int>(4 * static_cast<size_t>(plan->nt), tmp);
+  launch_p2p_close_count(plan->src_rel, plan->src_off, plan->tgt_rel, plan->p2p_work_wide, plan->n_p2p_work_wide,
+                         plan->depth, thr, counts, nullptr);
+  std::vector<int> h(4 * static_cast<size_t>(plan->nt));
+  cudaError_t e = cudaMemcpy(h.data(), counts, sizeof(int) * h.size(), cudaMemcpyDeviceToHost);
+  cudaFree(counts);
+  check(e, "close-pair count");
+  long long total[kCloseLevels] = {};
+  for (int i = 0; i < plan->nt; ++i)
+    for (int l = 0; l < kCloseLevels; ++l) total[l] += h[4 * static_cast<size_t>(i) + l];
+  int level = kCloseLevels - 1;
+  for (int l = 0; l < kCloseLevels; ++l)
+    if (total[l] <= 4LL * plan->nt + 1024) {
+      level = l;
+      break;
+    }
+  if (total[level] > 64LL * plan->nt + 1024) return;
+  plan->close_shift = kCloseShift + level;
+  if (total[level] == 0) return;
+  std::vector<int4> targets;
+  std::vector<int> first(static_cast<size_t>(plan->nt), 0);
+  int run = 0;
+  for (int i = 0; i < plan->nt; ++i) {
+    const int c = h[4 * static_cast<size_t>(i) + level];
+    first[static_cast<size_t>(i)] = run;
+    if (c > 0) targets.push_back(make_int4(i, run, c, 0));
+    run += c;
+  }
+  const std::vector<double> sabs = normalised_positions(desc->sorted_source_positions, static_cast<size_t>(plan->ns),
+                                                        plan->root_centre, plan->scale);
+  const std::vector<double> tabs = normalised_positions(desc->sorted_target_positions, static_cast<size_t>(plan->nt),
+                                                        plan->root_centre, plan->scale);
+  double *d_sabs = dalloc<double>(sabs.size(), tmp);
+  double *d_tabs = dalloc<double>(tabs.size(), tmp);
+  int *d_first = dalloc<int>(first.size(), tmp);
+  plan->close_r_fp32 = dalloc<float4>(static_cast<size_t>(run), bytes);
+  plan->close_r_exact = dalloc<float4>(static_cast<size_t>(run), bytes);
+  upload(d_sabs, sabs.data(), sabs.size(), h2d);
+  upload(d_tabs, tabs.data(), tabs.size(), h2d);
+  upload(d_first, first.data(), first.size(), h2d);
+  launch_p2p_close_write(plan->src_rel, plan->src_off, plan->tgt_rel, plan->p2p_work_wide, plan->n_p2p_work_wide,
+                         plan->depth, thr[level], d_first, d_sabs, d_tabs, plan->close_r_fp32, plan->close_r_exact,
+                         nullptr);
+  e = cudaDeviceSynchronize();
+  cudaFree(d_sabs);
+  cudaFree(d_tabs);
+  cudaFree(d_first);
+  check(e, "close-pair write");
+  plan->close_targets = dalloc<int4>(targets.size(), bytes);
+  upload(plan->close_targets, targets.data(), targets.size(), h2d);
+  plan->n_close_targets = static_cast<int>(targets.size());
+  plan->close_pairs = static_cast<uint64_t>(run);
 }
 
 void cdfmm_b200_record_error(cdfmm_b200_plan *plan, const std::string &msg) {
@@ -356,6 +438,8 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     {
       int sms = 0;
       check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device), "device attribute");
+      plan->sm_count = sms;
+      plan->p2p_next_unit = dalloc<int>(1, bytes);
       const std::vector<int4> work =
           p2p_work_units(desc->leaf_source_offsets, desc->leaf_target_offsets, plan->depth, sms, true);
       const std::vector<int4> wide =
@@ -372,6 +456,7 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
         plan->p2p_work_wide = dalloc<int4>(wide.size(), bytes);
         upload(plan->p2p_work_wide, wide.data(), wide.size(), h2d);
       }
+      build_close_pairs(plan, desc, bytes, h2d);
     }
     {
       std::vector<int> inv(static_cast<size_t>(std::max(plan->ns, plan->nt)), -1);
@@ -574,10 +659,11 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
       const int stages = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().stages;
       const int fuse0 = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().fuse;
       const int acc_stride = acc_stride_of(fuse0);
-      // AUTO uses the tensor cores from K = 8 states on: a plan that never
-      // evaluates 8 states at once does not allocate their operand buffers.
-      const bool wanted = desc->m2l_mode == CDFMM_B200_M2L_BF16X3 ||
-                          (desc->m2l_mode == CDFMM_B200_M2L_AUTO && desc->max_states >= 8);
+      // AUTO and BF16X3 run the M2L on the tensor cores for any K (fewer
+      // than 8 states fill 8-row groups of the MMA tile with zero rows: the
+      // tensor cores still beat the FP32 SIMT M2L several times over);
+      // FP32 keeps the SIMT M2L (the plain per-state path).
+      const bool wanted = desc->m2l_mode == CDFMM_B200_M2L_BF16X3 || desc->m2l_mode == CDFMM_B200_M2L_AUTO;
       plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 2 && wanted &&
                            configure_m2l_tc(smem);
       if (plan->tc_supported) {
@@ -693,7 +779,7 @@ static void upload_tc_tiles(cdfmm_b200_plan *plan, int Kp) {
 // give bit-identical results (the per-row MMA sequence is the same); the
 // fused form sums the hi*lo product in its own accumulator, a difference at
 // FP32 rounding level.
-static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
+static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s, size_t smem_budget) {
   const int Kp = round_up(K, 8);
   const int node_base = level_offset(2);
   TcArgs ta{};
@@ -714,7 +800,17 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
   ta.wait_limit = plan->tc_wait_limit;
   float best = 0.0F;
   int best_i = -1;
+  // candidates within the budget (all of them if none fits)
+  auto launch_smem = [&](const cdfmm_b200_plan::TcShape &c) {
+    const int acc = round_up(c.fuse ? 2 * plan->tc_Npad : plan->tc_Npad, 32);
+    size_t b = m2l_tc_smem_bytes(plan->tc_Npad, c.m_tiles, c.stages);
+    if (tmem_columns(c.m_tiles, acc) > 256) b = std::max<size_t>(b, 120 * 1024);
+    return b;
+  };
+  bool any_fits = false;
+  for (const cdfmm_b200_plan::TcShape &c : plan->tc_candidates) any_fits = any_fits || launch_smem(c) <= smem_budget;
   for (size_t c = 0; c < plan->tc_candidates.size(); ++c) {
+    if (any_fits && launch_smem(plan->tc_candidates[c]) > smem_budget) continue;
     const int mt = plan->tc_candidates[c].m_tiles;
     const std::vector<int4> tiles = build_tc_tiles(plan->depth, mt * (128 / Kp));
     grow(plan->tc_tiles, plan->tc_tiles_capacity, tiles.size(), "cudaMalloc tiles");
@@ -765,24 +861,71 @@ static int enqueue_upward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool tim
   return launches;
 }
 
+static CloseGeometry close_geometry(const cdfmm_b200_plan *plan) {
+  return CloseGeometry{plan->close_targets, plan->n_close_targets, plan->close_r_fp32, plan->close_r_exact};
+}
+
+// Whether K states take the tensor-core M2L.
+static bool m2l_on_tensor_cores(const cdfmm_b200_plan *plan, int K) {
+  return plan->depth >= 2 && plan->tc_supported && K <= 128 &&
+         (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || plan->m2l_mode == CDFMM_B200_M2L_AUTO);
+}
+
+// Near/far schedule of one evaluation (cdfmm_b200_set_schedule): the
+// co-resident schedule needs the tensor-core M2L (whose CTA fits beside two
+// co-resident near-field CTAs); other evaluations run SEPARATE.
+static int resolved_schedule(const cdfmm_b200_plan *plan, int K) {
+  if (K <= 1 || !m2l_on_tensor_cores(plan, K)) return CDFMM_B200_SCHEDULE_SEPARATE;
+  return plan->schedule == CDFMM_B200_SCHEDULE_AUTO ? CDFMM_B200_SCHEDULE_CORUN : plan->schedule;
+}
+
+// Shared memory one tensor-core M2L CTA may use to sit beside two
+// co-resident near-field CTAs on one SM.
+static size_t corun_m2l_smem_budget(const cdfmm_b200_plan *plan, int K) {
+  int per_sm = 0, reserved = 0;
+  cudaDeviceGetAttribute(&per_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, plan->device);
+  cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, plan->device);
+  const size_t near = p2p_corun_cta_smem(K) + static_cast<size_t>(reserved);
+  const size_t used = 2 * near + static_cast<size_t>(reserved);
+  return static_cast<size_t>(per_sm) > used ? static_cast<size_t>(per_sm) - used : 0;
+}
+
+// Tensor-core M2L operands: packs the scaled multipoles into BF16 hi/lo boxes
+// and, on the first use for this K (or after a schedule change), chooses the
+// pipeline shape -- the fastest candidate whose shared memory fits beside
+// the co-resident near field when K states run CORUN -- and builds its work
+// tiles.  Every path of the plan (device or host arrays, backward) then
+// uses that shape.  Returns the launch count.
+static int prepare_m2l(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
+  if (!m2l_on_tensor_cores(plan, K)) return 0;
+  const size_t smem_budget =
+      resolved_schedule(plan, K) == CDFMM_B200_SCHEDULE_CORUN ? corun_m2l_smem_budget(plan, K) : SIZE_MAX;
+  const int Kp = round_up(K, 8);
+  const int node_base = level_offset(2);
+  const int boxes = plan->n_nodes - node_base;
+  launch_m2l_pack(plan->M, plan->scale_m, plan->basis, plan->tc_a_hi, plan->tc_a_lo, plan->n, K, Kp, plan->tc_Kpad,
+                  plan->depth, node_base, boxes, s);
+  if (plan->tc_tiles_Kp != Kp || (!plan->tc_pinned && plan->tc_tuned_budget != smem_budget)) {
+    check(cudaStreamSynchronize(s), "sync");
+    if (plan->tc_candidates.size() > 1 && !plan->tc_pinned) tune_m2l_tc(plan, K, s, smem_budget);
+    plan->tc_tuned_budget = smem_budget;
+    upload_tc_tiles(plan, Kp);
+  }
+  return 1;
+}
+
 // Downward pass: M2L (tensor cores or FP32 SIMT) and L2L, leaving the leaf
-// local expansions in plan->L.  Returns the launch count.
-static int enqueue_downward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing) {
+// local expansions in plan->L.  prepared: prepare_m2l already ran for this
+// evaluation.  Returns the launch count.
+static int enqueue_downward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing, bool prepared = false) {
   const int n = plan->n;
   int launches = 0;
-    const bool use_tc = plan->depth >= 2 && plan->tc_supported && K <= 128 &&
-                        (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || (plan->m2l_mode == CDFMM_B200_M2L_AUTO && K >= 8));
+    const bool use_tc = m2l_on_tensor_cores(plan, K);
     if (use_tc) {
+      if (!prepared) launches += prepare_m2l(plan, K, s);
       const int Kp = round_up(K, 8);
       const int node_base = level_offset(2);
       const int boxes = plan->n_nodes - node_base;
-      launch_m2l_pack(plan->M, plan->scale_m, plan->basis, plan->tc_a_hi, plan->tc_a_lo, n, K, Kp, plan->tc_Kpad,
-                      plan->depth, node_base, boxes, s);
-      if (plan->tc_tiles_Kp != Kp) {
-        check(cudaStreamSynchronize(s), "sync");
-        if (plan->tc_candidates.size() > 1 && !plan->tc_pinned) tune_m2l_tc(plan, K, s);
-        upload_tc_tiles(plan, Kp);
-      }
       TcArgs ta{};
       ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
       ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
@@ -806,7 +949,7 @@ static int enqueue_downward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool t
       ta.box_bytes = static_cast<uint32_t>(Kp) * static_cast<uint32_t>(plan->tc_Kpad) * 2u;
       ta.wait_limit = plan->tc_wait_limit;
       launch_m2l_tc(ta, plan->tc_n_tiles, s);
-      launches += 2;
+      launches += 1;
       plan->stats.m2l_tc_m_tiles = plan->tc_m_tiles;
       plan->stats.m2l_tc_stages = plan->tc_stages;
       plan->stats.m2l_tc_fused = plan->tc_fuse;
@@ -831,11 +974,6 @@ static int enqueue_far(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing
   return launches + enqueue_downward(plan, K, s, timing);
 }
 
-// Near/far schedule of one evaluation of K > 1 states (cdfmm_b200_set_schedule).
-static int resolved_schedule(const cdfmm_b200_plan *plan, int K) {
-  if (K <= 1) return CDFMM_B200_SCHEDULE_SEPARATE;
-  return plan->schedule == CDFMM_B200_SCHEDULE_AUTO ? CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST : plan->schedule;
-}
 
 // Enqueues one evaluation of K states on stream s: device-resident moments
 // ([K][ns][3], dtype) -> gather -> (list-1 P2P on the near stream || P2M, M2M,
@@ -855,20 +993,24 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   // stage timing enabled it runs first on the main stream instead, so that
   // each stage's events measure that stage alone.
   //   SEPARATE: the full-size near-field kernel (two CTAs fill an SM) beside
-  //     the far field on a high-priority stream;
-  //   CORUN: the co-resident near-field form, two CTAs of which leave room
-  //     on every SM for one tensor-core M2L CTA, so the FP32 near field and
-  //     the tensor-core far field run side by side;
-  //   CORUN_UPWARD_FIRST: as CORUN, with P2M and M2M (short, HBM-bound, and
-  //     too large to sit beside the near field) run on all SMs first.
+  //     the far field on a high-priority stream (which in practice takes
+  //     most SMs while it runs: the two share the GPU by turns);
+  //   CORUN: P2M, M2M and the M2L operand pack run first on all SMs; then
+  //     the co-resident near-field form on the high-priority stream -- two
+  //     of its CTAs per SM, which leave room for exactly one tensor-core M2L
+  //     CTA -- beside M2L and L2L on a normal-priority stream, so an M2L CTA
+  //     only ever takes the slot the near field leaves free and the FP32
+  //     near field and the tensor-core far field run side by side on every
+  //     SM (the M2L's pipeline shape is chosen among those that fit there).
   const int schedule = timing ? CDFMM_B200_SCHEDULE_SEPARATE : resolved_schedule(plan, K);
-  const bool corun = schedule != CDFMM_B200_SCHEDULE_SEPARATE;
+  const bool corun = schedule == CDFMM_B200_SCHEDULE_CORUN;
   const bool trace = plan->trace && !timing;
-  cudaStream_t ns = timing ? s : plan->near_stream;
-  cudaStream_t fs = timing ? s : plan->far_stream;
-  if (schedule == CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST) {
+  cudaStream_t ns = timing ? s : (corun ? plan->far_stream : plan->near_stream);
+  cudaStream_t fs = timing ? s : (corun ? plan->near_stream : plan->far_stream);
+  if (corun) {
     if (trace) check(cudaEventRecord(plan->ev_t[kTraceFarBegin], s), "event");
     launches += enqueue_upward(plan, K, s, false);
+    launches += prepare_m2l(plan, K, s);
   }
   if (!timing) {
     check(cudaEventRecord(plan->ev_fork, s), "event");
@@ -881,9 +1023,11 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   // (same results bit for bit: a K = 1 target's sum does not depend on how
   // its leaf is cut into units).
   const bool wide = plan->in_batch && K == 1;
+  const CorunLaunch corun_launch{2 * plan->sm_count, plan->p2p_next_unit};
   launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, wide ? plan->p2p_work_wide : plan->p2p_work,
              wide ? plan->n_p2p_work_wide : plan->n_p2p_work, plan->has_self ? plan->self_idx : nullptr,
-             plan->leaf_self, plan->depth, K, want_phi, plan->near, ns, 0, -1, 0, 1.0F, corun);
+             plan->leaf_self, close_geometry(plan), plan->depth, K, want_phi, plan->near, ns, 0, -1, 0, 1.0F,
+             corun ? &corun_launch : nullptr);
   ++launches;
   if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
   if (trace) check(cudaEventRecord(plan->ev_t[kTraceP2pEnd], ns), "event");
@@ -891,9 +1035,9 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   if (!timing) check(cudaEventRecord(plan->ev_join, ns), "event");
 
   // far field
-  if (schedule == CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST) {
+  if (corun) {
     if (trace) check(cudaEventRecord(plan->ev_t[kTraceM2lBegin], fs), "event");
-    launches += enqueue_downward(plan, K, fs, false);
+    launches += enqueue_downward(plan, K, fs, false, true);
   } else {
     if (trace) check(cudaEventRecord(plan->ev_t[kTraceFarBegin], fs), "event");
     launches += enqueue_upward(plan, K, fs, timing);
@@ -1019,7 +1163,8 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
       auto near_part = [&](int j, bool accumulate) {
         const int k0 = bounds[j], kc = bounds[j + 1] - bounds[j];
         launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
-                   plan->has_self ? plan->self_idx : nullptr, plan->leaf_self, plan->depth, K, want_phi_p, plan->near, s, k0, k0 + kc,
+                   plan->has_self ? plan->self_idx : nullptr, plan->leaf_self, close_geometry(plan), plan->depth, K,
+                   want_phi_p, plan->near, s, k0, k0 + kc,
                    accumulate ? ((a->output & CDFMM_B200_OUTPUT_FIELD) != 0u ? 1 : 2) : 0, plan->phi_scale);
         ++launches;
       };
@@ -1334,7 +1479,7 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
       if (!reuse) enqueue_far(plan, K, s, false);
       plan->stats.backward_reused_forward = reuse ? 1 : 0;
       launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
-                      plan->has_self ? plan->self_idx : nullptr, plan->depth, K, W, gpart, s);
+                      plan->has_self ? plan->self_idx : nullptr, close_geometry(plan), plan->depth, K, W, gpart, s);
       launch_l2p_grad(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, W, gpart, G, plan->n, plan->p, K,
                       plan->nt, plan->depth, static_cast<float>(1.0 / plan->scale), out, s);
       check(cudaGetLastError(), "kernel launch");
@@ -1394,7 +1539,7 @@ int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled) {
 
 int cdfmm_b200_set_schedule(cdfmm_b200_plan *plan, int32_t schedule) {
   if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
-  if (schedule < CDFMM_B200_SCHEDULE_AUTO || schedule > CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST)
+  if (schedule < CDFMM_B200_SCHEDULE_AUTO || schedule > CDFMM_B200_SCHEDULE_CORUN)
     return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT, "unknown schedule");
   plan->schedule = schedule;
   return CDFMM_B200_OK;

@@ -34,7 +34,7 @@ MOMENTS_ON_HOST = 1
 RESULTS_ON_HOST = 2
 LAYOUT_SEPARATE = 0
 LAYOUT_INTERLEAVED = 1
-SCHEDULE_AUTO, SCHEDULE_SEPARATE, SCHEDULE_CORUN, SCHEDULE_CORUN_UPWARD_FIRST = 0, 1, 2, 3
+SCHEDULE_AUTO, SCHEDULE_SEPARATE, SCHEDULE_CORUN = 0, 1, 2
 
 EXPORTED = (
     "cdfmm_b200_device_count", "cdfmm_b200_device_info", "cdfmm_b200_plan_create",

@@ -49,7 +49,7 @@ extern "C" {
 #define CDFMM_B200_OUTPUT_FIELD 2u
 
 /* M2L arithmetic. */
-#define CDFMM_B200_M2L_AUTO 0        /* split-BF16 tensor cores where supported, else FP32 */
+#define CDFMM_B200_M2L_AUTO 0        /* split-BF16 tensor cores where supported (any K), else FP32 */
 #define CDFMM_B200_M2L_FP32 1        /* FP32 SIMT (the plain per-state path) */
 #define CDFMM_B200_M2L_BF16X3 2      /* tcgen05, BF16 hi/lo with three products, FP32 accumulate */
 
@@ -58,10 +58,10 @@ extern "C" {
 #define CDFMM_B200_RESULTS_ON_HOST 2u
 
 /* Near/far schedule of an evaluation of K > 1 states (cdfmm_b200_set_schedule). */
-#define CDFMM_B200_SCHEDULE_AUTO 0                 /* CORUN_UPWARD_FIRST */
-#define CDFMM_B200_SCHEDULE_SEPARATE 1             /* full-size near-field CTAs beside a high-priority far field */
-#define CDFMM_B200_SCHEDULE_CORUN 2                /* near-field CTAs sized to leave one far-field CTA per SM */
-#define CDFMM_B200_SCHEDULE_CORUN_UPWARD_FIRST 3   /* CORUN, with P2M and M2M on all SMs before the near field */
+#define CDFMM_B200_SCHEDULE_AUTO 0      /* CORUN where the M2L runs on the tensor cores, else SEPARATE */
+#define CDFMM_B200_SCHEDULE_SEPARATE 1  /* full-size near-field CTAs beside a high-priority far field */
+#define CDFMM_B200_SCHEDULE_CORUN 2     /* upward pass first; then near-field CTAs sized to leave one
+                                           tensor-core M2L CTA per SM, the near field at high priority */
 
 /* Result layout (cdfmm_b200_eval_args.layout). */
 #define CDFMM_B200_LAYOUT_SEPARATE 0    /* field[K][Nt][3] and potential[K][Nt] */
@@ -286,9 +286,10 @@ int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled);
 /* Near/far schedule for evaluations of K > 1 states (no counterpart in the
  * reference, which overlaps a cuSPARSE near field with its M2L on two
  * streams, src/cuda_fmm.cu:3295-3300, 3386-3391 upstream):
- * CDFMM_B200_SCHEDULE_*.  All schedules compute the same sums; the near
- * field's summation order differs between SEPARATE and the CORUN forms
- * (state blocks of 64 vs 32), at FP32 rounding level. */
+ * CDFMM_B200_SCHEDULE_*.  Both schedules compute the same sums; the near
+ * field's summation order differs between them (state blocks of 64 vs 32)
+ * and the M2L pipeline shape may too, at FP32 rounding level.  Evaluations
+ * whose M2L runs on the FP32 SIMT path always run SEPARATE. */
 int cdfmm_b200_set_schedule(cdfmm_b200_plan *plan, int32_t schedule);
 
 int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out);

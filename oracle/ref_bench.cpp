@@ -1,17 +1,21 @@
-// CpuStatic driver for the upstream dip-fmm reference (test / baseline
+// Timing driver for the upstream dip-fmm reference (test / baseline
 // infrastructure only; built by oracle/ref.mk into oracle/_ref/).
 //
 // It builds cdfmm::UniformFmm(sources, targets, options) exactly as a
 // reference user would (include/cdfmm/uniform_fmm.hpp:180-182 upstream), runs
 // `warmup` untimed and `steps` timed evaluate_into / evaluate_into_float32
 // calls (src/uniform_fmm.cpp:1065-1257 and :1281-1457 upstream), and writes
-// the last results plus a one-line JSON timing summary.
+// the last results plus a one-line JSON timing summary.  A timed step
+// evaluates every state once.  With the CudaFull backend (the reference's
+// own GPU path, src/cuda_fmm.cu:3457-3655 upstream; FP32, field only) the
+// summary also gives the median per-evaluation device-kernel, H2D and D2H
+// seconds the reference itself records (UniformFmm::last_timings).
 //
 // Input file (little endian), written by tests/ and bench.py:
 //   char[8]  "CDFMMIN1"
 //   int32    n_src, n_tgt, order, depth, precision(0=f32,1=f64),
 //            output_flags(1=phi,2=H,3=both), n_states, warmup, steps,
-//            use_fixed_map, has_root, backend(0=CpuStatic,1=CpuReference)
+//            use_fixed_map, has_root, backend(0=CpuStatic,1=CpuReference,2=CudaFull)
 //   float64  root_centre[3], root_half_width
 //   float64  sources[n_src][3], targets[n_tgt][3]
 //   float64  moments[n_states][n_src][3]
@@ -83,8 +87,9 @@ int main(int argc, char **argv) {
                                        : cdfmm::StaticPrecision::Float64;
     options.expansion_order = order;
     options.tree.max_level = depth;
-    options.backend = backend == 1 ? cdfmm::ExecutionBackend::CpuReference
-                                   : cdfmm::ExecutionBackend::CpuStatic;
+    options.backend = backend == 1   ? cdfmm::ExecutionBackend::CpuReference
+                      : backend == 2 ? cdfmm::ExecutionBackend::CudaFull
+                                     : cdfmm::ExecutionBackend::CpuStatic;
     if (backend == 1) options.m2l_backend = cdfmm::M2LBackend::Reference;
     if (has_root) {
       options.tree.root_centre = cdfmm::Vec3{root[0], root[1], root[2]};
@@ -126,12 +131,24 @@ int main(int argc, char **argv) {
       }
     };
     for (int w = 0; w < warmup; ++w) run_state(w % n_states);
-    std::vector<double> step_s;
+    std::vector<double> step_s, kernel_s, h2d_s, d2h_s;
     for (int s = 0; s < steps; ++s) {
       const auto a = std::chrono::steady_clock::now();
-      for (int k = 0; k < n_states; ++k) run_state(k);
+      for (int k = 0; k < n_states; ++k) {
+        run_state(k);
+        if (backend == 2) {
+          const cdfmm::EvaluationTimings &t = fmm.last_timings();
+          kernel_s.push_back(t.cuda_kernel.total_seconds);
+          h2d_s.push_back(t.cuda_h2d.total_seconds);
+          d2h_s.push_back(t.cuda_d2h.total_seconds);
+        }
+      }
       step_s.push_back(std::chrono::duration<double>(std::chrono::steady_clock::now() - a).count());
     }
+    auto median_of = [](std::vector<double> v) {
+      std::sort(v.begin(), v.end());
+      return v.empty() ? 0.0 : v[v.size() / 2];
+    };
     for (int k = 0; k < n_states; ++k) {
       run_state(k);
       store_state(k);
@@ -155,10 +172,12 @@ int main(int argc, char **argv) {
 #endif
     std::printf("{\"setup_s\": %.6f, \"steps\": %d, \"states_per_step\": %d, "
                 "\"median_step_s\": %.6f, \"total_timed_s\": %.6f, \"threads\": %d, "
-                "\"m2l_classes\": %zu, \"m2l_interactions\": %zu}\n",
+                "\"m2l_classes\": %zu, \"m2l_interactions\": %zu, \"backend\": %d, "
+                "\"median_kernel_s\": %.6f, \"median_h2d_s\": %.6f, \"median_d2h_s\": %.6f}\n",
                 setup_s, steps, n_states, median, total, threads,
                 fmm.static_plan_statistics().transfer_classes,
-                fmm.static_plan_statistics().interactions);
+                fmm.static_plan_statistics().interactions, backend, median_of(kernel_s), median_of(h2d_s),
+                median_of(d2h_s));
     return 0;
   } catch (const std::exception &e) {
     std::fprintf(stderr, "ref_bench error: %s\n", e.what());
