@@ -126,7 +126,7 @@ size_t p2p_corun_cta_smem(int K);
 int p2p_grad_groups(int K);
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                      const int4 *work, int n_work, const int *self_idx, const CloseGeometry &cg, int depth, int K,
-                     const float4 *W, float4 *gpart, cudaStream_t s);
+                     const float4 *W, float4 *gpart, cudaStream_t s, const CorunLaunch *corun = nullptr);
 // Far part (second derivatives of the leaf local expansions) plus the near
 // partial sums, scaled by inv_scale, written as out[user target][3].
 void launch_l2p_grad(const float *L, const float4 *tgt_rel, const int *tgt_off, const int *tgt_perm,

@@ -314,11 +314,13 @@ constexpr int kStateBlock = 64;     // states per state block (bounds shared mem
 constexpr int kKbThreads = 256;
 // Co-resident form: two CTAs of this kernel leave room on every SM for one
 // CTA of a far-field kernel (the tensor-core M2L: 128 threads, <= 56
-// registers, <= 100 KB of shared memory), so the near field and the far
+// registers, up to ~105 KB of shared memory), so the near field and the far
 // field run side by side instead of taking SMs from each other: state blocks
-// of 32 (61 KB of shared memory per CTA) and at most 112 registers per thread
-// (2 x 256 x 112 + 128 x 56 <= 65,536).
+// of 32 (58 KB of shared memory per CTA; moment chunks of 24 sources, 47.5
+// KB, were measured slower with no gain for the M2L beside them) and at most
+// 112 registers per thread (2 x 256 x 112 + 128 x 56 <= 65,536).
 constexpr int kStateBlockCorun = 32;
+constexpr int kChunkCorun = 32;
 constexpr int kKbRegsCorun = 112;
 
 // Shared-memory position of state k within a staged moment row (one pad
@@ -334,7 +336,7 @@ template <int KG> __host__ __device__ __forceinline__ int mrow_stride(int Kw) {
 // groups start at multiples of 8), rows Kr float4 apart.  FULL: all KG states
 // valid (no per-state predicate).
 template <int KG, bool PHI, bool FULL>
-__device__ __forceinline__ void p2p_kb_chunk(const float4 &ti, int self, const float4 *sPos, const int *sIdx,
+__device__ __forceinline__ void p2p_kb_chunk(const float4 &ti, int self, const float4 *sPos,
                                              const float4 *m_row0, int Kr, int qbeg, int sn, int F, int kvalid,
                                              float (&acc)[KG][4]) {
 #pragma unroll 2
@@ -342,7 +344,7 @@ __device__ __forceinline__ void p2p_kb_chunk(const float4 &ti, int self, const f
     const float4 s = sPos[q];
     const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const bool is_self = sIdx[q] == self;
+    const bool is_self = __float_as_int(s.w) == self;
     const float rinv = is_self ? 0.0F : rsqrtf(r2);
     const float v = rinv * rinv * rinv;
     const float f = 3.0F * v * rinv * rinv;
@@ -411,7 +413,7 @@ __device__ __forceinline__ void p2p_kb_chunk_x2(const float4 &ti, int self_q, co
 // C = sum(w.m), P = sum(a b) over the states.  Self pairs give zero; a
 // coincident non-self pair gives NaN like the forward field.
 template <int KG, bool FULL, bool PAIRED>
-__device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const float4 *sPos, const int *sIdx,
+__device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const float4 *sPos,
                                                const float4 *m_row0, int Kr, int qbeg, int sn, int F, int kvalid,
                                                const float (&w)[KG][3], float (&g)[3]) {
 #pragma unroll 2
@@ -419,7 +421,7 @@ __device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const
     const float4 s = sPos[q];
     const float dx = ti.x - s.x, dy = ti.y - s.y, dz = ti.z - s.z;
     const float r2 = fmaf(dx, dx, fmaf(dy, dy, dz * dz));
-    const bool is_self = sIdx[q] == self;
+    const bool is_self = __float_as_int(s.w) == self;
     const float rinv = is_self ? 0.0F : rsqrtf(r2);
     const float r2inv = rinv * rinv;
     const float f5 = 3.0F * r2inv * r2inv * rinv;
@@ -457,9 +459,10 @@ __device__ __forceinline__ void p2p_grad_chunk(const float4 &ti, int self, const
 //    gpart[nt][G] (G = ceil(K / KG)) from the weights W[nt][K] (plain layout).
 // PAIRED: the sorted moments use the paired layout (rows of round_up(K, 2)
 // float4), K >= 4.
-// SB: states per state block (kStateBlock, or kStateBlockCorun for the
-// co-resident form).
-template <int KG, int MODE, bool PAIRED, int SB>
+// SB: states per state block, CB: sources per moment chunk at the widest
+// state window (kStateBlock, kChunkB; or kStateBlockCorun, kChunkCorun for
+// the co-resident form).
+template <int KG, int MODE, bool PAIRED, int SB, int CB>
 __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, const float4 *__restrict__ mom,
                                             const int *__restrict__ src_off, const float4 *__restrict__ tgt_rel,
                                             const int4 *__restrict__ work, const int *__restrict__ self_idx,
@@ -470,8 +473,7 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
   constexpr bool GRAD = MODE == 2;
   extern __shared__ float4 dynb[];
   float4 *sPos = dynb;                                            // [kNeighbourCap]
-  int *sIdx = reinterpret_cast<int *>(sPos + kNeighbourCap);      // [kNeighbourCap]
-  float4 *sMom = reinterpret_cast<float4 *>(sIdx + kNeighbourCap); // [kBufs][kChunkB][Kr <= SB + 9]
+  float4 *sMom = sPos + kNeighbourCap;                            // [kBufs][CB][Kr <= SB + 9]
   __shared__ Neighbours nb;
   const int4 unit = work[unit_index];
   const int leaf = unit.x;
@@ -512,10 +514,10 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
       const int k_hi = min(Kc, ((ib + r - 1) / nt + 1) * KG);
       const int Kw = PAIRED ? (k_hi - k_lo + 1) & ~1 : k_hi - k_lo; // staged float4 units per source
       const int Kr = mrow_stride<KG>(Kw);
-      // sources per chunk: kChunkB at the widest window, more for narrower
-      // windows (a chunk buffer holds kChunkB rows of the widest stride), so
+      // sources per chunk: CB at the widest window, more for narrower
+      // windows (a chunk buffer holds CB rows of the widest stride), so
       // each chunk carries about the same work between barriers
-      const int chunkB = kChunkB * (mrow_stride<KG>((min(K, SB) + 1) & ~1) / Kr);
+      const int chunkB = CB * (mrow_stride<KG>((min(K, SB) + 1) & ~1) / Kr);
       const int mrow = PAIRED ? (K + 1) & ~1 : K;                   // global row length (float4)
       const int i = t0 + t;
       const float4 ti = tgt_rel[i];
@@ -553,7 +555,6 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
             int j;
             stage_source(nb, pass + q, src_rel, pos, j);
             sPos[q] = pos;
-            sIdx[q] = j;
           }
           __syncthreads();
           staged = true;
@@ -569,7 +570,8 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
           float4 *dst = sMom + (c % kBufs) * chunkB * Kr;
           int q = cq0, k = ck0;
           while (q < sn) {
-            cp_async16(dst + q * Kr + mrow_pos<KG>(k), mom + static_cast<long long>(sIdx[q0 + q]) * mrow + kblk + k_lo + k);
+            cp_async16(dst + q * Kr + mrow_pos<KG>(k),
+                       mom + static_cast<long long>(__float_as_int(sPos[q0 + q].w)) * mrow + kblk + k_lo + k);
             q += cqs;
             k += cks;
             if (k >= Kw) {
@@ -598,10 +600,10 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
             const float4 *m_row0 = sMom + (c % kBufs) * chunkB * Kr + mrow_pos<KG>(kb - k_lo);
             if constexpr (GRAD) {
               if (kvalid == KG)
-                p2p_grad_chunk<KG, true, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
+                p2p_grad_chunk<KG, true, PAIRED>(ti, self, sPos + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
                                                  gacc);
               else
-                p2p_grad_chunk<KG, false, PAIRED>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
+                p2p_grad_chunk<KG, false, PAIRED>(ti, self, sPos + q0, m_row0, Kr, f, sn, F, kvalid, wreg,
                                                   gacc);
             } else if constexpr (PAIRED) {
               const int self_q = self_g >= 0 ? self_g - pass - q0 : -1;
@@ -611,9 +613,9 @@ __device__ __forceinline__ void p2p_kb_body(const float4 *__restrict__ src_rel, 
                 p2p_kb_chunk_x2<KG, PHI, false>(ti, self_q, sPos + q0, m_row0, Kr, f, sn, F, kvalid, acc2);
             } else {
               if (kvalid == KG)
-                p2p_kb_chunk<KG, PHI, true>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc);
+                p2p_kb_chunk<KG, PHI, true>(ti, self, sPos + q0, m_row0, Kr, f, sn, F, kvalid, acc);
               else
-                p2p_kb_chunk<KG, PHI, false>(ti, self, sPos + q0, sIdx + q0, m_row0, Kr, f, sn, F, kvalid, acc);
+                p2p_kb_chunk<KG, PHI, false>(ti, self, sPos + q0, m_row0, Kr, f, sn, F, kvalid, acc);
             }
           }
         }
@@ -670,7 +672,7 @@ __global__ void __launch_bounds__(kKbThreads, 2)
                   const int4 *__restrict__ work, const int *__restrict__ self_idx, int depth, int K,
                   float4 *__restrict__ near, const float4 *__restrict__ W, int k_begin, int k_end, int accumulate,
                   float acc_phi_scale) {
-  p2p_kb_body<KG, MODE, PAIRED, kStateBlock>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W,
+  p2p_kb_body<KG, MODE, PAIRED, kStateBlock, kChunkB>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W,
                                              k_begin, k_end, accumulate, acc_phi_scale, blockIdx.x);
 }
 
@@ -694,7 +696,7 @@ __global__ void __maxnreg__(kKbRegsCorun)
     __syncthreads();
     const int u = s_unit;
     if (u >= n_work) break;
-    p2p_kb_body<KG, MODE, PAIRED, kStateBlockCorun>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near,
+    p2p_kb_body<KG, MODE, PAIRED, kStateBlockCorun, kChunkCorun>(src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near,
                                                     W, k_begin, k_end, accumulate, acc_phi_scale, u);
   }
 }
@@ -817,11 +819,10 @@ __global__ void __launch_bounds__(256) direct_grad_fp64_kernel(const double *__r
   }
 }
 
-template <int KG> size_t p2p_kb_smem_bytes(int K, int state_block) {
+template <int KG> size_t p2p_kb_smem_bytes(int K, int state_block, int chunk) {
   const int Kc = (std::min(K, state_block) + 1) & ~1; // widest window (paired rows round up)
   const int Kr = mrow_stride<KG>(Kc);
-  return sizeof(float4) * kNeighbourCap + sizeof(int) * kNeighbourCap +
-         sizeof(float4) * kBufs * kChunkB * static_cast<size_t>(Kr);
+  return sizeof(float4) * kNeighbourCap + sizeof(float4) * kBufs * chunk * static_cast<size_t>(Kr);
 }
 
 template <int KG, bool PAIRED, int MODE>
@@ -832,11 +833,11 @@ void launch_kb_mode(const float4 *src_rel, const float4 *mom, const int *src_off
   if (corun != nullptr) {
     cudaMemsetAsync(corun->next_unit, 0, sizeof(int), s);
     const int grid = std::min(n_work, corun->ctas);
-    p2p_kb_corun_kernel<KG, MODE, PAIRED><<<grid, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlockCorun), s>>>(
+    p2p_kb_corun_kernel<KG, MODE, PAIRED><<<grid, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlockCorun, kChunkCorun), s>>>(
         src_rel, mom, src_off, tgt_rel, work, n_work, corun->next_unit, self_idx, depth, K, near, W, k_begin, k_end,
         accumulate, acc_phi_scale);
   } else
-    p2p_kb_kernel<KG, MODE, PAIRED><<<n_work, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlock), s>>>(
+    p2p_kb_kernel<KG, MODE, PAIRED><<<n_work, kKbThreads, p2p_kb_smem_bytes<KG>(K, kStateBlock, kChunkB), s>>>(
         src_rel, mom, src_off, tgt_rel, work, self_idx, depth, K, near, W, k_begin, k_end, accumulate, acc_phi_scale);
 }
 
@@ -1084,8 +1085,9 @@ int p2p_grad_groups(int K) { return K >= 8 ? (K + 7) / 8 : (K + 3) / 4; }
 
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                      const int4 *work, int n_work, const int *self_idx, const CloseGeometry &cg, int depth, int K,
-                     const float4 *W, float4 *gpart, cudaStream_t s) {
-  launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, 2, gpart, W, s);
+                     const float4 *W, float4 *gpart, cudaStream_t s, const CorunLaunch *corun) {
+  launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, 2, gpart, W, s, 0, -1, 0, 1.0F,
+                corun);
   launch_close_correction<2>(mom, cg, self_idx, K, gpart, W, p2p_grad_groups(K), 0, K, 0, 1.0F, s);
 }
 
@@ -1194,10 +1196,10 @@ size_t p2p_corun_cta_smem(int K) {
   cudaFuncAttributes attr{};
   if (K >= 8) {
     cudaFuncGetAttributes(&attr, p2p_kb_corun_kernel<8, 1, true>);
-    return p2p_kb_smem_bytes<8>(K, kStateBlockCorun) + attr.sharedSizeBytes;
+    return p2p_kb_smem_bytes<8>(K, kStateBlockCorun, kChunkCorun) + attr.sharedSizeBytes;
   }
   cudaFuncGetAttributes(&attr, p2p_kb_corun_kernel<4, 1, true>);
-  return p2p_kb_smem_bytes<4>(K, kStateBlockCorun) + attr.sharedSizeBytes;
+  return p2p_kb_smem_bytes<4>(K, kStateBlockCorun, kChunkCorun) + attr.sharedSizeBytes;
 }
 
 void configure_p2p(size_t max_smem) {
