@@ -774,23 +774,38 @@ def multi_geometry_leg(args, stream, local):
     rng = np.random.default_rng(args.seed + 77)
     count = args.multi_problems
     sizes = np.round(np.exp(rng.uniform(math.log(8192), math.log(524288), size=count))).astype(int)
+    points = [clustered_points(rng, int(n)) for n in sizes]
+    depths = [max(1, int(round(math.log(int(n) / 32.0, 8)))) for n in sizes]
+    # plan set-up from the host tree (cdfmm.UniformTree + self map + plan)
     t0 = time.perf_counter()
-    probs, items = [], []
-    for n in sizes:
-        n = int(n)
-        x = clustered_points(rng, n)
+    for x, depth in zip(points, depths):
         o = cdfmm.UniformTreeOptions()
-        o.max_level = max(1, int(round(math.log(n / 32.0, 8))))
+        o.max_level = depth
         tree = cdfmm.UniformTree(x, x, o)
         plan = cdfmm_b200.DevicePlan.from_tree(tree, 6, max_states=1, device=local)
         plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
+        plan.close()
+    setup_host_s = time.perf_counter() - t0
+    # plan set-up with the octree built on the device (the plans used below)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    plans = [cdfmm_b200.DevicePlan.from_points(x, 6, depth, max_states=1, device=local)
+             for x, depth in zip(points, depths)]
+    setup_s = time.perf_counter() - t0
+    phases = {}
+    for plan in plans:
+        for key, v in plan.stats().items():
+            if key.startswith("setup_ms_"):
+                phases[key[9:]] = phases.get(key[9:], 0.0) + v
+    probs, items = [], []
+    for x, plan in zip(points, plans):
+        n = len(x)
         d = rng.normal(size=(1, n, 3))
         d /= np.linalg.norm(d, axis=2, keepdims=True)
         dm = torch.from_numpy(d.astype(np.float32)).cuda()
         dH = torch.empty((1, n, 3), dtype=torch.float32, device="cuda")
         probs.append((x, plan, d, dH))
         items.append((plan, dm, dH, None))
-    setup_s = time.perf_counter() - t0
     batch = cdfmm_b200.Batch(items, output="field")
     for _ in range(3):
         batch.launch(stream=stream.cuda_stream, synchronize=False)
@@ -834,7 +849,10 @@ def multi_geometry_leg(args, stream, local):
             "order": 6, "states": 1, "output": "field", "graph_launches_per_step": 1, "ms_per_launch": ms,
             "ms_sequential_calls": ms_seq,
             "value": total / (ms * 1e-3), "unit": "target evals/s", "rel_l2_H_max_checked": worst,
-            "plan_setup_s": setup_s,
+            "plan_setup_s": setup_s, "plan_setup_host_tree_s": setup_host_s,
+            "plan_setup_phases_ms": {k: round(v, 1) for k, v in phases.items()},
+            "plan_setup_note": "device octree (cdfmm_b200_plan_create_from_points) vs host tree + from_tree + self "
+                               "map; point generation excluded",
             "data": "synthetic: 8 Gaussian clusters (sigma 0.05, centres U[0.1,0.9]^3, out-of-cube points redrawn)"}
 
 

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <string>
 #include <utility>
+#include <memory>
 #include <vector>
 
 #include "cdfmm_b200.h"
@@ -50,15 +51,30 @@ struct HostOperators {
   // Normalised M2L matrices T^(t)[beta][alpha] = D^{alpha+beta} G(t) for the
   // 7x7x7 integer translation stencil (slot = (tx+3)*49 + (ty+3)*7 + (tz+3));
   // slots inside the 3x3x3 near stencil are zero and never used.
-  // Stored FP32 as [slot][alpha][beta_pad] with beta_pad = m2l_ld.
+  // Stored FP32 as [slot][alpha][beta_pad] with beta_pad = m2l_ld.  Both
+  // tables depend on the order alone and are shared by every plan of that
+  // order (see m2l_matrices); null for depth < 2 (no M2L).
   int m2l_ld = 0;
-  std::vector<float> m2l_T;
+  std::shared_ptr<const std::vector<float>> m2l_T;
   // The same matrices in FP64, [slot][alpha][beta] with leading dimension n
   // (input of the BF16 hi/lo split of the tensor-core path).
-  std::vector<double> m2l_T64;
+  std::shared_ptr<const std::vector<double>> m2l_T64;
 };
 
 HostOperators build_host_operators(int p, int depth, int m2l_ld_multiple);
+
+// Where m2l_matrices found the tables of an order.
+enum class OperatorSource { Computed = 0, Process = 1, Disk = 2 };
+
+// The normalised FP64 M2L matrices of order p ([343][n][n], near-stencil
+// slots zero).  Computed once per process and order; when the environment
+// variable CDFMM_B200_OPERATOR_CACHE names a directory they are also kept
+// there, one file per order, and read back by later processes (a file whose
+// header, size or checksum does not match is ignored and rewritten).
+std::shared_ptr<const std::vector<double>> m2l_matrices(int p, OperatorSource *source = nullptr);
+// Their FP32 copy with rows padded to ld (zero padding), also shared.
+std::shared_ptr<const std::vector<float>> m2l_matrices_fp32(int p, int ld,
+                                                            const std::shared_ptr<const std::vector<double>> &T64);
 
 // D^gamma G(R) for G = 1/(4 pi |R|) and every gamma of total degree <= order,
 // in basis order (FP64).  Cartesian recurrence for the Taylor coefficients
@@ -81,6 +97,25 @@ cudaError_t cdfmm_b200_collect_status(cdfmm_b200_plan *plan, cudaStream_t s, uns
 // record counts as reported).  Failures of earlier calls are left for
 // cdfmm_b200_poll_status.
 std::string cdfmm_b200_own_status(cdfmm_b200_plan *plan, unsigned long long call);
+
+// Batch building blocks: a one-state evaluation (device arrays, already
+// validated by a plain evaluate of the same arguments) split around its M2L,
+// which the batch runs for several plans of one depth and order at once
+// (their multipoles stacked as the states of one tensor-core M2L).  upward:
+// gather, the near field (forked onto the plan's near stream), P2M, M2M on s;
+// downward: L2L, the join with the near field, L2P, the status record, on s.
+namespace cdfmm_b200 {
+// Tensor-core M2L work tiles (per level, deepest first: runs of T parents, the
+// 8 parity classes of a run adjacent) and the TMEM columns of m_tiles
+// accumulators acc_stride apart.
+std::vector<int4> tc_work_tiles(int depth, int T);
+uint32_t tc_tmem_columns(int m_tiles, int acc_stride);
+} // namespace cdfmm_b200
+
+extern "C" {
+void cdfmm_b200_stacked_upward(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a, cudaStream_t s);
+void cdfmm_b200_stacked_downward(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a, cudaStream_t s);
+}
 
 // The opaque ABI handle.
 struct cdfmm_b200_plan {
@@ -201,11 +236,14 @@ struct cdfmm_b200_plan {
   void *stage_out = nullptr;   // device results before D2H
   size_t stage_out_bytes = 0;
 
-  // reverse mode: host copy of the sorted geometry (to build the transposed
-  // plan on first use), that plan -- its sources are this plan's targets and
-  // vice versa -- and the buffers of the position gradient
-  std::vector<double> h_src_pos, h_tgt_pos;    // [n][3] Morton-sorted
-  std::vector<int> h_src_perm, h_tgt_perm, h_src_off, h_tgt_off;
+  // Morton-sorted FP64 positions (device, [n][3]): the exact geometry of the
+  // close pairs and the input of the transposed plan; host copy of the leaf
+  // ranges
+  double *src_pos64 = nullptr, *tgt_pos64 = nullptr;
+  std::vector<int> h_src_off, h_tgt_off;
+  // reverse mode: the transposed plan (built on first use; its sources are
+  // this plan's targets and vice versa) and the buffers of the position
+  // gradient
   std::vector<int> h_self;                     // sorted self map as last set (empty: none)
   int self_version = 0;                        // bumped by every set_self_indices
   cdfmm_b200_plan *adjoint = nullptr;

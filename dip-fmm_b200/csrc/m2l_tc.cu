@@ -375,7 +375,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
       const int tt = m * T + tr;
       if (tr < T && tt < count && k < args.K) {
         const long long base = static_cast<long long>(tgt_node[tt]) * args.n * args.K + k;
-        for (int b = 0; b < args.n; ++b) args.L[base + static_cast<long long>(b) * args.K] = __int_as_float(0x7fc00000);
+        for (int b = 0; b < args.n; ++b) {
+          if (args.L_list != nullptr)
+            args.L_list[k][static_cast<long long>(tgt_node[tt]) * args.n + b] = __int_as_float(0x7fc00000);
+          else
+            args.L[base + static_cast<long long>(b) * args.K] = __int_as_float(0x7fc00000);
+        }
       }
     }
   } else {
@@ -389,6 +394,8 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
       const bool valid = tr < T && tt < count && k < args.K;
       const int node = valid ? tgt_node[tt] : 0;
       const long long base = static_cast<long long>(node) * args.n * args.K + k;
+      float *const out_k = (args.L_list != nullptr && valid) ? args.L_list[k] + static_cast<long long>(node) * args.n
+                                                              : nullptr;
       for (int c0 = 0; c0 < args.Npad; c0 += 16) {
         float v[16];
         const uint32_t tcol = tmem + (static_cast<uint32_t>(warp * 32) << 16) + static_cast<uint32_t>(m * args.acc_stride + c0);
@@ -407,7 +414,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
 #pragma unroll
           for (int j = 0; j < 16; ++j) {
             const int b = c0 + j;
-            if (b < args.n) args.L[base + static_cast<long long>(b) * args.K] = v[j] * sl[b];
+            if (b < args.n) {
+              if (out_k != nullptr)
+                out_k[b] = v[j] * sl[b];
+              else
+                args.L[base + static_cast<long long>(b) * args.K] = v[j] * sl[b];
+            }
           }
         }
       }
@@ -433,6 +445,7 @@ constexpr int kPackThreads = 256;
 constexpr int kPackMaxKp = 128;
 
 __global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__restrict__ M,
+                                                                const float *const *__restrict__ M_list,
                                                                 const float *__restrict__ scale_m,
                                                                 uint4 *__restrict__ hi, uint4 *__restrict__ lo, int n,
                                                                 int K, int Kp, int Kpad, int depth, int node_base,
@@ -443,7 +456,7 @@ __global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__r
   const int node = node_base + box;
   int level = 0;
   while (level < depth && level_offset_d(level + 1) <= node) ++level;
-  const float *src = M + static_cast<long long>(node) * n * K;
+  const float *src = M != nullptr ? M + static_cast<long long>(node) * n * K : nullptr;
   const long long box_vec = static_cast<long long>(box) * Kp * Kpad / 8; // 16-byte vectors before this box
   const int nkc = (Kpad + kKChunk - 1) / kKChunk;
   for (int kc = 0; kc < nkc; ++kc) {
@@ -454,8 +467,10 @@ __global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__r
       const int al = e / Kp;
       const int k = e - al * Kp;
       const int a = kc * kKChunk + al;
-      tile[al][k] = (box < n_boxes && a < n && k < K) ? src[static_cast<long long>(a) * K + k] * scale_m[level * n + a]
-                                                     : 0.0F;
+      float m = 0.0F;
+      if (box < n_boxes && a < n && k < K)
+        m = M_list != nullptr ? M_list[k][static_cast<long long>(node) * n + a] : src[static_cast<long long>(a) * K + k];
+      tile[al][k] = m * scale_m[level * n + a];
     }
     __syncthreads();
     const long long chunk_vec = box_vec + static_cast<long long>(kc) * Kp * kKChunk / 8;
@@ -490,11 +505,13 @@ size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages) {
 }
 
 void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,
-                     int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s) {
+                     int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s,
+                     const float *const *M_list) {
   (void)basis;
   if (Kp > kPackMaxKp || Kp % 8 != 0 || Kpad % 16 != 0) return; // the plan keeps Kp <= 128, multiples of 8
-  m2l_pack_kernel<<<n_boxes + 1, kPackThreads, 0, s>>>(M, scale_m, static_cast<uint4 *>(hi), static_cast<uint4 *>(lo),
-                                                        n, K, Kp, Kpad, depth, node_base, n_boxes);
+  m2l_pack_kernel<<<n_boxes + 1, kPackThreads, 0, s>>>(M, M_list, scale_m, static_cast<uint4 *>(hi),
+                                                        static_cast<uint4 *>(lo), n, K, Kp, Kpad, depth, node_base,
+                                                        n_boxes);
 }
 
 void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s) {

@@ -17,6 +17,7 @@ struct TcArgs {
   const int4 *tiles;       // per CTA: (level, class, first parent Morton index, target count)
   const float *scale_l;    // [depth+1][n] exact powers of two
   float *L;                // [node][n][K] FP32 locals (overwritten)
+  float *const *L_list;    // or (stacked problems, one state each): state k's locals at L_list[k][node][n]
   int *error_flag;         // set nonzero if a bounded wait expired
   int n, K, Kp, Kpad, Npad;
   int node_base;           // flat node index of packed box 0
@@ -38,7 +39,8 @@ constexpr int kTcMaxTargets = 64;
 
 size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages);
 void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,
-                     int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s);
+                     int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s,
+                     const float *const *M_list = nullptr);
 void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s);
 bool configure_m2l_tc(size_t max_smem);
 // Runs a kernel whose bounded mbarrier wait must expire (nothing arrives)

@@ -17,8 +17,17 @@
 //    coefficients of 1/|R| (our own method; upstream uses Taylor-jet
 //    arithmetic, src/taylor_jet.cpp:68-148); both give the same derivatives,
 //    which the tests check against the reference's matrices.
+#include <unistd.h>
+
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 #include "fmm_internal.hpp"
@@ -139,29 +148,137 @@ HostOperators build_host_operators(int p, int depth, int m2l_ld_multiple) {
 
   // Normalised M2L matrices for the 7^3 stencil (near slots left zero).
   ops.m2l_ld = round_up(n, m2l_ld_multiple);
-  const int ld = ops.m2l_ld;
-  ops.m2l_T.assign(static_cast<std::size_t>(343) * n * ld, 0.0F);
-  if (depth >= 2) ops.m2l_T64.assign(static_cast<std::size_t>(343) * n * n, 0.0);
   if (depth >= 2) {
-    const BasisTable D(2 * p);
-    for (int tx = -3; tx <= 3; ++tx)
-      for (int ty = -3; ty <= 3; ++ty)
-        for (int tz = -3; tz <= 3; ++tz) {
-          if (std::abs(tx) <= 1 && std::abs(ty) <= 1 && std::abs(tz) <= 1) continue;
-          const double R[3] = {static_cast<double>(tx), static_cast<double>(ty), static_cast<double>(tz)};
-          const std::vector<double> deriv = laplace_derivatives(2 * p, R);
-          const int slot = (tx + 3) * 49 + (ty + 3) * 7 + (tz + 3);
-          float *T = ops.m2l_T.data() + static_cast<std::size_t>(slot) * n * ld;
-          double *T64 = ops.m2l_T64.data() + static_cast<std::size_t>(slot) * n * n;
-          for (int a = 0; a < n; ++a)
-            for (int b = 0; b < n; ++b) {
-              const double v = deriv[BasisTable::rank(B.ax[a] + B.ax[b], B.ay[a] + B.ay[b], B.az[a] + B.az[b])];
-              T[static_cast<std::size_t>(a) * ld + b] = static_cast<float>(v);
-              T64[static_cast<std::size_t>(a) * n + b] = v;
-            }
-        }
+    ops.m2l_T64 = m2l_matrices(p);
+    ops.m2l_T = m2l_matrices_fp32(p, ops.m2l_ld, ops.m2l_T64);
   }
   return ops;
+}
+
+namespace {
+
+std::mutex g_operator_mutex;
+std::map<int, std::shared_ptr<const std::vector<double>>> g_m2l64;
+std::map<std::pair<int, int>, std::shared_ptr<const std::vector<float>>> g_m2l32;
+
+constexpr char kCacheMagic[8] = {'C', 'D', 'F', 'M', 'M', 'M', '2', 'L'};
+constexpr uint32_t kCacheVersion = 1;
+
+struct CacheHeader {
+  char magic[8];
+  uint32_t version;
+  int32_t order;
+  int32_t n;
+  uint32_t reserved;
+  uint64_t checksum; // FNV-1a 64 of the matrix bytes
+};
+
+uint64_t fnv1a(const void *data, std::size_t bytes) {
+  const unsigned char *b = static_cast<const unsigned char *>(data);
+  uint64_t h = 1469598103934665603ULL;
+  for (std::size_t i = 0; i < bytes; ++i) {
+    h ^= b[i];
+    h *= 1099511628211ULL;
+  }
+  return h;
+}
+
+std::string cache_file(int p) {
+  const char *dir = std::getenv("CDFMM_B200_OPERATOR_CACHE");
+  if (dir == nullptr || *dir == '\0') return std::string();
+  return std::string(dir) + "/m2l_p" + std::to_string(p) + ".bin";
+}
+
+bool read_cache(const std::string &path, int p, int n, std::vector<double> &out) {
+  std::FILE *f = std::fopen(path.c_str(), "rb");
+  if (f == nullptr) return false;
+  CacheHeader h{};
+  const std::size_t count = static_cast<std::size_t>(343) * n * n;
+  out.assign(count, 0.0);
+  bool ok = std::fread(&h, sizeof h, 1, f) == 1 && std::memcmp(h.magic, kCacheMagic, 8) == 0 &&
+            h.version == kCacheVersion && h.order == p && h.n == n &&
+            std::fread(out.data(), sizeof(double), count, f) == count;
+  if (ok) {
+    char extra;
+    ok = std::fread(&extra, 1, 1, f) == 0 && fnv1a(out.data(), count * sizeof(double)) == h.checksum;
+  }
+  std::fclose(f);
+  if (!ok) out.clear();
+  return ok;
+}
+
+// Writes the file under a temporary name and renames it into place, so a
+// reader never sees a partial file; failures leave no file and are ignored.
+void write_cache(const std::string &path, int p, int n, const std::vector<double> &T) {
+  const std::string tmp = path + ".tmp." + std::to_string(static_cast<long>(getpid()));
+  std::FILE *f = std::fopen(tmp.c_str(), "wb");
+  if (f == nullptr) return;
+  CacheHeader h{};
+  std::memcpy(h.magic, kCacheMagic, 8);
+  h.version = kCacheVersion;
+  h.order = p;
+  h.n = n;
+  h.checksum = fnv1a(T.data(), T.size() * sizeof(double));
+  const bool ok = std::fwrite(&h, sizeof h, 1, f) == 1 && std::fwrite(T.data(), sizeof(double), T.size(), f) == T.size();
+  const bool closed = std::fclose(f) == 0;
+  if (!ok || !closed || std::rename(tmp.c_str(), path.c_str()) != 0) std::remove(tmp.c_str());
+}
+
+std::vector<double> compute_m2l_matrices(int p) {
+  const BasisTable B(p);
+  const int n = B.size();
+  std::vector<double> T64(static_cast<std::size_t>(343) * n * n, 0.0);
+  for (int tx = -3; tx <= 3; ++tx)
+    for (int ty = -3; ty <= 3; ++ty)
+      for (int tz = -3; tz <= 3; ++tz) {
+        if (std::abs(tx) <= 1 && std::abs(ty) <= 1 && std::abs(tz) <= 1) continue;
+        const double R[3] = {static_cast<double>(tx), static_cast<double>(ty), static_cast<double>(tz)};
+        const std::vector<double> deriv = laplace_derivatives(2 * p, R);
+        const int slot = (tx + 3) * 49 + (ty + 3) * 7 + (tz + 3);
+        double *T = T64.data() + static_cast<std::size_t>(slot) * n * n;
+        for (int a = 0; a < n; ++a)
+          for (int b = 0; b < n; ++b)
+            T[static_cast<std::size_t>(a) * n + b] =
+                deriv[BasisTable::rank(B.ax[a] + B.ax[b], B.ay[a] + B.ay[b], B.az[a] + B.az[b])];
+      }
+  return T64;
+}
+
+} // namespace
+
+std::shared_ptr<const std::vector<double>> m2l_matrices(int p, OperatorSource *source) {
+  std::lock_guard<std::mutex> lock(g_operator_mutex);
+  auto it = g_m2l64.find(p);
+  if (it != g_m2l64.end()) {
+    if (source) *source = OperatorSource::Process;
+    return it->second;
+  }
+  const int n = BasisTable(p).size();
+  const std::string path = cache_file(p);
+  auto T = std::make_shared<std::vector<double>>();
+  if (!path.empty() && read_cache(path, p, n, *T)) {
+    if (source) *source = OperatorSource::Disk;
+  } else {
+    *T = compute_m2l_matrices(p);
+    if (!path.empty()) write_cache(path, p, n, *T);
+    if (source) *source = OperatorSource::Computed;
+  }
+  g_m2l64[p] = T;
+  return T;
+}
+
+// FP32 copy of the matrices with rows padded to `ld` (zero padding).
+std::shared_ptr<const std::vector<float>> m2l_matrices_fp32(int p, int ld,
+                                                            const std::shared_ptr<const std::vector<double>> &T64) {
+  std::lock_guard<std::mutex> lock(g_operator_mutex);
+  auto it = g_m2l32.find({p, ld});
+  if (it != g_m2l32.end()) return it->second;
+  const int n = BasisTable(p).size();
+  auto T = std::make_shared<std::vector<float>>(static_cast<std::size_t>(343) * n * ld, 0.0F);
+  for (std::size_t sa = 0; sa < static_cast<std::size_t>(343) * n; ++sa)
+    for (int b = 0; b < n; ++b) (*T)[sa * ld + b] = static_cast<float>((*T64)[sa * n + b]);
+  g_m2l32[{p, ld}] = T;
+  return T;
 }
 
 } // namespace cdfmm_b200

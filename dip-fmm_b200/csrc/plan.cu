@@ -10,16 +10,22 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <cmath>
 #include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
 #include <new>
 #include <stdexcept>
 #include <string>
+#include <tuple>
 #include <vector>
 
 #include "cdfmm_b200.h"
 #include "far_kernels.hpp"
 #include "fmm_internal.hpp"
+#include "geometry.hpp"
 #include "kernels.cuh"
 #include "m2l_tc.hpp"
 
@@ -101,7 +107,7 @@ void free_plan(cdfmm_b200_plan *p) {
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
                   p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
-                  p->close_targets, p->close_r_fp32, p->close_r_exact};
+                  p->close_targets, p->close_r_fp32, p->close_r_exact, p->src_pos64, p->tgt_pos64};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
   if (p->p2p_work_wide != nullptr && p->p2p_work_wide != p->p2p_work) cudaFree(p->p2p_work_wide);
@@ -120,45 +126,6 @@ void free_plan(cdfmm_b200_plan *p) {
   if (p->ev_far) cudaEventDestroy(p->ev_far);
   if (p->stream) cudaStreamDestroy(p->stream);
   delete p;
-}
-
-// Normalised (root width = 1) coordinates relative to the centre of the leaf
-// that holds each point; the FP64 subtraction order follows the reference's
-// FP32 normalisation (src/uniform_fmm.cpp:379-417 upstream).
-std::vector<float4> relative_positions(const double *pos, const int32_t *leaf_off, int n_leaves,
-                                       int depth, const double centre[3], double hw, double scale) {
-  const int side = 1 << depth;
-  std::vector<float4> out(static_cast<size_t>(leaf_off[n_leaves]));
-  const double inv = 1.0 / scale;
-  for (int m = 0; m < n_leaves; ++m) {
-    if (leaf_off[m + 1] == leaf_off[m]) continue;
-    int ix, iy, iz;
-    demorton3(static_cast<uint32_t>(m), ix, iy, iz);
-    const int c3[3] = {ix, iy, iz};
-    double nc[3];
-    for (int a = 0; a < 3; ++a) {
-      const double offset = ((static_cast<double>(c3[a]) + 0.5) / static_cast<double>(side) - 0.5) * 2.0 * hw;
-      const double leaf_centre = centre[a] + offset;
-      nc[a] = (leaf_centre - centre[a]) * inv;
-    }
-    for (int j = leaf_off[m]; j < leaf_off[m + 1]; ++j) {
-      double np[3];
-      for (int a = 0; a < 3; ++a) np[a] = (pos[3 * static_cast<size_t>(j) + a] - centre[a]) * inv;
-      out[static_cast<size_t>(j)] = make_float4(static_cast<float>(np[0] - nc[0]), static_cast<float>(np[1] - nc[1]),
-                                                static_cast<float>(np[2] - nc[2]), 0.0F);
-    }
-  }
-  return out;
-}
-
-// Root-normalised FP64 positions ((x - centre) / scale), [n][3]: the exact
-// geometry of pairs much closer than a leaf (see p2p_close_r2).
-std::vector<double> normalised_positions(const double *pos, size_t n, const double centre[3], double scale) {
-  std::vector<double> out(3 * n);
-  const double inv = 1.0 / scale;
-  for (size_t j = 0; j < n; ++j)
-    for (int a = 0; a < 3; ++a) out[3 * j + a] = (pos[3 * j + a] - centre[a]) * inv;
-  return out;
 }
 
 int fail(cdfmm_b200_plan *plan, int code, const std::string &msg) {
@@ -221,8 +188,7 @@ std::string cdfmm_b200_own_status(cdfmm_b200_plan *plan, unsigned long long call
 // need the exact r most, are always inside it), and writes the list.  A
 // geometry with more than 64 pairs per target even at the smallest
 // threshold keeps no list (close_shift = -1).
-static void build_close_pairs(cdfmm_b200_plan *plan, const cdfmm_b200_plan_desc *desc, uint64_t &bytes,
-                              uint64_t &h2d) {
+static void build_close_pairs(cdfmm_b200_plan *plan, uint64_t &bytes, uint64_t &h2d) {
   plan->n_close_targets = 0;
   plan->close_pairs = 0;
   plan->close_shift = -1;
@@ -259,17 +225,13 @@ static void build_close_pairs(cdfmm_b200_plan *plan, const cdfmm_b200_plan_desc 
     if (c > 0) targets.push_back(make_int4(i, run, c, 0));
     run += c;
   }
-  const std::vector<double> sabs = normalised_positions(desc->sorted_source_positions, static_cast<size_t>(plan->ns),
-                                                        plan->root_centre, plan->scale);
-  const std::vector<double> tabs = normalised_positions(desc->sorted_target_positions, static_cast<size_t>(plan->nt),
-                                                        plan->root_centre, plan->scale);
-  double *d_sabs = dalloc<double>(sabs.size(), tmp);
-  double *d_tabs = dalloc<double>(tabs.size(), tmp);
+  double *d_sabs = dalloc<double>(3 * static_cast<size_t>(plan->ns), tmp);
+  double *d_tabs = dalloc<double>(3 * static_cast<size_t>(plan->nt), tmp);
   int *d_first = dalloc<int>(first.size(), tmp);
   plan->close_r_fp32 = dalloc<float4>(static_cast<size_t>(run), bytes);
   plan->close_r_exact = dalloc<float4>(static_cast<size_t>(run), bytes);
-  upload(d_sabs, sabs.data(), sabs.size(), h2d);
-  upload(d_tabs, tabs.data(), tabs.size(), h2d);
+  launch_normalised_positions(plan->src_pos64, plan->ns, plan->root_centre, 1.0 / plan->scale, d_sabs, nullptr);
+  launch_normalised_positions(plan->tgt_pos64, plan->nt, plan->root_centre, 1.0 / plan->scale, d_tabs, nullptr);
   upload(d_first, first.data(), first.size(), h2d);
   launch_p2p_close_write(plan->src_rel, plan->src_off, plan->tgt_rel, plan->p2p_work_wide, plan->n_p2p_work_wide,
                          plan->depth, thr[level], d_first, d_sabs, d_tabs, plan->close_r_fp32, plan->close_r_exact,
@@ -323,8 +285,378 @@ int cdfmm_b200_device_info(int32_t device, char *name, size_t name_len, int32_t 
 
 static size_t corun_m2l_smem_budget(const cdfmm_b200_plan *plan, int K);
 
+// BF16 hi/lo B tiles of the tensor-core M2L per (order, Npad, Kpad), packed
+// once per process and shared by the plans of that order.
+static std::shared_ptr<const std::vector<uint16_t>> packed_b_tiles(int p, const HostOperators &ops, int Npad,
+                                                                    int Kpad) {
+  static std::mutex mutex;
+  static std::map<std::tuple<int, int, int>, std::shared_ptr<const std::vector<uint16_t>>> cache;
+  std::lock_guard<std::mutex> lock(mutex);
+  auto &slot = cache[std::make_tuple(p, Npad, Kpad)];
+  if (!slot) slot = std::make_shared<const std::vector<uint16_t>>(pack_m2l_b_tiles(*ops.m2l_T64, ops.n, Npad, Kpad));
+  return slot;
+}
+
+// A new plan's sizes, streams and events (root cube, geometry, operators
+// and buffers are set by the creators below).
+static cdfmm_b200_plan *new_plan(int ns, int nt, int order, int depth, int max_states, int device) {
+  cdfmm_b200_plan *plan = new cdfmm_b200_plan();
+  try {
+    plan->device = device;
+    plan->ns = ns;
+    plan->nt = nt;
+    plan->p = order;
+    plan->depth = depth;
+    plan->n_leaves = 1 << (3 * depth);
+    plan->n_nodes = level_offset(depth + 1);
+    plan->max_states = max_states;
+    plan->m2l_mode = CDFMM_B200_M2L_FP32; // tensor-core M2L is selected in finish_plan when available
+
+    check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&plan->near_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+    {
+      // The far field runs on a high-priority stream so its CTAs are
+      // dispatched into SM slots as they free up while the (FP32-bound) near
+      // field runs at the default priority: tensor-core M2L and P2P overlap.
+      int least = 0, greatest = 0;
+      check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
+      check(cudaStreamCreateWithPriority(&plan->far_stream, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
+      check(cudaEventCreateWithFlags(&plan->ev_far, cudaEventDisableTiming), "cudaEventCreate");
+    }
+    check(cudaStreamCreateWithFlags(&plan->io_in, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaStreamCreateWithFlags(&plan->io_out, cudaStreamNonBlocking), "cudaStreamCreate");
+    check(cudaEventCreateWithFlags(&plan->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
+    check(cudaEventCreateWithFlags(&plan->ev_join, cudaEventDisableTiming), "cudaEventCreate");
+    for (cudaEvent_t &e : plan->ev_t) check(cudaEventCreate(&e), "cudaEventCreate");
+  } catch (...) {
+    free_plan(plan);
+    throw;
+  }
+  return plan;
+}
+
+static void set_root(cdfmm_b200_plan *plan, const double centre[3], double half_width) {
+  for (int a = 0; a < 3; ++a) plan->root_centre[a] = centre[a];
+  plan->root_half_width = half_width;
+  plan->scale = 2.0 * half_width;
+  plan->inv_scale3 = static_cast<float>(1.0 / (plan->scale * plan->scale * plan->scale));
+  plan->phi_scale = static_cast<float>(plan->scale);
+}
+
+// Everything that follows from the plan's Morton-ordered geometry (src_pos64,
+// tgt_pos64, src_perm, tgt_perm, src_off, tgt_off on the device, h_src_off,
+// h_tgt_off on the host): leaf-relative FP32 positions, inverse
+// permutations, near-field work units, close pairs, operators, interaction
+// statistics, state buffers and the tensor-core M2L set-up.
+static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
+  const int n_leaves = plan->n_leaves;
+  auto mark = std::chrono::steady_clock::now();
+  auto lap = [&mark](double &slot) {
+    const auto now = std::chrono::steady_clock::now();
+    slot += std::chrono::duration<double, std::milli>(now - mark).count();
+    mark = now;
+  };
+
+  HostOperators &ops = plan->ops;
+  ops = build_host_operators(plan->p, plan->depth, 16);
+  plan->n = ops.n;
+  const int n = ops.n;
+  const int J = m2l_simt_beta_per_thread(n);
+  if (ops.m2l_ld < 16 * J) {
+    ops = build_host_operators(plan->p, plan->depth, 16 * J);
+  }
+  uint64_t &bytes = plan->stats.persistent_device_bytes;
+  uint64_t &h2d = plan->stats.setup_h2d_bytes;
+  lap(plan->stats.setup_ms_operators);
+
+  // geometry: leaf-relative positions and inverse permutations on the device
+  {
+    const double inv_scale = 1.0 / plan->scale;
+    plan->src_rel = dalloc<float4>(plan->ns, bytes);
+    plan->tgt_rel = dalloc<float4>(plan->nt, bytes);
+    launch_relative_positions(plan->src_pos64, plan->src_off, n_leaves, plan->ns, plan->depth, plan->root_centre,
+                              plan->root_half_width, inv_scale, plan->src_rel, nullptr);
+    launch_relative_positions(plan->tgt_pos64, plan->tgt_off, n_leaves, plan->nt, plan->depth, plan->root_centre,
+                              plan->root_half_width, inv_scale, plan->tgt_rel, nullptr);
+    plan->src_inv = dalloc<int>(plan->ns, bytes);
+    plan->tgt_inv = dalloc<int>(plan->nt, bytes);
+    check(cudaMemset(plan->src_inv, 0xff, sizeof(int) * std::max(plan->ns, 1)), "cudaMemset");
+    check(cudaMemset(plan->tgt_inv, 0xff, sizeof(int) * std::max(plan->nt, 1)), "cudaMemset");
+    uint64_t tmp = 0;
+    int *flags = dalloc<int>(2, tmp);
+    int h_flags[2] = {0, 0};
+    cudaError_t e = cudaMemset(flags, 0, 2 * sizeof(int));
+    if (e == cudaSuccess) {
+      launch_inverse_permutation(plan->src_perm, plan->ns, plan->src_inv, flags, nullptr);
+      launch_inverse_permutation(plan->tgt_perm, plan->nt, plan->tgt_inv, flags + 1, nullptr);
+      e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpy(h_flags, flags, sizeof h_flags, cudaMemcpyDeviceToHost);
+    cudaFree(flags);
+    check(e, "plan geometry");
+    require((h_flags[0] & 1) == 0, "source_permutation out of range");
+    require((h_flags[1] & 1) == 0, "target_permutation out of range");
+    require((h_flags[0] & 2) == 0, "source_permutation is not a permutation");
+    require((h_flags[1] & 2) == 0, "target_permutation is not a permutation");
+    plan->self_idx = dalloc<int>(plan->nt, bytes);
+    plan->leaf_self = dalloc<int2>(n_leaves, bytes);
+  }
+  lap(plan->stats.setup_ms_geometry);
+
+  {
+    int sms = 0;
+    check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device), "device attribute");
+    plan->sm_count = sms;
+    plan->p2p_next_unit = dalloc<int>(1, bytes);
+    const std::vector<int4> work =
+        p2p_work_units(plan->h_src_off.data(), plan->h_tgt_off.data(), plan->depth, sms, true);
+    const std::vector<int4> wide =
+        p2p_work_units(plan->h_src_off.data(), plan->h_tgt_off.data(), plan->depth, sms, false);
+    plan->n_p2p_work = static_cast<int>(work.size());
+    plan->n_p2p_work_wide = static_cast<int>(wide.size());
+    if (!work.empty()) {
+      plan->p2p_work = dalloc<int4>(work.size(), bytes);
+      upload(plan->p2p_work, work.data(), work.size(), h2d);
+    }
+    if (wide.size() == work.size()) {
+      plan->p2p_work_wide = plan->p2p_work; // no unit was capped: the same units
+    } else {
+      plan->p2p_work_wide = dalloc<int4>(wide.size(), bytes);
+      upload(plan->p2p_work_wide, wide.data(), wide.size(), h2d);
+    }
+    build_close_pairs(plan, bytes, h2d);
+  }
+  lap(plan->stats.setup_ms_near);
+
+  // operators
+  std::vector<int8_t> basis(static_cast<size_t>(n) * 4);
+  for (int a = 0; a < n; ++a) {
+    basis[4 * a] = static_cast<int8_t>(ops.ax[a]);
+    basis[4 * a + 1] = static_cast<int8_t>(ops.ay[a]);
+    basis[4 * a + 2] = static_cast<int8_t>(ops.az[a]);
+    basis[4 * a + 3] = static_cast<int8_t>(ops.ax[a] + ops.ay[a] + ops.az[a]);
+  }
+  std::vector<int> m2m_pair(ops.m2m_pair_g.size()), l2l_pair(ops.l2l_pair_g.size());
+  for (size_t e = 0; e < m2m_pair.size(); ++e) m2m_pair[e] = ops.m2m_pair_g[e] | (ops.m2m_pair_in[e] << 16);
+  for (size_t e = 0; e < l2l_pair.size(); ++e) l2l_pair[e] = ops.l2l_pair_g[e] | (ops.l2l_pair_in[e] << 16);
+  plan->basis = dalloc<int8_t>(basis.size(), bytes);
+  plan->m2m_off = dalloc<int>(ops.m2m_off.size(), bytes);
+  plan->l2l_off = dalloc<int>(ops.l2l_off.size(), bytes);
+  plan->m2m_pair = dalloc<int>(m2m_pair.size(), bytes);
+  plan->l2l_pair = dalloc<int>(l2l_pair.size(), bytes);
+  plan->m2m_coef = dalloc<float>(ops.m2m_coef.size(), bytes);
+  plan->l2l_coef = dalloc<float>(ops.l2l_coef.size(), bytes);
+  upload(plan->basis, basis.data(), basis.size(), h2d);
+  upload(plan->m2m_off, ops.m2m_off.data(), ops.m2m_off.size(), h2d);
+  upload(plan->l2l_off, ops.l2l_off.data(), ops.l2l_off.size(), h2d);
+  upload(plan->m2m_pair, m2m_pair.data(), m2m_pair.size(), h2d);
+  upload(plan->l2l_pair, l2l_pair.data(), l2l_pair.size(), h2d);
+  upload(plan->m2m_coef, ops.m2m_coef.data(), ops.m2m_coef.size(), h2d);
+  upload(plan->l2l_coef, ops.l2l_coef.data(), ops.l2l_coef.size(), h2d);
+
+  // M2L: matrices, exact power-of-two level scalings, and the work tiles.
+  std::vector<float> sm(static_cast<size_t>(plan->depth + 1) * n), sl(sm.size());
+  for (int level = 0; level <= plan->depth; ++level)
+    for (int a = 0; a < n; ++a) {
+      const int deg = ops.ax[a] + ops.ay[a] + ops.az[a];
+      sm[static_cast<size_t>(level) * n + a] = std::ldexp(1.0F, level * deg);
+      sl[static_cast<size_t>(level) * n + a] = std::ldexp(1.0F, level * (deg + 1));
+    }
+  std::vector<int4> tiles;
+  for (int level = plan->depth; level >= 2; --level) {
+    const int pside = 1 << (level - 1);
+    for (int cls = 0; cls < 8; ++cls)
+      for (int pz = 0; pz < pside; pz += 4)
+        for (int py = 0; py < pside; py += 4)
+          for (int px = 0; px < pside; px += 4) tiles.push_back(make_int4(level, cls, px | (py << 10) | (pz << 20), 0));
+  }
+  plan->n_tiles = static_cast<int>(tiles.size());
+  plan->scale_m = dalloc<float>(sm.size(), bytes);
+  plan->scale_l = dalloc<float>(sl.size(), bytes);
+  plan->m2l_tiles = dalloc<int4>(tiles.size(), bytes);
+  upload(plan->scale_m, sm.data(), sm.size(), h2d);
+  upload(plan->scale_l, sl.data(), sl.size(), h2d);
+  upload(plan->m2l_tiles, tiles.data(), tiles.size(), h2d);
+  if (plan->depth >= 2) {
+    plan->m2l_T = dalloc<float>(ops.m2l_T->size(), bytes);
+    upload(plan->m2l_T, ops.m2l_T->data(), ops.m2l_T->size(), h2d);
+    plan->stats.m2l_matrix_bytes = ops.m2l_T->size() * sizeof(float);
+  }
+
+  lap(plan->stats.setup_ms_operators);
+  // statistics of the implicit interaction lists (counted on the host)
+  {
+    uint64_t classes = 0, inter = 0, pairs = 0;
+    bool used[343] = {};
+    const int32_t *so = plan->h_src_off.data();
+    const int32_t *to = plan->h_tgt_off.data();
+    // occupancy of every level for sources and targets
+    std::vector<std::vector<int>> socc(plan->depth + 1), tocc(plan->depth + 1);
+    for (int level = 0; level <= plan->depth; ++level) {
+      socc[level].assign(static_cast<size_t>(1) << (3 * level), 0);
+      tocc[level].assign(static_cast<size_t>(1) << (3 * level), 0);
+    }
+    for (int m = 0; m < n_leaves; ++m) {
+      for (int level = 0; level <= plan->depth; ++level) {
+        const int shift = 3 * (plan->depth - level);
+        socc[level][m >> shift] += so[m + 1] - so[m];
+        tocc[level][m >> shift] += to[m + 1] - to[m];
+      }
+    }
+    for (int level = 2; level <= plan->depth; ++level) {
+      const int side = 1 << level;
+      for (int t = 0; t < side * side * side; ++t) {
+        if (tocc[level][t] == 0) continue;
+        int tx, ty, tz;
+        demorton3(static_cast<uint32_t>(t), tx, ty, tz);
+        for (int sz = 2 * (tz >> 1) - 2; sz <= 2 * (tz >> 1) + 3; ++sz)
+          for (int sy = 2 * (ty >> 1) - 2; sy <= 2 * (ty >> 1) + 3; ++sy)
+            for (int sx = 2 * (tx >> 1) - 2; sx <= 2 * (tx >> 1) + 3; ++sx) {
+              if (sx < 0 || sy < 0 || sz < 0 || sx >= side || sy >= side || sz >= side) continue;
+              if (std::abs(sx - tx) <= 1 && std::abs(sy - ty) <= 1 && std::abs(sz - tz) <= 1) continue;
+              if (socc[level][morton3(sx, sy, sz)] == 0) continue;
+              ++inter;
+              const int slot = (tx - sx + 3) * 49 + (ty - sy + 3) * 7 + (tz - sz + 3);
+              if (!used[slot]) {
+                used[slot] = true;
+                ++classes;
+              }
+            }
+      }
+    }
+    const int side = 1 << plan->depth;
+    for (int m = 0; m < n_leaves; ++m) {
+      const int nt_leaf = to[m + 1] - to[m];
+      if (nt_leaf == 0) continue;
+      int x, y, z;
+      demorton3(static_cast<uint32_t>(m), x, y, z);
+      for (int dz = -1; dz <= 1; ++dz)
+        for (int dy = -1; dy <= 1; ++dy)
+          for (int dx = -1; dx <= 1; ++dx) {
+            const int a = x + dx, b = y + dy, c = z + dz;
+            if (a < 0 || b < 0 || c < 0 || a >= side || b >= side || c >= side) continue;
+            const uint32_t q = morton3(a, b, c);
+            pairs += static_cast<uint64_t>(nt_leaf) * static_cast<uint64_t>(so[q + 1] - so[q]);
+          }
+    }
+    plan->stats.m2l_classes = classes;
+    plan->stats.m2l_interactions = inter;
+    plan->stats.p2p_pairs = pairs;
+  }
+
+  lap(plan->stats.setup_ms_statistics);
+  // state buffers sized for max_states
+  const size_t K = static_cast<size_t>(plan->max_states);
+  plan->mom = dalloc<float4>(static_cast<size_t>(plan->ns) * ((K + 1) & ~static_cast<size_t>(1)), bytes); // paired rows
+  plan->M = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
+  plan->L = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
+  plan->near = dalloc<float4>(static_cast<size_t>(plan->nt) * K, bytes);
+  check(cudaMemset(plan->M, 0, static_cast<size_t>(plan->n_nodes) * n * K * sizeof(float)), "cudaMemset");
+  check(cudaMemset(plan->L, 0, static_cast<size_t>(plan->n_nodes) * n * K * sizeof(float)), "cudaMemset");
+  check(cudaMemset(plan->near, 0, static_cast<size_t>(std::max(plan->nt, 1)) * K * sizeof(float4)), "cudaMemset");
+
+  const size_t smem = device_smem_optin(plan->device);
+  configure_far_kernels(smem);
+  configure_m2l_simt(smem);
+  configure_p2p(smem);
+  plan->p2m_chunk = 64;
+  while (plan->p2m_chunk > 8 && p2m_smem_bytes(n, plan->p, static_cast<int>(K), plan->p2m_chunk) > smem) plan->p2m_chunk /= 2;
+  require(p2m_smem_bytes(n, plan->p, 4, plan->p2m_chunk) <= smem && l2p_smem_bytes(n, plan->p, 4) <= smem,
+          "order exceeds the shared-memory budget of one CTA");
+  check(cudaDeviceSynchronize(), "plan upload");
+  plan->error_flag = dalloc<int>(1, bytes);
+  check(cudaMemset(plan->error_flag, 0, sizeof(int)), "cudaMemset");
+  check(cudaHostAlloc(reinterpret_cast<void **>(&plan->status), sizeof(cdfmm_b200_plan::StatusRecord),
+                      cudaHostAllocMapped), "cudaHostAlloc");
+  std::memset(plan->status, 0, sizeof(cdfmm_b200_plan::StatusRecord));
+  check(cudaHostGetDevicePointer(reinterpret_cast<void **>(&plan->status_dev), plan->status, 0),
+        "cudaHostGetDevicePointer");
+  plan->tc_wait_limit = kTcWaitLimit;
+
+  lap(plan->stats.setup_ms_buffers);
+  // Tensor-core M2L: sm_100 devices, order <= 9 (N = 16 * ceil(n/16) <= 256
+  // accumulator columns) and at least one pipeline stage in shared memory.
+  {
+    int major = 0;
+    cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, plan->device);
+    const int Kpad = round_up(n, 16);
+    const int Npad = round_up(n, 16);
+    // Pipeline shapes: 1, 2 or 4 128-row accumulators per CTA sharing each
+    // B tile, with as many stages as fit one CTA per SM, or half / a third
+    // of that for two / three CTAs per SM; each with the three products as
+    // three MMAs of N = Npad, or (when 2 Npad <= 256) A_hi x [B_hi | B_lo]
+    // fused into one MMA of N = 2 Npad plus A_lo x B_hi (two larger MMAs
+    // instead of three: fewer instructions for the one issuing thread;
+    // twice the TMEM columns).  Default: two accumulators, two CTAs per SM,
+    // three MMAs; the autotuner times the candidates on first use for
+    // each K.
+    auto acc_stride_of = [&](int fuse) { return round_up(fuse ? 2 * Npad : Npad, 32); };
+    auto max_stages = [&](int mt, size_t budget) {
+      int st = 0;
+      while (st < 8 && m2l_tc_smem_bytes(Npad, mt, st + 1) <= budget) ++st;
+      return st;
+    };
+    const size_t one_cta = std::min<size_t>(smem, 224 * 1024), two_cta = 112 * 1024, three_cta = 74 * 1024;
+    // one CTA beside two co-resident near-field CTAs (schedule CORUN)
+    const size_t corun_cta = corun_m2l_smem_budget(plan, std::min(plan->max_states, 64));
+    plan->tc_candidates.clear();
+    for (int fuse : {0, 1}) {
+      if (fuse && 2 * Npad > 256) continue; // MMA N <= 256
+      const int acc = acc_stride_of(fuse);
+      for (int mt : {2, 1, 4}) {
+        if (mt * acc > 512) continue;
+        const int s1 = max_stages(mt, one_cta);
+        const int s2 = max_stages(mt, two_cta);
+        const int s3 = max_stages(mt, three_cta);
+        const int sc = max_stages(mt, corun_cta);
+        if (s2 >= 2 && s2 < s1 && tmem_columns(mt, acc) <= 256) plan->tc_candidates.push_back({mt, s2, fuse});
+        if (s1 >= 2) plan->tc_candidates.push_back({mt, s1, fuse});
+        if (s3 >= 2 && s3 < s2 && 3 * tmem_columns(mt, acc) <= 512) plan->tc_candidates.push_back({mt, s3, fuse});
+        if (sc >= 2 && sc != s1 && sc != s2 && sc != s3) plan->tc_candidates.push_back({mt, sc, fuse});
+      }
+    }
+    const int m_tiles = plan->tc_candidates.empty() ? 1 : plan->tc_candidates.front().m_tiles;
+    const int stages = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().stages;
+    const int fuse0 = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().fuse;
+    const int acc_stride = acc_stride_of(fuse0);
+    // AUTO and BF16X3 run the M2L on the tensor cores for any K (fewer
+    // than 8 states fill 8-row groups of the MMA tile with zero rows: the
+    // tensor cores still beat the FP32 SIMT M2L several times over);
+    // FP32 keeps the SIMT M2L (the plain per-state path).
+    const bool wanted = m2l_mode == CDFMM_B200_M2L_BF16X3 || m2l_mode == CDFMM_B200_M2L_AUTO;
+    plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 2 && wanted &&
+                         configure_m2l_tc(smem);
+    if (plan->tc_supported) {
+      plan->tc_Kpad = Kpad;
+      plan->tc_Npad = Npad;
+      plan->tc_stages = stages;
+      plan->tc_m_tiles = m_tiles;
+      plan->tc_acc_stride = acc_stride;
+      plan->tc_fuse = fuse0;
+      plan->tc_tmem_cols = tmem_columns(m_tiles, acc_stride);
+      plan->tc_Kp_max = round_up(std::min(plan->max_states, 128), 8);
+      const size_t boxes = static_cast<size_t>(plan->n_nodes - level_offset(2)) + 1;
+      const size_t box_elems = static_cast<size_t>(plan->tc_Kp_max) * Kpad;
+      plan->tc_a_hi = dalloc<uint16_t>(boxes * box_elems, bytes);
+      plan->tc_a_lo = dalloc<uint16_t>(boxes * box_elems, bytes);
+      const std::shared_ptr<const std::vector<uint16_t>> bt = packed_b_tiles(plan->p, ops, Npad, Kpad);
+      plan->tc_b = dalloc<uint16_t>(bt->size(), bytes);
+      upload(static_cast<uint16_t *>(plan->tc_b), bt->data(), bt->size(), h2d);
+    } else if (m2l_mode == CDFMM_B200_M2L_BF16X3) {
+      throw AbiError(CDFMM_B200_ERR_RUNTIME,
+                     "split-BF16 tensor-core M2L needs an sm_100 device, depth >= 2 and order <= 9");
+    }
+  }
+  ops.m2l_T64.reset();
+  lap(plan->stats.setup_ms_m2l);
+  plan->m2l_mode = m2l_mode;
+  plan->stats.m2l_mode_resolved = plan->tc_supported ? (m2l_mode == CDFMM_B200_M2L_FP32 ? CDFMM_B200_M2L_FP32 : CDFMM_B200_M2L_BF16X3)
+                                                     : CDFMM_B200_M2L_FP32;
+}
+
 int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **out_plan) {
   cdfmm_b200_plan *plan = nullptr;
+  const auto t_begin = std::chrono::steady_clock::now();
   try {
     require(desc != nullptr && out_plan != nullptr, "desc and out_plan must not be NULL");
     *out_plan = nullptr;
@@ -356,348 +688,30 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
     require(desc->device >= 0 && desc->device < devices, "device ordinal out of range");
     check(cudaSetDevice(desc->device), "cudaSetDevice");
 
-    plan = new cdfmm_b200_plan();
-    plan->device = desc->device;
-    plan->ns = desc->n_sources;
-    plan->nt = desc->n_targets;
-    plan->p = desc->order;
-    plan->depth = desc->depth;
-    plan->n_leaves = n_leaves;
-    plan->n_nodes = level_offset(desc->depth + 1);
-    plan->max_states = desc->max_states;
-    plan->m2l_mode = CDFMM_B200_M2L_FP32; // tensor-core M2L is selected below when available
-    for (int a = 0; a < 3; ++a) plan->root_centre[a] = desc->root_centre[a];
-    plan->root_half_width = desc->root_half_width;
-    plan->scale = 2.0 * desc->root_half_width;
-    plan->inv_scale3 = static_cast<float>(1.0 / (plan->scale * plan->scale * plan->scale));
-    plan->phi_scale = static_cast<float>(plan->scale);
-    // Host copy of the geometry: the transposed (reverse-mode) plan is built
-    // from it on the first backward call.
-    if (plan->ns > 0) {
-      plan->h_src_pos.assign(desc->sorted_source_positions, desc->sorted_source_positions + 3 * static_cast<size_t>(plan->ns));
-      plan->h_src_perm.assign(desc->source_permutation, desc->source_permutation + plan->ns);
-    }
-    if (plan->nt > 0) {
-      plan->h_tgt_pos.assign(desc->sorted_target_positions, desc->sorted_target_positions + 3 * static_cast<size_t>(plan->nt));
-      plan->h_tgt_perm.assign(desc->target_permutation, desc->target_permutation + plan->nt);
-    }
-    plan->h_src_off.assign(desc->leaf_source_offsets, desc->leaf_source_offsets + n_leaves + 1);
-    plan->h_tgt_off.assign(desc->leaf_target_offsets, desc->leaf_target_offsets + n_leaves + 1);
-
-    HostOperators &ops = plan->ops;
-    ops = build_host_operators(plan->p, plan->depth, 16);
-    plan->n = ops.n;
-    const int n = ops.n;
-    const int J = m2l_simt_beta_per_thread(n);
-    if (ops.m2l_ld < 16 * J) {
-      ops = build_host_operators(plan->p, plan->depth, 16 * J);
-    }
+    plan = new_plan(desc->n_sources, desc->n_targets, desc->order, desc->depth, desc->max_states, desc->device);
+    set_root(plan, desc->root_centre, desc->root_half_width);
     uint64_t &bytes = plan->stats.persistent_device_bytes;
     uint64_t &h2d = plan->stats.setup_h2d_bytes;
-
-    check(cudaStreamCreateWithFlags(&plan->stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    check(cudaStreamCreateWithFlags(&plan->near_stream, cudaStreamNonBlocking), "cudaStreamCreate");
-    {
-      // The far field runs on a high-priority stream so its CTAs are
-      // dispatched into SM slots as they free up while the (FP32-bound) near
-      // field runs at the default priority: tensor-core M2L and P2P overlap.
-      int least = 0, greatest = 0;
-      check(cudaDeviceGetStreamPriorityRange(&least, &greatest), "stream priorities");
-      check(cudaStreamCreateWithPriority(&plan->far_stream, cudaStreamNonBlocking, greatest), "cudaStreamCreate");
-      check(cudaEventCreateWithFlags(&plan->ev_far, cudaEventDisableTiming), "cudaEventCreate");
-    }
-    check(cudaStreamCreateWithFlags(&plan->io_in, cudaStreamNonBlocking), "cudaStreamCreate");
-    check(cudaStreamCreateWithFlags(&plan->io_out, cudaStreamNonBlocking), "cudaStreamCreate");
-    check(cudaEventCreateWithFlags(&plan->ev_fork, cudaEventDisableTiming), "cudaEventCreate");
-    check(cudaEventCreateWithFlags(&plan->ev_join, cudaEventDisableTiming), "cudaEventCreate");
-    for (cudaEvent_t &e : plan->ev_t) check(cudaEventCreate(&e), "cudaEventCreate");
-
-    // geometry
-    const std::vector<float4> srel = relative_positions(desc->sorted_source_positions, desc->leaf_source_offsets,
-                                                        n_leaves, plan->depth, plan->root_centre,
-                                                        plan->root_half_width, plan->scale);
-    const std::vector<float4> trel = relative_positions(desc->sorted_target_positions, desc->leaf_target_offsets,
-                                                        n_leaves, plan->depth, plan->root_centre,
-                                                        plan->root_half_width, plan->scale);
-    for (int j = 0; j < plan->ns; ++j)
-      require(desc->source_permutation[j] >= 0 && desc->source_permutation[j] < plan->ns, "source_permutation out of range");
-    for (int j = 0; j < plan->nt; ++j)
-      require(desc->target_permutation[j] >= 0 && desc->target_permutation[j] < plan->nt, "target_permutation out of range");
-    plan->src_rel = dalloc<float4>(plan->ns, bytes);
-    plan->tgt_rel = dalloc<float4>(plan->nt, bytes);
-    plan->src_off = dalloc<int>(n_leaves + 1, bytes);
-    plan->tgt_off = dalloc<int>(n_leaves + 1, bytes);
+    plan->src_pos64 = dalloc<double>(3 * static_cast<size_t>(plan->ns), bytes);
+    plan->tgt_pos64 = dalloc<double>(3 * static_cast<size_t>(plan->nt), bytes);
     plan->src_perm = dalloc<int>(plan->ns, bytes);
     plan->tgt_perm = dalloc<int>(plan->nt, bytes);
-    plan->self_idx = dalloc<int>(plan->nt, bytes);
-    plan->leaf_self = dalloc<int2>(n_leaves, bytes);
-    upload(plan->src_rel, srel.data(), srel.size(), h2d);
-    upload(plan->tgt_rel, trel.data(), trel.size(), h2d);
-    upload(plan->src_off, desc->leaf_source_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
-    upload(plan->tgt_off, desc->leaf_target_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
+    plan->src_off = dalloc<int>(n_leaves + 1, bytes);
+    plan->tgt_off = dalloc<int>(n_leaves + 1, bytes);
+    upload(plan->src_pos64, desc->sorted_source_positions, 3 * static_cast<size_t>(plan->ns), h2d);
+    upload(plan->tgt_pos64, desc->sorted_target_positions, 3 * static_cast<size_t>(plan->nt), h2d);
     upload(plan->src_perm, desc->source_permutation, static_cast<size_t>(plan->ns), h2d);
     upload(plan->tgt_perm, desc->target_permutation, static_cast<size_t>(plan->nt), h2d);
-    {
-      int sms = 0;
-      check(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, plan->device), "device attribute");
-      plan->sm_count = sms;
-      plan->p2p_next_unit = dalloc<int>(1, bytes);
-      const std::vector<int4> work =
-          p2p_work_units(desc->leaf_source_offsets, desc->leaf_target_offsets, plan->depth, sms, true);
-      const std::vector<int4> wide =
-          p2p_work_units(desc->leaf_source_offsets, desc->leaf_target_offsets, plan->depth, sms, false);
-      plan->n_p2p_work = static_cast<int>(work.size());
-      plan->n_p2p_work_wide = static_cast<int>(wide.size());
-      if (!work.empty()) {
-        plan->p2p_work = dalloc<int4>(work.size(), bytes);
-        upload(plan->p2p_work, work.data(), work.size(), h2d);
-      }
-      if (wide.size() == work.size()) {
-        plan->p2p_work_wide = plan->p2p_work; // no unit was capped: the same units
-      } else {
-        plan->p2p_work_wide = dalloc<int4>(wide.size(), bytes);
-        upload(plan->p2p_work_wide, wide.data(), wide.size(), h2d);
-      }
-      build_close_pairs(plan, desc, bytes, h2d);
-    }
-    {
-      std::vector<int> inv(static_cast<size_t>(std::max(plan->ns, plan->nt)), -1);
-      for (int j = 0; j < plan->ns; ++j) {
-        require(inv[static_cast<size_t>(desc->source_permutation[j])] < 0, "source_permutation is not a permutation");
-        inv[static_cast<size_t>(desc->source_permutation[j])] = j;
-      }
-      plan->src_inv = dalloc<int>(plan->ns, bytes);
-      upload(plan->src_inv, inv.data(), static_cast<size_t>(plan->ns), h2d);
-      std::fill(inv.begin(), inv.end(), -1);
-      for (int j = 0; j < plan->nt; ++j) {
-        require(inv[static_cast<size_t>(desc->target_permutation[j])] < 0, "target_permutation is not a permutation");
-        inv[static_cast<size_t>(desc->target_permutation[j])] = j;
-      }
-      plan->tgt_inv = dalloc<int>(plan->nt, bytes);
-      upload(plan->tgt_inv, inv.data(), static_cast<size_t>(plan->nt), h2d);
-    }
+    upload(plan->src_off, desc->leaf_source_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
+    upload(plan->tgt_off, desc->leaf_target_offsets, static_cast<size_t>(n_leaves) + 1, h2d);
+    plan->h_src_off.assign(desc->leaf_source_offsets, desc->leaf_source_offsets + n_leaves + 1);
+    plan->h_tgt_off.assign(desc->leaf_target_offsets, desc->leaf_target_offsets + n_leaves + 1);
+    plan->stats.setup_ms_geometry =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+    finish_plan(plan, desc->m2l_mode);
+    plan->stats.setup_ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
 
-    // operators
-    std::vector<int8_t> basis(static_cast<size_t>(n) * 4);
-    for (int a = 0; a < n; ++a) {
-      basis[4 * a] = static_cast<int8_t>(ops.ax[a]);
-      basis[4 * a + 1] = static_cast<int8_t>(ops.ay[a]);
-      basis[4 * a + 2] = static_cast<int8_t>(ops.az[a]);
-      basis[4 * a + 3] = static_cast<int8_t>(ops.ax[a] + ops.ay[a] + ops.az[a]);
-    }
-    std::vector<int> m2m_pair(ops.m2m_pair_g.size()), l2l_pair(ops.l2l_pair_g.size());
-    for (size_t e = 0; e < m2m_pair.size(); ++e) m2m_pair[e] = ops.m2m_pair_g[e] | (ops.m2m_pair_in[e] << 16);
-    for (size_t e = 0; e < l2l_pair.size(); ++e) l2l_pair[e] = ops.l2l_pair_g[e] | (ops.l2l_pair_in[e] << 16);
-    plan->basis = dalloc<int8_t>(basis.size(), bytes);
-    plan->m2m_off = dalloc<int>(ops.m2m_off.size(), bytes);
-    plan->l2l_off = dalloc<int>(ops.l2l_off.size(), bytes);
-    plan->m2m_pair = dalloc<int>(m2m_pair.size(), bytes);
-    plan->l2l_pair = dalloc<int>(l2l_pair.size(), bytes);
-    plan->m2m_coef = dalloc<float>(ops.m2m_coef.size(), bytes);
-    plan->l2l_coef = dalloc<float>(ops.l2l_coef.size(), bytes);
-    upload(plan->basis, basis.data(), basis.size(), h2d);
-    upload(plan->m2m_off, ops.m2m_off.data(), ops.m2m_off.size(), h2d);
-    upload(plan->l2l_off, ops.l2l_off.data(), ops.l2l_off.size(), h2d);
-    upload(plan->m2m_pair, m2m_pair.data(), m2m_pair.size(), h2d);
-    upload(plan->l2l_pair, l2l_pair.data(), l2l_pair.size(), h2d);
-    upload(plan->m2m_coef, ops.m2m_coef.data(), ops.m2m_coef.size(), h2d);
-    upload(plan->l2l_coef, ops.l2l_coef.data(), ops.l2l_coef.size(), h2d);
-
-    // M2L: matrices, exact power-of-two level scalings, and the work tiles.
-    std::vector<float> sm(static_cast<size_t>(plan->depth + 1) * n), sl(sm.size());
-    for (int level = 0; level <= plan->depth; ++level)
-      for (int a = 0; a < n; ++a) {
-        const int deg = ops.ax[a] + ops.ay[a] + ops.az[a];
-        sm[static_cast<size_t>(level) * n + a] = std::ldexp(1.0F, level * deg);
-        sl[static_cast<size_t>(level) * n + a] = std::ldexp(1.0F, level * (deg + 1));
-      }
-    std::vector<int4> tiles;
-    for (int level = plan->depth; level >= 2; --level) {
-      const int pside = 1 << (level - 1);
-      for (int cls = 0; cls < 8; ++cls)
-        for (int pz = 0; pz < pside; pz += 4)
-          for (int py = 0; py < pside; py += 4)
-            for (int px = 0; px < pside; px += 4) tiles.push_back(make_int4(level, cls, px | (py << 10) | (pz << 20), 0));
-    }
-    plan->n_tiles = static_cast<int>(tiles.size());
-    plan->scale_m = dalloc<float>(sm.size(), bytes);
-    plan->scale_l = dalloc<float>(sl.size(), bytes);
-    plan->m2l_tiles = dalloc<int4>(tiles.size(), bytes);
-    upload(plan->scale_m, sm.data(), sm.size(), h2d);
-    upload(plan->scale_l, sl.data(), sl.size(), h2d);
-    upload(plan->m2l_tiles, tiles.data(), tiles.size(), h2d);
-    if (plan->depth >= 2) {
-      plan->m2l_T = dalloc<float>(ops.m2l_T.size(), bytes);
-      upload(plan->m2l_T, ops.m2l_T.data(), ops.m2l_T.size(), h2d);
-      plan->stats.m2l_matrix_bytes = ops.m2l_T.size() * sizeof(float);
-    }
-
-    // statistics of the implicit interaction lists (counted on the host)
-    {
-      uint64_t classes = 0, inter = 0, pairs = 0;
-      bool used[343] = {};
-      const int32_t *so = desc->leaf_source_offsets;
-      const int32_t *to = desc->leaf_target_offsets;
-      // occupancy of every level for sources and targets
-      std::vector<std::vector<int>> socc(plan->depth + 1), tocc(plan->depth + 1);
-      for (int level = 0; level <= plan->depth; ++level) {
-        socc[level].assign(static_cast<size_t>(1) << (3 * level), 0);
-        tocc[level].assign(static_cast<size_t>(1) << (3 * level), 0);
-      }
-      for (int m = 0; m < n_leaves; ++m) {
-        for (int level = 0; level <= plan->depth; ++level) {
-          const int shift = 3 * (plan->depth - level);
-          socc[level][m >> shift] += so[m + 1] - so[m];
-          tocc[level][m >> shift] += to[m + 1] - to[m];
-        }
-      }
-      for (int level = 2; level <= plan->depth; ++level) {
-        const int side = 1 << level;
-        for (int t = 0; t < side * side * side; ++t) {
-          if (tocc[level][t] == 0) continue;
-          int tx, ty, tz;
-          demorton3(static_cast<uint32_t>(t), tx, ty, tz);
-          for (int sz = 2 * (tz >> 1) - 2; sz <= 2 * (tz >> 1) + 3; ++sz)
-            for (int sy = 2 * (ty >> 1) - 2; sy <= 2 * (ty >> 1) + 3; ++sy)
-              for (int sx = 2 * (tx >> 1) - 2; sx <= 2 * (tx >> 1) + 3; ++sx) {
-                if (sx < 0 || sy < 0 || sz < 0 || sx >= side || sy >= side || sz >= side) continue;
-                if (std::abs(sx - tx) <= 1 && std::abs(sy - ty) <= 1 && std::abs(sz - tz) <= 1) continue;
-                if (socc[level][morton3(sx, sy, sz)] == 0) continue;
-                ++inter;
-                const int slot = (tx - sx + 3) * 49 + (ty - sy + 3) * 7 + (tz - sz + 3);
-                if (!used[slot]) {
-                  used[slot] = true;
-                  ++classes;
-                }
-              }
-        }
-      }
-      const int side = 1 << plan->depth;
-      for (int m = 0; m < n_leaves; ++m) {
-        const int nt_leaf = to[m + 1] - to[m];
-        if (nt_leaf == 0) continue;
-        int x, y, z;
-        demorton3(static_cast<uint32_t>(m), x, y, z);
-        for (int dz = -1; dz <= 1; ++dz)
-          for (int dy = -1; dy <= 1; ++dy)
-            for (int dx = -1; dx <= 1; ++dx) {
-              const int a = x + dx, b = y + dy, c = z + dz;
-              if (a < 0 || b < 0 || c < 0 || a >= side || b >= side || c >= side) continue;
-              const uint32_t q = morton3(a, b, c);
-              pairs += static_cast<uint64_t>(nt_leaf) * static_cast<uint64_t>(so[q + 1] - so[q]);
-            }
-      }
-      plan->stats.m2l_classes = classes;
-      plan->stats.m2l_interactions = inter;
-      plan->stats.p2p_pairs = pairs;
-    }
-
-    // state buffers sized for max_states
-    const size_t K = static_cast<size_t>(plan->max_states);
-    plan->mom = dalloc<float4>(static_cast<size_t>(plan->ns) * ((K + 1) & ~static_cast<size_t>(1)), bytes); // paired rows
-    plan->M = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
-    plan->L = dalloc<float>(static_cast<size_t>(plan->n_nodes) * n * K, bytes);
-    plan->near = dalloc<float4>(static_cast<size_t>(plan->nt) * K, bytes);
-    check(cudaMemset(plan->M, 0, static_cast<size_t>(plan->n_nodes) * n * K * sizeof(float)), "cudaMemset");
-    check(cudaMemset(plan->L, 0, static_cast<size_t>(plan->n_nodes) * n * K * sizeof(float)), "cudaMemset");
-    check(cudaMemset(plan->near, 0, static_cast<size_t>(std::max(plan->nt, 1)) * K * sizeof(float4)), "cudaMemset");
-
-    const size_t smem = device_smem_optin(plan->device);
-    configure_far_kernels(smem);
-    configure_m2l_simt(smem);
-    configure_p2p(smem);
-    plan->p2m_chunk = 64;
-    while (plan->p2m_chunk > 8 && p2m_smem_bytes(n, plan->p, static_cast<int>(K), plan->p2m_chunk) > smem) plan->p2m_chunk /= 2;
-    require(p2m_smem_bytes(n, plan->p, 4, plan->p2m_chunk) <= smem && l2p_smem_bytes(n, plan->p, 4) <= smem,
-            "order exceeds the shared-memory budget of one CTA");
-    check(cudaDeviceSynchronize(), "plan upload");
-    plan->error_flag = dalloc<int>(1, bytes);
-    check(cudaMemset(plan->error_flag, 0, sizeof(int)), "cudaMemset");
-    check(cudaHostAlloc(reinterpret_cast<void **>(&plan->status), sizeof(cdfmm_b200_plan::StatusRecord),
-                        cudaHostAllocMapped), "cudaHostAlloc");
-    std::memset(plan->status, 0, sizeof(cdfmm_b200_plan::StatusRecord));
-    check(cudaHostGetDevicePointer(reinterpret_cast<void **>(&plan->status_dev), plan->status, 0),
-          "cudaHostGetDevicePointer");
-    plan->tc_wait_limit = kTcWaitLimit;
-
-    // Tensor-core M2L: sm_100 devices, order <= 9 (N = 16 * ceil(n/16) <= 256
-    // accumulator columns) and at least one pipeline stage in shared memory.
-    {
-      int major = 0;
-      cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, plan->device);
-      const int Kpad = round_up(n, 16);
-      const int Npad = round_up(n, 16);
-      // Pipeline shapes: 1, 2 or 4 128-row accumulators per CTA sharing each
-      // B tile, with as many stages as fit one CTA per SM, or half / a third
-      // of that for two / three CTAs per SM; each with the three products as
-      // three MMAs of N = Npad, or (when 2 Npad <= 256) A_hi x [B_hi | B_lo]
-      // fused into one MMA of N = 2 Npad plus A_lo x B_hi (two larger MMAs
-      // instead of three: fewer instructions for the one issuing thread;
-      // twice the TMEM columns).  Default: two accumulators, two CTAs per SM,
-      // three MMAs; the autotuner times the candidates on first use for
-      // each K.
-      auto acc_stride_of = [&](int fuse) { return round_up(fuse ? 2 * Npad : Npad, 32); };
-      auto max_stages = [&](int mt, size_t budget) {
-        int st = 0;
-        while (st < 8 && m2l_tc_smem_bytes(Npad, mt, st + 1) <= budget) ++st;
-        return st;
-      };
-      const size_t one_cta = std::min<size_t>(smem, 224 * 1024), two_cta = 112 * 1024, three_cta = 74 * 1024;
-      // one CTA beside two co-resident near-field CTAs (schedule CORUN)
-      const size_t corun_cta = corun_m2l_smem_budget(plan, std::min(plan->max_states, 64));
-      plan->tc_candidates.clear();
-      for (int fuse : {0, 1}) {
-        if (fuse && 2 * Npad > 256) continue; // MMA N <= 256
-        const int acc = acc_stride_of(fuse);
-        for (int mt : {2, 1, 4}) {
-          if (mt * acc > 512) continue;
-          const int s1 = max_stages(mt, one_cta);
-          const int s2 = max_stages(mt, two_cta);
-          const int s3 = max_stages(mt, three_cta);
-          const int sc = max_stages(mt, corun_cta);
-          if (s2 >= 2 && s2 < s1 && tmem_columns(mt, acc) <= 256) plan->tc_candidates.push_back({mt, s2, fuse});
-          if (s1 >= 2) plan->tc_candidates.push_back({mt, s1, fuse});
-          if (s3 >= 2 && s3 < s2 && 3 * tmem_columns(mt, acc) <= 512) plan->tc_candidates.push_back({mt, s3, fuse});
-          if (sc >= 2 && sc != s1 && sc != s2 && sc != s3) plan->tc_candidates.push_back({mt, sc, fuse});
-        }
-      }
-      const int m_tiles = plan->tc_candidates.empty() ? 1 : plan->tc_candidates.front().m_tiles;
-      const int stages = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().stages;
-      const int fuse0 = plan->tc_candidates.empty() ? 0 : plan->tc_candidates.front().fuse;
-      const int acc_stride = acc_stride_of(fuse0);
-      // AUTO and BF16X3 run the M2L on the tensor cores for any K (fewer
-      // than 8 states fill 8-row groups of the MMA tile with zero rows: the
-      // tensor cores still beat the FP32 SIMT M2L several times over);
-      // FP32 keeps the SIMT M2L (the plain per-state path).
-      const bool wanted = desc->m2l_mode == CDFMM_B200_M2L_BF16X3 || desc->m2l_mode == CDFMM_B200_M2L_AUTO;
-      plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 2 && wanted &&
-                           configure_m2l_tc(smem);
-      if (plan->tc_supported) {
-        plan->tc_Kpad = Kpad;
-        plan->tc_Npad = Npad;
-        plan->tc_stages = stages;
-        plan->tc_m_tiles = m_tiles;
-        plan->tc_acc_stride = acc_stride;
-        plan->tc_fuse = fuse0;
-        plan->tc_tmem_cols = tmem_columns(m_tiles, acc_stride);
-        plan->tc_Kp_max = round_up(std::min(plan->max_states, 128), 8);
-        const size_t boxes = static_cast<size_t>(plan->n_nodes - level_offset(2)) + 1;
-        const size_t box_elems = static_cast<size_t>(plan->tc_Kp_max) * Kpad;
-        plan->tc_a_hi = dalloc<uint16_t>(boxes * box_elems, bytes);
-        plan->tc_a_lo = dalloc<uint16_t>(boxes * box_elems, bytes);
-        const std::vector<uint16_t> bt = pack_m2l_b_tiles(ops.m2l_T64, n, Npad, Kpad);
-        plan->tc_b = dalloc<uint16_t>(bt.size(), bytes);
-        upload(static_cast<uint16_t *>(plan->tc_b), bt.data(), bt.size(), h2d);
-      } else if (desc->m2l_mode == CDFMM_B200_M2L_BF16X3) {
-        throw AbiError(CDFMM_B200_ERR_RUNTIME,
-                       "split-BF16 tensor-core M2L needs an sm_100 device, depth >= 2 and order <= 9");
-      }
-    }
-    ops.m2l_T64.clear();
-    ops.m2l_T64.shrink_to_fit();
-    plan->m2l_mode = desc->m2l_mode;
-    plan->stats.m2l_mode_resolved = plan->tc_supported ? (desc->m2l_mode == CDFMM_B200_M2L_FP32 ? CDFMM_B200_M2L_FP32 : CDFMM_B200_M2L_BF16X3)
-                                                       : CDFMM_B200_M2L_FP32;
     *out_plan = plan;
     return CDFMM_B200_OK;
   } catch (const AbiError &e) {
@@ -709,6 +723,151 @@ int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **o
   } catch (const std::exception &e) {
     free_plan(plan);
     return fail(nullptr, CDFMM_B200_ERR_RUNTIME, e.what());
+  }
+}
+
+int cdfmm_b200_plan_create_from_points(const cdfmm_b200_points_desc *desc, cdfmm_b200_plan **out_plan) {
+  const auto t_begin = std::chrono::steady_clock::now();
+  cdfmm_b200_plan *plan = nullptr;
+  void *staged = nullptr;
+  SortedPopulation src, tgt;
+  auto release = [&]() {
+    for (void *q : {static_cast<void *>(src.positions), static_cast<void *>(src.permutation),
+                    static_cast<void *>(src.offsets), static_cast<void *>(tgt.positions),
+                    static_cast<void *>(tgt.permutation), static_cast<void *>(tgt.offsets), staged})
+      if (q != nullptr) cudaFree(q);
+    free_plan(plan);
+  };
+  try {
+    require(desc != nullptr && out_plan != nullptr, "desc and out_plan must not be NULL");
+    *out_plan = nullptr;
+    require(desc->struct_size == static_cast<int32_t>(sizeof(cdfmm_b200_points_desc)), "desc.struct_size mismatch");
+    require(desc->n_sources >= 0 && desc->n_targets >= 0, "negative population size");
+    require(desc->order >= 0 && desc->order <= kMaxOrder, "order must be in [0, 10]");
+    require(desc->depth >= 0 && desc->depth <= kMaxDepth, "depth must be in [0, 8]");
+    require(desc->max_states >= 1 && desc->max_states <= 1024, "max_states must be in [1, 1024]");
+    require(desc->m2l_mode >= CDFMM_B200_M2L_AUTO && desc->m2l_mode <= CDFMM_B200_M2L_BF16X3, "unknown m2l_mode");
+    require(desc->root_flags >= 0 && desc->root_flags <= (CDFMM_B200_ROOT_CENTRE | CDFMM_B200_ROOT_HALF_WIDTH),
+            "unknown root_flags");
+    require((desc->root_flags & CDFMM_B200_ROOT_HALF_WIDTH) == 0 ||
+                (desc->root_half_width > 0.0 && std::isfinite(desc->root_half_width)),
+            "UniformTreeOptions.root_half_width must be positive");
+    const bool same = desc->target_positions == nullptr;
+    require(desc->n_sources == 0 || desc->source_positions != nullptr, "source_positions are required");
+    require(same || desc->n_targets == 0 || desc->target_positions != nullptr, "target_positions are required");
+    require(desc->self_map == 0 || same, "the identity self map needs targets == sources (target_positions NULL)");
+    const int ns = desc->n_sources;
+    const int nt = same ? ns : desc->n_targets;
+
+    int devices = 0;
+    if (cudaGetDeviceCount(&devices) != cudaSuccess || devices == 0) {
+      cudaGetLastError();
+      throw AbiError(CDFMM_B200_ERR_NO_DEVICE, "no CUDA device is available");
+    }
+    require(desc->device >= 0 && desc->device < devices, "device ordinal out of range");
+    check(cudaSetDevice(desc->device), "cudaSetDevice");
+
+    cudaGetLastError(); // a stale error of an earlier call must not fail this one's checks
+    plan = new_plan(ns, nt, desc->order, desc->depth, desc->max_states, desc->device);
+    const auto t_tree = std::chrono::steady_clock::now();
+    uint64_t &bytes = plan->stats.persistent_device_bytes;
+    uint64_t &h2d = plan->stats.setup_h2d_bytes;
+    const double *sp = desc->source_positions;
+    const double *tp = same ? nullptr : desc->target_positions;
+    if (desc->positions_on_host) {
+      const size_t sb = 24 * static_cast<size_t>(ns), tb = same ? 0 : 24 * static_cast<size_t>(nt);
+      check(cudaMalloc(&staged, std::max<size_t>(sb + tb, 8)), "cudaMalloc positions");
+      char *d = static_cast<char *>(staged);
+      if (sb) check(cudaMemcpyAsync(d, sp, sb, cudaMemcpyHostToDevice, plan->stream), "H2D positions");
+      if (tb) check(cudaMemcpyAsync(d + sb, tp, tb, cudaMemcpyHostToDevice, plan->stream), "H2D positions");
+      h2d += sb + tb;
+      sp = reinterpret_cast<const double *>(d);
+      tp = same ? nullptr : reinterpret_cast<const double *>(d + sb);
+    }
+    RootRequest root;
+    root.has_centre = (desc->root_flags & CDFMM_B200_ROOT_CENTRE) != 0;
+    root.has_half_width = (desc->root_flags & CDFMM_B200_ROOT_HALF_WIDTH) != 0;
+    for (int a = 0; a < 3; ++a) root.centre[a] = desc->root_centre[a];
+    root.half_width = desc->root_half_width;
+    double centre[3], half_width = 0.0;
+    const std::string err =
+        build_device_tree(sp, ns, tp, same ? 0 : nt, desc->depth, root, centre, half_width, src, tgt, plan->stream);
+    if (staged != nullptr) {
+      cudaFree(staged);
+      staged = nullptr;
+    }
+    require(err.empty(), err);
+    require(half_width > 0.0 && std::isfinite(half_width),
+            "the points span no volume (root half width 0); give root_half_width explicitly");
+    set_root(plan, centre, half_width);
+    plan->src_pos64 = src.positions;
+    plan->src_perm = src.permutation;
+    plan->src_off = src.offsets;
+    plan->tgt_pos64 = tgt.positions;
+    plan->tgt_perm = tgt.permutation;
+    plan->tgt_off = tgt.offsets;
+    plan->h_src_off = std::move(src.host_offsets);
+    plan->h_tgt_off = std::move(tgt.host_offsets);
+    src = SortedPopulation();
+    tgt = SortedPopulation();
+    bytes += 28 * (static_cast<uint64_t>(ns) + static_cast<uint64_t>(nt)) +
+             8 * (static_cast<uint64_t>(plan->n_leaves) + 1);
+    plan->stats.setup_ms_tree =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_tree).count();
+    finish_plan(plan, desc->m2l_mode);
+    if (desc->self_map != 0) {
+      launch_identity_self(nt, plan->tgt_off, plan->n_leaves, plan->self_idx, plan->leaf_self, nullptr);
+      check(cudaGetLastError(), "identity self map");
+      check(cudaDeviceSynchronize(), "identity self map");
+      plan->h_self.resize(static_cast<size_t>(nt));
+      for (int i = 0; i < nt; ++i) plan->h_self[static_cast<size_t>(i)] = i;
+      plan->has_self = true;
+      plan->self_version += 1;
+    }
+    plan->stats.setup_ms_total =
+        std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - t_begin).count();
+    *out_plan = plan;
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    release();
+    return fail(nullptr, e.code, e.what());
+  } catch (const std::bad_alloc &) {
+    release();
+    return fail(nullptr, CDFMM_B200_ERR_OUT_OF_MEMORY, "allocation failed");
+  } catch (const std::exception &e) {
+    release();
+    return fail(nullptr, CDFMM_B200_ERR_RUNTIME, e.what());
+  }
+}
+
+int cdfmm_b200_plan_tree(cdfmm_b200_plan *plan, double *root, int32_t *source_permutation,
+                         int32_t *target_permutation, int32_t *leaf_source_offsets, int32_t *leaf_target_offsets,
+                         double *sorted_source_positions, double *sorted_target_positions) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  try {
+    check(cudaSetDevice(plan->device), "cudaSetDevice");
+    if (root != nullptr) {
+      for (int a = 0; a < 3; ++a) root[a] = plan->root_centre[a];
+      root[3] = plan->root_half_width;
+    }
+    const size_t ns = static_cast<size_t>(plan->ns), nt = static_cast<size_t>(plan->nt);
+    const size_t nl = static_cast<size_t>(plan->n_leaves) + 1;
+    if (leaf_source_offsets) std::memcpy(leaf_source_offsets, plan->h_src_off.data(), nl * sizeof(int32_t));
+    if (leaf_target_offsets) std::memcpy(leaf_target_offsets, plan->h_tgt_off.data(), nl * sizeof(int32_t));
+    check(cudaDeviceSynchronize(), "sync");
+    if (source_permutation && ns)
+      check(cudaMemcpy(source_permutation, plan->src_perm, ns * sizeof(int32_t), cudaMemcpyDeviceToHost), "D2H");
+    if (target_permutation && nt)
+      check(cudaMemcpy(target_permutation, plan->tgt_perm, nt * sizeof(int32_t), cudaMemcpyDeviceToHost), "D2H");
+    if (sorted_source_positions && ns)
+      check(cudaMemcpy(sorted_source_positions, plan->src_pos64, 3 * ns * sizeof(double), cudaMemcpyDeviceToHost),
+            "D2H");
+    if (sorted_target_positions && nt)
+      check(cudaMemcpy(sorted_target_positions, plan->tgt_pos64, 3 * nt * sizeof(double), cudaMemcpyDeviceToHost),
+            "D2H");
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(plan, e.code, e.what());
   }
 }
 
@@ -1069,6 +1228,37 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   return launches;
 }
 
+void cdfmm_b200_stacked_upward(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a, cudaStream_t s) {
+  const bool want_phi = (a->output & CDFMM_B200_OUTPUT_POTENTIAL) != 0u;
+  ++plan->call_seq;
+  launch_gather_moments(a->moments, a->moments_dtype, plan->src_inv, plan->ns, 1, plan->scale, plan->mom, s, false);
+  check(cudaEventRecord(plan->ev_fork, s), "event");
+  check(cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0), "wait");
+  // inside a batch graph: the uncapped work units (see enqueue_evaluation)
+  launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work_wide, plan->n_p2p_work_wide,
+             plan->has_self ? plan->self_idx : nullptr, plan->leaf_self, close_geometry(plan), plan->depth, 1, want_phi,
+             plan->near, plan->near_stream);
+  check(cudaEventRecord(plan->ev_join, plan->near_stream), "event");
+  enqueue_upward(plan, 1, s, false);
+  check(cudaGetLastError(), "kernel launch");
+}
+
+void cdfmm_b200_stacked_downward(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a, cudaStream_t s) {
+  for (int level = 3; level <= plan->depth; ++level)
+    launch_l2l(plan->L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, plan->n, 1, level,
+               static_cast<int>(plan->ops.l2l_pair_g.size()), s);
+  check(cudaStreamWaitEvent(s, plan->ev_join, 0), "wait");
+  launch_l2p(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, plan->tgt_inv, plan->near, plan->basis, plan->n,
+             plan->p, 1, plan->nt, plan->depth, a->output, a->layout, plan->phi_scale, a->field, a->potential, s);
+  check(cdfmm_b200_collect_status(plan, s, plan->call_seq), "status kernel launch");
+  check(cudaGetLastError(), "kernel launch");
+  plan->last_m2l_tc = true;
+  plan->last_schedule = CDFMM_B200_SCHEDULE_SEPARATE;
+  plan->exp_state0 = 0;
+  plan->last_K = 1;
+  plan->stats.evaluations += 1;
+}
+
 int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
   if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
   try {
@@ -1361,27 +1551,36 @@ int cdfmm_b200_evaluate(cdfmm_b200_plan *plan, const cdfmm_b200_eval_args *a) {
 // the uniform tree, and the dipole pair tensor is symmetric and even in r.
 static void ensure_adjoint(cdfmm_b200_plan *plan) {
   if (plan->adjoint == nullptr) {
-    cdfmm_b200_plan_desc d{};
-    d.struct_size = sizeof d;
-    d.n_sources = plan->nt;
-    d.n_targets = plan->ns;
-    d.order = plan->p;
-    d.depth = plan->depth;
-    d.max_states = plan->max_states;
-    d.m2l_mode = plan->m2l_mode;
-    d.device = plan->device;
-    for (int a = 0; a < 3; ++a) d.root_centre[a] = plan->root_centre[a];
-    d.root_half_width = plan->root_half_width;
-    d.sorted_source_positions = plan->h_tgt_pos.data();
-    d.sorted_target_positions = plan->h_src_pos.data();
-    d.source_permutation = plan->h_tgt_perm.data();
-    d.target_permutation = plan->h_src_perm.data();
-    d.leaf_source_offsets = plan->h_tgt_off.data();
-    d.leaf_target_offsets = plan->h_src_off.data();
     cdfmm_b200_plan *adj = nullptr;
-    const int rc = cdfmm_b200_plan_create(&d, &adj);
-    if (rc != CDFMM_B200_OK)
-      throw AbiError(rc, std::string("transposed plan: ") + cdfmm_b200_last_error(nullptr));
+    try {
+      adj = new_plan(plan->nt, plan->ns, plan->p, plan->depth, plan->max_states, plan->device);
+      set_root(adj, plan->root_centre, plan->root_half_width);
+      uint64_t &bytes = adj->stats.persistent_device_bytes;
+      const size_t nl = static_cast<size_t>(plan->n_leaves) + 1;
+      adj->src_pos64 = dalloc<double>(3 * static_cast<size_t>(adj->ns), bytes);
+      adj->tgt_pos64 = dalloc<double>(3 * static_cast<size_t>(adj->nt), bytes);
+      adj->src_perm = dalloc<int>(adj->ns, bytes);
+      adj->tgt_perm = dalloc<int>(adj->nt, bytes);
+      adj->src_off = dalloc<int>(nl, bytes);
+      adj->tgt_off = dalloc<int>(nl, bytes);
+      check(cudaDeviceSynchronize(), "sync");
+      const cudaMemcpyKind dd = cudaMemcpyDeviceToDevice;
+      check(cudaMemcpy(adj->src_pos64, plan->tgt_pos64, 24 * static_cast<size_t>(adj->ns), dd), "D2D");
+      check(cudaMemcpy(adj->tgt_pos64, plan->src_pos64, 24 * static_cast<size_t>(adj->nt), dd), "D2D");
+      check(cudaMemcpy(adj->src_perm, plan->tgt_perm, 4 * static_cast<size_t>(adj->ns), dd), "D2D");
+      check(cudaMemcpy(adj->tgt_perm, plan->src_perm, 4 * static_cast<size_t>(adj->nt), dd), "D2D");
+      check(cudaMemcpy(adj->src_off, plan->tgt_off, 4 * nl, dd), "D2D");
+      check(cudaMemcpy(adj->tgt_off, plan->src_off, 4 * nl, dd), "D2D");
+      adj->h_src_off = plan->h_tgt_off;
+      adj->h_tgt_off = plan->h_src_off;
+      finish_plan(adj, plan->m2l_mode);
+    } catch (const AbiError &e) {
+      free_plan(adj);
+      throw AbiError(e.code, std::string("transposed plan: ") + e.what());
+    } catch (...) {
+      free_plan(adj);
+      throw;
+    }
     plan->adjoint = adj;
     plan->adjoint_self_version = -1;
   }
@@ -1775,9 +1974,29 @@ int cdfmm_b200_m2l_matrix(int32_t order, const double *R, double *out, size_t ou
   }
 }
 
+int cdfmm_b200_m2l_stencil(int32_t order, double *out, size_t out_count, int32_t *source) {
+  try {
+    require(order >= 0 && order <= kMaxOrder, "order must be in [0, 10]");
+    const int n = basis_size(order);
+    require(out == nullptr || out_count >= static_cast<size_t>(343) * n * n, "output buffer too small");
+    OperatorSource from = OperatorSource::Computed;
+    const std::shared_ptr<const std::vector<double>> T = m2l_matrices(order, &from);
+    if (out != nullptr) std::memcpy(out, T->data(), T->size() * sizeof(double));
+    if (source != nullptr) *source = static_cast<int32_t>(from);
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(nullptr, e.code, e.what());
+  } catch (const std::exception &e) {
+    return fail(nullptr, CDFMM_B200_ERR_RUNTIME, e.what());
+  }
+}
+
 const char *cdfmm_b200_last_error(const cdfmm_b200_plan *plan) {
   if (plan != nullptr) return plan->last_error.c_str();
   return g_last_error.c_str();
 }
 
 } // extern "C"
+
+std::vector<int4> cdfmm_b200::tc_work_tiles(int depth, int T) { return build_tc_tiles(depth, T); }
+uint32_t cdfmm_b200::tc_tmem_columns(int m_tiles, int acc_stride) { return tmem_columns(m_tiles, acc_stride); }

@@ -44,8 +44,11 @@ EXPORTED = (
     "cdfmm_b200_evaluate_noalloc", "cdfmm_b200_backward", "cdfmm_b200_batch_create",
     "cdfmm_b200_batch_launch", "cdfmm_b200_batch_destroy", "cdfmm_b200_direct_grad_fp64",
     "cdfmm_b200_selftest_bounded_wait", "cdfmm_b200_m2l_shapes", "cdfmm_b200_set_m2l_shape",
-    "cdfmm_b200_poll_status", "cdfmm_b200_set_wait_limit", "cdfmm_b200_set_schedule",
+    "cdfmm_b200_poll_status", "cdfmm_b200_set_wait_limit", "cdfmm_b200_set_schedule", "cdfmm_b200_batch_groups",
+    "cdfmm_b200_plan_create_from_points", "cdfmm_b200_plan_tree", "cdfmm_b200_m2l_stencil",
 )
+
+ROOT_CENTRE, ROOT_HALF_WIDTH = 1, 2
 
 # Scratch capacity of cdfmm_b200_evaluate_noalloc (bytes).
 NOALLOC_SCRATCH_BYTES = 64 << 20
@@ -60,6 +63,18 @@ class PlanDesc(ctypes.Structure):
         ("sorted_source_positions", ctypes.c_void_p), ("sorted_target_positions", ctypes.c_void_p),
         ("source_permutation", ctypes.c_void_p), ("target_permutation", ctypes.c_void_p),
         ("leaf_source_offsets", ctypes.c_void_p), ("leaf_target_offsets", ctypes.c_void_p),
+    ]
+
+
+class PointsDesc(ctypes.Structure):
+    _fields_ = [
+        ("struct_size", ctypes.c_int32), ("n_sources", ctypes.c_int32), ("n_targets", ctypes.c_int32),
+        ("order", ctypes.c_int32), ("depth", ctypes.c_int32), ("max_states", ctypes.c_int32),
+        ("m2l_mode", ctypes.c_int32), ("device", ctypes.c_int32), ("root_flags", ctypes.c_int32),
+        ("positions_on_host", ctypes.c_int32),
+        ("root_centre", ctypes.c_double * 3), ("root_half_width", ctypes.c_double),
+        ("source_positions", ctypes.c_void_p), ("target_positions", ctypes.c_void_p),
+        ("self_map", ctypes.c_int32), ("reserved0", ctypes.c_int32),
     ]
 
 
@@ -99,6 +114,10 @@ class Stats(ctypes.Structure):
         ("trace_far_begin", ctypes.c_double), ("trace_m2l_begin", ctypes.c_double),
         ("trace_far_end", ctypes.c_double), ("trace_end", ctypes.c_double),
         ("schedule_last", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+        ("setup_ms_tree", ctypes.c_double), ("setup_ms_geometry", ctypes.c_double),
+        ("setup_ms_near", ctypes.c_double), ("setup_ms_operators", ctypes.c_double),
+        ("setup_ms_statistics", ctypes.c_double), ("setup_ms_buffers", ctypes.c_double),
+        ("setup_ms_m2l", ctypes.c_double), ("setup_ms_total", ctypes.c_double),
     ]
 
     def as_dict(self):
@@ -126,6 +145,9 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_device_count.argtypes = [ctypes.POINTER(i32)]
     lib.cdfmm_b200_device_info.argtypes = [i32, ctypes.c_char_p, u64, ctypes.POINTER(i32), ctypes.POINTER(i32)]
     lib.cdfmm_b200_plan_create.argtypes = [ctypes.POINTER(PlanDesc), ctypes.POINTER(vp)]
+    lib.cdfmm_b200_plan_create_from_points.argtypes = [ctypes.POINTER(PointsDesc), ctypes.POINTER(vp)]
+    lib.cdfmm_b200_plan_tree.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.cdfmm_b200_m2l_stencil.argtypes = [i32, vp, u64, ctypes.POINTER(i32)]
     lib.cdfmm_b200_plan_destroy.argtypes = [vp]
     lib.cdfmm_b200_plan_destroy.restype = None
     lib.cdfmm_b200_set_self_indices.argtypes = [vp, vp]
@@ -134,6 +156,7 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_backward.argtypes = [vp, ctypes.POINTER(BackwardArgs)]
     lib.cdfmm_b200_batch_create.argtypes = [ctypes.POINTER(vp), ctypes.POINTER(EvalArgs), i32, ctypes.POINTER(vp)]
     lib.cdfmm_b200_batch_launch.argtypes = [vp, vp, i32]
+    lib.cdfmm_b200_batch_groups.argtypes = [vp, ctypes.POINTER(i32), i32]
     lib.cdfmm_b200_batch_destroy.argtypes = [vp]
     lib.cdfmm_b200_batch_destroy.restype = None
     lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
@@ -183,6 +206,20 @@ def m2l_matrix(order: int, R) -> np.ndarray:
     Rv = np.ascontiguousarray(R, dtype=np.float64)
     _check(library().cdfmm_b200_m2l_matrix(order, _ptr(Rv), _ptr(out), out.size))
     return out.reshape(n, n).T.copy()
+
+
+STENCIL_COMPUTED, STENCIL_PROCESS, STENCIL_DISK = 0, 1, 2
+
+
+def m2l_stencil(order: int):
+    """The 343 normalised M2L matrices of `order` as plans use them,
+    (343, n, n) FP64, and where they came from (STENCIL_*): computed, this
+    process's cache, or the CDFMM_B200_OPERATOR_CACHE directory."""
+    n = (order + 1) * (order + 2) * (order + 3) // 6
+    out = np.zeros((343, n, n))
+    src = ctypes.c_int32(-1)
+    _check(library().cdfmm_b200_m2l_stencil(order, _ptr(out), out.size, ctypes.byref(src)))
+    return out, src.value
 
 
 def direct_fp64(sources, moments, targets, self_indices=None, device=0):
@@ -256,6 +293,82 @@ class DevicePlan:
         rc = tree.root_centre
         return cls(tree.sorted_source_positions(), tree.sorted_target_positions(), tree.source_permutation,
                    tree.target_permutation, soff, toff, (rc.x, rc.y, rc.z), tree.root_half_width, order, depth, **kw)
+
+    @classmethod
+    def from_points(cls, sources, order, depth, targets=None, root_centre=None, root_half_width=None,
+                    self_map=None, max_states=1, m2l_mode=M2L_AUTO, device=0):
+        """Builds the uniform octree on the device from user-order FP64
+        positions ((n, 3) numpy array, or a contiguous float64 CUDA tensor
+        with any array interface exposing data_ptr()) and the plan on it
+        (cdfmm_b200_plan_create_from_points).  targets None: the targets are
+        the sources, and self_map (default True then) excludes each point's
+        own source from its near field.  The tree equals cdfmm.UniformTree's
+        for the same points and options."""
+        lib = library()
+
+        def view(a):
+            if hasattr(a, "data_ptr"):
+                if a.dtype.__repr__() != "torch.float64" or not a.is_contiguous() or a.dim() != 2 or a.shape[1] != 3:
+                    raise ValueError("device positions must be a contiguous (n, 3) float64 tensor")
+                return a, a.data_ptr(), int(a.shape[0]), 0
+            h = np.ascontiguousarray(a, dtype=np.float64).reshape(-1, 3)
+            return h, h.ctypes.data, len(h), 1
+
+        ks, sp, ns, host_s = view(sources)
+        d = PointsDesc()
+        d.struct_size = ctypes.sizeof(PointsDesc)
+        d.n_sources = ns
+        d.order, d.depth, d.max_states, d.m2l_mode, d.device = order, depth, max_states, m2l_mode, device
+        d.positions_on_host = host_s
+        d.source_positions = sp
+        keep = [ks]
+        if targets is not None:
+            kt, tp, nt, host_t = view(targets)
+            if host_t != host_s:
+                raise ValueError("sources and targets must both be host arrays or both device arrays")
+            keep.append(kt)
+            d.n_targets, d.target_positions = nt, tp
+            if self_map:
+                raise ValueError("self_map needs targets=None (targets are the sources)")
+        else:
+            d.n_targets = ns
+            d.self_map = 1 if self_map in (None, True) else 0
+        flags = 0
+        if root_centre is not None:
+            flags |= ROOT_CENTRE
+            for a in range(3):
+                d.root_centre[a] = float(root_centre[a])
+        if root_half_width is not None:
+            flags |= ROOT_HALF_WIDTH
+            d.root_half_width = float(root_half_width)
+        d.root_flags = flags
+        handle = ctypes.c_void_p()
+        _check(lib.cdfmm_b200_plan_create_from_points(ctypes.byref(d), ctypes.byref(handle)))
+        self = cls.__new__(cls)
+        self._h = handle
+        self.n_sources, self.n_targets, self.order, self.depth = ns, d.n_targets, order, depth
+        self.n_coefficients = (order + 1) * (order + 2) * (order + 3) // 6
+        self.n_nodes = ((1 << (3 * (depth + 1))) - 1) // 7
+        self.max_states = max_states
+        self._keep = None
+        return self
+
+    def tree(self) -> dict:
+        """The plan's tree (cdfmm_b200_plan_tree): root centre and half
+        width, permutations, leaf offsets and Morton-sorted positions."""
+        nl = (1 << (3 * self.depth)) + 1
+        root = np.zeros(4)
+        sp = np.zeros(self.n_sources, dtype=np.int32)
+        tp = np.zeros(self.n_targets, dtype=np.int32)
+        so = np.zeros(nl, dtype=np.int32)
+        to = np.zeros(nl, dtype=np.int32)
+        sx = np.zeros((self.n_sources, 3))
+        tx = np.zeros((self.n_targets, 3))
+        _check(library().cdfmm_b200_plan_tree(self._h, *[a.ctypes.data for a in (root, sp, tp, so, to, sx, tx)]),
+               self._h)
+        return {"root_centre": root[:3].copy(), "root_half_width": float(root[3]), "source_permutation": sp,
+                "target_permutation": tp, "leaf_source_offsets": so, "leaf_target_offsets": to,
+                "sorted_source_positions": sx, "sorted_target_positions": tx}
 
     def close(self):
         if getattr(self, "_h", None):
@@ -462,6 +575,15 @@ class Batch:
 
     def launch(self, stream=None, synchronize=True):
         _check(library().cdfmm_b200_batch_launch(self._h, stream, 1 if synchronize else 0))
+
+    def groups(self) -> list:
+        """Stacked-M2L group of each plan (-1: evaluated on its own)."""
+        n = len(self._keep)
+        buf = (ctypes.c_int32 * max(n, 1))()
+        got = library().cdfmm_b200_batch_groups(self._h, buf, n)
+        if got < 0:
+            _check(got)
+        return [int(buf[i]) for i in range(n)]
 
     def close(self):
         if getattr(self, "_h", None):

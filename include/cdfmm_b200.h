@@ -136,6 +136,12 @@ typedef struct cdfmm_b200_stats {
   double trace_p2p_begin, trace_p2p_end, trace_far_begin, trace_m2l_begin, trace_far_end, trace_end;
   int32_t schedule_last;         /* CDFMM_B200_SCHEDULE_* the last evaluate ran */
   int32_t reserved0;
+  /* Plan construction, host wall-clock ms: the device octree (points plans),
+   * positions / permutations, near-field work units and close pairs,
+   * operators, interaction statistics, state buffers and kernel set-up, the
+   * tensor-core M2L set-up, and the whole call. */
+  double setup_ms_tree, setup_ms_geometry, setup_ms_near, setup_ms_operators, setup_ms_statistics,
+      setup_ms_buffers, setup_ms_m2l, setup_ms_total;
 } cdfmm_b200_stats;
 
 /* Library / device probing.  Returns OK and *count = 0 when no device. */
@@ -149,6 +155,54 @@ int cdfmm_b200_device_info(int32_t device, char *name, size_t name_len, int32_t 
 /* Build operators and upload the geometry (the reference's CudaFullPlan ctor,
  * src/cuda_fmm.cu:2937-3155 upstream).  Host arrays may be freed on return. */
 int cdfmm_b200_plan_create(const cdfmm_b200_plan_desc *desc, cdfmm_b200_plan **out_plan);
+
+/* Root cube parts a cdfmm_b200_points_desc gives explicitly
+ * (UniformTreeOptions.root_centre / root_half_width, include/cdfmm/
+ * uniform_tree.hpp upstream); parts not given come from the bounding box. */
+#define CDFMM_B200_ROOT_CENTRE 1
+#define CDFMM_B200_ROOT_HALF_WIDTH 2
+
+/* Plan geometry given as raw user-order positions: the uniform octree is
+ * built on the device.  The root cube, leaf keys, stable leaf ordering and
+ * leaf ranges equal upstream UniformTree's (src/uniform_tree.cpp:129-357)
+ * bit for bit, so the plan is the one cdfmm_b200_plan_create builds from the
+ * host tree of the same points. */
+typedef struct cdfmm_b200_points_desc {
+  int32_t struct_size;             /* sizeof(cdfmm_b200_points_desc) */
+  int32_t n_sources;               /* >= 0 */
+  int32_t n_targets;               /* >= 0; ignored when target_positions is NULL */
+  int32_t order;                   /* expansion order p, 0..10 */
+  int32_t depth;                   /* tree max_level, 0..8 */
+  int32_t max_states;              /* largest K passed to one evaluate call, >= 1 */
+  int32_t m2l_mode;                /* CDFMM_B200_M2L_* */
+  int32_t device;                  /* CUDA device ordinal */
+  int32_t root_flags;              /* CDFMM_B200_ROOT_* bits */
+  int32_t positions_on_host;       /* nonzero: positions are host arrays, else device arrays */
+  double root_centre[3];           /* used with CDFMM_B200_ROOT_CENTRE */
+  double root_half_width;          /* used with CDFMM_B200_ROOT_HALF_WIDTH, > 0 */
+  const double *source_positions;  /* [n_sources][3] FP64, user order */
+  const double *target_positions;  /* [n_targets][3] FP64, user order; NULL: the targets are the sources */
+  int32_t self_map;                /* nonzero (targets NULL only): target i is source i, as upstream's
+                                      identity policy sets it for targets == sources
+                                      (src/uniform_fmm.cpp:1028-1043) */
+  int32_t reserved0;
+} cdfmm_b200_points_desc;
+
+/* Builds the tree on the device and then the plan as cdfmm_b200_plan_create
+ * does (the reference's UniformFmm constructor, src/uniform_fmm.cpp:370-717,
+ * plus CudaFullPlan's set-up).  A point outside an explicit root box, or a
+ * non-finite coordinate, is CDFMM_B200_ERR_INVALID_ARGUMENT ("Point lies
+ * outside the requested root box", the host tree's message).  Device
+ * positions must be complete when the call is made. */
+int cdfmm_b200_plan_create_from_points(const cdfmm_b200_points_desc *desc, cdfmm_b200_plan **out_plan);
+
+/* The plan's tree, for callers that built it with
+ * cdfmm_b200_plan_create_from_points: root (centre x, y, z, half width),
+ * permutations (sorted index -> user index), leaf offsets ([8^depth + 1])
+ * and Morton-sorted FP64 positions ([n][3]).  Any NULL output is skipped. */
+int cdfmm_b200_plan_tree(cdfmm_b200_plan *plan, double *root, int32_t *source_permutation,
+                         int32_t *target_permutation, int32_t *leaf_source_offsets, int32_t *leaf_target_offsets,
+                         double *sorted_source_positions, double *sorted_target_positions);
 
 /* Releases every device allocation of the plan.  NULL is ignored. */
 void cdfmm_b200_plan_destroy(cdfmm_b200_plan *plan);
@@ -265,6 +319,15 @@ int cdfmm_b200_batch_create(cdfmm_b200_plan *const *plans, const cdfmm_b200_eval
  * evaluation of every plan of the batch (the `evaluations` counter), so a
  * backward call cannot reuse expansions from before the launch. */
 int cdfmm_b200_batch_launch(cdfmm_b200_batch *batch, void *stream, int32_t synchronize);
+/* Stacked M2L groups of a batch: plans evaluated with one state each whose
+ * M2L runs on the tensor cores are grouped by (depth, order); a group of two
+ * or more runs ONE M2L with its plans as the states (their normalised M2L
+ * operators are the same), instead of one M2L per plan.  Writes each plan's
+ * group (or -1: evaluated on its own) into out[capacity] and returns the
+ * plan count.  A stacked plan's results may differ from its own evaluate at
+ * FP32 rounding level (the group's M2L pipeline shape is chosen for the
+ * group). */
+int cdfmm_b200_batch_groups(const cdfmm_b200_batch *batch, int32_t *out, int32_t capacity);
 void cdfmm_b200_batch_destroy(cdfmm_b200_batch *batch);
 
 /* Copies the FP32 multipole (which = 0) or local (which = 1) expansions of one
@@ -336,6 +399,16 @@ int cdfmm_b200_direct_grad_fp64(int32_t device, int32_t n_sources, const double 
  * (the reference's build_static_m2l_matrix, src/static_operators.cpp:159-184,
  * and its Python static_m2l_matrix, python/bindings.cpp:932-943).  Host only. */
 int cdfmm_b200_m2l_matrix(int32_t order, const double *R, double *out, size_t out_count);
+
+/* The 343 normalised M2L matrices of one order as plans use them
+ * ([343][n][n], slot (tx+3)*49 + (ty+3)*7 + (tz+3) for the translation
+ * t = target box - source box; slots inside the 3x3x3 near stencil are zero).
+ * They are computed once per process and order, and kept on disk, one file
+ * per order, when the environment variable CDFMM_B200_OPERATOR_CACHE names a
+ * directory (a file that fails its header or checksum check is recomputed
+ * and rewritten).  *source (optional) = 0 computed, 1 from this process's
+ * cache, 2 read from the directory.  Host only. */
+int cdfmm_b200_m2l_stencil(int32_t order, double *out, size_t out_count, int32_t *source);
 
 /* Message of the last failure on this plan (or of the last failure of a call
  * without a plan, on this thread, when plan is NULL).  Never NULL. */
