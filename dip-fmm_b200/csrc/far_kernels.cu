@@ -113,6 +113,58 @@ __device__ inline void monomials_part(float dx, float dy, float dz, int q, float
   }
 }
 
+// Cuboid sources (upstream docs/math.md "Finite cuboid geometry";
+// src/static_operators.cpp:222-255): the point monomial d^mu/mu! is replaced
+// by its average over the source cuboid (side lengths h centred at d),
+// J_mu(d, h) = prod over axes of j(mu_axis), where per axis
+//   j(a) = sum_{g even <= a} d^(a-g)/(a-g)! * (h/2)^g/(g+1)!
+// (the average of (d+u)^a/a! over u in [-h/2, h/2]).  q <= 9.
+__device__ inline void cuboid_axis(float d, float h, int q, float (&j)[10]) {
+  float pw[10], c[10];
+  pw[0] = 1.0F;
+  c[0] = 1.0F;
+  c[1] = 0.0F;
+  const float hh = 0.25F * h * h;
+#pragma unroll
+  for (int i = 1; i < 10; ++i) pw[i] = i <= q ? pw[i - 1] * d * kInvInt[i] : 0.0F;
+#pragma unroll
+  for (int g = 2; g < 10; ++g) c[g] = (g & 1) ? 0.0F : c[g - 2] * hh * kInvInt[g] * kInvInt[g + 1];
+#pragma unroll
+  for (int a = 0; a < 10; ++a) {
+    float v = 0.0F;
+#pragma unroll
+    for (int g = 0; g <= a; g += 2) v = fmaf(pw[a - g], c[g], v);
+    j[a] = v;
+  }
+}
+
+// The cuboid-averaged monomials of x-degree a in part r of 4 (the split of
+// monomials_part), or all of them for r < 0.
+__device__ inline void cuboid_monomials_part(float dx, float dy, float dz, float4 h, int q, float *out, int r) {
+  float jx[10], jy[10], jz[10];
+  cuboid_axis(dx, h.x, q, jx);
+  cuboid_axis(dy, h.y, q, jy);
+  cuboid_axis(dz, h.z, q, jz);
+  for (int a = 0; a <= q; ++a) {
+    if (r >= 0) {
+      const int m8 = a & 7;
+      if (m8 != r && m8 != 7 - r) continue;
+    }
+    float xa = 0.0F;
+#pragma unroll
+    for (int i = 0; i < 10; ++i) xa = i == a ? jx[i] : xa;
+    for (int b = 0; a + b <= q; ++b) {
+      float yb = 0.0F;
+#pragma unroll
+      for (int i = 0; i < 10; ++i) yb = i == b ? jy[i] : yb;
+      const float xy = xa * yb;
+#pragma unroll
+      for (int c = 0; c < 10; ++c)
+        if (a + b + c <= q) out[rank3(a, b, c)] = xy * jz[c];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------
 // P2M (upstream docs/math.md P2M; src/static_operators.cpp:186-220):
 //   M_alpha = (-1)^|alpha| sum_j sum_{k: alpha_k > 0} m_jk d_j^(alpha-e_k)/(alpha-e_k)!
@@ -135,7 +187,8 @@ __global__ void __launch_bounds__(128) p2m_small_kernel(const float4 *__restrict
                                                         const float4 *__restrict__ mom,
                                                         const int *__restrict__ src_off,
                                                         const int8_t *__restrict__ basis, float *__restrict__ M,
-                                                        int n, int p, int K, int leaf_node_base) {
+                                                        int n, int p, int K, int leaf_node_base,
+                                                        const float4 *__restrict__ size, int size_step) {
   __shared__ float mono[kP2mChunk * 220];
   __shared__ float4 smom[kP2mChunk * 3];
   const int nm1 = basis_size_d(p - 1);
@@ -159,7 +212,12 @@ __global__ void __launch_bounds__(128) p2m_small_kernel(const float4 *__restrict
       __syncthreads();
       for (int j = threadIdx.x; j < cn; j += blockDim.x) {
         const float4 d = src_rel[c0 + j];
-        if (nm1 > 0) monomials(d.x, d.y, d.z, p - 1, mono + j * nm1);
+        if (nm1 > 0) {
+          if (size != nullptr)
+            cuboid_monomials_part(d.x, d.y, d.z, size[(c0 + j) * size_step], p - 1, mono + j * nm1, -1);
+          else
+            monomials(d.x, d.y, d.z, p - 1, mono + j * nm1);
+        }
       }
       for (int e = threadIdx.x; e < cn * K; e += blockDim.x) smom[e] = mom[static_cast<long long>(c0) * K + e];
       __syncthreads();
@@ -181,7 +239,8 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
                                                           const float4 *__restrict__ mom,
                                                           const int *__restrict__ src_off,
                                                           const int8_t *__restrict__ basis, float *__restrict__ M,
-                                                          int n, int p, int K, int leaf_node_base, int Kb) {
+                                                          int n, int p, int K, int leaf_node_base, int Kb,
+                                                          const float4 *__restrict__ size, int size_step) {
   extern __shared__ float4 p2m_smem[];
   const int nm1 = basis_size_d(p - 1);
   const int nm1p = (nm1 + 3) & ~3;
@@ -206,7 +265,12 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
         const int r = w / cn;
         const int j = w - r * cn;
         const float4 d = src_rel[c0 + j];
-        if (nm1 > 0) monomials_part(d.x, d.y, d.z, p - 1, mono + j * nm1p, 1, r, false);
+        if (nm1 > 0) {
+          if (size != nullptr)
+            cuboid_monomials_part(d.x, d.y, d.z, size[(c0 + j) * size_step], p - 1, mono + j * nm1p, r);
+          else
+            monomials_part(d.x, d.y, d.z, p - 1, mono + j * nm1p, 1, r, false);
+        }
         if (r == 0)
           for (int q = nm1; q < nm1p; ++q) mono[j * nm1p + q] = 0.0F;
       }
@@ -934,11 +998,13 @@ size_t p2m_smem_bytes(int n, int p, int K, int chunk) {
 }
 
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
-                float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s) {
+                float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s, const float4 *size,
+                int size_step) {
   (void)chunk;
   const int leaves = 1 << (3 * depth);
   if (K < 4) {
-    p2m_small_kernel<<<leaves, 128, 0, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth));
+    p2m_small_kernel<<<leaves, 128, 0, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), size,
+                                            size_step);
     return;
   }
   // State blocks of <= 32 keep a CTA within 64 KB (several CTAs per SM hide
@@ -947,7 +1013,8 @@ void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, co
   const size_t smem = p2m_smem_bytes(n, p, Kb, 0);
   const int nm1p = (basis_size_d(p - 1) + 3) & ~3;
   const int threads = (nm1p / 4) * ((Kb + 3) / 4) <= 128 ? 128 : kP2mThreads;
-  p2m_kernel<<<leaves, threads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb);
+  p2m_kernel<<<leaves, threads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb, size,
+                                           size_step);
 }
 
 static size_t pair_smem(int n, int n_pairs) {

@@ -25,8 +25,12 @@ inline int moment_row(int K) { return moments_paired(K) ? (K + 1) & ~1 : K; }
 void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, int K,
                            double scale, float4 *mom, cudaStream_t s, bool paired, int k0 = 0, int k_total = -1);
 size_t p2m_smem_bytes(int n, int p, int K, int chunk);
+// size != nullptr: uniformly magnetised cuboid sources, the monomials
+// averaged over each source's cuboid (normalised side lengths, size[j] per
+// source when size_step is 1, size[0] for all when 0).
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
-                float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s);
+                float *M, int n, int p, int K, int depth, int chunk, cudaStream_t s,
+                const float4 *size = nullptr, int size_step = 0);
 void launch_m2m(float *M, const int *pair_off, const int *pairs, const float *coef, int n, int K,
                 int parent_level, int n_pairs, cudaStream_t s);
 void launch_l2l(float *L, const int *pair_off, const int *pairs, const float *coef, int n, int K,
@@ -94,12 +98,33 @@ struct CorunLaunch {
 // index) and r from the FP64 positions; a correction pass after every
 // near-field launch swaps each pair's field at the FP32 r for its field at
 // the exact r.  targets: (sorted target, first pair, pairs, 0).
+// Cuboid sources: the near field applies per-pair moment-to-field tensors
+// of the plan (FP32, computed once in FP64 by launch_cuboid_tensors) over
+// its own work units; T of unit u, neighbourhood source g (flattened in
+// build_neighbours order), component c (xx, xy, xz, yy, yz, zz) and target
+// t of the unit is at T[base[u] + (g * 6 + c) * targets(u) + t].
+struct CuboidNear {
+  const float *T = nullptr;
+  const long long *base = nullptr;
+  const int4 *work = nullptr;
+  int n_work = 0;
+};
 struct CloseGeometry {
   const int4 *targets;
   int n_targets;
   const float4 *r_fp32;
   const float4 *r_exact;
+  CuboidNear cuboid; // T == nullptr: point-dipole sources
 };
+// Pair tensors of cuboid sources (see CuboidNear) from the Morton-sorted FP64
+// positions (r = (x_t - x_s) * inv_scale) and the root-normalised FP64 side
+// lengths (size[3 j + c], j = 0 for one common size when size_step is 0).
+void launch_cuboid_tensors(const int4 *work, int n_work, const long long *base, const int *src_off, int depth,
+                           const double *src_pos, const double *tgt_pos, double inv_scale, const double *size,
+                           int size_step, float *T, cudaStream_t s);
+// Near-field work of a cuboid-source plan per unit: neighbourhood sources of
+// each unit (the tensor storage needed is 6 floats per (source, target)).
+std::vector<long long> cuboid_unit_sources(const int *src_off, const std::vector<int4> &work, int depth);
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
                 const int2 *leaf_self, const CloseGeometry &cg, int depth, int K,

@@ -98,6 +98,13 @@ cudaError_t cdfmm_b200_collect_status(cdfmm_b200_plan *plan, cudaStream_t s, uns
 // cdfmm_b200_poll_status.
 std::string cdfmm_b200_own_status(cdfmm_b200_plan *plan, unsigned long long call);
 
+// Near-field geometry of a plan as launch_p2p takes it: the close pairs and,
+// for cuboid sources, the pair tensors.
+namespace cdfmm_b200 {
+struct CloseGeometry;
+}
+cdfmm_b200::CloseGeometry cdfmm_b200_near_geometry(const cdfmm_b200_plan *plan);
+
 // Batch building blocks: a one-state evaluation (device arrays, already
 // validated by a plain evaluate of the same arguments) split around its M2L,
 // which the batch runs for several plans of one depth and order at once
@@ -236,6 +243,19 @@ struct cdfmm_b200_plan {
   void *stage_out = nullptr;   // device results before D2H
   size_t stage_out_bytes = 0;
 
+  // Uniformly magnetised cuboid sources (cdfmm_b200_set_source_cuboids):
+  // root-normalised side lengths (FP32 for the P2M, FP64 for the pair
+  // tensors; one entry for all sources when size_step is 0, else one per
+  // sorted source), whether the P2M averages over them, and the near-field
+  // pair tensors of the work units p2p_work (see CuboidNear).
+  bool cuboid = false;
+  bool cuboid_p2m = false;
+  int size_step = 0;
+  float4 *src_size = nullptr;
+  double *src_size64 = nullptr;
+  float *cuboid_T = nullptr;
+  long long *cuboid_base = nullptr;
+  uint64_t cuboid_T_bytes = 0;
   // Morton-sorted FP64 positions (device, [n][3]): the exact geometry of the
   // close pairs and the input of the transposed plan; host copy of the leaf
   // ranges

@@ -1057,11 +1057,254 @@ void launch_close_correction(const float4 *mom, const CloseGeometry &cg, const i
 
 } // namespace
 
+// ---------------------------------------------------------------------------
+// Uniformly magnetised cuboid sources (upstream SourceGeometry::UniformCuboid:
+// src/cuboid.cpp:150-180 for the tensor, src/static_operators.cpp:405-470 for
+// the near-field pairs).  A source j is a cuboid of side lengths h centred at
+// x_j carrying the total moment m_j (magnetisation m_j / V).  Its field at a
+// point r = x - x_j is H = T(r) m_j with T the cuboid's moment-to-field
+// tensor, from the magnetic surface charges of the faces (the classical
+// closed form of the prism's demagnetising tensor):
+//   T_xx = 1/(4 pi V) sum_corners s atan(Y Z / (X R))
+//   T_xy = -1/(4 pi V) sum_corners s asinh(Z / hypot(X, Y))   (xz: Y / hypot(X, Z), yz: X / hypot(Y, Z))
+// over the corners (X, Y, Z) = r - (sx hx, sy hy, sz hz) / 2, sx, sy, sz = +-1,
+// s = sx sy sz, R = |(X, Y, Z)|, with the limiting values 0 (0/0) and
+// +-pi/2 (X = 0) the reference uses on faces and edges.  Self pairs are
+// included (a cube's own field at its centre is -m / (3 V)); the potential
+// is the point dipole's, (m.r) / (4 pi |r|^3), and 0 at r = 0, as upstream.
+// The tensors are computed once per plan in FP64 and stored in FP32 (the
+// reference's FP32 static plan stores the same), then applied by an FP32
+// kernel in every evaluation.
+namespace {
+
+__device__ inline double atan_limit(double num, double den) {
+  if (den != 0.0) return atan(num / den);
+  if (num == 0.0) return 0.0;
+  return copysign(1.5707963267948966, num);
+}
+
+__device__ inline double asinh_limit(double num, double a, double b) {
+  const double d = hypot(a, b);
+  return d == 0.0 ? 0.0 : asinh(num / d);
+}
+
+// Tensor (xx, xy, xz, yy, yz, zz) at r of a cuboid with half sides (a, b, c),
+// times 4 pi V.
+__device__ void cuboid_tensor_4piV(double x, double y, double z, double a, double b, double c, double (&t)[6]) {
+  for (int q = 0; q < 6; ++q) t[q] = 0.0;
+  for (int corner = 0; corner < 8; ++corner) {
+    const double sx = (corner & 1) ? 1.0 : -1.0, sy = (corner & 2) ? 1.0 : -1.0, sz = (corner & 4) ? 1.0 : -1.0;
+    const double X = x - sx * a, Y = y - sy * b, Z = z - sz * c;
+    const double s = sx * sy * sz;
+    const double R = sqrt(X * X + Y * Y + Z * Z);
+    t[0] += s * atan_limit(Y * Z, X * R);
+    t[3] += s * atan_limit(X * Z, Y * R);
+    t[5] += s * atan_limit(X * Y, Z * R);
+    t[1] -= s * asinh_limit(Z, X, Y);
+    t[2] -= s * asinh_limit(Y, X, Z);
+    t[4] -= s * asinh_limit(X, Y, Z);
+  }
+}
+
+// One CTA per work unit, one thread per target: walks the unit's flattened
+// neighbourhood and writes each pair's tensor.
+__global__ void __launch_bounds__(128) cuboid_tensor_kernel(const int4 *__restrict__ work,
+                                                            const long long *__restrict__ base,
+                                                            const int *__restrict__ src_off, int depth,
+                                                            const double *__restrict__ src_pos,
+                                                            const double *__restrict__ tgt_pos, double inv_scale,
+                                                            const double *__restrict__ size, int size_step,
+                                                            float *__restrict__ T) {
+  __shared__ Neighbours nb;
+  const int4 unit = work[blockIdx.x];
+  if (threadIdx.x < 32) build_neighbours(nb, unit.x, depth, src_off, threadIdx.x);
+  __syncthreads();
+  const int t = threadIdx.x;
+  if (t >= unit.z) return;
+  const int i = unit.y + t;
+  const double xt = tgt_pos[3LL * i], yt = tgt_pos[3LL * i + 1], zt = tgt_pos[3LL * i + 2];
+  const int total = nb.prefix[nb.count];
+  float *out = T + base[blockIdx.x];
+  int b = 0;
+  for (int g = 0; g < total; ++g) {
+    while (b + 1 < nb.count && nb.prefix[b + 1] <= g) ++b;
+    const int j = nb.begin[b] + (g - nb.prefix[b]);
+    const double *h = size + 3LL * j * size_step;
+    const double rx = (xt - src_pos[3LL * j]) * inv_scale, ry = (yt - src_pos[3LL * j + 1]) * inv_scale,
+                 rz = (zt - src_pos[3LL * j + 2]) * inv_scale;
+    double v[6];
+    cuboid_tensor_4piV(rx, ry, rz, 0.5 * h[0], 0.5 * h[1], 0.5 * h[2], v);
+    const double f = 1.0 / (4.0 * 3.14159265358979323846 * h[0] * h[1] * h[2]);
+    for (int q = 0; q < 6; ++q) out[(static_cast<long long>(g) * 6 + q) * unit.z + t] = static_cast<float>(v[q] * f);
+  }
+}
+
+constexpr int kCuboidChunk = 128; // staged sources per pass
+
+// Near field of cuboid sources: one CTA per work unit, one thread per target,
+// states in blocks of KC (sources staged in chunks; each pair's tensor is
+// read once per state block).  Output as the point kernels write it (see
+// p2p_close_correction_kernel for `accumulate`).
+template <bool PHI, bool PAIRED, int KC>
+__global__ void __launch_bounds__(128) p2p_cuboid_kernel(const float4 *__restrict__ src_rel,
+                                                         const float4 *__restrict__ mom,
+                                                         const int *__restrict__ src_off,
+                                                         const float4 *__restrict__ tgt_rel,
+                                                         const int4 *__restrict__ work,
+                                                         const long long *__restrict__ base,
+                                                         const float *__restrict__ T, int depth, int K,
+                                                         float4 *__restrict__ near, int k_begin, int k_end,
+                                                         int accumulate, float acc_phi_scale) {
+  __shared__ Neighbours nb;
+  __shared__ float4 sPos[kCuboidChunk];
+  __shared__ float4 sMom[kCuboidChunk * KC];
+  const int4 unit = work[blockIdx.x];
+  if (threadIdx.x < 32) build_neighbours(nb, unit.x, depth, src_off, threadIdx.x);
+  __syncthreads();
+  const int total = nb.prefix[nb.count];
+  const int t = threadIdx.x;
+  const bool mine = t < unit.z;
+  const int i = unit.y + (mine ? t : 0);
+  const float4 tp = tgt_rel[i];
+  const float *Tu = T + base[blockIdx.x];
+  for (int k0 = k_begin; k0 < k_end; k0 += KC) {
+    float acc[KC][4];
+#pragma unroll
+    for (int kk = 0; kk < KC; ++kk) acc[kk][0] = acc[kk][1] = acc[kk][2] = acc[kk][3] = 0.0F;
+    for (int sc = 0; sc < total; sc += kCuboidChunk) {
+      const int sn = min(kCuboidChunk, total - sc);
+      __syncthreads();
+      for (int q = threadIdx.x; q < sn; q += blockDim.x) {
+        float4 pos;
+        int j;
+        stage_source(nb, sc + q, src_rel, pos, j);
+        sPos[q] = pos;
+#pragma unroll
+        for (int kk = 0; kk < KC; ++kk) {
+          const int k = k0 + kk;
+          const float3 m = k < k_end ? moment_of<PAIRED>(mom, j, K, k) : make_float3(0.0F, 0.0F, 0.0F);
+          sMom[q * KC + kk] = make_float4(m.x, m.y, m.z, 0.0F);
+        }
+      }
+      __syncthreads();
+      if (!mine) continue;
+      for (int q = 0; q < sn; ++q) {
+        const long long g6 = static_cast<long long>(sc + q) * 6 * unit.z + t;
+        const float txx = Tu[g6], txy = Tu[g6 + unit.z], txz = Tu[g6 + 2 * unit.z];
+        const float tyy = Tu[g6 + 3 * unit.z], tyz = Tu[g6 + 4 * unit.z], tzz = Tu[g6 + 5 * unit.z];
+        float rx = 0.0F, ry = 0.0F, rz = 0.0F, v = 0.0F;
+        if (PHI) {
+          const float4 p = sPos[q];
+          rx = tp.x - p.x;
+          ry = tp.y - p.y;
+          rz = tp.z - p.z;
+          const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+          const float rinv = r2 > 0.0F ? rsqrtf(r2) : 0.0F;
+          v = rinv * rinv * rinv * kInvFourPiF;
+        }
+#pragma unroll
+        for (int kk = 0; kk < KC; ++kk) {
+          const float4 m = sMom[q * KC + kk];
+          if (PHI) acc[kk][0] = fmaf(fmaf(m.x, rx, fmaf(m.y, ry, m.z * rz)), v, acc[kk][0]);
+          acc[kk][1] = fmaf(txx, m.x, fmaf(txy, m.y, fmaf(txz, m.z, acc[kk][1])));
+          acc[kk][2] = fmaf(txy, m.x, fmaf(tyy, m.y, fmaf(tyz, m.z, acc[kk][2])));
+          acc[kk][3] = fmaf(txz, m.x, fmaf(tyz, m.y, fmaf(tzz, m.z, acc[kk][3])));
+        }
+      }
+    }
+    if (mine) {
+#pragma unroll
+      for (int kk = 0; kk < KC; ++kk) {
+        const int k = k0 + kk;
+        if (k >= k_end) continue;
+        float4 &o = near[static_cast<long long>(i) * K + k];
+        if (accumulate != 0) {
+          float4 w = o;
+          if (PHI) w.x = fmaf(acc[kk][0], acc_phi_scale, w.x);
+          if (accumulate == 1) {
+            w.y += acc[kk][1];
+            w.z += acc[kk][2];
+            w.w += acc[kk][3];
+          }
+          o = w;
+        } else {
+          o = make_float4(PHI ? acc[kk][0] : 0.0F, acc[kk][1], acc[kk][2], acc[kk][3]);
+        }
+      }
+    }
+  }
+}
+
+template <bool PHI, bool PAIRED>
+void launch_cuboid_kb(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
+                      const CuboidNear &c, int depth, int K, float4 *near, int kb, int ke, int accumulate,
+                      float phi_scale, cudaStream_t s) {
+  if (ke - kb >= 8)
+    p2p_cuboid_kernel<PHI, PAIRED, 8><<<c.n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, c.work, c.base, c.T,
+                                                              depth, K, near, kb, ke, accumulate, phi_scale);
+  else if (ke - kb >= 4)
+    p2p_cuboid_kernel<PHI, PAIRED, 4><<<c.n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, c.work, c.base, c.T,
+                                                              depth, K, near, kb, ke, accumulate, phi_scale);
+  else
+    p2p_cuboid_kernel<PHI, PAIRED, 1><<<c.n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, c.work, c.base, c.T,
+                                                              depth, K, near, kb, ke, accumulate, phi_scale);
+}
+
+} // namespace
+
+void launch_cuboid_tensors(const int4 *work, int n_work, const long long *base, const int *src_off, int depth,
+                           const double *src_pos, const double *tgt_pos, double inv_scale, const double *size,
+                           int size_step, float *T, cudaStream_t s) {
+  if (n_work == 0) return;
+  cuboid_tensor_kernel<<<n_work, 128, 0, s>>>(work, base, src_off, depth, src_pos, tgt_pos, inv_scale, size,
+                                              size_step, T);
+}
+
+std::vector<long long> cuboid_unit_sources(const int *src_off, const std::vector<int4> &work, int depth) {
+  std::vector<long long> out(work.size(), 0);
+  const int side = 1 << depth;
+  for (size_t u = 0; u < work.size(); ++u) {
+    int ix, iy, iz;
+    demorton3(static_cast<uint32_t>(work[u].x), ix, iy, iz);
+    long long n = 0;
+    for (int dz = -1; dz <= 1; ++dz)
+      for (int dy = -1; dy <= 1; ++dy)
+        for (int dx = -1; dx <= 1; ++dx) {
+          const int x = ix + dx, y = iy + dy, z = iz + dz;
+          if (x < 0 || y < 0 || z < 0 || x >= side || y >= side || z >= side) continue;
+          const uint32_t m = morton3(x, y, z);
+          n += src_off[m + 1] - src_off[m];
+        }
+    out[u] = n;
+  }
+  return out;
+}
+
 void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
                 const int2 *leaf_self, const CloseGeometry &cg, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end, int accumulate,
                 float phi_scale, const CorunLaunch *corun) {
+  if (cg.cuboid.T != nullptr) {
+    const int kb = k_begin, ke = k_end < 0 ? K : k_end;
+    if (cg.cuboid.n_work == 0 || ke <= kb) return;
+    if (K >= 4) {
+      if (want_phi)
+        launch_cuboid_kb<true, true>(src_rel, mom, src_off, tgt_rel, cg.cuboid, depth, K, near, kb, ke, accumulate,
+                                     phi_scale, s);
+      else
+        launch_cuboid_kb<false, true>(src_rel, mom, src_off, tgt_rel, cg.cuboid, depth, K, near, kb, ke, accumulate,
+                                      phi_scale, s);
+    } else {
+      if (want_phi)
+        launch_cuboid_kb<true, false>(src_rel, mom, src_off, tgt_rel, cg.cuboid, depth, K, near, kb, ke, accumulate,
+                                      phi_scale, s);
+      else
+        launch_cuboid_kb<false, false>(src_rel, mom, src_off, tgt_rel, cg.cuboid, depth, K, near, kb, ke,
+                                       accumulate, phi_scale, s);
+    }
+    return;
+  }
   if (n_work == 0) return;
   if (K == 1) {
     if (want_phi)

@@ -177,11 +177,12 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   cudaStreamWaitEvent(plan->near_stream, plan->ev_fork, 0);
   launch_p2p(plan->src_rel, mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
              plan->has_self ? plan->self_idx : nullptr, plan->leaf_self,
-             CloseGeometry{plan->close_targets, plan->n_close_targets, plan->close_r_fp32, plan->close_r_exact},
+             cdfmm_b200_near_geometry(plan),
              plan->depth, K, want_phi, near,
              plan->near_stream);
   cudaEventRecord(plan->ev_join, plan->near_stream);
-  launch_p2m(plan->src_rel, mom, plan->src_off, plan->basis, M, n, plan->p, K, plan->depth, plan->p2m_chunk, s);
+  launch_p2m(plan->src_rel, mom, plan->src_off, plan->basis, M, n, plan->p, K, plan->depth, plan->p2m_chunk, s,
+             plan->cuboid_p2m ? plan->src_size : nullptr, plan->size_step);
   for (int level = plan->depth - 1; level >= 0; --level)
     launch_m2m(M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level, static_cast<int>(plan->ops.m2m_pair_g.size()), s);
   if (use_tc) {

@@ -107,7 +107,8 @@ void free_plan(cdfmm_b200_plan *p) {
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
                   p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
-                  p->close_targets, p->close_r_fp32, p->close_r_exact, p->src_pos64, p->tgt_pos64};
+                  p->close_targets, p->close_r_fp32, p->close_r_exact, p->src_pos64, p->tgt_pos64,
+                  p->src_size, p->src_size64, p->cuboid_T, p->cuboid_base};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
   if (p->p2p_work_wide != nullptr && p->p2p_work_wide != p->p2p_work) cudaFree(p->p2p_work_wide);
@@ -878,6 +879,83 @@ void cdfmm_b200_plan_destroy(cdfmm_b200_plan *plan) {
   free_plan(plan);
 }
 
+int cdfmm_b200_set_source_cuboids(cdfmm_b200_plan *plan, const double *sizes, int32_t count, int32_t cuboid_p2m) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  try {
+    require(count == 0 || count == 1 || count == plan->ns, "cuboid sizes must contain one or one per source");
+    require(count == 0 || sizes != nullptr, "sizes must not be NULL");
+    for (int64_t i = 0; i < 3 * static_cast<int64_t>(count); ++i)
+      require(std::isfinite(sizes[i]) && sizes[i] > 0.0, "source cuboid dimensions must be positive");
+    check(cudaSetDevice(plan->device), "cudaSetDevice");
+    check(cudaDeviceSynchronize(), "sync");
+    uint64_t &bytes = plan->stats.persistent_device_bytes;
+    for (void *q : {static_cast<void *>(plan->src_size), static_cast<void *>(plan->src_size64),
+                    static_cast<void *>(plan->cuboid_T), static_cast<void *>(plan->cuboid_base)})
+      if (q != nullptr) cudaFree(q);
+    plan->src_size = nullptr;
+    plan->src_size64 = nullptr;
+    plan->cuboid_T = nullptr;
+    plan->cuboid_base = nullptr;
+    bytes -= std::min(bytes, plan->cuboid_T_bytes);
+    plan->cuboid_T_bytes = 0;
+    plan->cuboid = false;
+    plan->cuboid_p2m = false;
+    if (count == 0) return CDFMM_B200_OK;
+
+    // side lengths in sorted order, normalised by the root width
+    const int m = count == 1 ? 1 : plan->ns;
+    std::vector<int> perm(static_cast<size_t>(plan->ns));
+    if (count > 1 && plan->ns > 0)
+      check(cudaMemcpy(perm.data(), plan->src_perm, sizeof(int) * perm.size(), cudaMemcpyDeviceToHost), "D2H");
+    const double inv = 1.0 / plan->scale;
+    std::vector<double> h64(3 * static_cast<size_t>(m));
+    std::vector<float4> h32(static_cast<size_t>(m));
+    for (int j = 0; j < m; ++j) {
+      const size_t u = count == 1 ? 0 : static_cast<size_t>(perm[static_cast<size_t>(j)]);
+      for (int c = 0; c < 3; ++c) h64[3 * static_cast<size_t>(j) + c] = sizes[3 * u + c] * inv;
+      h32[static_cast<size_t>(j)] = make_float4(static_cast<float>(h64[3 * j]), static_cast<float>(h64[3 * j + 1]),
+                                                static_cast<float>(h64[3 * j + 2]), 0.0F);
+    }
+    // pair tensors of the near-field work units
+    std::vector<int4> work(static_cast<size_t>(plan->n_p2p_work));
+    if (!work.empty())
+      check(cudaMemcpy(work.data(), plan->p2p_work, sizeof(int4) * work.size(), cudaMemcpyDeviceToHost), "D2H");
+    const std::vector<long long> sources = cuboid_unit_sources(plan->h_src_off.data(), work, plan->depth);
+    std::vector<long long> base(work.size() + 1, 0);
+    for (size_t u = 0; u < work.size(); ++u) base[u + 1] = base[u] + 6 * sources[u] * work[u].z;
+    const uint64_t tensor_bytes = sizeof(float) * static_cast<uint64_t>(base.back());
+    size_t free_b = 0, total_b = 0;
+    check(cudaMemGetInfo(&free_b, &total_b), "cudaMemGetInfo");
+    if (tensor_bytes > free_b / 10 * 9)
+      throw AbiError(CDFMM_B200_ERR_OUT_OF_MEMORY,
+                     "the cuboid near-field pair tensors need " + std::to_string(tensor_bytes >> 20) + " MiB (" +
+                         std::to_string(free_b >> 20) + " MiB free)");
+    uint64_t added = 0;
+    plan->src_size = dalloc<float4>(h32.size(), added);
+    plan->src_size64 = dalloc<double>(h64.size(), added);
+    plan->cuboid_base = dalloc<long long>(base.size(), added);
+    plan->cuboid_T = dalloc<float>(static_cast<size_t>(base.back()), added);
+    upload(plan->src_size, h32.data(), h32.size(), plan->stats.setup_h2d_bytes);
+    upload(plan->src_size64, h64.data(), h64.size(), plan->stats.setup_h2d_bytes);
+    upload(plan->cuboid_base, base.data(), base.size(), plan->stats.setup_h2d_bytes);
+    launch_cuboid_tensors(plan->p2p_work, plan->n_p2p_work, plan->cuboid_base, plan->src_off, plan->depth,
+                          plan->src_pos64, plan->tgt_pos64, inv, plan->src_size64, count == 1 ? 0 : 1,
+                          plan->cuboid_T, nullptr);
+    check(cudaGetLastError(), "cuboid tensors");
+    check(cudaDeviceSynchronize(), "cuboid tensors");
+    plan->cuboid_T_bytes = added;
+    bytes += added;
+    plan->size_step = count == 1 ? 0 : 1;
+    plan->cuboid = true;
+    plan->cuboid_p2m = cuboid_p2m != 0;
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(plan, e.code, e.what());
+  } catch (const std::bad_alloc &) {
+    return fail(plan, CDFMM_B200_ERR_OUT_OF_MEMORY, "host allocation failed");
+  }
+}
+
 int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_self) {
   if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
   try {
@@ -1015,7 +1093,7 @@ static int enqueue_upward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool tim
   const int n = plan->n;
   int launches = 0;
   launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
-             plan->p2m_chunk, s);
+             plan->p2m_chunk, s, plan->cuboid_p2m ? plan->src_size : nullptr, plan->size_step);
   ++launches;
   if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
   for (int level = plan->depth - 1; level >= 0; --level) {
@@ -1027,9 +1105,7 @@ static int enqueue_upward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool tim
   return launches;
 }
 
-static CloseGeometry close_geometry(const cdfmm_b200_plan *plan) {
-  return CloseGeometry{plan->close_targets, plan->n_close_targets, plan->close_r_fp32, plan->close_r_exact};
-}
+static CloseGeometry close_geometry(const cdfmm_b200_plan *plan) { return cdfmm_b200_near_geometry(plan); }
 
 // Whether K states take the tensor-core M2L.
 static bool m2l_on_tensor_cores(const cdfmm_b200_plan *plan, int K) {
@@ -1041,7 +1117,8 @@ static bool m2l_on_tensor_cores(const cdfmm_b200_plan *plan, int K) {
 // co-resident schedule needs the tensor-core M2L (whose CTA fits beside two
 // co-resident near-field CTAs); other evaluations run SEPARATE.
 static int resolved_schedule(const cdfmm_b200_plan *plan, int K) {
-  if (K <= 1 || !m2l_on_tensor_cores(plan, K)) return CDFMM_B200_SCHEDULE_SEPARATE;
+  // cuboid sources: their near-field kernel has no co-resident form
+  if (K <= 1 || !m2l_on_tensor_cores(plan, K) || plan->cuboid) return CDFMM_B200_SCHEDULE_SEPARATE;
   return plan->schedule == CDFMM_B200_SCHEDULE_AUTO ? CDFMM_B200_SCHEDULE_CORUN : plan->schedule;
 }
 
@@ -1613,6 +1690,7 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
     require(a->grad_moments != nullptr || a->grad_target_positions != nullptr,
             "request grad_moments and/or grad_target_positions");
     require(plan->nt == 0 || a->grad_field != nullptr, "grad_field is NULL");
+    if (plan->cuboid) throw AbiError(CDFMM_B200_ERR_LOGIC, "reverse mode supports point-dipole sources only");
     const bool want_x = a->grad_target_positions != nullptr;
     // The forward's sorted moments and leaf locals are still in the plan if
     // no evaluate ran since and that one held all K states.
@@ -2000,3 +2078,11 @@ const char *cdfmm_b200_last_error(const cdfmm_b200_plan *plan) {
 
 std::vector<int4> cdfmm_b200::tc_work_tiles(int depth, int T) { return build_tc_tiles(depth, T); }
 uint32_t cdfmm_b200::tc_tmem_columns(int m_tiles, int acc_stride) { return tmem_columns(m_tiles, acc_stride); }
+
+cdfmm_b200::CloseGeometry cdfmm_b200_near_geometry(const cdfmm_b200_plan *plan) {
+  using cdfmm_b200::CloseGeometry;
+  using cdfmm_b200::CuboidNear;
+  CloseGeometry g{plan->close_targets, plan->n_close_targets, plan->close_r_fp32, plan->close_r_exact, CuboidNear{}};
+  if (plan->cuboid) g.cuboid = CuboidNear{plan->cuboid_T, plan->cuboid_base, plan->p2p_work, plan->n_p2p_work};
+  return g;
+}

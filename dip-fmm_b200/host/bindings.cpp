@@ -238,6 +238,13 @@ PYBIND11_MODULE(cdfmm, m) {
   py::enum_<SourceGeometry>(m, "SourceGeometry")
       .value("POINT_DIPOLE", SourceGeometry::PointDipole)
       .value("UNIFORM_CUBOID", SourceGeometry::UniformCuboid);
+  py::class_<CuboidSize>(m, "CuboidSize")
+      .def(py::init([](double hx, double hy, double hz) { return CuboidSize{hx, hy, hz}; }), py::arg("hx"),
+           py::arg("hy"), py::arg("hz"))
+      .def_readwrite("hx", &CuboidSize::hx)
+      .def_readwrite("hy", &CuboidSize::hy)
+      .def_readwrite("hz", &CuboidSize::hz)
+      .def_property_readonly("volume", [](const CuboidSize &h) { return h.hx * h.hy * h.hz; });
   py::enum_<StaticPrecision>(m, "StaticPrecision")
       .value("FLOAT32", StaticPrecision::Float32)
       .value("FLOAT64", StaticPrecision::Float64);
@@ -319,6 +326,7 @@ PYBIND11_MODULE(cdfmm, m) {
       .def_readwrite("static_matrix_backend", &UniformFmmOptions::static_matrix_backend)
       .def_readwrite("backend", &UniformFmmOptions::backend)
       .def_readwrite("source_geometry", &UniformFmmOptions::source_geometry)
+      .def_readwrite("source_sizes", &UniformFmmOptions::source_sizes)
       .def_readwrite("use_cuboid_p2m", &UniformFmmOptions::use_cuboid_p2m)
       .def_readwrite("fixed_target_source_indices", &UniformFmmOptions::fixed_target_source_indices)
       .def_readwrite("cuda_p2p_bsr_max_bytes", &UniformFmmOptions::cuda_p2p_bsr_max_bytes)

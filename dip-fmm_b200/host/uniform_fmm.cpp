@@ -104,11 +104,14 @@ void UniformFmm::construct(const UniformFmmOptions &options) {
   if (options.precision != StaticPrecision::Float32) {
     throw std::invalid_argument("the B200 backend evaluates FP32 plans; set precision to Float32");
   }
-  if (options.source_geometry != SourceGeometry::PointDipole) {
-    throw std::invalid_argument("the B200 backend evaluates point-dipole sources only");
-  }
-  if (!options.source_sizes.empty()) {
+  // Source geometry (upstream src/uniform_fmm.cpp:296-328).
+  cuboid_sources_ = options.source_geometry == SourceGeometry::UniformCuboid;
+  if (!cuboid_sources_ && !options.source_sizes.empty()) {
     throw std::invalid_argument("point-dipole sources do not accept cuboid sizes");
+  }
+  if (cuboid_sources_ && options.source_sizes.size() != 1 &&
+      options.source_sizes.size() != tree_.sorted_source_positions().size()) {
+    throw std::invalid_argument("cuboid sizes must contain one or one per source");
   }
   if (options.max_states < 1) {
     throw std::invalid_argument("UniformFmmOptions.max_states must be >= 1");
@@ -128,7 +131,8 @@ void UniformFmm::construct(const UniformFmmOptions &options) {
         throw std::invalid_argument("fixed_target_source_indices contains an invalid source index");
       }
     }
-    fixed_identities_ = ids;
+    // finite cuboid self fields are physical: the map is checked, not kept
+    if (!cuboid_sources_) fixed_identities_ = ids;
   }
   m2l_mode_ = options.b200_m2l;
   max_states_ = options.max_states;
@@ -173,6 +177,18 @@ void UniformFmm::construct(const UniformFmmOptions &options) {
   const int status = cdfmm_b200_plan_create(&d, &raw);
   if (status != CDFMM_B200_OK) throw_status(status, cdfmm_b200_last_error(nullptr));
   plan_.reset(raw);
+  if (cuboid_sources_) {
+    std::vector<double> sizes;
+    sizes.reserve(3 * options.source_sizes.size());
+    for (const CuboidSize &h : options.source_sizes) {
+      sizes.push_back(h.hx);
+      sizes.push_back(h.hy);
+      sizes.push_back(h.hz);
+    }
+    check_plan(cdfmm_b200_set_source_cuboids(plan_.get(), sizes.data(), static_cast<int32_t>(options.source_sizes.size()),
+                                             options.use_cuboid_p2m ? 1 : 0),
+               plan_.get());
+  }
 
   if (fixed_identities_.has_value()) {
     bind_identities(fixed_identities_.value(), ns);
@@ -201,6 +217,11 @@ void UniformFmm::construct(const UniformFmmOptions &options) {
 // :1290-1305) and uploads its sorted form when it differs from the bound one
 // (src/uniform_fmm.cpp:1028-1043 builds the same sorted map).
 void UniformFmm::bind_identities(std::span<const int> ids, std::size_t moment_count) {
+  // cuboid sources: identities are not applied (upstream resolve_self_indices)
+  if (cuboid_sources_) {
+    identities_bound_ = true;
+    return;
+  }
   const std::size_t nt = tree_.sorted_target_positions().size();
   if (fixed_identities_.has_value()) {
     const std::vector<int> &fixed = fixed_identities_.value();

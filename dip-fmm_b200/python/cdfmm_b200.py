@@ -46,6 +46,7 @@ EXPORTED = (
     "cdfmm_b200_selftest_bounded_wait", "cdfmm_b200_m2l_shapes", "cdfmm_b200_set_m2l_shape",
     "cdfmm_b200_poll_status", "cdfmm_b200_set_wait_limit", "cdfmm_b200_set_schedule", "cdfmm_b200_batch_groups",
     "cdfmm_b200_plan_create_from_points", "cdfmm_b200_plan_tree", "cdfmm_b200_m2l_stencil",
+    "cdfmm_b200_set_source_cuboids",
 )
 
 ROOT_CENTRE, ROOT_HALF_WIDTH = 1, 2
@@ -148,6 +149,7 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_plan_create_from_points.argtypes = [ctypes.POINTER(PointsDesc), ctypes.POINTER(vp)]
     lib.cdfmm_b200_plan_tree.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     lib.cdfmm_b200_m2l_stencil.argtypes = [i32, vp, u64, ctypes.POINTER(i32)]
+    lib.cdfmm_b200_set_source_cuboids.argtypes = [vp, vp, i32, i32]
     lib.cdfmm_b200_plan_destroy.argtypes = [vp]
     lib.cdfmm_b200_plan_destroy.restype = None
     lib.cdfmm_b200_set_self_indices.argtypes = [vp, vp]
@@ -380,6 +382,16 @@ class DevicePlan:
             self.close()
         except Exception:
             pass
+
+    def set_source_cuboids(self, sizes, cuboid_p2m=True):
+        """Uniformly magnetised cuboid sources (cdfmm_b200_set_source_cuboids):
+        sizes (n_sources, 3) or (3,) / (1, 3) side lengths in user order;
+        None returns to point dipoles."""
+        if sizes is None:
+            _check(library().cdfmm_b200_set_source_cuboids(self._h, None, 0, 0), self._h)
+            return
+        a = np.ascontiguousarray(sizes, dtype=np.float64).reshape(-1, 3)
+        _check(library().cdfmm_b200_set_source_cuboids(self._h, _ptr(a), len(a), 1 if cuboid_p2m else 0), self._h)
 
     def set_self_indices(self, sorted_self):
         if sorted_self is None:

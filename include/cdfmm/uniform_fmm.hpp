@@ -60,8 +60,9 @@ struct StaticExecutionPlan {
   StaticOperatorExecutor p2p{StaticOperatorExecutor::Cuda};
 };
 
-/// Physical model of a source (upstream include/cdfmm/cuboid.hpp).  Only
-/// point dipoles are evaluated by this library.
+/// Physical model of a source (upstream include/cdfmm/cuboid.hpp): point
+/// dipoles, or uniformly magnetised axis-aligned cuboids (total moments;
+/// side lengths in UniformFmmOptions.source_sizes).
 enum class SourceGeometry { PointDipole, UniformCuboid };
 struct CuboidSize {
   double hx{0.0};
@@ -203,6 +204,7 @@ private:
   std::optional<std::vector<int>> fixed_identities_{};
   std::vector<int> fixed_sorted_self_{};
   bool identities_bound_{false};
+  bool cuboid_sources_{false}; // identity maps do not apply to cuboid sources
   StaticPlanStatistics static_stats_{};
   mutable CudaPlanStatistics cuda_stats_{};
   EvaluationTimings last_timings_{};

@@ -207,6 +207,22 @@ int cdfmm_b200_plan_tree(cdfmm_b200_plan *plan, double *root, int32_t *source_pe
 /* Releases every device allocation of the plan.  NULL is ignored. */
 void cdfmm_b200_plan_destroy(cdfmm_b200_plan *plan);
 
+/* Uniformly magnetised cuboid sources (upstream SourceGeometry::UniformCuboid,
+ * include/cdfmm/cuboid.hpp; UniformFmmOptions.source_sizes / use_cuboid_p2m).
+ * sizes: [count][3] side lengths (hx, hy, hz) > 0 in physical units, one per
+ * source in USER order (count == n_sources) or one for all (count == 1);
+ * count == 0 returns to point dipoles.  Moments stay total moments (m = V M).
+ * The near field then applies each pair's exact cuboid -> point
+ * moment-to-field tensor (upstream src/cuboid.cpp:150-180), computed once
+ * here in FP64 from the FP64 positions and kept in FP32 on the device
+ * (24 bytes per list-1 pair; ERR_OUT_OF_MEMORY when they do not fit); self
+ * pairs are included (the self map is not applied, as upstream) and the
+ * potential stays the point dipole's.  cuboid_p2m nonzero: the multipoles
+ * average each source's monomials over its cuboid (upstream
+ * src/static_operators.cpp:222-255), else they treat sources as points.
+ * Reverse mode is refused for cuboid sources (ERR_LOGIC). */
+int cdfmm_b200_set_source_cuboids(cdfmm_b200_plan *plan, const double *sizes, int32_t count, int32_t cuboid_p2m);
+
 /* Sets the target -> source self-exclusion map in SORTED numbering
  * ([n_targets], -1 = no self source), or clears it when NULL.  The list1 P2P
  * skips exactly that source for each target (upstream

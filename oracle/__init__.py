@@ -44,6 +44,10 @@ def library() -> ctypes.CDLL:
     lib.oracle_lists.argtypes = [i, P(i), P(i), P(i), P(i)]
     lib.oracle_direct.argtypes = [i, P(d), P(d), i, P(d), P(i), i, P(d), P(d)]
     lib.oracle_direct_grad.argtypes = [i, P(d), P(d), i, P(d), P(i), P(d), P(d)]
+    lib.oracle_cuboid_tensor.argtypes = [P(d), P(d), P(d)]
+    lib.oracle_cuboid_monomial.argtypes = [i, i, i, P(d), P(d)]
+    lib.oracle_cuboid_monomial.restype = d
+    lib.oracle_direct_cuboid.argtypes = [i, P(d), P(d), P(d), i, i, P(d), P(d), P(d)]
     lib.oracle_fmm.argtypes = [i, P(d), i, P(d), i, i, i, P(d), d, P(d), P(i), i, P(d), P(d), P(d), P(d)]
     lib.oracle_fmm.restype = i
     _LIB = lib
@@ -166,6 +170,29 @@ def fmm(sources, targets, moments, order, depth, identities=None, flags=3, root_
     if expansions:
         out["M"], out["L"] = M, L
     return out
+
+
+def cuboid_tensor(r, h) -> np.ndarray:
+    """(3, 3) [field][moment] field per unit total moment of a uniformly
+    magnetised cuboid of side lengths h at r from its centre."""
+    out = np.zeros(9)
+    library().oracle_cuboid_tensor(_dp(_f64(r)), _dp(_f64(h)), _dp(out))
+    return out.reshape(3, 3)
+
+
+def cuboid_monomial(alpha, d, h) -> float:
+    """(d + u)^alpha / alpha! averaged over u in the cuboid of side lengths h."""
+    return library().oracle_cuboid_monomial(int(alpha[0]), int(alpha[1]), int(alpha[2]), _dp(_f64(d)), _dp(_f64(h)))
+
+
+def direct_cuboid(sources, moments, sizes, targets):
+    """FP64 direct sum over cuboid sources: (phi, H) at the targets."""
+    s, m, t = _f64(sources), _f64(moments), _f64(targets)
+    h = _f64(sizes).reshape(-1, 3)
+    phi = np.zeros(len(t))
+    H = np.zeros((len(t), 3))
+    library().oracle_direct_cuboid(len(s), _dp(s), _dp(m), _dp(h), len(h), len(t), _dp(t), _dp(phi), _dp(H))
+    return phi, H
 
 
 def rel_l2(a, b) -> float:

@@ -388,6 +388,93 @@ void oracle_direct(int ns, const double *src, const double *mom, int nt, const d
   }
 }
 
+/* --------------------------------------------------------------- cuboids */
+/* Uniformly magnetised cuboid sources (src/cuboid.cpp:150-180 and
+ * docs/math.md "Finite cuboid geometry").  The field of a cuboid of side
+ * lengths h = 2 (a, b, c) centred at the origin with total moment m, at r,
+ * is T(r) m; T is the classical closed form of the prism's demagnetising
+ * tensor from the magnetic surface charges on its faces: with the corners
+ * (X, Y, Z) = r - (sx a, sy b, sz c), sx, sy, sz = +-1, s = sx sy sz,
+ * R = |(X, Y, Z)| and V = 8 a b c,
+ *   4 pi V T_xx = sum s atan(Y Z / (X R))
+ *   4 pi V T_xy = -sum s asinh(Z / sqrt(X^2 + Y^2))
+ * (the other components by permuting the axes).  On faces and edges the
+ * reference's limits are kept: atan(num / 0) = sign(num) pi / 2 (0 for
+ * 0 / 0) and asinh(num / 0) = 0.  T is written [field][moment], row-major. */
+static double atan_lim(double num, double den) {
+  if (den != 0.0) return atan(num / den);
+  if (num == 0.0) return 0.0;
+  return num > 0.0 ? 1.5707963267948966 : -1.5707963267948966;
+}
+static double asinh_lim(double num, double p, double q) {
+  const double d = sqrt(p * p + q * q);
+  return d == 0.0 ? 0.0 : asinh(num / d);
+}
+void oracle_cuboid_tensor(const double *r, const double *h, double *T) {
+  const double half[3] = {0.5 * h[0], 0.5 * h[1], 0.5 * h[2]};
+  double d[3] = {0.0, 0.0, 0.0}, o[3] = {0.0, 0.0, 0.0}; /* diagonal; xy, xz, yz */
+  for (int sx = -1; sx <= 1; sx += 2)
+    for (int sy = -1; sy <= 1; sy += 2)
+      for (int sz = -1; sz <= 1; sz += 2) {
+        const double X = r[0] - sx * half[0], Y = r[1] - sy * half[1], Z = r[2] - sz * half[2];
+        const double R = sqrt(X * X + Y * Y + Z * Z);
+        const double s = (double)(sx * sy * sz);
+        d[0] += s * atan_lim(Y * Z, X * R);
+        d[1] += s * atan_lim(X * Z, Y * R);
+        d[2] += s * atan_lim(X * Y, Z * R);
+        o[0] -= s * asinh_lim(Z, X, Y);
+        o[1] -= s * asinh_lim(Y, X, Z);
+        o[2] -= s * asinh_lim(X, Y, Z);
+      }
+  const double f = ORACLE_INV_4PI / (h[0] * h[1] * h[2]);
+  T[0] = f * d[0];
+  T[4] = f * d[1];
+  T[8] = f * d[2];
+  T[1] = T[3] = f * o[0];
+  T[2] = T[6] = f * o[1];
+  T[5] = T[7] = f * o[2];
+}
+
+/* static_operators.cpp:222-255 (cuboid P2M entries) via cuboid.cpp:251-268:
+ * the average over the cuboid (side lengths h, centred at d) of the monomial
+ * (d + u)^alpha / alpha!, a product over axes of
+ *   sum_{g even <= a} d^(a-g) / (a-g)! * (h/2)^g / (g+1)!. */
+double oracle_cuboid_monomial(int a, int b, int c, const double *d, const double *h) {
+  const int e[3] = {a, b, c};
+  double v = 1.0;
+  for (int axis = 0; axis < 3; ++axis) {
+    double sum = 0.0;
+    for (int g = 0; g <= e[axis]; g += 2)
+      sum += pow(d[axis], e[axis] - g) / fact(e[axis] - g) * pow(0.5 * h[axis], g) / fact(g + 1);
+    v *= sum;
+  }
+  return v;
+}
+
+/* Direct sum over cuboid sources (sizes: one per source, or one for all when
+ * n_sizes == 1): H_i = sum_j T(x_i - x_j; h_j) m_j over every pair (self
+ * pairs included); phi_i = the point dipoles' potential, pairs at r = 0
+ * contributing 0 (static_operators.cpp:447-463). */
+void oracle_direct_cuboid(int ns, const double *src, const double *mom, const double *sizes, int n_sizes, int nt,
+                          const double *tgt, double *phi, double *H) {
+#pragma omp parallel for schedule(dynamic, 64)
+  for (int i = 0; i < nt; ++i) {
+    double p = 0.0, hsum[3] = {0.0, 0.0, 0.0};
+    for (int j = 0; j < ns; ++j) {
+      const double r[3] = {tgt[3 * i] - src[3 * j], tgt[3 * i + 1] - src[3 * j + 1], tgt[3 * i + 2] - src[3 * j + 2]};
+      const double *m = mom + 3 * j;
+      double T[9];
+      oracle_cuboid_tensor(r, sizes + 3 * (n_sizes == 1 ? 0 : j), T);
+      for (int a = 0; a < 3; ++a) hsum[a] += T[3 * a] * m[0] + T[3 * a + 1] * m[1] + T[3 * a + 2] * m[2];
+      const double r2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+      if (r2 > 0.0) p += ORACLE_INV_4PI * (m[0] * r[0] + m[1] * r[1] + m[2] * r[2]) / (r2 * sqrt(r2));
+    }
+    if (phi != NULL) phi[i] = p;
+    if (H != NULL)
+      for (int a = 0; a < 3; ++a) H[3 * i + a] = hsum[a];
+  }
+}
+
 /* Position gradient of L = sum_i w_i . H_i (direct sum, FP64) with respect
  * to the target positions.  The reference has no reverse mode; this is the
  * analytic derivative of the pair field of pair_add:
