@@ -139,7 +139,9 @@ cudaError_t upload_tiles(StackGroup &g, int depth) {
   if (g.tiles) cudaFree(g.tiles);
   g.tiles = nullptr;
   cudaError_t e = cudaMalloc(reinterpret_cast<void **>(&g.tiles), t.size() * sizeof(int4));
+  // (a pageable copy may return before its DMA lands: wait for it)
   if (e == cudaSuccess) e = cudaMemcpy(g.tiles, t.data(), t.size() * sizeof(int4), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy);
   g.n_tiles = static_cast<int>(t.size());
   return e;
 }
@@ -164,6 +166,7 @@ cudaError_t prepare_group(cdfmm_b200_batch *b, StackGroup &g) {
   if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void **>(&g.L_list), K * sizeof(float *));
   if (e == cudaSuccess) e = cudaMemcpy(g.M_list, M.data(), K * sizeof(float *), cudaMemcpyHostToDevice);
   if (e == cudaSuccess) e = cudaMemcpy(g.L_list, L.data(), K * sizeof(float *), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(cudaStreamLegacy); // the copies have landed
   if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&g.stream, cudaStreamNonBlocking);
   if (e == cudaSuccess) e = cudaEventCreateWithFlags(&g.done, cudaEventDisableTiming);
   g.up.assign(static_cast<size_t>(K), nullptr);

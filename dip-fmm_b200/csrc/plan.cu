@@ -59,9 +59,20 @@ template <typename T> T *dalloc(size_t count, uint64_t &bytes) {
   return static_cast<T *>(p);
 }
 
+// Host -> device copy that has landed when it returns.  cudaMemcpy from
+// pageable host memory may return once the data is in the driver's staging
+// buffer, before the DMA into device memory is done; it is ordered only on
+// the legacy default stream, and the evaluator's kernels run on non-blocking
+// streams that do not wait for that stream.
+void copy_to_device(void *dst, const void *src, size_t bytes, const char *what) {
+  if (bytes == 0) return;
+  check(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), what);
+  check(cudaStreamSynchronize(cudaStreamLegacy), what);
+}
+
 template <typename T> void upload(T *dst, const T *src, size_t count, uint64_t &bytes) {
   if (count == 0) return;
-  check(cudaMemcpy(dst, src, count * sizeof(T), cudaMemcpyHostToDevice), "cudaMemcpy H2D");
+  copy_to_device(dst, src, count * sizeof(T), "cudaMemcpy H2D");
   bytes += count * sizeof(T);
 }
 
@@ -649,6 +660,9 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
     }
   }
   ops.m2l_T64.reset();
+  // every set-up copy, memset and kernel (legacy default stream) is complete
+  // before the plan's non-blocking streams can read what they wrote
+  check(cudaDeviceSynchronize(), "plan set-up");
   lap(plan->stats.setup_ms_m2l);
   plan->m2l_mode = m2l_mode;
   plan->stats.m2l_mode_resolved = plan->tc_supported ? (m2l_mode == CDFMM_B200_M2L_FP32 ? CDFMM_B200_M2L_FP32 : CDFMM_B200_M2L_BF16X3)
@@ -970,7 +984,7 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
       require(sorted_self[i] >= -1 && sorted_self[i] < plan->ns, "self index out of range");
     check(cudaDeviceSynchronize(), "sync");
     if (plan->nt > 0)
-      check(cudaMemcpy(plan->self_idx, sorted_self, sizeof(int) * plan->nt, cudaMemcpyHostToDevice), "cudaMemcpy");
+      copy_to_device(plan->self_idx, sorted_self, sizeof(int) * plan->nt, "cudaMemcpy");
     {
       // per leaf: the lowest and highest self source of its targets
       std::vector<int2> range(static_cast<size_t>(plan->n_leaves), make_int2(0x7fffffff, -1));
@@ -981,8 +995,7 @@ int cdfmm_b200_set_self_indices(cdfmm_b200_plan *plan, const int32_t *sorted_sel
             r.x = std::min(r.x, sorted_self[i]);
             r.y = std::max(r.y, sorted_self[i]);
           }
-      check(cudaMemcpy(plan->leaf_self, range.data(), sizeof(int2) * range.size(), cudaMemcpyHostToDevice),
-            "cudaMemcpy");
+      copy_to_device(plan->leaf_self, range.data(), sizeof(int2) * range.size(), "cudaMemcpy");
     }
     plan->h_self.assign(sorted_self, sorted_self + plan->nt);
     plan->has_self = true;
@@ -1009,7 +1022,7 @@ static std::vector<int4> build_tc_tiles(int depth, int T) {
 static void upload_tc_tiles(cdfmm_b200_plan *plan, int Kp) {
   const std::vector<int4> tiles = build_tc_tiles(plan->depth, plan->tc_m_tiles * (128 / Kp));
   grow(plan->tc_tiles, plan->tc_tiles_capacity, tiles.size(), "cudaMalloc tiles");
-  check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
+  copy_to_device(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), "tiles");
   plan->tc_tiles_Kp = Kp;
   plan->tc_n_tiles = static_cast<int>(tiles.size());
 }
@@ -1058,7 +1071,7 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s, size_t sme
     const int mt = plan->tc_candidates[c].m_tiles;
     const std::vector<int4> tiles = build_tc_tiles(plan->depth, mt * (128 / Kp));
     grow(plan->tc_tiles, plan->tc_tiles_capacity, tiles.size(), "cudaMalloc tiles");
-    check(cudaMemcpy(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice), "tiles");
+    copy_to_device(plan->tc_tiles, tiles.data(), tiles.size() * sizeof(int4), "tiles");
     ta.tiles = plan->tc_tiles;
     ta.m_tiles = mt;
     ta.stages = plan->tc_candidates[c].stages;

@@ -164,7 +164,7 @@ def test_cuboid_states_batched_like_single_calls(K):
     rng = np.random.default_rng(K)
     m = rng.normal(size=(K, len(c["sources"]), 3)) * 1e-3
     f = cuboid_fmm(c, max_states=K)
-    r = f.evaluate(m, output="both")
+    r = f.evaluate_states(m.astype(np.float32), output="both")
     g = cuboid_fmm(c)
     for k in (0, K - 1):
         s = g.evaluate(m[k], output="both")
@@ -186,7 +186,7 @@ def test_cuboid_plan_api():
     with pytest.raises(ValueError, match="dimensions must be positive"):
         plan.set_source_cuboids([0.1, 0.0, 0.1])
     with pytest.raises(cdfmm_b200.CdfmmError, match="point-dipole sources only"):
-        plan.backward(np.ones((1, len(x), 3), np.float32), m.astype(np.float32), grad_moments=True)
+        plan.backward(np.ones((1, len(x), 3), np.float32), m.astype(np.float32))
     plan.set_source_cuboids(None)
     again = plan.evaluate(m, output="both")
     np.testing.assert_array_equal(point["H"], again["H"])
