@@ -252,7 +252,7 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
   const int s0 = src_off[leaf];
   const int s1 = src_off[leaf + 1];
   float *out = M + static_cast<long long>(leaf_node_base + leaf) * n * K;
-  for (int kblk = 0; kblk < K; kblk += Kb) {
+  for (int kblk = blockIdx.y * Kb; kblk < K; kblk += Kb * gridDim.y) {
     const int Kc = min(Kb, K - kblk);
     const int Kq = (Kc + 3) >> 2;
     const int tiles = (nm1p >> 2) * Kq;
@@ -653,7 +653,7 @@ __global__ void __launch_bounds__(kL2pThreads) l2p_kernel(const float *__restric
   const bool want_phi = (output & 1u) != 0u;
   const bool want_h = (output & 2u) != 0u;
   const float *src = L + static_cast<long long>(leaf_node_base + leaf) * n * K;
-  for (int kblk = k_begin; kblk < k_end; kblk += Kb) {
+  for (int kblk = k_begin + blockIdx.y * Kb; kblk < k_end; kblk += Kb * gridDim.y) {
     const int Kc = min(Kb, k_end - kblk);
     const int Kcp = (Kc + 3) & ~3;
     const int Kq = Kcp >> 2;
@@ -983,8 +983,20 @@ void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, 
 
 // State block of the P2M kernel for K states: the largest of 64, 32, ...
 // (<= K) whose shared memory stays within 100 KB (two CTAs per SM).
+#ifndef CDFMM_P2M_KB
+#define CDFMM_P2M_KB 32
+#endif
+#ifndef CDFMM_P2M_SPLIT
+#define CDFMM_P2M_SPLIT 0
+#endif
+#ifndef CDFMM_L2P_KB
+#define CDFMM_L2P_KB 64
+#endif
+#ifndef CDFMM_L2P_SPLIT
+#define CDFMM_L2P_SPLIT 0
+#endif
 static int p2m_state_block(int p, int K) {
-  int Kb = std::min(K, 32);
+  int Kb = std::min(K, CDFMM_P2M_KB);
   while (Kb > 4 && p2m_smem_bytes(0, p, Kb, 0) > 64 * 1024) Kb = (Kb + 1) / 2;
   return Kb;
 }
@@ -1013,8 +1025,9 @@ void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, co
   const size_t smem = p2m_smem_bytes(n, p, Kb, 0);
   const int nm1p = (basis_size_d(p - 1) + 3) & ~3;
   const int threads = (nm1p / 4) * ((Kb + 3) / 4) <= 128 ? 128 : kP2mThreads;
-  p2m_kernel<<<leaves, threads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb, size,
-                                           size_step);
+  const dim3 grid(leaves, CDFMM_P2M_SPLIT ? (K + Kb - 1) / Kb : 1);
+  p2m_kernel<<<grid, threads, smem, s>>>(src_rel, mom, src_off, basis, M, n, p, K, level_offset_d(depth), Kb, size,
+                                         size_step);
 }
 
 static size_t pair_smem(int n, int n_pairs) {
@@ -1065,10 +1078,12 @@ void launch_l2p(const float *L, const float4 *tgt_rel, const int *tgt_off, const
                                             output, layout, phi_scale, field, potential);
     return;
   }
-  int Kb = std::min(K, 64);
+  int Kb = std::min(K, CDFMM_L2P_KB);
   while (Kb > 4 && l2p_smem_bytes(n, p, Kb) > 60 * 1024) Kb = (Kb + 1) / 2;
   const size_t smem = l2p_smem_bytes(n, p, Kb);
-  l2p_kernel<<<leaves, kL2pThreads, smem, s>>>(L, tgt_rel, tgt_off, near, basis, n, p, K, level_offset_d(depth), output,
+  const dim3 grid(leaves, CDFMM_L2P_SPLIT ? (k_end - k_begin + Kb - 1) / Kb : 1);
+  if (k_end > k_begin)
+    l2p_kernel<<<grid, kL2pThreads, smem, s>>>(L, tgt_rel, tgt_off, near, basis, n, p, K, level_offset_d(depth), output,
                                                phi_scale, Kb, k_begin, k_end, k_near_end);
   if (unsort) launch_unsort(near, tgt_inv, nt, K, output, layout, field, potential, s, k_begin, k_end);
 }

@@ -467,10 +467,13 @@ __global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__r
       const int al = e / Kp;
       const int k = e - al * Kp;
       const int a = kc * kKChunk + al;
+      // padding alphas (a >= n), padding states (k >= K) and the zero box are
+      // zero; scale_m holds n entries per level (no padding)
       float m = 0.0F;
       if (box < n_boxes && a < n && k < K)
-        m = M_list != nullptr ? M_list[k][static_cast<long long>(node) * n + a] : src[static_cast<long long>(a) * K + k];
-      tile[al][k] = m * scale_m[level * n + a];
+        m = (M_list != nullptr ? M_list[k][static_cast<long long>(node) * n + a] : src[static_cast<long long>(a) * K + k]) *
+            scale_m[level * n + a];
+      tile[al][k] = m;
     }
     __syncthreads();
     const long long chunk_vec = box_vec + static_cast<long long>(kc) * Kp * kKChunk / 8;
