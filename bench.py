@@ -76,6 +76,8 @@ def parse_args():
     ap.add_argument("--no-multi", action="store_true")
     ap.add_argument("--no-lattice", action="store_true")
     ap.add_argument("--no-reference-gpu", action="store_true")
+    ap.add_argument("--nvtx", action="store_true",
+                    help="mark the timed steps with the NVTX range 'timed_steps' (for ncu --nvtx-include)")
     ap.add_argument("--corun-shape-sweep", action="store_true",
                     help="time every M2L pipeline shape under the co-resident schedule")
     ap.add_argument("--multi-problems", type=int, default=48)
@@ -368,8 +370,12 @@ def b200_arm(args):
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    if args.nvtx:
+        torch.cuda.nvtx.range_push("timed_steps")
     for _ in range(args.steps):
         step()
+    if args.nvtx:
+        torch.cuda.nvtx.range_pop()
     e1.record(stream)
     torch.cuda.synchronize()
     barrier()
