@@ -245,18 +245,30 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
   const int nm1 = basis_size_d(p - 1);
   const int nm1p = (nm1 + 3) & ~3;
   float4 *smom = p2m_smem;                                              // [chunk][Kc]
-  float *P = reinterpret_cast<float *>(smom + kP2mChunk * Kb);          // [3][nm1p][Kc]
-  float *mono = P + 3 * nm1p * Kb;                                      // [chunk][nm1p]
+  float *P = reinterpret_cast<float *>(smom + kP2mChunk * Kb);          // [3][nm1p][Kc + 2]
+  float *mono = P + 3 * nm1p * (Kb + 2);                                // [chunk][nm1p]
+  short *sidx = reinterpret_cast<short *>(mono + kP2mChunk * nm1p);     // [n][4] P rows of alpha - e_c (-1: none), sign
   const int tid = threadIdx.x;
   const int leaf = blockIdx.x;
   const int s0 = src_off[leaf];
   const int s1 = src_off[leaf + 1];
   float *out = M + static_cast<long long>(leaf_node_base + leaf) * n * K;
+  // the P rows each output coefficient combines (once per CTA)
+  for (int a = tid; a < n; a += blockDim.x) {
+    const int ax = basis[4 * a], ay = basis[4 * a + 1], az = basis[4 * a + 2];
+    sidx[4 * a] = static_cast<short>(ax > 0 ? rank3(ax - 1, ay, az) : -1);
+    sidx[4 * a + 1] = static_cast<short>(ay > 0 ? nm1p + rank3(ax, ay - 1, az) : -1);
+    sidx[4 * a + 2] = static_cast<short>(az > 0 ? 2 * nm1p + rank3(ax, ay, az - 1) : -1);
+    sidx[4 * a + 3] = static_cast<short>(((ax + ay + az) & 1) ? -1 : 1);
+  }
   for (int kblk = blockIdx.y * Kb; kblk < K; kblk += Kb * gridDim.y) {
     const int Kc = min(Kb, K - kblk);
     const int Kq = (Kc + 3) >> 2;
+    // P row stride Kc + 2: the 4 monomial quads of a warp's tile updates
+    // fall in different banks
+    const int Ps = Kc + 2;
     const int tiles = (nm1p >> 2) * Kq;
-    for (int q = tid; q < 3 * nm1p * Kc; q += blockDim.x) P[q] = 0.0F;
+    for (int q = tid; q < 3 * nm1p * Ps; q += blockDim.x) P[q] = 0.0F;
     for (int c0 = s0; c0 < s1; c0 += kP2mChunk) {
       const int cn = min(kP2mChunk, s1 - c0);
       __syncthreads();
@@ -344,7 +356,7 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
             for (int c = 0; c < 3; ++c)
 #pragma unroll
               for (int u = 0; u < 4; ++u)
-                P[(c * nm1p + mu0 + u) * Kc + k] += (u & 1) ? acc[c][u >> 1][kk].y : acc[c][u >> 1][kk].x;
+                P[(c * nm1p + mu0 + u) * Ps + k] += (u & 1) ? acc[c][u >> 1][kk].y : acc[c][u >> 1][kk].x;
           }
         }
       }
@@ -353,12 +365,12 @@ __global__ void __launch_bounds__(kP2mThreads) p2m_kernel(const float4 *__restri
     for (int q = tid; q < n * Kc; q += blockDim.x) {
       const int a = q / Kc;
       const int k = q - a * Kc;
-      const int ax = basis[4 * a], ay = basis[4 * a + 1], az = basis[4 * a + 2];
+      const short *ix = sidx + 4 * a;
       float v = 0.0F;
-      if (ax > 0) v += P[(0 * nm1p + rank3(ax - 1, ay, az)) * Kc + k];
-      if (ay > 0) v += P[(1 * nm1p + rank3(ax, ay - 1, az)) * Kc + k];
-      if (az > 0) v += P[(2 * nm1p + rank3(ax, ay, az - 1)) * Kc + k];
-      out[static_cast<long long>(a) * K + kblk + k] = ((ax + ay + az) & 1) ? -v : v;
+      if (ix[0] >= 0) v += P[ix[0] * Ps + k];
+      if (ix[1] >= 0) v += P[ix[1] * Ps + k];
+      if (ix[2] >= 0) v += P[ix[2] * Ps + k];
+      out[static_cast<long long>(a) * K + kblk + k] = ix[3] < 0 ? -v : v;
     }
     __syncthreads();
   }
@@ -1006,7 +1018,8 @@ size_t p2m_smem_bytes(int n, int p, int K, int chunk) {
   (void)chunk;
   const int nm1p = (basis_size_d(p - 1) + 3) & ~3;
   const size_t Kb = static_cast<size_t>(std::min(K, 32));
-  return sizeof(float4) * kP2mChunk * Kb + sizeof(float) * (3 * nm1p * Kb + static_cast<size_t>(kP2mChunk) * nm1p);
+  return sizeof(float4) * kP2mChunk * Kb + sizeof(float) * (3 * nm1p * (Kb + 2) + static_cast<size_t>(kP2mChunk) * nm1p) +
+         sizeof(short) * 4 * static_cast<size_t>(basis_size_d(p));
 }
 
 void launch_p2m(const float4 *src_rel, const float4 *mom, const int *src_off, const int8_t *basis,
