@@ -1007,9 +1007,12 @@ void launch_gather_moments(const void *user, int dtype, const int *inv, int ns, 
 #ifndef CDFMM_L2P_SPLIT
 #define CDFMM_L2P_SPLIT 0
 #endif
+#ifndef CDFMM_P2M_SMEM_CAP
+#define CDFMM_P2M_SMEM_CAP (64 * 1024)
+#endif
 static int p2m_state_block(int p, int K) {
   int Kb = std::min(K, CDFMM_P2M_KB);
-  while (Kb > 4 && p2m_smem_bytes(0, p, Kb, 0) > 64 * 1024) Kb = (Kb + 1) / 2;
+  while (Kb > 4 && p2m_smem_bytes(0, p, Kb, 0) > CDFMM_P2M_SMEM_CAP) Kb = (Kb + 1) / 2;
   return Kb;
 }
 
@@ -1017,7 +1020,7 @@ size_t p2m_smem_bytes(int n, int p, int K, int chunk) {
   (void)n;
   (void)chunk;
   const int nm1p = (basis_size_d(p - 1) + 3) & ~3;
-  const size_t Kb = static_cast<size_t>(std::min(K, 32));
+  const size_t Kb = static_cast<size_t>(std::min(K, CDFMM_P2M_KB));
   return sizeof(float4) * kP2mChunk * Kb + sizeof(float) * (3 * nm1p * (Kb + 2) + static_cast<size_t>(kP2mChunk) * nm1p) +
          sizeof(short) * 4 * static_cast<size_t>(basis_size_d(p));
 }
