@@ -572,3 +572,46 @@ def test_near_far_schedules_give_the_same_field(K):
     with pytest.raises(ValueError, match="unknown schedule"):
         plan.set_schedule(7)
     plan.close()
+
+
+def test_results_do_not_depend_on_other_live_plans():
+    """Plans created while other plans stay alive land on other memory; a
+    kernel that reads past one of its own arrays would then see whatever lies
+    there.  Regression of the M2L operand pack, which read its level-scale
+    table past the deepest level for the zero padding (stale non-finite
+    words there made every local NaN): each new plan must give the same
+    finite field as the first."""
+    rng = np.random.default_rng(9)
+    n, K = 2000, 8
+    x = rng.uniform(0, 1, (n, 3))
+    m = rng.normal(size=(K, n, 3)).astype(np.float32)
+    o = cdfmm.UniformTreeOptions()
+    o.max_level = 3
+    tree = cdfmm.UniformTree(x, x, o)
+    self_map = np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)]
+    big = np.random.default_rng(10).random((50000, 3))
+    mb = np.random.default_rng(11).normal(size=(1, 50000, 3))
+    side = np.random.default_rng(12).random((3000, 3))
+    alive, first, first_big = [], None, None
+    for it in range(6):
+        plan = cdfmm_b200.DevicePlan.from_tree(tree, 4, max_states=K)
+        plan.set_self_indices(self_map)
+        plan.set_m2l_shape(*plan.m2l_shapes()[0])
+        H = plan.evaluate(m, output="field")["H"]
+        plan.close()
+        assert np.isfinite(H).all(), f"iteration {it}"
+        if first is None:
+            first = H
+        np.testing.assert_array_equal(H, first)
+        p6 = cdfmm_b200.DevicePlan.from_points(big, 6, 3)
+        p6.set_m2l_shape(*p6.m2l_shapes()[0])
+        Hb = p6.evaluate(mb, output="field")["H"]
+        p6.close()
+        assert np.isfinite(Hb).all(), f"iteration {it}"
+        if first_big is None:
+            first_big = Hb
+        np.testing.assert_array_equal(Hb, first_big)
+        # a plan of another order kept alive for the rest of the test
+        alive.append(cdfmm_b200.DevicePlan.from_points(side, 5, 3))
+    for p in alive:
+        p.close()
