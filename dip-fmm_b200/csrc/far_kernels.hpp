@@ -89,6 +89,7 @@ std::vector<int4> p2p_work_units(const int *src_off, const int *tgt_off, int dep
 // from the device counter `next_unit`, each CTA leaving room on its SM for
 // one far-field CTA (same results up to the summation order of the state
 // blocks).
+struct NearTcLaunch; // tensor-core near field (near_tc.hpp)
 struct CorunLaunch {
   int ctas;        // grid size: two per SM
   int *next_unit;  // device counter (reset on the launch stream)
@@ -129,7 +130,8 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
                 const int2 *leaf_self, const CloseGeometry &cg, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin = 0, int k_end = -1,
-                int accumulate = 0, float phi_scale = 1.0F, const CorunLaunch *corun = nullptr);
+                int accumulate = 0, float phi_scale = 1.0F, const CorunLaunch *corun = nullptr,
+                const NearTcLaunch *tc = nullptr);
 // Close-pair search (once per plan), over work units covering every
 // target, with r formed as the near-field kernels form it.  Count pass:
 // counts[i][l] = pairs of target i with 0 < r^2 < thresholds[l]; write pass:

@@ -182,6 +182,18 @@ struct cdfmm_b200_plan {
   int4 *p2p_work_wide = nullptr;
   int n_p2p_work_wide = 0;
   bool in_batch = false;
+  // tensor-core near field (states 8..128): sources in blocks of 4 per leaf,
+  // work units of <= 32 targets, TF32 hi / lo moment operands; built on
+  // first use
+  int near_mode = CDFMM_B200_NEAR_AUTO;
+  bool ntc_supported = false;
+  bool ntc_built = false;
+  int *ntc_blk_off = nullptr;
+  int *ntc_blk_src = nullptr;
+  float4 *ntc_blk_pos = nullptr;
+  int4 *ntc_work = nullptr;
+  int ntc_n_blocks = 0, ntc_n_work = 0;
+  void *ntc_b = nullptr;
 
   // operators (device)
   int *m2m_off = nullptr, *m2m_pair = nullptr; // pair = g | (in << 16)

@@ -37,6 +37,7 @@
 #include "far_kernels.hpp"
 #include "kernels.cuh"
 #include "m2l_tc.hpp"
+#include "tcgen05.cuh"
 
 namespace cdfmm_b200 {
 
@@ -46,90 +47,22 @@ constexpr int kTcThreads = 128;
 constexpr uint32_t kWaitLimit = kTcWaitLimit; // ~2 s with the back-off below
 constexpr int kKChunk = 32;               // alphas per pipeline unit
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
+using tc::bulk_g2s;
+using tc::fence_proxy_async;
+using tc::instr_desc_bf16;
+using tc::mbar_expect_tx;
+using tc::mbar_init;
+using tc::mma_bf16;
+using tc::mma_commit;
+using tc::smem_desc;
+using tc::smem_u32;
+using tc::tc_fence_after;
+using tc::tc_fence_before;
+using tc::tmem_ld16;
 
-__device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
-               : "memory");
-}
-
-// Bounded wait for the phase with the given parity to complete.
+// Bounded wait (by default with the full limit).
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, uint32_t limit = kWaitLimit) {
-  const uint32_t addr = smem_u32(bar);
-  for (uint32_t i = 0; i < limit; ++i) {
-    uint32_t done;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(done)
-        : "r"(addr), "r"(parity)
-        : "memory");
-    if (done) return true;
-    if (i > 64) __nanosleep(32);
-  }
-  return false;
-}
-
-__device__ __forceinline__ void bulk_g2s(void *smem_dst, const void *gmem_src, uint32_t bytes, uint64_t *bar) {
-  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-                   smem_u32(smem_dst)),
-               "l"(gmem_src), "r"(bytes), "r"(smem_u32(bar))
-               : "memory");
-}
-
-// Shared-memory matrix descriptor, K-major, no swizzle: 8x16-byte core
-// matrices; lbo = byte distance between K-adjacent core matrices, sbo =
-// between 8-row groups (both multiples of 16); version 1 (sm_100).
-__device__ __forceinline__ uint64_t smem_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
-  uint64_t d = 0;
-  d |= static_cast<uint64_t>((addr >> 4) & 0x3fffu);
-  d |= static_cast<uint64_t>((lbo >> 4) & 0x3fffu) << 16;
-  d |= static_cast<uint64_t>((sbo >> 4) & 0x3fffu) << 32;
-  d |= static_cast<uint64_t>(1u) << 46; // version
-  // base offset 0, lbo mode 0, layout type 0 (SWIZZLE_NONE)
-  return d;
-}
-
-// Instruction descriptor: kind::f16, A = B = BF16, D = F32, K-major A and B, M = 128.
-__host__ __device__ constexpr uint32_t instr_desc_bf16(int n) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | (static_cast<uint32_t>(n >> 3) << 17) | (static_cast<uint32_t>(128 >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t tmem_d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t accumulate) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}" ::"r"(tmem_d),
-      "l"(a), "l"(b), "r"(idesc), "r"(accumulate)
-      : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint64_t *bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
-               : "memory");
-}
-
-__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
-__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
-  uint32_t r[16];
-  asm volatile(
-      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, [%16];"
-      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
-        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
-      : "r"(taddr));
-  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-#pragma unroll
-  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+  return tc::mbar_wait(bar, parity, limit);
 }
 
 // Pipeline unit = (offset, alpha chunk of kKChunk = 32, the last chunk

@@ -21,6 +21,7 @@
 
 #include "far_kernels.hpp"
 #include "kernels.cuh"
+#include "near_tc.hpp"
 
 namespace cdfmm_b200 {
 
@@ -1284,7 +1285,7 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
                 const float4 *tgt_rel, const int4 *work, int n_work, const int *self_idx,
                 const int2 *leaf_self, const CloseGeometry &cg, int depth, int K,
                 bool want_phi, float4 *near, cudaStream_t s, int k_begin, int k_end, int accumulate,
-                float phi_scale, const CorunLaunch *corun) {
+                float phi_scale, const CorunLaunch *corun, const NearTcLaunch *tc) {
   if (cg.cuboid.T != nullptr) {
     const int kb = k_begin, ke = k_end < 0 ? K : k_end;
     if (cg.cuboid.n_work == 0 || ke <= kb) return;
@@ -1313,6 +1314,9 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
     else
       p2p_k1_kernel<false><<<n_work, 128, 0, s>>>(src_rel, mom, src_off, tgt_rel, work, self_idx, leaf_self, depth,
                                                   near);
+  } else if (tc != nullptr && K >= kNearTcMinStates && K <= kNearTcMaxStates && k_begin == 0 &&
+             (k_end < 0 || k_end == K) && accumulate == 0) {
+    launch_near_tc(*tc, mom, tgt_rel, self_idx, depth, K, want_phi, near, s);
   } else {
     launch_kb_any(src_rel, mom, src_off, tgt_rel, work, n_work, self_idx, depth, K, want_phi ? 1 : 0, near, nullptr, s,
                   k_begin, k_end, accumulate, phi_scale, corun);

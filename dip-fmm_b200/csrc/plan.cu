@@ -28,6 +28,7 @@
 #include "geometry.hpp"
 #include "kernels.cuh"
 #include "m2l_tc.hpp"
+#include "near_tc.hpp"
 
 namespace {
 
@@ -119,7 +120,8 @@ void free_plan(cdfmm_b200_plan *p) {
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
                   p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
                   p->close_targets, p->close_r_fp32, p->close_r_exact, p->src_pos64, p->tgt_pos64,
-                  p->src_size, p->src_size64, p->cuboid_T, p->cuboid_base};
+                  p->src_size, p->src_size64, p->cuboid_T, p->cuboid_base, p->ntc_blk_off, p->ntc_blk_src,
+                  p->ntc_blk_pos, p->ntc_work, p->ntc_b};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
   if (p->p2p_work_wide != nullptr && p->p2p_work_wide != p->p2p_work) cudaFree(p->p2p_work_wide);
@@ -658,6 +660,8 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
       throw AbiError(CDFMM_B200_ERR_RUNTIME,
                      "split-BF16 tensor-core M2L needs an sm_100 device, depth >= 2 and order <= 9");
     }
+    // tensor-core near field: sm_100 devices (layout and buffers on first use)
+    plan->ntc_supported = major == 10 && configure_near_tc(smem);
   }
   ops.m2l_T64.reset();
   // every set-up copy, memset and kernel (legacy default stream) is complete
@@ -1126,12 +1130,58 @@ static bool m2l_on_tensor_cores(const cdfmm_b200_plan *plan, int K) {
          (plan->m2l_mode == CDFMM_B200_M2L_BF16X3 || plan->m2l_mode == CDFMM_B200_M2L_AUTO);
 }
 
+// Whether an evaluation of K states takes the tensor-core near field.
+static bool near_on_tensor_cores(const cdfmm_b200_plan *plan, int K) {
+  return plan->ntc_supported && plan->near_mode != CDFMM_B200_NEAR_FP32 && K >= kNearTcMinStates &&
+         K <= kNearTcMaxStates && !plan->cuboid && plan->n_p2p_work > 0;
+}
+
+// Blocks, work units and operand buffers of the tensor-core near field
+// (once per plan, on first use).
+static void ensure_near_tc(cdfmm_b200_plan *plan) {
+  if (plan->ntc_built) return;
+  const NearTcLayout lay = near_tc_layout(plan->h_src_off.data(), plan->h_tgt_off.data(), plan->depth);
+  uint64_t bytes = 0, h2d = 0;
+  plan->ntc_blk_off = dalloc<int>(lay.blk_off.size(), bytes);
+  upload(plan->ntc_blk_off, lay.blk_off.data(), lay.blk_off.size(), h2d);
+  plan->ntc_blk_src = dalloc<int>(lay.blk_src.size(), bytes);
+  upload(plan->ntc_blk_src, lay.blk_src.data(), lay.blk_src.size(), h2d);
+  plan->ntc_blk_pos = dalloc<float4>(lay.blk_src.size(), bytes);
+  plan->ntc_work = dalloc<int4>(lay.work.size(), bytes);
+  upload(plan->ntc_work, lay.work.data(), lay.work.size(), h2d);
+  const size_t ob = near_tc_operand_bytes(lay.n_blocks, std::min(plan->max_states, kNearTcMaxStates));
+  plan->ntc_b = dalloc<uint8_t>(ob, bytes);
+  launch_near_tc_positions(plan->src_rel, plan->ntc_blk_src, lay.n_blocks, plan->ntc_blk_pos, plan->stream);
+  check(cudaGetLastError(), "kernel launch");
+  check(cudaStreamSynchronize(plan->stream), "near-field blocks");
+  plan->ntc_n_blocks = lay.n_blocks;
+  plan->ntc_n_work = static_cast<int>(lay.work.size());
+  plan->stats.persistent_device_bytes += bytes;
+  plan->stats.setup_h2d_bytes += h2d;
+  plan->ntc_built = true;
+}
+
+static NearTcLaunch near_tc_launch(const cdfmm_b200_plan *plan) {
+  NearTcLaunch l{};
+  l.blk_pos = plan->ntc_blk_pos;
+  l.blk_off = plan->ntc_blk_off;
+  l.blk_src = plan->ntc_blk_src;
+  l.n_blocks = plan->ntc_n_blocks;
+  l.work = plan->ntc_work;
+  l.n_work = plan->ntc_n_work;
+  l.b_ops = plan->ntc_b;
+  l.error_flag = plan->error_flag;
+  l.wait_limit = plan->tc_wait_limit;
+  return l;
+}
+
 // Near/far schedule of one evaluation (cdfmm_b200_set_schedule): the
 // co-resident schedule needs the tensor-core M2L (whose CTA fits beside two
 // co-resident near-field CTAs); other evaluations run SEPARATE.
 static int resolved_schedule(const cdfmm_b200_plan *plan, int K) {
-  // cuboid sources: their near-field kernel has no co-resident form
-  if (K <= 1 || !m2l_on_tensor_cores(plan, K) || plan->cuboid) return CDFMM_B200_SCHEDULE_SEPARATE;
+  // cuboid sources and the tensor-core near field: no co-resident form
+  if (K <= 1 || !m2l_on_tensor_cores(plan, K) || plan->cuboid || near_on_tensor_cores(plan, K))
+    return CDFMM_B200_SCHEDULE_SEPARATE;
   return plan->schedule == CDFMM_B200_SCHEDULE_AUTO ? CDFMM_B200_SCHEDULE_CORUN : plan->schedule;
 }
 
@@ -1280,10 +1330,14 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   // its leaf is cut into units).
   const bool wide = plan->in_batch && K == 1;
   const CorunLaunch corun_launch{2 * plan->sm_count, plan->p2p_next_unit};
+  const bool near_tc = near_on_tensor_cores(plan, K);
+  if (near_tc) ensure_near_tc(plan);
+  const NearTcLaunch near_tc_args = near_tc_launch(plan);
   launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, wide ? plan->p2p_work_wide : plan->p2p_work,
              wide ? plan->n_p2p_work_wide : plan->n_p2p_work, plan->has_self ? plan->self_idx : nullptr,
              plan->leaf_self, close_geometry(plan), plan->depth, K, want_phi, plan->near, ns, 0, -1, 0, 1.0F,
-             corun ? &corun_launch : nullptr);
+             corun ? &corun_launch : nullptr, near_tc ? &near_tc_args : nullptr);
+  plan->stats.near_tc_last = near_tc ? 1 : 0;
   ++launches;
   if (timing) check(cudaEventRecord(plan->ev_t[9], ns), "event");
   if (trace) check(cudaEventRecord(plan->ev_t[kTraceP2pEnd], ns), "event");
@@ -1843,6 +1897,16 @@ int cdfmm_b200_set_schedule(cdfmm_b200_plan *plan, int32_t schedule) {
   if (schedule < CDFMM_B200_SCHEDULE_AUTO || schedule > CDFMM_B200_SCHEDULE_CORUN)
     return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT, "unknown schedule");
   plan->schedule = schedule;
+  return CDFMM_B200_OK;
+}
+
+int cdfmm_b200_set_near_mode(cdfmm_b200_plan *plan, int32_t mode) {
+  if (plan == nullptr) return fail(nullptr, CDFMM_B200_ERR_INVALID_ARGUMENT, "plan is NULL");
+  if (mode < CDFMM_B200_NEAR_AUTO || mode > CDFMM_B200_NEAR_TF32X3)
+    return fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT, "unknown near-field mode");
+  if (mode == CDFMM_B200_NEAR_TF32X3 && !plan->ntc_supported)
+    return fail(plan, CDFMM_B200_ERR_RUNTIME, "the tensor-core near field needs an sm_100 device");
+  plan->near_mode = mode;
   return CDFMM_B200_OK;
 }
 

@@ -35,6 +35,7 @@ RESULTS_ON_HOST = 2
 LAYOUT_SEPARATE = 0
 LAYOUT_INTERLEAVED = 1
 SCHEDULE_AUTO, SCHEDULE_SEPARATE, SCHEDULE_CORUN = 0, 1, 2
+NEAR_AUTO, NEAR_FP32, NEAR_TF32X3 = 0, 1, 2
 
 EXPORTED = (
     "cdfmm_b200_device_count", "cdfmm_b200_device_info", "cdfmm_b200_plan_create",
@@ -46,7 +47,7 @@ EXPORTED = (
     "cdfmm_b200_selftest_bounded_wait", "cdfmm_b200_m2l_shapes", "cdfmm_b200_set_m2l_shape",
     "cdfmm_b200_poll_status", "cdfmm_b200_set_wait_limit", "cdfmm_b200_set_schedule", "cdfmm_b200_batch_groups",
     "cdfmm_b200_plan_create_from_points", "cdfmm_b200_plan_tree", "cdfmm_b200_m2l_stencil",
-    "cdfmm_b200_set_source_cuboids",
+    "cdfmm_b200_set_source_cuboids", "cdfmm_b200_set_near_mode",
 )
 
 ROOT_CENTRE, ROOT_HALF_WIDTH = 1, 2
@@ -114,7 +115,7 @@ class Stats(ctypes.Structure):
         ("trace_p2p_begin", ctypes.c_double), ("trace_p2p_end", ctypes.c_double),
         ("trace_far_begin", ctypes.c_double), ("trace_m2l_begin", ctypes.c_double),
         ("trace_far_end", ctypes.c_double), ("trace_end", ctypes.c_double),
-        ("schedule_last", ctypes.c_int32), ("reserved0", ctypes.c_int32),
+        ("schedule_last", ctypes.c_int32), ("near_tc_last", ctypes.c_int32),
         ("setup_ms_tree", ctypes.c_double), ("setup_ms_geometry", ctypes.c_double),
         ("setup_ms_near", ctypes.c_double), ("setup_ms_operators", ctypes.c_double),
         ("setup_ms_statistics", ctypes.c_double), ("setup_ms_buffers", ctypes.c_double),
@@ -164,6 +165,7 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_read_expansions.argtypes = [vp, i32, i32, vp, u64]
     lib.cdfmm_b200_set_timing.argtypes = [vp, i32]
     lib.cdfmm_b200_set_schedule.argtypes = [vp, i32]
+    lib.cdfmm_b200_set_near_mode.argtypes = [vp, i32]
     lib.cdfmm_b200_m2l_shapes.argtypes = [vp, ctypes.POINTER(i32), i32]
     lib.cdfmm_b200_set_m2l_shape.argtypes = [vp, i32, i32, i32]
     lib.cdfmm_b200_get_stats.argtypes = [vp, ctypes.POINTER(Stats)]
@@ -410,6 +412,11 @@ class DevicePlan:
     def set_schedule(self, schedule):
         """Near/far schedule of K > 1 evaluations (SCHEDULE_*)."""
         _check(library().cdfmm_b200_set_schedule(self._h, int(schedule)), self._h)
+
+    def set_near_mode(self, mode):
+        """Near-field arithmetic of evaluations of 8..128 states: NEAR_AUTO
+        (tensor cores where supported), NEAR_FP32 or NEAR_TF32X3."""
+        _check(library().cdfmm_b200_set_near_mode(self._h, int(mode)), self._h)
 
     def m2l_shapes(self) -> list:
         """Tensor-core M2L pipeline shapes of this plan as (accumulators per

@@ -53,6 +53,11 @@ extern "C" {
 #define CDFMM_B200_M2L_FP32 1        /* FP32 SIMT (the plain per-state path) */
 #define CDFMM_B200_M2L_BF16X3 2      /* tcgen05, BF16 hi/lo with three products, FP32 accumulate */
 
+/* Near-field arithmetic of evaluations of 8..128 states (cdfmm_b200_set_near_mode). */
+#define CDFMM_B200_NEAR_AUTO 0       /* tensor cores where supported, else FP32 */
+#define CDFMM_B200_NEAR_FP32 1       /* FP32 SIMT */
+#define CDFMM_B200_NEAR_TF32X3 2     /* tcgen05, TF32 hi/lo with three products, FP32 accumulate */
+
 /* Where the caller's arrays live (cdfmm_b200_eval_args.memory). */
 #define CDFMM_B200_MOMENTS_ON_HOST 1u
 #define CDFMM_B200_RESULTS_ON_HOST 2u
@@ -135,7 +140,7 @@ typedef struct cdfmm_b200_stats {
    * far field begin (P2M), M2L begin, far field end (after L2L), end. */
   double trace_p2p_begin, trace_p2p_end, trace_far_begin, trace_m2l_begin, trace_far_end, trace_end;
   int32_t schedule_last;         /* CDFMM_B200_SCHEDULE_* the last evaluate ran */
-  int32_t reserved0;
+  int32_t near_tc_last;          /* 1: the last evaluate's near field ran on the tensor cores */
   /* Plan construction, host wall-clock ms: the device octree (points plans),
    * positions / permutations, near-field work units and close pairs,
    * operators, interaction statistics, state buffers and kernel set-up, the
@@ -370,6 +375,21 @@ int cdfmm_b200_set_timing(cdfmm_b200_plan *plan, int32_t enabled);
  * and the M2L pipeline shape may too, at FP32 rounding level.  Evaluations
  * whose M2L runs on the FP32 SIMT path always run SEPARATE. */
 int cdfmm_b200_set_schedule(cdfmm_b200_plan *plan, int32_t schedule);
+
+/* Near-field arithmetic for evaluations of 8 <= K <= 128 states (no
+ * counterpart in the reference, whose CudaFull near field is an FP32
+ * cuSPARSE product with stored pair tensors, src/cuda_fmm.cu:3295-3300
+ * upstream): CDFMM_B200_NEAR_*.  The tensor-core form computes the pair
+ * tensors of each work unit of up to 32 targets on the fly and multiplies
+ * them with the states' moments as TF32 hi/lo splits (three products, FP32
+ * accumulation: FP32-level accuracy; results differ from the FP32 SIMT form
+ * at rounding level).  It takes the evaluations that compute every state in
+ * one near-field pass on the device (cdfmm_b200_evaluate with device arrays,
+ * K within the range); streamed host-array evaluations, backward passes,
+ * cuboid sources and cdfmm_b200_evaluate_noalloc keep the FP32 form.  Its
+ * per-plan blocks and operand buffers (about 96 bytes per source and state)
+ * are allocated on its first use. */
+int cdfmm_b200_set_near_mode(cdfmm_b200_plan *plan, int32_t mode);
 
 int cdfmm_b200_get_stats(const cdfmm_b200_plan *plan, cdfmm_b200_stats *out);
 

@@ -1,0 +1,155 @@
+"""Tensor-core near field (cdfmm_b200_set_near_mode): TF32 hi/lo pair-tensor
+products against the FP32 SIMT near field and the FP64 direct sum.
+
+The near field is the reference's list-1 P2P (upstream src/operators.cpp:
+178-199 pair formula, src/uniform_tree.cpp:455-480 neighbourhood); the
+tensor-core form must give the same sums at FP32-level accuracy: against the
+FP64 direct sum on a depth-1 tree (every pair is a near pair) it must be as
+accurate as the FP32 form, and on deeper trees it must agree with the FP32
+form to rounding level."""
+import numpy as np
+import pytest
+
+import cdfmm_b200
+import oracle
+
+pytestmark = pytest.mark.gpu
+
+torch = pytest.importorskip("torch")
+
+
+def _evaluate(plan, m, mode, output="both"):
+    plan.set_near_mode(mode)
+    K, n = m.shape[0], plan.n_targets
+    H = torch.full((K, n, 3), float("nan"), dtype=torch.float32, device="cuda")
+    phi = torch.full((K, n), float("nan"), dtype=torch.float32, device="cuda")
+    plan.evaluate(m, output=output, field=H, potential=phi, synchronize=True)
+    return H.cpu().numpy(), phi.cpu().numpy(), plan.stats()["near_tc_last"]
+
+
+def _points(kind, n, rng):
+    if kind == "uniform":
+        return rng.uniform(0, 1, (n, 3))
+    c = rng.uniform(0.2, 0.8, (4, 3))
+    return c[rng.integers(0, 4, n)] + rng.normal(0, 0.03, (n, 3))
+
+
+@pytest.mark.parametrize("kind", ["uniform", "clusters"])
+def test_near_field_alone_is_as_accurate_as_fp32(kind):
+    """Depth 1: the FMM is the near field alone.  Both forms against the FP64
+    direct sum (FP32 moments), every state checked on two of them."""
+    rng = np.random.default_rng(11)
+    n, K = 3000, 8
+    x = _points(kind, n, rng)
+    plan = cdfmm_b200.DevicePlan.from_points(x, 4, 1, max_states=K)
+    mm = rng.normal(size=(K, n, 3)).astype(np.float32)
+    m = torch.from_numpy(mm).cuda()
+    H32, p32, used32 = _evaluate(plan, m, cdfmm_b200.NEAR_FP32)
+    Htc, ptc, usedtc = _evaluate(plan, m, cdfmm_b200.NEAR_TF32X3)
+    assert (used32, usedtc) == (0, 1)
+    ids = np.arange(n, dtype=np.int32)
+    for k in (0, K - 1):
+        phi64, H64 = cdfmm_b200.direct_fp64(x, mm[k].astype(np.float64), x, ids)
+        e32, etc = oracle.rel_l2(H32[k], H64), oracle.rel_l2(Htc[k], H64)
+        assert etc < 2e-6 and etc < 2.0 * e32, (etc, e32)
+        assert oracle.rel_l2(ptc[k], phi64) < 2e-6
+    plan.close()
+
+
+@pytest.mark.parametrize("K", [8, 24, 64])
+def test_tensor_core_and_fp32_near_fields_agree(K):
+    """Depth 3 (far field present): the two near-field forms give the same
+    field and potential to rounding level for K rounded up to 16 (padding
+    states), and the result meets the FP32 bar against the FP64 oracle."""
+    rng = np.random.default_rng(100 + K)
+    n = 20000
+    x = rng.uniform(0, 1, (n, 3))
+    plan = cdfmm_b200.DevicePlan.from_points(x, 4, 3, max_states=K)
+    m = torch.from_numpy(rng.normal(size=(K, n, 3)).astype(np.float32)).cuda()
+    H32, p32, _ = _evaluate(plan, m, cdfmm_b200.NEAR_FP32)
+    Htc, ptc, used = _evaluate(plan, m, cdfmm_b200.NEAR_AUTO)
+    assert used == 1
+    assert oracle.rel_l2(Htc, H32) < 2e-6
+    assert oracle.rel_l2(ptc, p32) < 2e-6
+    sub = rng.choice(n, 500, replace=False)
+    k = K - 1
+    phi64, H64 = cdfmm_b200.direct_fp64(x, m[k].cpu().numpy().astype(np.float64), x[sub], sub.astype(np.int32))
+    assert oracle.rel_l2(Htc[k][sub], H64) < 3e-5
+    plan.close()
+
+
+def test_dense_neighbourhoods_and_separate_targets():
+    """Clustered points at depth 2: some neighbourhoods hold more than the
+    1,536 sources whose positions are staged in shared memory (the kernel
+    then reads them from global memory), and targets distinct from the
+    sources (no self pairs)."""
+    rng = np.random.default_rng(5)
+    ns, nt, K = 40000, 3000, 16
+    src = 0.5 + rng.normal(0, 0.06, (ns, 3))
+    tgt = 0.5 + rng.normal(0, 0.08, (nt, 3))
+    plan = cdfmm_b200.DevicePlan.from_points(src, 4, 2, targets=tgt, root_centre=(0.5, 0.5, 0.5),
+                                             root_half_width=0.6, max_states=K)
+    tree = plan.tree()
+    counts = np.diff(tree["leaf_source_offsets"])
+    assert counts.max() > 1536
+    m = torch.from_numpy(rng.normal(size=(K, ns, 3)).astype(np.float32)).cuda()
+    H32, p32, _ = _evaluate(plan, m, cdfmm_b200.NEAR_FP32)
+    Htc, ptc, used = _evaluate(plan, m, cdfmm_b200.NEAR_TF32X3)
+    assert used == 1 and np.isfinite(Htc).all()
+    assert oracle.rel_l2(Htc, H32) < 2e-6
+    assert oracle.rel_l2(ptc, p32) < 2e-6
+    plan.close()
+
+
+def test_field_only_output_and_state_range():
+    """Field-only output leaves the potential untouched by the near field;
+    K outside 8..64 keeps the FP32 near field."""
+    rng = np.random.default_rng(3)
+    n = 5000
+    x = rng.uniform(0, 1, (n, 3))
+    plan = cdfmm_b200.DevicePlan.from_points(x, 4, 2, max_states=72)
+    m8 = torch.from_numpy(rng.normal(size=(8, n, 3)).astype(np.float32)).cuda()
+    Hf, _, used = _evaluate(plan, m8, cdfmm_b200.NEAR_AUTO, output="field")
+    Hb, _, _ = _evaluate(plan, m8, cdfmm_b200.NEAR_AUTO, output="both")
+    assert used == 1
+    np.testing.assert_array_equal(Hf, Hb)
+    for K in (4, 72):
+        m = torch.from_numpy(rng.normal(size=(K, n, 3)).astype(np.float32)).cuda()
+        _, _, used = _evaluate(plan, m, cdfmm_b200.NEAR_AUTO)
+        assert used == 0
+    plan.close()
+
+
+def test_near_field_expired_waits_poison_and_recover():
+    """With the SIMT M2L (no tensor-core far field) and the injected wait
+    limit 0, the tensor-core near field's progress waits expire: the call
+    reports a timeout and its near-field targets read NaN; with the default
+    limit restored the next evaluation equals the one before."""
+    rng = np.random.default_rng(21)
+    n, K = 4000, 16
+    x = rng.uniform(0, 1, (n, 3))
+    plan = cdfmm_b200.DevicePlan.from_points(x, 4, 3, max_states=K, m2l_mode=cdfmm_b200.M2L_FP32)
+    plan.set_near_mode(cdfmm_b200.NEAR_TF32X3)
+    m = torch.from_numpy(rng.normal(size=(K, n, 3)).astype(np.float32)).cuda()
+    H = torch.empty((K, n, 3), dtype=torch.float32, device="cuda")
+    plan.evaluate(m, output="field", field=H, synchronize=True)
+    clean = H.cpu().numpy().copy()
+    assert np.isfinite(clean).all()
+    plan.set_wait_limit(0)
+    with pytest.raises(cdfmm_b200.CdfmmError) as err:
+        plan.evaluate(m, output="field", field=H, synchronize=True)
+    assert err.value.code == cdfmm_b200.ERR_TIMEOUT
+    assert np.isnan(H.cpu().numpy()).any()
+    plan.poll_status()
+    plan.set_wait_limit(-1)
+    plan.evaluate(m, output="field", field=H, synchronize=True)
+    np.testing.assert_array_equal(H.cpu().numpy(), clean)
+    plan.close()
+
+
+def test_set_near_mode_rejects_unknown_modes():
+    rng = np.random.default_rng(1)
+    plan = cdfmm_b200.DevicePlan.from_points(rng.uniform(0, 1, (100, 3)), 2, 1, max_states=8)
+    with pytest.raises(cdfmm_b200.CdfmmError):
+        plan.set_near_mode(7)
+    plan.close()
