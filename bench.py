@@ -19,6 +19,8 @@ Reported beside `value` (device-resident inputs):
   plain         the plain per-state FP32 path (K = 1 calls, FP32 SIMT M2L);
   rel_l2_*      accuracy of state 0 vs the FP64 direct sum on 16,384 targets;
   roofline      dominant kernel: algorithmic work / CUDA-event duration;
+  near_field    the step with the FP32 SIMT near field (co-resident with
+                the M2L) and with the tensor-core near field;
   cpu_baseline  the reference CpuStatic (oracle/_ref, built from the upstream
                 sources) on the host cores, on a bounded sample;
   backward      reverse mode on the same workload: device time of the field
@@ -68,6 +70,8 @@ def parse_args():
     ap.add_argument("--depth", type=int, default=5)
     ap.add_argument("--states", type=int, default=64)
     ap.add_argument("--m2l", choices=["auto", "fp32", "bf16x3"], default="auto")
+    ap.add_argument("--near", choices=["auto", "fp32", "tf32x3"], default="auto",
+                    help="near-field arithmetic of the K-state evaluation (auto: tensor cores)")
     ap.add_argument("--seed", type=int, default=314159)
     ap.add_argument("--plain-states", type=int, default=8)
     ap.add_argument("--no-cpu-baseline", action="store_true")
@@ -339,6 +343,9 @@ def b200_arm(args):
     sorted_self = np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)]
     plan = cdfmm_b200.DevicePlan.from_tree(tree, p, max_states=K, m2l_mode=mode, device=local)
     plan.set_self_indices(sorted_self)
+    near_mode = {"auto": cdfmm_b200.NEAR_AUTO, "fp32": cdfmm_b200.NEAR_FP32,
+                 "tf32x3": cdfmm_b200.NEAR_TF32X3}[args.near]
+    plan.set_near_mode(near_mode)
     moments = unit_moments(np.random.default_rng(rank_moment_seed(args.seed, rank)), K, N)
     # A dedicated stream: torch's events and our kernels are ordered on it.
     stream = torch.cuda.Stream()
@@ -392,9 +399,24 @@ def b200_arm(args):
     rel_h = float(np.sqrt(np.sum((H0 - H_ref) ** 2) / np.sum(H_ref ** 2)))
     rel_phi = float(np.sqrt(np.sum((phi0 - phi_ref) ** 2) / np.sum(phi_ref ** 2)))
 
-    # near/far schedules: device time per step of each, and one concurrent
-    # trace each (per-stream events: when the near field and the M2L ran)
+    near_tc_used = bool(plan.stats()["near_tc_last"])
+    # near/far schedules (with the FP32 near field, which has a co-resident
+    # form): device time per step of each, and one concurrent trace each
+    # (per-stream events: when the near field and the M2L ran)
+    plan.set_near_mode(cdfmm_b200.NEAR_FP32)
     schedules = schedule_leg(plan, step, stream, args.steps, max_over_ranks, args.corun_shape_sweep)
+    # the step with each near-field form (FP32 SIMT in its automatic
+    # schedule, tensor cores beside the far field)
+    near_field = {"used": "tf32x3" if near_tc_used else "fp32"}
+    for name, nm in (("fp32", cdfmm_b200.NEAR_FP32), ("tf32x3", cdfmm_b200.NEAR_TF32X3)):
+        try:
+            plan.set_near_mode(nm)
+        except cdfmm_b200.CdfmmError:
+            continue
+        near_field[name + "_ms_per_step"] = timed_steps(step, stream, args.steps, max_over_ranks)
+    plan.set_near_mode(near_mode)
+    step()
+    torch.cuda.synchronize()
 
     # per-stage device times (separate, instrumented evaluations)
     plan.set_timing(True)
@@ -521,13 +543,21 @@ def b200_arm(args):
     n = (p + 1) * (p + 2) * (p + 3) // 6
     m2l_flop = 2.0 * n * n * st["m2l_interactions"] * K
     p2p_flop = (st["p2p_pairs"] - N) * (13.0 + 20.0 * K)
-    cand = {"m2l": (stages.get("m2l", 0.0), m2l_flop), "p2p": (stages.get("p2p", 0.0), p2p_flop)}
+    near_key = "near_tc" if near_tc_used else "p2p"
+    cand = {"m2l": (stages.get("m2l", 0.0), m2l_flop), near_key: (stages.get("p2p", 0.0), p2p_flop)}
     dom = max(cand, key=lambda k: cand[k][0])
     ms_dom, flop_dom = cand[dom]
     if dom == "m2l":
         peak = peaks.get("bf16_tflops_sustained", FALLBACK_PEAKS["bf16_tflops_sustained"])
         roofline = {"kernel": "m2l", "bound": "tensor", "unit": "TFLOP/s",
                     "algorithmic_flop": m2l_flop, "peak_source": f"{peak_kind} bf16_tflops_sustained"}
+    elif dom == "near_tc":
+        # TF32 MMAs run at half the BF16 rate on this part (nominal 1.1 vs
+        # 2.25 PFLOP/s dense)
+        peak = 0.5 * peaks.get("bf16_tflops_sustained", FALLBACK_PEAKS["bf16_tflops_sustained"])
+        roofline = {"kernel": "near_tc", "bound": "tensor", "unit": "TFLOP/s", "algorithmic_flop": p2p_flop,
+                    "peak_source": f"{peak_kind} bf16_tflops_sustained / 2 (TF32 rate)",
+                    "fp32_fma_frac": p2p_flop / (ms_dom * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS if ms_dom > 0 else None}
     else:
         peak = FP32_NOMINAL_TFLOPS
         roofline = {"kernel": "p2p", "bound": "fp32", "unit": "TFLOP/s", "algorithmic_flop": p2p_flop,
@@ -585,7 +615,7 @@ def b200_arm(args):
         "rel_l2_H": rel_h, "rel_l2_phi": rel_phi,
         "e2e": e2e, "gpu_launches": int(launches), "clocks": clock_info, "roofline": roofline,
         "cpu_baseline": cpu, "reference_gpu": reference_gpu, "stages_ms": stages, "hbm_stages": hbm,
-        "schedules": schedules,
+        "schedules": schedules, "near_field": near_field,
         "plain": {"value": plain_value, "unit": UNIT, "ms_per_state": ms_state_plain, "states_timed": ks,
                   "m2l": "fp32"},
         "batched_over_plain": value / plain_value,
@@ -693,6 +723,21 @@ def reference_gpu_leg(args, stream, local):
 
 
 SCHEDULE_NAMES = {1: "separate", 2: "corun"}
+
+
+def timed_steps(step, stream, steps, max_over_ranks):
+    """Device ms per step over `steps` steps after one untimed step."""
+    import torch
+
+    step()
+    torch.cuda.synchronize()
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    a.record(stream)
+    for _ in range(max(1, steps)):
+        step()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return max_over_ranks(a.elapsed_time(b) / max(1, steps))
 
 
 def schedule_leg(plan, step, stream, steps, max_over_ranks, shape_sweep=False):

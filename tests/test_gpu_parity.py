@@ -533,7 +533,9 @@ def test_near_far_schedules_give_the_same_field(K):
     results agree to FP32 rounding (the co-resident form sums each target's
     state blocks of 32 in another order, and the M2L may take another
     pipeline shape) and meet the FP32 bar against the FP64 oracle FMM.  The
-    concurrent trace reports each stream's interval in order."""
+    concurrent trace reports each stream's interval in order.  The schedules
+    are those of the FP32 near field; with the tensor-core near field every
+    schedule runs SEPARATE."""
     torch = pytest.importorskip("torch")
     rng = np.random.default_rng(400 + K)
     n = 6000
@@ -544,6 +546,7 @@ def test_near_far_schedules_give_the_same_field(K):
     plan = cdfmm_b200.DevicePlan.from_tree(tree, 5, max_states=K)
     plan.set_self_indices(np.array(tree.source_inverse_permutation)[np.array(tree.target_permutation)])
     m = torch.from_numpy(rng.normal(size=(K, n, 3)).astype(np.float32)).cuda()
+    plan.set_near_mode(cdfmm_b200.NEAR_FP32)
     out = {}
     for sched in (cdfmm_b200.SCHEDULE_SEPARATE, cdfmm_b200.SCHEDULE_CORUN, cdfmm_b200.SCHEDULE_AUTO):
         plan.set_schedule(sched)
@@ -569,6 +572,12 @@ def test_near_far_schedules_give_the_same_field(K):
     h, p = out[cdfmm_b200.SCHEDULE_AUTO]
     assert oracle.rel_l2(h[K - 1], ref["H"]) < FP32_REL_L2
     assert oracle.rel_l2(p[K - 1], ref["phi"]) < FP32_REL_L2
+    plan.set_near_mode(cdfmm_b200.NEAR_AUTO)
+    plan.set_schedule(cdfmm_b200.SCHEDULE_CORUN)
+    plan.evaluate(m, output="both", field=H, potential=phi, synchronize=True)
+    assert plan.stats()["near_tc_last"] == 1
+    assert plan.stats()["schedule_last"] == cdfmm_b200.SCHEDULE_SEPARATE
+    assert oracle.rel_l2(H.cpu().numpy(), base_h) < 2e-6
     with pytest.raises(ValueError, match="unknown schedule"):
         plan.set_schedule(7)
     plan.close()
