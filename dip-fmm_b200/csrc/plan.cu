@@ -1779,6 +1779,7 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
     if (a->grad_moments != nullptr) {
       // dL/dm = A^t dL/dH: the transposed plan evaluated on the weights.
       ensure_adjoint(plan);
+      plan->adjoint->near_mode = plan->near_mode;
       cdfmm_b200_eval_args e{};
       e.moments = a->grad_field;
       e.moments_dtype = 0;
