@@ -78,7 +78,19 @@ constexpr int kNtThreads = 32 * (kNtDrainWarp + 4);
 constexpr uint32_t kNtTmemCols = kNtCtasPerSm == 2 ? 256 : 512;
 constexpr int kNtStageStride = 33;    // epilogue transpose row (32 targets + 1)
 constexpr int kNtPosCap = 384;        // neighbourhood blocks whose positions are staged in shared memory
-constexpr int kNtBSlots = kNtCtasPerSm == 2 ? 4 : 8; // moment operand ring
+// Blocks of 4 sources per pipeline chunk (even), and whether a k-step's
+// hi x hi and hi x lo products run as one MMA of width 2 K (A_hi x
+// [B_hi | B_lo]; twice the accumulator columns) or as two.
+#ifndef CDFMM_NTC_CB
+#define CDFMM_NTC_CB 4
+#endif
+#ifndef CDFMM_NTC_FUSE
+#define CDFMM_NTC_FUSE 0
+#endif
+constexpr int kNtCB = CDFMM_NTC_CB;
+constexpr bool kNtFuse = CDFMM_NTC_FUSE != 0;
+constexpr int kNtAW = 24 * kNtCB;                                     // A-slot columns (hi, then lo)
+constexpr int kNtBSlots = (kNtCtasPerSm == 2 ? 8 : 16) / kNtCB;        // moment operand ring
 constexpr uint32_t kNtMiscBytes = 640;
 
 // Chunks (8 sources, 9 MMAs) accumulated in one tensor-memory buffer before
@@ -86,7 +98,7 @@ constexpr uint32_t kNtMiscBytes = 640;
 // accumulation is not round-to-nearest, so its error grows with the number
 // of MMAs summed into one accumulator at its magnitude.
 #ifndef CDFMM_NTC_GROUP
-#define CDFMM_NTC_GROUP 4
+#define CDFMM_NTC_GROUP 2
 #endif
 
 // Accumulator buffers: 2 (the MMAs of the next group run while a group is
@@ -99,8 +111,9 @@ constexpr int kNtDBuf = CDFMM_NTC_DBUF;
 __host__ __device__ inline int nt_N(int K) { return (K + 15) / 16 * 16; }
 // A-operand slots in tensor memory after the accumulators (2 N columns
 // each: hi x [B_hi | B_lo] side by side), 48 columns each (24 hi + 24 lo).
+__host__ __device__ inline int nt_acc_cols(int N) { return kNtFuse ? 2 * N : N; }
 __host__ __device__ inline int nt_slots(int N) {
-  const int s = (static_cast<int>(kNtTmemCols) - 2 * kNtDBuf * N) / 48;
+  const int s = (static_cast<int>(kNtTmemCols) - kNtDBuf * nt_acc_cols(N)) / kNtAW;
   return s < 8 ? s : 8;
 }
 
@@ -114,9 +127,9 @@ struct NtSmem {
 };
 __host__ __device__ inline NtSmem nt_smem(int N, int SA) {
   NtSmem m;
-  m.slot_bytes = 192u * static_cast<uint32_t>(N);
+  m.slot_bytes = 96u * kNtCB * static_cast<uint32_t>(N);
   m.pos_off = kNtBSlots * m.slot_bytes;
-  m.stage_off = m.pos_off + (kNtPosCap + 1) * 64u + 4u * kNtWg * 128u;
+  m.stage_off = m.pos_off + (kNtPosCap + kNtCB) * 64u + 4u * kNtWg * 128u;
   m.bar_off = m.stage_off + 4u * 16u * kNtStageStride * 4u;
   m.misc_off = m.bar_off + (2u * kNtBSlots + 2u * static_cast<uint32_t>(SA) + 6u) * 8u;
   m.total = m.misc_off + kNtMiscBytes;
@@ -321,10 +334,11 @@ __global__ void __launch_bounds__(kNtThreads, kNtCtasPerSm) near_tc_kernel(const
   const uint32_t tmem = *tmem_slot;
   const int n_nb = *nb_count;
   const int n_blk = nb_prefix[n_nb];
-  const int chunks = (n_blk + 1) / 2;
+  const int chunks = (n_blk + kNtCB - 1) / kNtCB;
   const int groups = (chunks + G - 1) / G;
   const bool staged = n_blk <= kNtPosCap; // positions in shared memory (else read from global memory)
-  const uint32_t acol0 = 2u * kNtDBuf * static_cast<uint32_t>(N); // first A slot column
+  const uint32_t acc_cols = static_cast<uint32_t>(nt_acc_cols(N));
+  const uint32_t acol0 = kNtDBuf * acc_cols; // first A slot column
 
   if (warp == kNtCopyWarp) {
     // Copies: the neighbourhood's positions once (one bulk copy per leaf),
@@ -349,23 +363,21 @@ __global__ void __launch_bounds__(kNtThreads, kNtCtasPerSm) near_tc_kernel(const
       }
       ok = __shfl_sync(0xffffffffu, ok, 0);
       if (!ok) break;
-      int blk0 = a.zero_block, blk1 = a.zero_block;
-      {
-        const int g = 2 * i;
-        while (nbi + 1 < n_nb && nb_prefix[nbi + 1] <= g) ++nbi;
-        blk0 = nb_first[nbi] + (g - nb_prefix[nbi]);
-        if (g + 1 < n_blk) {
-          while (nbi + 1 < n_nb && nb_prefix[nbi + 1] <= g + 1) ++nbi;
-          blk1 = nb_first[nbi] + (g + 1 - nb_prefix[nbi]);
+      // block of this lane (lanes < kNtCB): neighbourhood block CB i + lane
+      int blk = a.zero_block;
+      for (int b = 0; b < kNtCB; ++b) {
+        const int g = kNtCB * i + b;
+        if (g < n_blk) {
+          while (nbi + 1 < n_nb && nb_prefix[nbi + 1] <= g) ++nbi;
+          if (lane == b) blk = nb_first[nbi] + (g - nb_prefix[nbi]);
         }
       }
       uint8_t *st = smem + static_cast<uint32_t>(s) * lay.slot_bytes;
-      if (lane == 0) mbar_expect_tx(&bfull[s], 2u * blk_bytes);
+      if (lane == 0) mbar_expect_tx(&bfull[s], kNtCB * blk_bytes);
       __syncwarp();
-      if (lane < 2) {
-        const size_t gb = static_cast<size_t>(lane ? blk1 : blk0);
-        bulk_g2s(st + static_cast<uint32_t>(lane) * blk_bytes, a.b_ops + gb * blk_bytes, blk_bytes, &bfull[s]);
-      }
+      if (lane < kNtCB)
+        bulk_g2s(st + static_cast<uint32_t>(lane) * blk_bytes, a.b_ops + static_cast<size_t>(blk) * blk_bytes, blk_bytes,
+                 &bfull[s]);
       __syncwarp();
       if (lane == 0) last_chunk[s] = i;
     }
@@ -399,15 +411,20 @@ __global__ void __launch_bounds__(kNtThreads, kNtCtasPerSm) near_tc_kernel(const
           break;
         }
         tc_fence_after();
-        const uint32_t dcol = tmem + static_cast<uint32_t>(2 * db * N);
+        const uint32_t dcol = tmem + static_cast<uint32_t>(db) * acc_cols;
         const uint64_t bd = desc0 + ((static_cast<uint32_t>(sb) * lay.slot_bytes) >> 4);
-        const uint32_t acol = tmem + acol0 + 48u * static_cast<uint32_t>(sa);
+        const uint32_t acol = tmem + acol0 + kNtAW * static_cast<uint32_t>(sa);
 #pragma unroll
-        for (int j = 0; j < 3; ++j) {
+        for (int j = 0; j < 3 * kNtCB / 2; ++j) {
           const uint64_t bj = bd + ((2u * static_cast<uint32_t>(j) * 32u * static_cast<uint32_t>(N)) >> 4);
           const uint32_t ah = acol + 8u * static_cast<uint32_t>(j);
-          const uint32_t al = ah + 24u;
-          mma_tf32_ts(dcol, ah, bj, idesc2, (first && j == 0) ? 0u : 1u);
+          const uint32_t al = ah + 12u * kNtCB;
+          if (kNtFuse) {
+            mma_tf32_ts(dcol, ah, bj, idesc2, (first && j == 0) ? 0u : 1u);
+          } else {
+            mma_tf32_ts(dcol, ah, bj, idesc, (first && j == 0) ? 0u : 1u);
+            mma_tf32_ts(dcol, ah, bj + ((16u * static_cast<uint32_t>(N)) >> 4), idesc, 1); // B_lo
+          }
           mma_tf32_ts(dcol, al, bj, idesc, 1);
         }
         mma_commit(&bempty[sb]);
@@ -444,10 +461,10 @@ __global__ void __launch_bounds__(kNtThreads, kNtCtasPerSm) near_tc_kernel(const
           const float4 q = spos[e];
           spos[e] = make_float4(q.x + nb_off[3 * n], q.y + nb_off[3 * n + 1], q.z + nb_off[3 * n + 2], q.w);
         }
-      if (at < 4) spos[4 * n_blk + at] = far_slot();
+      if (at < 4 * kNtCB) spos[4 * n_blk + at] = far_slot();
       agen_bar();
     }
-    float4 *scratch = spos + 4 * (kNtPosCap + 1) + 8 * warp; // this warp's 8 positions (unstaged)
+    float4 *scratch = spos + 4 * (kNtPosCap + kNtCB) + 8 * warp; // this warp's 8 positions (unstaged)
     for (int i = wg; ok && i < chunks; i += kNtWg) {
       const int sa = i % SA;
       // the MMAs that read this slot's previous A (chunk i - SA) have completed
@@ -461,37 +478,42 @@ __global__ void __launch_bounds__(kNtThreads, kNtCtasPerSm) near_tc_kernel(const
       go = __shfl_sync(0xffffffffu, go, 0);
       if (!go) break;
       tc_fence_after();
-      const float4 *p8 = spos + 8 * i;
-      if (!staged) {
-        // a neighbourhood beyond the staging capacity: lane q < 8 forms
-        // position q of the chunk from global memory
-        if (lane < 8) {
-          const int g = 2 * i + (lane >> 2);
-          float4 q = far_slot();
-          if (g < n_blk) {
-            int n = 0;
-            while (n + 1 < n_nb && nb_prefix[n + 1] <= g) ++n;
-            q = a.blk_pos[4LL * (nb_first[n] + (g - nb_prefix[n])) + (lane & 3)];
-            q = make_float4(q.x + nb_off[3 * n], q.y + nb_off[3 * n + 1], q.z + nb_off[3 * n + 2], q.w);
+      const uint32_t ta = tmem + lane_base + acol0 + kNtAW * static_cast<uint32_t>(sa);
+      // the chunk in sub-chunks of 8 sources (2 blocks): k columns 24 h ...
+      for (int h = 0; h < kNtCB / 2; ++h) {
+        const int g0 = kNtCB * i + 2 * h; // first block of the sub-chunk
+        const float4 *p8 = spos + 4 * g0;
+        if (!staged) {
+          // a neighbourhood beyond the staging capacity: lane q < 8 forms
+          // position q of the sub-chunk from global memory
+          if (lane < 8) {
+            const int g = g0 + (lane >> 2);
+            float4 q = far_slot();
+            if (g < n_blk) {
+              int n = 0;
+              while (n + 1 < n_nb && nb_prefix[n + 1] <= g) ++n;
+              q = a.blk_pos[4LL * (nb_first[n] + (g - nb_prefix[n])) + (lane & 3)];
+              q = make_float4(q.x + nb_off[3 * n], q.y + nb_off[3 * n + 1], q.z + nb_off[3 * n + 2], q.w);
+            }
+            scratch[lane] = q;
           }
-          scratch[lane] = q;
+          __syncwarp();
+          p8 = scratch;
         }
-        __syncwarp();
-        p8 = scratch;
+        float hv[24], lv[24];
+        switch (c) {
+        case 0: chunk_tensors<0>(p8, ntx, nty, ntz, self, hv, lv); break;
+        case 1: chunk_tensors<1>(p8, ntx, nty, ntz, self, hv, lv); break;
+        case 2: chunk_tensors<2>(p8, ntx, nty, ntz, self, hv, lv); break;
+        default: chunk_tensors<3>(p8, ntx, nty, ntz, self, hv, lv); break;
+        }
+        if (!staged) __syncwarp(); // scratch reads done before the next sub-chunk overwrites it
+        const uint32_t th = ta + 24u * static_cast<uint32_t>(h);
+        tmem_st16(th, hv);
+        tmem_st8(th + 16u, hv + 16);
+        tmem_st16(th + 12u * kNtCB, lv);
+        tmem_st8(th + 12u * kNtCB + 16u, lv + 16);
       }
-      float hv[24], lv[24];
-      switch (c) {
-      case 0: chunk_tensors<0>(p8, ntx, nty, ntz, self, hv, lv); break;
-      case 1: chunk_tensors<1>(p8, ntx, nty, ntz, self, hv, lv); break;
-      case 2: chunk_tensors<2>(p8, ntx, nty, ntz, self, hv, lv); break;
-      default: chunk_tensors<3>(p8, ntx, nty, ntz, self, hv, lv); break;
-      }
-      if (!staged) __syncwarp(); // scratch reads done before the next chunk overwrites it
-      const uint32_t ta = tmem + lane_base + acol0 + 48u * static_cast<uint32_t>(sa);
-      tmem_st16(ta, hv);
-      tmem_st8(ta + 16u, hv + 16);
-      tmem_st16(ta + 24u, lv);
-      tmem_st8(ta + 40u, lv + 16);
       tmem_wait_st();
       tc_fence_before();
       __syncwarp();
@@ -525,9 +547,9 @@ __global__ void __launch_bounds__(kNtThreads, kNtCtasPerSm) near_tc_kernel(const
       for (int q = 0; q < 4; ++q) {
         if (16 * q < N) {
 #pragma unroll
-          for (int h = 0; h < 2; ++h) {
+          for (int h = 0; h < (kNtFuse ? 2 : 1); ++h) {
             float v[16];
-            tmem_ld16(tmem + lane_base + static_cast<uint32_t>((2 * db + h) * N + 16 * q), v);
+            tmem_ld16(tmem + lane_base + static_cast<uint32_t>(db) * acc_cols + static_cast<uint32_t>(h * N + 16 * q), v);
 #pragma unroll
             for (int kk = 0; kk < 16; ++kk) acc[q][kk] += v[kk];
           }
