@@ -151,6 +151,10 @@ size_t p2p_corun_cta_smem(int K);
 // Position gradient of sum_k W_k . H_k, near part: partial sums per state
 // group, gpart[nt][p2p_grad_groups(K)] (normalised units, 1/(4 pi) applied).
 int p2p_grad_groups(int K);
+// The close-pair correction of the position gradient (added to gpart's
+// group 0), for a gradient computed by another near-field kernel.
+void launch_p2p_grad_close(const float4 *mom, const CloseGeometry &cg, const int *self_idx, int K, const float4 *W,
+                           float4 *gpart, cudaStream_t s);
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                      const int4 *work, int n_work, const int *self_idx, const CloseGeometry &cg, int depth, int K,
                      const float4 *W, float4 *gpart, cudaStream_t s, const CorunLaunch *corun = nullptr);

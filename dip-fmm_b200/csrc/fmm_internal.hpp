@@ -194,6 +194,14 @@ struct cdfmm_b200_plan {
   int4 *ntc_work = nullptr;
   int ntc_n_blocks = 0, ntc_n_work = 0;
   void *ntc_b = nullptr;
+  // tensor-core position gradient of the near field: blocks of 16 sources
+  bool ngt_supported = false;
+  bool ngt_built = false;
+  int *ngt_blk_off = nullptr;
+  int *ngt_blk_src = nullptr;
+  float4 *ngt_blk_pos = nullptr;
+  int ngt_n_blocks = 0;
+  void *ngt_b = nullptr;
 
   // operators (device)
   int *m2m_off = nullptr, *m2m_pair = nullptr; // pair = g | (in << 16)

@@ -1330,6 +1330,11 @@ void launch_p2p(const float4 *src_rel, const float4 *mom, const int *src_off,
 
 int p2p_grad_groups(int K) { return K >= 8 ? (K + 7) / 8 : (K + 3) / 4; }
 
+void launch_p2p_grad_close(const float4 *mom, const CloseGeometry &cg, const int *self_idx, int K, const float4 *W,
+                           float4 *gpart, cudaStream_t s) {
+  launch_close_correction<2>(mom, cg, self_idx, K, gpart, W, p2p_grad_groups(K), 0, K, 0, 1.0F, s);
+}
+
 void launch_p2p_grad(const float4 *src_rel, const float4 *mom, const int *src_off, const float4 *tgt_rel,
                      const int4 *work, int n_work, const int *self_idx, const CloseGeometry &cg, int depth, int K,
                      const float4 *W, float4 *gpart, cudaStream_t s, const CorunLaunch *corun) {

@@ -28,6 +28,7 @@
 #include "geometry.hpp"
 #include "kernels.cuh"
 #include "m2l_tc.hpp"
+#include "near_grad_tc.hpp"
 #include "near_tc.hpp"
 
 namespace {
@@ -121,7 +122,8 @@ void free_plan(cdfmm_b200_plan *p) {
                   p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
                   p->close_targets, p->close_r_fp32, p->close_r_exact, p->src_pos64, p->tgt_pos64,
                   p->src_size, p->src_size64, p->cuboid_T, p->cuboid_base, p->ntc_blk_off, p->ntc_blk_src,
-                  p->ntc_blk_pos, p->ntc_work, p->ntc_b};
+                  p->ntc_blk_pos, p->ntc_work, p->ntc_b, p->ngt_blk_off, p->ngt_blk_src, p->ngt_blk_pos,
+                  p->ngt_b};
   for (void *q : ptrs)
     if (q != nullptr) cudaFree(q);
   if (p->p2p_work_wide != nullptr && p->p2p_work_wide != p->p2p_work) cudaFree(p->p2p_work_wide);
@@ -662,6 +664,7 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
     }
     // tensor-core near field: sm_100 devices (layout and buffers on first use)
     plan->ntc_supported = major == 10 && configure_near_tc(smem);
+    plan->ngt_supported = plan->ntc_supported && configure_near_grad_tc(smem);
   }
   ops.m2l_T64.reset();
   // every set-up copy, memset and kernel (legacy default stream) is complete
@@ -1159,6 +1162,29 @@ static void ensure_near_tc(cdfmm_b200_plan *plan) {
   plan->stats.persistent_device_bytes += bytes;
   plan->stats.setup_h2d_bytes += h2d;
   plan->ntc_built = true;
+}
+
+// Blocks of 16 sources and the operand buffer of the tensor-core position
+// gradient (once per plan, on first use; its work units are the forward's).
+static void ensure_near_grad_tc(cdfmm_b200_plan *plan) {
+  ensure_near_tc(plan);
+  if (plan->ngt_built) return;
+  const NearGradLayout lay = near_grad_layout(plan->h_src_off.data(), plan->depth);
+  uint64_t bytes = 0, h2d = 0;
+  plan->ngt_blk_off = dalloc<int>(lay.blk_off.size(), bytes);
+  upload(plan->ngt_blk_off, lay.blk_off.data(), lay.blk_off.size(), h2d);
+  plan->ngt_blk_src = dalloc<int>(lay.blk_src.size(), bytes);
+  upload(plan->ngt_blk_src, lay.blk_src.data(), lay.blk_src.size(), h2d);
+  plan->ngt_blk_pos = dalloc<float4>(lay.blk_src.size(), bytes);
+  plan->ngt_b = dalloc<uint8_t>(near_grad_operand_bytes(lay.n_blocks, std::min(plan->max_states, kNearTcMaxStates)),
+                                bytes);
+  launch_near_grad_positions(plan->src_rel, plan->ngt_blk_src, lay.n_blocks, plan->ngt_blk_pos, plan->stream);
+  check(cudaGetLastError(), "kernel launch");
+  check(cudaStreamSynchronize(plan->stream), "near-field gradient blocks");
+  plan->ngt_n_blocks = lay.n_blocks;
+  plan->stats.persistent_device_bytes += bytes;
+  plan->stats.setup_h2d_bytes += h2d;
+  plan->ngt_built = true;
 }
 
 static NearTcLaunch near_tc_launch(const cdfmm_b200_plan *plan) {
@@ -1834,8 +1860,26 @@ int cdfmm_b200_backward(cdfmm_b200_plan *plan, const cdfmm_b200_backward_args *a
       // and far fields) measured 127.6 against 119.8 ms on the 1M-point
       // K = 64 bench workload.
       if (!reuse) enqueue_far(plan, K, s, false);
-      launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
-                      plan->has_self ? plan->self_idx : nullptr, close_geometry(plan), plan->depth, K, W, gpart, s);
+      if (plan->ngt_supported && near_on_tensor_cores(plan, K)) {
+        ensure_near_grad_tc(plan);
+        NearGradLaunch l{};
+        l.blk_pos = plan->ngt_blk_pos;
+        l.blk_off = plan->ngt_blk_off;
+        l.blk_src = plan->ngt_blk_src;
+        l.n_blocks = plan->ngt_n_blocks;
+        l.work = plan->ntc_work;
+        l.n_work = plan->ntc_n_work;
+        l.b_ops = plan->ngt_b;
+        l.error_flag = plan->error_flag;
+        l.wait_limit = plan->tc_wait_limit;
+        launch_near_grad_tc(l, plan->mom, plan->tgt_rel, plan->has_self ? plan->self_idx : nullptr, plan->depth, K, W,
+                            gpart, G, s);
+        launch_p2p_grad_close(plan->mom, close_geometry(plan), plan->has_self ? plan->self_idx : nullptr, K, W, gpart,
+                              s);
+      } else {
+        launch_p2p_grad(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, plan->p2p_work, plan->n_p2p_work,
+                        plan->has_self ? plan->self_idx : nullptr, close_geometry(plan), plan->depth, K, W, gpart, s);
+      }
       launch_l2p_grad(plan->L, plan->tgt_rel, plan->tgt_off, plan->tgt_perm, W, gpart, G, plan->n, plan->p, K,
                       plan->nt, plan->depth, static_cast<float>(1.0 / plan->scale), out, s);
       check(cudaGetLastError(), "kernel launch");

@@ -154,3 +154,39 @@ def test_set_near_mode_rejects_unknown_modes():
     with pytest.raises(ValueError, match="unknown near-field mode"):
         plan.set_near_mode(7)
     plan.close()
+
+
+@pytest.mark.parametrize("kind", ["uniform", "clusters"])
+def test_position_gradient_on_tensor_cores(kind):
+    """The backward's near-field position gradient on the tensor cores
+    (X = sum_k w_k m_k^T per pair as one matrix product over the states):
+    on a depth-1 tree (every pair near) against the FP64 direct gradient
+    summed over the states, within 3x the FP32 kernel's error and below
+    2e-6, and against the FP32 kernel to rounding level.  The moment
+    gradient (transposed evaluation) is unchanged by the near-field form up
+    to rounding."""
+    rng = np.random.default_rng(3)
+    n, K = 3000, 8
+    x = _points(kind, n, rng)
+    plan = cdfmm_b200.DevicePlan.from_points(x, 4, 1, max_states=K)
+    mm = rng.normal(size=(K, n, 3)).astype(np.float32)
+    ww = rng.normal(size=(K, n, 3)).astype(np.float32)
+    m, w = torch.from_numpy(mm).cuda(), torch.from_numpy(ww).cuda()
+    out = {}
+    for mode in (cdfmm_b200.NEAR_FP32, cdfmm_b200.NEAR_TF32X3):
+        plan.set_near_mode(mode)
+        gx = torch.full((n, 3), float("nan"), dtype=torch.float32, device="cuda")
+        gm = torch.full((K, n, 3), float("nan"), dtype=torch.float32, device="cuda")
+        plan.backward(w, moments=m, grad_moments=gm, grad_target_positions=gx, want_moments=True,
+                      want_positions=True, synchronize=True)
+        out[mode] = (gx.cpu().numpy(), gm.cpu().numpy())
+    ids = np.arange(n, dtype=np.int32)
+    ref = sum(cdfmm_b200.direct_grad_fp64(x, mm[k].astype(np.float64), x, ww[k].astype(np.float64), ids)
+              for k in range(K))
+    g32, gtc = out[cdfmm_b200.NEAR_FP32][0], out[cdfmm_b200.NEAR_TF32X3][0]
+    e32, etc = oracle.rel_l2(g32, ref), oracle.rel_l2(gtc, ref)
+    assert np.isfinite(gtc).all()
+    assert etc < 2e-6 and etc < 3.0 * e32, (etc, e32)
+    assert oracle.rel_l2(gtc, g32) < 2e-6
+    assert oracle.rel_l2(out[cdfmm_b200.NEAR_TF32X3][1], out[cdfmm_b200.NEAR_FP32][1]) < 2e-6
+    plan.close()
