@@ -386,8 +386,8 @@ int cdfmm_b200_set_schedule(cdfmm_b200_plan *plan, int32_t schedule);
  * at rounding level).  It takes the evaluations that compute every state in
  * one near-field pass on the device (cdfmm_b200_evaluate with device arrays,
  * or host arrays of fewer than 32 states; a backward pass's transposed
- * evaluation too); streamed host-array evaluations, the position-gradient
- * near field, cuboid sources and cdfmm_b200_evaluate_noalloc keep the FP32
+ * evaluation and its near-field position gradient too); streamed host-array
+ * evaluations, cuboid sources and cdfmm_b200_evaluate_noalloc keep the FP32
  * form.  Its
  * per-plan blocks and operand buffers (about 96 bytes per source and state)
  * are allocated on its first use. */
