@@ -49,6 +49,16 @@ constexpr int kNgRows = 3 * kNearGradSources; // 48 accumulator columns per chun
 constexpr int kNgBSlots = 3;
 constexpr int kNgPosCap = 96;         // neighbourhood blocks whose positions are staged
 constexpr uint32_t kNgMiscBytes = 640;
+// sources of the epilogue's loop unrolled at a time (code size vs ILP)
+#ifndef CDFMM_NGT_UNROLL
+#define CDFMM_NGT_UNROLL 16
+#endif
+constexpr int kNgUnroll = CDFMM_NGT_UNROLL;
+// epilogue rows: one run-time copy (1) or a template per row (0)
+#ifndef CDFMM_NGT_RUNTIME_ROW
+#define CDFMM_NGT_RUNTIME_ROW 1
+#endif
+constexpr bool kNgRuntimeRow = CDFMM_NGT_RUNTIME_ROW != 0;
 
 __host__ __device__ inline int ng_kpad(int K) { return (K + 7) / 8 * 8; }
 
@@ -119,10 +129,36 @@ __device__ __forceinline__ void pair_row_grad(float rx, float ry, float rz, floa
   g[2] = fmaf(f5, v2, fmaf(coef, rz, g[2]));
 }
 
+// The same with the row c chosen at run time (one copy of the unrolled loop
+// instead of three: a third of the code the epilogue streams through the
+// instruction cache).
+__device__ __forceinline__ void chunk_grad_any(int c, const float4 *p16, float tx, float ty, float tz, int self,
+                                               const float (&x)[kNgRows], float (&g)[3]) {
+  const float e0 = c == 0 ? 1.0F : 0.0F, e1 = c == 1 ? 1.0F : 0.0F, e2 = c == 2 ? 1.0F : 0.0F;
+#pragma unroll
+  for (int q = 0; q < kNearGradSources; ++q) {
+    const float4 p = p16[q];
+    const float rx = tx - p.x, ry = ty - p.y, rz = tz - p.z;
+    const float r2 = fmaf(rx, rx, fmaf(ry, ry, rz * rz));
+    const float rinv = __float_as_int(p.w) == self ? 0.0F : rsqrtf(r2);
+    const float r2inv = rinv * rinv;
+    const float f5 = 3.0F * r2inv * r2inv * rinv;
+    const float f7 = 5.0F * f5 * r2inv;
+    const float x0 = x[3 * q], x1 = x[3 * q + 1], x2 = x[3 * q + 2];
+    const float rc = fmaf(e0, rx, fmaf(e1, ry, e2 * rz));
+    const float xcc = fmaf(e0, x0, fmaf(e1, x1, e2 * x2));
+    const float xr = fmaf(x0, rx, fmaf(x1, ry, x2 * rz));
+    const float coef = fmaf(f5, xcc, -f7 * rc * xr);
+    g[0] = fmaf(f5, fmaf(rc, x0, e0 * xr), fmaf(coef, rx, g[0]));
+    g[1] = fmaf(f5, fmaf(rc, x1, e1 * xr), fmaf(coef, ry, g[1]));
+    g[2] = fmaf(f5, fmaf(rc, x2, e2 * xr), fmaf(coef, rz, g[2]));
+  }
+}
+
 template <int C>
 __device__ __forceinline__ void chunk_grad(const float4 *p16, float tx, float ty, float tz, int self,
                                            const float (&x)[kNgRows], float (&g)[3]) {
-#pragma unroll
+#pragma unroll kNgUnroll
   for (int q = 0; q < kNearGradSources; ++q) {
     const float4 p = p16[q];
     const float rx = tx - p.x, ry = ty - p.y, rz = tz - p.z;
@@ -384,7 +420,9 @@ __global__ void __launch_bounds__(kNgThreads, 2) near_grad_tc_kernel(const NgArg
         __syncwarp();
         p16 = scratch;
       }
-      if (c == 0)
+      if (kNgRuntimeRow)
+        chunk_grad_any(c, p16, tp.x, tp.y, tp.z, self, x, g);
+      else if (c == 0)
         chunk_grad<0>(p16, tp.x, tp.y, tp.z, self, x, g);
       else if (c == 1)
         chunk_grad<1>(p16, tp.x, tp.y, tp.z, self, x, g);
