@@ -190,3 +190,34 @@ def test_position_gradient_on_tensor_cores(kind):
     assert oracle.rel_l2(gtc, g32) < 2e-6
     assert oracle.rel_l2(out[cdfmm_b200.NEAR_TF32X3][1], out[cdfmm_b200.NEAR_FP32][1]) < 2e-6
     plan.close()
+
+
+def test_tensor_core_forms_across_state_counts_and_point_sets():
+    """One plan (max 64 states) called with K = 17 (padded to 32 MMA
+    columns), 64 and 8 in turn, targets distinct from the sources, depth 3
+    (neighbourhood positions staged in shared memory): field, potential and
+    position gradient of both near-field forms agree to rounding level on
+    every call."""
+    rng = np.random.default_rng(29)
+    ns, nt = 15000, 4000
+    src = rng.uniform(0, 1, (ns, 3))
+    tgt = rng.uniform(0, 1, (nt, 3))
+    plan = cdfmm_b200.DevicePlan.from_points(src, 4, 3, targets=tgt, root_centre=(0.5, 0.5, 0.5),
+                                             root_half_width=0.5, max_states=64)
+    for K in (17, 64, 8):
+        m = torch.from_numpy(rng.normal(size=(K, ns, 3)).astype(np.float32)).cuda()
+        w = torch.from_numpy(rng.normal(size=(K, nt, 3)).astype(np.float32)).cuda()
+        res = {}
+        for mode in (cdfmm_b200.NEAR_FP32, cdfmm_b200.NEAR_TF32X3):
+            H, phi, used = _evaluate(plan, m, mode)
+            assert used == (1 if mode == cdfmm_b200.NEAR_TF32X3 else 0)
+            gx = torch.full((nt, 3), float("nan"), dtype=torch.float32, device="cuda")
+            plan.backward(w, moments=m, grad_target_positions=gx, want_moments=False, want_positions=True,
+                          synchronize=True)
+            res[mode] = (H, phi, gx.cpu().numpy())
+        a, b = res[cdfmm_b200.NEAR_FP32], res[cdfmm_b200.NEAR_TF32X3]
+        assert np.isfinite(b[0]).all() and np.isfinite(b[2]).all()
+        assert oracle.rel_l2(b[0], a[0]) < 2e-6, K
+        assert oracle.rel_l2(b[1], a[1]) < 2e-6, K
+        assert oracle.rel_l2(b[2], a[2]) < 2e-6, K
+    plan.close()
