@@ -541,7 +541,12 @@ def b200_arm(args):
 
     peaks, peak_kind = load_peaks()
     n = (p + 1) * (p + 2) * (p + 3) // 6
-    m2l_flop = 2.0 * n * n * st["m2l_interactions"] * K
+    # the tensor-core M2L applies the traceless-reduced operator: (p+1)^2 - 1
+    # folded moments in, (p+1)^2 locals out (the other locals follow from the
+    # trace relations); the full-basis count 2 n^2 is kept beside it
+    m2l_full_flop = 2.0 * n * n * st["m2l_interactions"] * K
+    m2l_flop = (2.0 * ((p + 1) ** 2 - 1) * (p + 1) ** 2 * st["m2l_interactions"] * K if st["m2l_mode_resolved"] == 2
+                else m2l_full_flop)
     p2p_flop = (st["p2p_pairs"] - N) * (13.0 + 20.0 * K)
     near_key = "near_tc" if near_tc_used else "p2p"
     cand = {"m2l": (stages.get("m2l", 0.0), m2l_flop), near_key: (stages.get("p2p", 0.0), p2p_flop)}
@@ -550,7 +555,8 @@ def b200_arm(args):
     if dom == "m2l":
         peak = peaks.get("bf16_tflops_sustained", FALLBACK_PEAKS["bf16_tflops_sustained"])
         roofline = {"kernel": "m2l", "bound": "tensor", "unit": "TFLOP/s",
-                    "algorithmic_flop": m2l_flop, "peak_source": f"{peak_kind} bf16_tflops_sustained"}
+                    "algorithmic_flop": m2l_flop, "full_basis_flop": m2l_full_flop,
+                    "peak_source": f"{peak_kind} bf16_tflops_sustained"}
     elif dom == "near_tc":
         # TF32 MMAs run at half the BF16 rate on this part (nominal 1.1 vs
         # 2.25 PFLOP/s dense)

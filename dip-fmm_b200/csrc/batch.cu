@@ -104,6 +104,7 @@ TcArgs stacked_args(const cdfmm_b200_batch *b, const StackGroup &g) {
   ta.a_hi = static_cast<const uint8_t *>(g.a_hi);
   ta.a_lo = static_cast<const uint8_t *>(g.a_lo);
   ta.b_tiles = static_cast<const uint8_t *>(p0->tc_b);
+  set_m2l_reduction(ta, p0);
   ta.tiles = g.tiles;
   ta.scale_l = p0->scale_l;
   ta.L = nullptr;
@@ -129,7 +130,8 @@ TcArgs stacked_args(const cdfmm_b200_batch *b, const StackGroup &g) {
 void enqueue_stacked_m2l(const cdfmm_b200_batch *b, const StackGroup &g, cudaStream_t s) {
   const cdfmm_b200_plan *p0 = b->plans[static_cast<size_t>(g.members.front())];
   const int node_base = level_offset(2);
-  launch_m2l_pack(nullptr, p0->scale_m, p0->basis, g.a_hi, g.a_lo, p0->n, static_cast<int>(g.members.size()), g.Kp,
+  launch_m2l_pack(nullptr, p0->scale_m, p0->tc_fold_off, p0->tc_fold, p0->tc_n_in, g.a_hi, g.a_lo, p0->n,
+                  static_cast<int>(g.members.size()), g.Kp,
                   p0->tc_Kpad, p0->depth, node_base, p0->n_nodes - node_base, s, g.M_list);
   launch_m2l_tc(stacked_args(b, g), g.n_tiles, s);
 }
@@ -175,7 +177,8 @@ cudaError_t prepare_group(cdfmm_b200_batch *b, StackGroup &g) {
   // shape: the fastest candidate on this group's operands (the kernel
   // overwrites the members' locals, which the capture rewrites anyway)
   const int node_base = level_offset(2);
-  launch_m2l_pack(nullptr, p0->scale_m, p0->basis, g.a_hi, g.a_lo, p0->n, K, g.Kp, p0->tc_Kpad, p0->depth, node_base,
+  launch_m2l_pack(nullptr, p0->scale_m, p0->tc_fold_off, p0->tc_fold, p0->tc_n_in, g.a_hi, g.a_lo, p0->n, K, g.Kp,
+                  p0->tc_Kpad, p0->depth, node_base,
                   p0->n_nodes - node_base, g.stream, g.M_list);
   cudaEvent_t t0 = nullptr, t1 = nullptr;
   e = cudaEventCreate(&t0);

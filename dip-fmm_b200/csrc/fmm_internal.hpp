@@ -230,7 +230,9 @@ struct cdfmm_b200_plan {
   std::vector<TcShape> tc_candidates;     // pipeline shapes the autotuner tries
   uint32_t tc_tmem_cols = 0;
   void *tc_a_hi = nullptr, *tc_a_lo = nullptr; // [boxes + 1][Kp_max * Kpad] BF16
-  void *tc_b = nullptr;                        // [343][Kpad/32][2][Npad * 32] BF16
+  void *tc_b = nullptr;                        // [343][Kpad/32][2][Npad * 32] BF16 (reduced operator)
+  int *tc_fold_off = nullptr, *tc_fold = nullptr, *tc_expand = nullptr; // traceless reduction tables
+  int tc_n_in = 0, tc_n_out = 0, tc_n_derived = 0;
   int4 *tc_tiles = nullptr;
   size_t tc_tiles_capacity = 0;
   int tc_tiles_Kp = 0, tc_n_tiles = 0;

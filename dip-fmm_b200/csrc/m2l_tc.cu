@@ -97,7 +97,10 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
   const uint32_t b_bytes = static_cast<uint32_t>(args.Npad) * kKChunk * 2u;
   const uint32_t stage_bytes = 2u * a_bytes + 2u * b_bytes;
   uint8_t *stage0 = smem;
-  uint64_t *full = reinterpret_cast<uint64_t *>(smem + S * stage_bytes);
+  // the stages, reused after the last MMA by the epilogue's full-basis rows
+  const uint32_t epi_bytes = (128u * static_cast<uint32_t>(args.n) * 4u + 15u) & ~15u;
+  const uint32_t pipe_bytes = max(static_cast<uint32_t>(S) * stage_bytes, epi_bytes);
+  uint64_t *full = reinterpret_cast<uint64_t *>(smem + pipe_bytes);
   uint64_t *empty = full + S;
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(empty + S);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
@@ -298,9 +301,12 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     if (u >= 0) mbar_wait(&full[tid], static_cast<uint32_t>(u / S) & 1u);
   }
 
-  // Epilogue: warp w owns TMEM lanes 32w..32w+31 (rows of every M tile);
-  // scale by D_L and store.  After an expired wait the accumulators are
-  // incomplete: the tile's locals are written as NaN instead.
+  // Epilogue: warp w owns TMEM lanes 32w..32w+31 (rows of every M tile).
+  // A row's n_out reduced locals go to its column of the (now idle) stage
+  // memory at their full ranks, the other locals follow from the trace
+  // relations, and all n are scaled by D_L and stored.  After an expired
+  // wait the accumulators are incomplete: the tile's locals are written as
+  // NaN instead.
   if (*abort_flag != 0) {
     const int tr = tid / args.Kp;
     const int k = tid - tr * args.Kp;
@@ -322,6 +328,7 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
     const int tr = row / args.Kp;
     const int k = row - tr * args.Kp;
     const float *sl = args.scale_l + level * args.n;
+    float *const ep = reinterpret_cast<float *>(smem) + tid; // this row's locals, stride kTcThreads floats
     for (int m = 0; m < m_active; ++m) {
       const int tt = m * T + tr;
       const bool valid = tr < T && tt < count && k < args.K;
@@ -343,17 +350,21 @@ __global__ void __launch_bounds__(kTcThreads, 1) m2l_tc_kernel(const TcArgs args
 #pragma unroll
           for (int j = 0; j < 16; ++j) v[j] = 0.0F; // no source box in the grid: no MMA wrote the accumulator
         }
-        if (valid) {
 #pragma unroll
-          for (int j = 0; j < 16; ++j) {
-            const int b = c0 + j;
-            if (b < args.n) {
-              if (out_k != nullptr)
-                out_k[b] = v[j] * sl[b];
-              else
-                args.L[base + static_cast<long long>(b) * args.K] = v[j] * sl[b];
-            }
-          }
+        for (int j = 0; j < 16; ++j)
+          if (c0 + j < args.n_out) ep[__ldg(args.expand + c0 + j) * kTcThreads] = v[j];
+      }
+      for (int i = 0; i < args.n_derived; ++i) {
+        const int e = __ldg(args.expand + args.n_out + i);
+        ep[(e & 1023) * kTcThreads] = -(ep[((e >> 10) & 1023) * kTcThreads] + ep[(e >> 20) * kTcThreads]);
+      }
+      if (valid) {
+        for (int b = 0; b < args.n; ++b) {
+          const float x = ep[b * kTcThreads] * sl[b];
+          if (out_k != nullptr)
+            out_k[b] = x;
+          else
+            args.L[base + static_cast<long long>(b) * args.K] = x;
         }
       }
     }
@@ -380,6 +391,8 @@ constexpr int kPackMaxKp = 128;
 __global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__restrict__ M,
                                                                 const float *const *__restrict__ M_list,
                                                                 const float *__restrict__ scale_m,
+                                                                const int *__restrict__ fold_off,
+                                                                const int *__restrict__ fold, int n_in,
                                                                 uint4 *__restrict__ hi, uint4 *__restrict__ lo, int n,
                                                                 int K, int Kp, int Kpad, int depth, int node_base,
                                                                 int n_boxes) {
@@ -399,13 +412,23 @@ __global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__r
     for (int e = tid; e < w * Kp; e += kPackThreads) {
       const int al = e / Kp;
       const int k = e - al * Kp;
-      const int a = kc * kKChunk + al;
-      // padding alphas (a >= n), padding states (k >= K) and the zero box are
-      // zero; scale_m holds n entries per level (no padding)
+      const int j = kc * kKChunk + al;
+      // folded input j: sum of c M_a over its fold entries (all of one
+      // degree, the first one its own rank), then scaled (scale_m is one
+      // power of two per degree).  Padding inputs (j >= n_in), padding
+      // states (k >= K) and the zero box are zero.
       float m = 0.0F;
-      if (box < n_boxes && a < n && k < K)
-        m = (M_list != nullptr ? M_list[k][static_cast<long long>(node) * n + a] : src[static_cast<long long>(a) * K + k]) *
-            scale_m[level * n + a];
+      if (box < n_boxes && j < n_in && k < K) {
+        const int f0 = __ldg(fold_off + j), f1 = __ldg(fold_off + j + 1);
+        for (int f = f0; f < f1; ++f) {
+          const int ent = __ldg(fold + f);
+          const int a = ent & 0xffff;
+          const float x =
+              M_list != nullptr ? M_list[k][static_cast<long long>(node) * n + a] : src[static_cast<long long>(a) * K + k];
+          m = fmaf(static_cast<float>((ent >> 16) - 64), x, m);
+        }
+        m *= scale_m[level * n + (__ldg(fold + f0) & 0xffff)];
+      }
       tile[al][k] = m;
     }
     __syncthreads();
@@ -433,26 +456,26 @@ __global__ void __launch_bounds__(kPackThreads) m2l_pack_kernel(const float *__r
 
 } // namespace
 
-size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages) {
+size_t m2l_tc_smem_bytes(int Npad, int m_tiles, int stages, int n) {
   const size_t a = 128u * kKChunk * 2u * static_cast<size_t>(m_tiles);
   const size_t b = static_cast<size_t>(Npad) * kKChunk * 2u;
-  return static_cast<size_t>(stages) * (2 * a + 2 * b) + 2 * stages * sizeof(uint64_t) + 8 +
+  const size_t epi = (static_cast<size_t>(kTcThreads) * n * 4u + 15u) & ~static_cast<size_t>(15);
+  return std::max(static_cast<size_t>(stages) * (2 * a + 2 * b), epi) + 2 * stages * sizeof(uint64_t) + 8 +
          (2 * kTcMaxTargets + 216 + 1 + 8) * sizeof(int);
 }
 
-void launch_m2l_pack(const float *M, const float *scale_m, const int8_t *basis, void *hi, void *lo, int n, int K,
-                     int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s,
+void launch_m2l_pack(const float *M, const float *scale_m, const int *fold_off, const int *fold, int n_in, void *hi,
+                     void *lo, int n, int K, int Kp, int Kpad, int depth, int node_base, int n_boxes, cudaStream_t s,
                      const float *const *M_list) {
-  (void)basis;
   if (Kp > kPackMaxKp || Kp % 8 != 0 || Kpad % 16 != 0) return; // the plan keeps Kp <= 128, multiples of 8
-  m2l_pack_kernel<<<n_boxes + 1, kPackThreads, 0, s>>>(M, M_list, scale_m, static_cast<uint4 *>(hi),
-                                                        static_cast<uint4 *>(lo), n, K, Kp, Kpad, depth, node_base,
-                                                        n_boxes);
+  m2l_pack_kernel<<<n_boxes + 1, kPackThreads, 0, s>>>(M, M_list, scale_m, fold_off, fold, n_in,
+                                                        static_cast<uint4 *>(hi), static_cast<uint4 *>(lo), n, K, Kp,
+                                                        Kpad, depth, node_base, n_boxes);
 }
 
 void launch_m2l_tc(const TcArgs &args, int n_tiles, cudaStream_t s) {
   if (n_tiles == 0) return;
-  size_t smem = m2l_tc_smem_bytes(args.Npad, args.m_tiles, args.stages);
+  size_t smem = m2l_tc_smem_bytes(args.Npad, args.m_tiles, args.stages, args.n);
   // More than half of TMEM per CTA: request enough shared memory that a
   // second CTA never shares the SM (its tcgen05.alloc would wait for ours).
   if (args.tmem_cols > 256) smem = std::max<size_t>(smem, 120 * 1024);
@@ -491,7 +514,8 @@ bool configure_m2l_tc(size_t max_smem) {
 // Host: B tiles [slot][alpha chunk][hi, lo][Npad x 32 stride] BF16 from FP64
 // matrices T[slot][alpha][beta] (symmetric in alpha, beta); a chunk of width w
 // is stored as [beta group][w/8 column blocks][8 betas][8 alphas].
-std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, int Npad, int Kpad) {
+std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, const M2lTraceless &red, int Npad,
+                                       int Kpad) {
   const int nkc = (Kpad + kKChunk - 1) / kKChunk;
   const size_t btile = static_cast<size_t>(Npad) * kKChunk;
   std::vector<uint16_t> out(static_cast<size_t>(343) * nkc * 2 * btile, 0);
@@ -503,9 +527,11 @@ std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, in
   };
   for (int slot = 0; slot < 343; ++slot) {
     const double *Ts = T64.data() + static_cast<size_t>(slot) * n * n;
-    for (int beta = 0; beta < n; ++beta)
-      for (int alpha = 0; alpha < n; ++alpha) {
-        const double v = Ts[static_cast<size_t>(alpha) * n + beta];
+    const int n_out = static_cast<int>(red.out_set.size()), n_in = static_cast<int>(red.in_set.size());
+    for (int beta = 0; beta < n_out; ++beta)
+      for (int alpha = 0; alpha < n_in; ++alpha) {
+        const double v = Ts[static_cast<size_t>(red.in_set[static_cast<size_t>(alpha)]) * n +
+                            red.out_set[static_cast<size_t>(beta)]];
         const __nv_bfloat16 h = __float2bfloat16_rn(static_cast<float>(v));
         const float l = static_cast<float>(v - static_cast<double>(__bfloat162float(h)));
         const int kc = alpha / kKChunk;
@@ -519,6 +545,67 @@ std::vector<uint16_t> pack_m2l_b_tiles(const std::vector<double> &T64, int n, in
       }
   }
   return out;
+}
+
+M2lTraceless m2l_traceless(int p) {
+  const int n = basis_size_d(p);
+  std::vector<int> ex(static_cast<size_t>(n)), ey(static_cast<size_t>(n)), ez(static_cast<size_t>(n));
+  for (int d = 0; d <= p; ++d)
+    for (int a = 0; a <= d; ++a)
+      for (int b = 0; a + b <= d; ++b) {
+        const size_t r = static_cast<size_t>(rank3(a, b, d - a - b));
+        ex[r] = a;
+        ey[r] = b;
+        ez[r] = d - a - b;
+      }
+  M2lTraceless t;
+  std::vector<int> in_pos(static_cast<size_t>(n), -1);
+  for (int r = 0; r < n; ++r) {
+    if (ez[static_cast<size_t>(r)] > 1) continue;
+    t.out_set.push_back(r);
+    if (r > 0) {
+      in_pos[static_cast<size_t>(r)] = static_cast<int>(t.in_set.size());
+      t.in_set.push_back(r);
+    }
+  }
+  // fold every moment a >= 1 onto the reduced inputs: repeatedly move the
+  // weight on an exponent with z >= 2 to (x + 2, z - 2) and (y + 2, z - 2)
+  // with the sign flipped, from the highest z down
+  std::vector<std::vector<std::pair<int, int>>> per_in(t.in_set.size());
+  for (int a = 1; a < n; ++a) {
+    std::vector<int> w(static_cast<size_t>(n), 0);
+    w[static_cast<size_t>(a)] = 1;
+    for (int z = p; z >= 2; --z)
+      for (int r = 0; r < n; ++r) {
+        const size_t rr = static_cast<size_t>(r);
+        if (ez[rr] != z || w[rr] == 0) continue;
+        w[static_cast<size_t>(rank3(ex[rr] + 2, ey[rr], z - 2))] -= w[rr];
+        w[static_cast<size_t>(rank3(ex[rr], ey[rr] + 2, z - 2))] -= w[rr];
+        w[rr] = 0;
+      }
+    for (int r = 0; r < n; ++r)
+      if (w[static_cast<size_t>(r)] != 0) per_in[static_cast<size_t>(in_pos[static_cast<size_t>(r)])].push_back({a, w[static_cast<size_t>(r)]});
+  }
+  t.fold_off.push_back(0);
+  for (size_t j = 0; j < per_in.size(); ++j) {
+    // its own rank first (coefficient 1), then the folded ranks ascending
+    std::stable_sort(per_in[j].begin(), per_in[j].end(), [&](const std::pair<int, int> &x, const std::pair<int, int> &y) {
+      const bool xs = x.first == t.in_set[j], ys = y.first == t.in_set[j];
+      return xs != ys ? xs : x.first < y.first;
+    });
+    for (const auto &e : per_in[j]) t.fold.push_back(e.first | ((e.second + 64) << 16));
+    t.fold_off.push_back(static_cast<int>(t.fold.size()));
+  }
+  t.expand = t.out_set;
+  for (int z = 2; z <= p; ++z)
+    for (int r = 0; r < n; ++r) {
+      const size_t rr = static_cast<size_t>(r);
+      if (ez[rr] != z) continue;
+      const int s1 = rank3(ex[rr] + 2, ey[rr], z - 2), s2 = rank3(ex[rr], ey[rr] + 2, z - 2);
+      t.expand.push_back(r | (s1 << 10) | (s2 << 20));
+      ++t.n_derived;
+    }
+  return t;
 }
 
 } // namespace cdfmm_b200

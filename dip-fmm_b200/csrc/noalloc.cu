@@ -186,11 +186,13 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   for (int level = plan->depth - 1; level >= 0; --level)
     launch_m2m(M, plan->m2m_off, plan->m2m_pair, plan->m2m_coef, n, K, level, static_cast<int>(plan->ops.m2m_pair_g.size()), s);
   if (use_tc) {
-    launch_m2l_pack(M, plan->scale_m, plan->basis, a_hi, a_lo, n, K, Kp, plan->tc_Kpad, plan->depth, node_base, boxes, s);
+    launch_m2l_pack(M, plan->scale_m, plan->tc_fold_off, plan->tc_fold, plan->tc_n_in, a_hi, a_lo, n, K, Kp,
+                    plan->tc_Kpad, plan->depth, node_base, boxes, s);
     TcArgs ta{};
     ta.a_hi = static_cast<const uint8_t *>(a_hi);
     ta.a_lo = static_cast<const uint8_t *>(a_lo);
     ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b);
+    set_m2l_reduction(ta, plan);
     ta.tiles = dtiles;
     ta.scale_l = plan->scale_l;
     ta.L = L;

@@ -119,7 +119,7 @@ void free_plan(cdfmm_b200_plan *p) {
                   p->self_idx, p->leaf_self, p->p2p_work, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
-                  p->tc_b, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
+                  p->tc_b, p->tc_fold_off, p->tc_fold, p->tc_expand, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
                   p->close_targets, p->close_r_fp32, p->close_r_exact, p->src_pos64, p->tgt_pos64,
                   p->src_size, p->src_size64, p->cuboid_T, p->cuboid_base, p->ntc_blk_off, p->ntc_blk_src,
                   p->ntc_blk_pos, p->ntc_work, p->ntc_b, p->ngt_blk_off, p->ngt_blk_src, p->ngt_blk_pos,
@@ -303,13 +303,13 @@ static size_t corun_m2l_smem_budget(const cdfmm_b200_plan *plan, int K);
 
 // BF16 hi/lo B tiles of the tensor-core M2L per (order, Npad, Kpad), packed
 // once per process and shared by the plans of that order.
-static std::shared_ptr<const std::vector<uint16_t>> packed_b_tiles(int p, const HostOperators &ops, int Npad,
-                                                                    int Kpad) {
+static std::shared_ptr<const std::vector<uint16_t>> packed_b_tiles(int p, const HostOperators &ops,
+                                                                    const M2lTraceless &red, int Npad, int Kpad) {
   static std::mutex mutex;
   static std::map<std::tuple<int, int, int>, std::shared_ptr<const std::vector<uint16_t>>> cache;
   std::lock_guard<std::mutex> lock(mutex);
   auto &slot = cache[std::make_tuple(p, Npad, Kpad)];
-  if (!slot) slot = std::make_shared<const std::vector<uint16_t>>(pack_m2l_b_tiles(*ops.m2l_T64, ops.n, Npad, Kpad));
+  if (!slot) slot = std::make_shared<const std::vector<uint16_t>>(pack_m2l_b_tiles(*ops.m2l_T64, ops.n, red, Npad, Kpad));
   return slot;
 }
 
@@ -590,13 +590,17 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
   plan->tc_wait_limit = kTcWaitLimit;
 
   lap(plan->stats.setup_ms_buffers);
-  // Tensor-core M2L: sm_100 devices, order <= 9 (N = 16 * ceil(n/16) <= 256
-  // accumulator columns) and at least one pipeline stage in shared memory.
+  // Tensor-core M2L: sm_100 devices and at least two pipeline stages in
+  // shared memory (the traceless operator's N = 16 ceil((p+1)^2 / 16) <= 128
+  // accumulator columns for every order up to 10).  AUTO keeps order 10 on
+  // the FP32 SIMT M2L, whose products are exact FP32.
   {
     int major = 0;
     cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, plan->device);
-    const int Kpad = round_up(n, 16);
-    const int Npad = round_up(n, 16);
+    // traceless reduction: (p+1)^2 - 1 folded moments in, (p+1)^2 locals out
+    const M2lTraceless red = m2l_traceless(plan->p);
+    const int Kpad = std::max(16, round_up(static_cast<int>(red.in_set.size()), 16));
+    const int Npad = round_up(static_cast<int>(red.out_set.size()), 16);
     // Pipeline shapes: 1, 2 or 4 128-row accumulators per CTA sharing each
     // B tile, with as many stages as fit one CTA per SM, or half / a third
     // of that for two / three CTAs per SM; each with the three products as
@@ -609,7 +613,7 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
     auto acc_stride_of = [&](int fuse) { return round_up(fuse ? 2 * Npad : Npad, 32); };
     auto max_stages = [&](int mt, size_t budget) {
       int st = 0;
-      while (st < 8 && m2l_tc_smem_bytes(Npad, mt, st + 1) <= budget) ++st;
+      while (st < 8 && m2l_tc_smem_bytes(Npad, mt, st + 1, n) <= budget) ++st;
       return st;
     };
     const size_t one_cta = std::min<size_t>(smem, 224 * 1024), two_cta = 112 * 1024, three_cta = 74 * 1024;
@@ -639,7 +643,7 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
     // than 8 states fill 8-row groups of the MMA tile with zero rows: the
     // tensor cores still beat the FP32 SIMT M2L several times over);
     // FP32 keeps the SIMT M2L (the plain per-state path).
-    const bool wanted = m2l_mode == CDFMM_B200_M2L_BF16X3 || m2l_mode == CDFMM_B200_M2L_AUTO;
+    const bool wanted = m2l_mode == CDFMM_B200_M2L_BF16X3 || (m2l_mode == CDFMM_B200_M2L_AUTO && plan->p <= 9);
     plan->tc_supported = major == 10 && plan->depth >= 2 && Npad <= 256 && stages >= 2 && wanted &&
                          configure_m2l_tc(smem);
     if (plan->tc_supported) {
@@ -655,12 +659,21 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
       const size_t box_elems = static_cast<size_t>(plan->tc_Kp_max) * Kpad;
       plan->tc_a_hi = dalloc<uint16_t>(boxes * box_elems, bytes);
       plan->tc_a_lo = dalloc<uint16_t>(boxes * box_elems, bytes);
-      const std::shared_ptr<const std::vector<uint16_t>> bt = packed_b_tiles(plan->p, ops, Npad, Kpad);
+      const std::shared_ptr<const std::vector<uint16_t>> bt = packed_b_tiles(plan->p, ops, red, Npad, Kpad);
       plan->tc_b = dalloc<uint16_t>(bt->size(), bytes);
       upload(static_cast<uint16_t *>(plan->tc_b), bt->data(), bt->size(), h2d);
+      plan->tc_n_in = static_cast<int>(red.in_set.size());
+      plan->tc_n_out = static_cast<int>(red.out_set.size());
+      plan->tc_n_derived = red.n_derived;
+      plan->tc_fold_off = dalloc<int>(red.fold_off.size(), bytes);
+      upload(plan->tc_fold_off, red.fold_off.data(), red.fold_off.size(), h2d);
+      plan->tc_fold = dalloc<int>(std::max<size_t>(red.fold.size(), 1), bytes);
+      upload(plan->tc_fold, red.fold.data(), red.fold.size(), h2d);
+      plan->tc_expand = dalloc<int>(red.expand.size(), bytes);
+      upload(plan->tc_expand, red.expand.data(), red.expand.size(), h2d);
     } else if (m2l_mode == CDFMM_B200_M2L_BF16X3) {
       throw AbiError(CDFMM_B200_ERR_RUNTIME,
-                     "split-BF16 tensor-core M2L needs an sm_100 device, depth >= 2 and order <= 9");
+                     "split-BF16 tensor-core M2L needs an sm_100 device and depth >= 2");
     }
     // tensor-core near field: sm_100 devices (layout and buffers on first use)
     plan->ntc_supported = major == 10 && configure_near_tc(smem);
@@ -1048,7 +1061,7 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s, size_t sme
   TcArgs ta{};
   ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
   ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
-  ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b);
+  ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b); set_m2l_reduction(ta, plan);
   ta.scale_l = plan->scale_l;
   ta.L = plan->L;
   ta.error_flag = plan->error_flag;
@@ -1066,7 +1079,7 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s, size_t sme
   // candidates within the budget (all of them if none fits)
   auto launch_smem = [&](const cdfmm_b200_plan::TcShape &c) {
     const int acc = round_up(c.fuse ? 2 * plan->tc_Npad : plan->tc_Npad, 32);
-    size_t b = m2l_tc_smem_bytes(plan->tc_Npad, c.m_tiles, c.stages);
+    size_t b = m2l_tc_smem_bytes(plan->tc_Npad, c.m_tiles, c.stages, plan->n);
     if (tmem_columns(c.m_tiles, acc) > 256) b = std::max<size_t>(b, 120 * 1024);
     return b;
   };
@@ -1239,7 +1252,8 @@ static int prepare_m2l(cdfmm_b200_plan *plan, int K, cudaStream_t s) {
   const int Kp = round_up(K, 8);
   const int node_base = level_offset(2);
   const int boxes = plan->n_nodes - node_base;
-  launch_m2l_pack(plan->M, plan->scale_m, plan->basis, plan->tc_a_hi, plan->tc_a_lo, plan->n, K, Kp, plan->tc_Kpad,
+  launch_m2l_pack(plan->M, plan->scale_m, plan->tc_fold_off, plan->tc_fold, plan->tc_n_in, plan->tc_a_hi, plan->tc_a_lo,
+                  plan->n, K, Kp, plan->tc_Kpad,
                   plan->depth, node_base, boxes, s);
   if (plan->tc_tiles_Kp != Kp || (!plan->tc_pinned && plan->tc_tuned_budget != smem_budget)) {
     check(cudaStreamSynchronize(s), "sync");
@@ -1265,7 +1279,7 @@ static int enqueue_downward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool t
       TcArgs ta{};
       ta.a_hi = static_cast<const uint8_t *>(plan->tc_a_hi);
       ta.a_lo = static_cast<const uint8_t *>(plan->tc_a_lo);
-      ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b);
+      ta.b_tiles = static_cast<const uint8_t *>(plan->tc_b); set_m2l_reduction(ta, plan);
       ta.tiles = plan->tc_tiles;
       ta.scale_l = plan->scale_l;
       ta.L = plan->L;

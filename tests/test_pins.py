@@ -5,10 +5,11 @@ from the reference's CpuStatic FP32 / FP64 backends and FP64 direct sum):
   - the host tree at depth 5 and at the headline size (N = 1,048,576), bit
     for bit (SHA-256 of the permutations and node ranges);
   - p = 8 on a jittered lattice (8 per leaf), where the tensor-core M2L runs
-    its p = 8 shape (n = 165 padded to 176, no fused hi/lo MMA);
+    its p = 8 shape (80 folded moments, 81 locals padded to 96);
   - depth 5 at p = 6 (the level that carries 90 % of the bench's M2L work);
-  - p = 9 (the largest tensor-core shape, n = 220 padded to 224) and p = 10
-    (FP32 SIMT M2L only);
+  - p = 9 (the largest shape the tensor-core M2L takes by default: the
+    traceless operator's 99 folded moments padded to 112, 100 locals padded
+    to 112) and p = 10 (FP32 SIMT M2L by default; split BF16 on request);
   - the bench's batched split-precision workload (64^3 lattice, p = 8,
     depth 5, K = 64): its error against the FP64 direct sum is the p = 8
     expansion's own, equal to the reference FP64 FMM's;
@@ -165,8 +166,15 @@ def test_tensor_core_m2l_at_high_order_matches_reference(name):
 def test_order_10_runs_the_fp32_m2l_and_matches_reference():
     g, x, m, order, depth, sample = golden_inputs("small_p10_d3")
     tree = tree_of(x, depth)
-    with pytest.raises(cdfmm_b200.CdfmmError, match="order <= 9"):
-        device_plan(tree, order, 8, m2l=cdfmm_b200.M2L_BF16X3)
+    # split BF16 on request: 120 folded moments, 121 locals (both padded to 128)
+    plan = device_plan(tree, order, 8, m2l=cdfmm_b200.M2L_BF16X3)
+    H, phi = evaluate_copies(plan, m)
+    assert plan.stats()["m2l_mode_resolved"] == cdfmm_b200.M2L_BF16X3
+    plan.close()
+    check_scaled_copies(H, phi)
+    for k in (0, 7):
+        assert_fp32_parity(H[k] / SCALES[k], phi[k] / SCALES[k], g, sample)
+    # AUTO: the FP32 SIMT M2L
     plan = device_plan(tree, order, 8)
     H, phi = evaluate_copies(plan, m)
     st = plan.stats()
