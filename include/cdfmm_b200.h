@@ -49,9 +49,11 @@ extern "C" {
 #define CDFMM_B200_OUTPUT_FIELD 2u
 
 /* M2L arithmetic. */
-#define CDFMM_B200_M2L_AUTO 0        /* split-BF16 tensor cores where supported (any K), else FP32 */
+#define CDFMM_B200_M2L_AUTO 0        /* split-BF16 tensor cores on sm_100, depth >= 2, order <= 9 (any K), else FP32 */
 #define CDFMM_B200_M2L_FP32 1        /* FP32 SIMT (the plain per-state path) */
-#define CDFMM_B200_M2L_BF16X3 2      /* tcgen05, BF16 hi/lo with three products, FP32 accumulate */
+#define CDFMM_B200_M2L_BF16X3 2      /* tcgen05, BF16 hi/lo with three products, FP32 accumulate; applies the
+                                        traceless-reduced operator ((p+1)^2 - 1 folded moments in, (p+1)^2
+                                        locals out, the rest from the trace relations); any order */
 
 /* Near-field arithmetic of evaluations of 8..128 states (cdfmm_b200_set_near_mode). */
 #define CDFMM_B200_NEAR_AUTO 0       /* tensor cores where supported, else FP32 */
