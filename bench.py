@@ -561,9 +561,14 @@ def b200_arm(args):
         # TF32 MMAs run at half the BF16 rate on this part (nominal 1.1 vs
         # 2.25 PFLOP/s dense)
         peak = 0.5 * peaks.get("bf16_tflops_sustained", FALLBACK_PEAKS["bf16_tflops_sustained"])
+        # issued tensor work: 128 rows x 3 split products x the units' padded
+        # reduction length x the states padded to 16
+        issued = 2.0 * 128 * 3 * st["near_tc_k_cols"] * (16 * ((K + 15) // 16))
         roofline = {"kernel": "near_tc", "bound": "tensor", "unit": "TFLOP/s", "algorithmic_flop": p2p_flop,
                     "peak_source": f"{peak_kind} bf16_tflops_sustained / 2 (TF32 rate)",
-                    "fp32_fma_frac": p2p_flop / (ms_dom * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS if ms_dom > 0 else None}
+                    "fp32_fma_frac": p2p_flop / (ms_dom * 1e-3) / 1e12 / FP32_NOMINAL_TFLOPS if ms_dom > 0 else None,
+                    "issued_flop": issued,
+                    "issued_frac": issued / (ms_dom * 1e-3) / 1e12 / peak if ms_dom > 0 else None}
     else:
         peak = FP32_NOMINAL_TFLOPS
         roofline = {"kernel": "p2p", "bound": "fp32", "unit": "TFLOP/s", "algorithmic_flop": p2p_flop,

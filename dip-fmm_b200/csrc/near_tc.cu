@@ -703,8 +703,10 @@ NearTcLayout near_tc_layout(const int *src_off, const int *tgt_off, int depth) {
           const uint32_t m = morton3(static_cast<uint32_t>(x), static_cast<uint32_t>(y), static_cast<uint32_t>(z));
           cost += lay.blk_off[m + 1] - lay.blk_off[m];
         }
-    for (int t = 0; t < tn; t += kNearTcTargets)
+    for (int t = 0; t < tn; t += kNearTcTargets) {
       lay.work.push_back(make_int4(l, tgt_off[l] + t, std::min(kNearTcTargets, tn - t), cost));
+      lay.k_cols += 3u * 4u * static_cast<uint64_t>(kNtCB) * static_cast<uint64_t>((cost + kNtCB - 1) / kNtCB);
+    }
   }
   return lay;
 }

@@ -24,6 +24,7 @@ struct NearTcLayout {
   std::vector<int> blk_src; // [(n_blocks + 1) * 4] sorted source index of each slot, -1: empty
   std::vector<int4> work;   // (leaf, first target, targets <= 32, neighbourhood blocks) in leaf order
   int n_blocks = 0;         // block n_blocks is the all-empty block
+  uint64_t k_cols = 0;      // sum over units of the MMA reduction length (3 x chunk-padded sources)
 };
 NearTcLayout near_tc_layout(const int *src_off, const int *tgt_off, int depth);
 

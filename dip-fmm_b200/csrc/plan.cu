@@ -1176,6 +1176,7 @@ static void ensure_near_tc(cdfmm_b200_plan *plan) {
   check(cudaStreamSynchronize(plan->stream), "near-field blocks");
   plan->ntc_n_blocks = lay.n_blocks;
   plan->ntc_n_work = static_cast<int>(lay.work.size());
+  plan->stats.near_tc_k_cols = lay.k_cols;
   plan->stats.persistent_device_bytes += bytes;
   plan->stats.setup_h2d_bytes += h2d;
   plan->ntc_built = true;

@@ -120,6 +120,7 @@ class Stats(ctypes.Structure):
         ("setup_ms_near", ctypes.c_double), ("setup_ms_operators", ctypes.c_double),
         ("setup_ms_statistics", ctypes.c_double), ("setup_ms_buffers", ctypes.c_double),
         ("setup_ms_m2l", ctypes.c_double), ("setup_ms_total", ctypes.c_double),
+        ("near_tc_k_cols", ctypes.c_uint64),
     ]
 
     def as_dict(self):

@@ -149,6 +149,11 @@ typedef struct cdfmm_b200_stats {
    * tensor-core M2L set-up, and the whole call. */
   double setup_ms_tree, setup_ms_geometry, setup_ms_near, setup_ms_operators, setup_ms_statistics,
       setup_ms_buffers, setup_ms_m2l, setup_ms_total;
+  /* Tensor-core near field (set when its layout is built): the sum over work
+   * units of the MMA reduction length, 3 x the unit's sources padded to whole
+   * chunks.  Issued tensor work per evaluation = 2 x 128 rows x 3 products x
+   * near_tc_k_cols x 16 ceil(K / 16) FLOP. */
+  uint64_t near_tc_k_cols;
 } cdfmm_b200_stats;
 
 /* Library / device probing.  Returns OK and *count = 0 when no device. */
