@@ -231,6 +231,7 @@ struct cdfmm_b200_plan {
   uint32_t tc_tmem_cols = 0;
   void *tc_a_hi = nullptr, *tc_a_lo = nullptr; // [boxes + 1][Kp_max * Kpad] BF16
   void *tc_b = nullptr;                        // [343][Kpad/32][2][Npad * 32] BF16 (reduced operator)
+  bool p2m_tc_ok = false;                      // tensor-core P2M configured (beside the tensor-core near field)
   int *tc_fold_off = nullptr, *tc_fold = nullptr, *tc_expand = nullptr; // traceless reduction tables
   int tc_n_in = 0, tc_n_out = 0, tc_n_derived = 0;
   int4 *tc_tiles = nullptr;

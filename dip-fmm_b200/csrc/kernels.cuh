@@ -93,6 +93,49 @@ __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commi
 template <int N> __device__ __forceinline__ void cp_async_wait() {
   asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory");
 }
+
+// Monomials d^mu / mu! for every |mu| <= q, written into out[rank(mu)].
+__device__ inline void monomials(float dx, float dy, float dz, int q, float *out) {
+  float xa = 1.0F;
+  for (int a = 0; a <= q; ++a) {
+    float xb = xa;
+    for (int b = 0; a + b <= q; ++b) {
+      float xc = xb;
+      for (int c = 0; a + b + c <= q; ++c) {
+        out[rank3(a, b, c)] = xc;
+        xc = xc * dz * kInvInt[c + 1];
+      }
+      xb = xb * dy * kInvInt[b + 1];
+    }
+    xa = xa * dx * kInvInt[a + 1];
+  }
+}
+
+// The monomials of monomials() whose x-degree a belongs to part r of 4:
+// a = r, 7 - r, 8 + r, 15 - r, ... (part 0 takes a = 0, the largest group;
+// for q = 6 the parts hold 28, 22, 18 and 16 of the 84 monomials).  Four
+// threads per point share the work; each runs the serial recurrences, so the
+// values are bit-identical to monomials().  zero: store zeros instead.
+__device__ inline void monomials_part(float dx, float dy, float dz, int q, float *out, int stride, int r, bool zero) {
+  for (int a0 = 0; a0 <= q; a0 += 8) {
+    for (int h = 0; h < 2; ++h) {
+      const int a = a0 + (h == 0 ? r : 7 - r);
+      if (a > q) continue;
+      float xa = 1.0F;
+      for (int i = 0; i < a; ++i) xa = xa * dx * kInvInt[i + 1];
+      float xb = xa;
+      for (int b = 0; a + b <= q; ++b) {
+        float xc = xb;
+        for (int c = 0; a + b + c <= q; ++c) {
+          out[rank3(a, b, c) * stride] = zero ? 0.0F : xc;
+          xc = xc * dz * kInvInt[c + 1];
+        }
+        xb = xb * dy * kInvInt[b + 1];
+      }
+    }
+  }
+}
+
 #endif
 
 } // namespace cdfmm_b200

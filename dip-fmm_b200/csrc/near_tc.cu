@@ -721,13 +721,19 @@ void launch_near_tc_positions(const float4 *src_rel, const int *blk_src, int n_b
   near_tc_positions_kernel<<<(slots + 255) / 256, 256, 0, s>>>(src_rel, blk_src, slots, blk_pos);
 }
 
-void launch_near_tc(const NearTcLaunch &a, const float4 *mom, const float4 *tgt_rel, const int *self_idx, int depth,
-                    int K, bool want_phi, float4 *near, cudaStream_t s) {
-  if (a.n_work == 0 || K < kNearTcMinStates || K > kNearTcMaxStates) return;
+void launch_near_tc_pack(const NearTcLaunch &a, const float4 *mom, int K, cudaStream_t s) {
+  if (K < kNearTcMinStates || K > kNearTcMaxStates) return;
   const int N = nt_N(K);
   const long long total = static_cast<long long>(a.n_blocks + 1) * 3 * N;
   const unsigned grid = static_cast<unsigned>((total + 255) / 256);
   near_tc_pack_kernel<true><<<grid, 256, 0, s>>>(mom, a.blk_src, total, K, N, static_cast<float4 *>(a.b_ops));
+}
+
+void launch_near_tc(const NearTcLaunch &a, const float4 *mom, const float4 *tgt_rel, const int *self_idx, int depth,
+                    int K, bool want_phi, float4 *near, cudaStream_t s) {
+  if (a.n_work == 0 || K < kNearTcMinStates || K > kNearTcMaxStates) return;
+  const int N = nt_N(K);
+  if (!a.packed) launch_near_tc_pack(a, mom, K, s);
   NtArgs args{};
   args.blk_pos = a.blk_pos;
   args.blk_off = a.blk_off;

@@ -39,6 +39,7 @@ struct NearTcLaunch {
   void *b_ops;           // [(n_blocks + 1)][3][hi, lo][N][4] TF32 moments (96 N bytes per block)
   int *error_flag;
   uint32_t wait_limit;
+  bool packed;           // b_ops already holds this call's moments (launch_near_tc_pack ran)
 };
 
 // Bytes of b_ops for states up to K.
@@ -46,8 +47,10 @@ size_t near_tc_operand_bytes(int n_blocks, int K);
 // Block positions from the leaf-relative source positions.
 void launch_near_tc_positions(const float4 *src_rel, const int *blk_src, int n_blocks, float4 *blk_pos,
                               cudaStream_t s);
-// Moments (sorted, scaled; paired rows for K >= 4) -> TF32 hi / lo blocks,
-// then the near field near[nt][K] = (phi, H) / 4 pi of every target.
+// Moments (sorted, scaled; paired rows for K >= 4) -> TF32 hi / lo blocks.
+void launch_near_tc_pack(const NearTcLaunch &a, const float4 *mom, int K, cudaStream_t s);
+// The blocks (unless a.packed), then the near field near[nt][K] =
+// (phi, H) / 4 pi of every target.
 void launch_near_tc(const NearTcLaunch &a, const float4 *mom, const float4 *tgt_rel, const int *self_idx, int depth,
                     int K, bool want_phi, float4 *near, cudaStream_t s);
 bool configure_near_tc(size_t max_smem);

@@ -28,6 +28,7 @@
 #include "geometry.hpp"
 #include "kernels.cuh"
 #include "m2l_tc.hpp"
+#include "p2m_tc.hpp"
 #include "near_grad_tc.hpp"
 #include "near_tc.hpp"
 
@@ -678,6 +679,7 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
     // tensor-core near field: sm_100 devices (layout and buffers on first use)
     plan->ntc_supported = major == 10 && configure_near_tc(smem);
     plan->ngt_supported = plan->ntc_supported && configure_near_grad_tc(smem);
+    plan->p2m_tc_ok = plan->ntc_supported && configure_p2m_tc(smem);
   }
   ops.m2l_T64.reset();
   // every set-up copy, memset and kernel (legacy default stream) is complete
@@ -1126,11 +1128,17 @@ static void tune_m2l_tc(cdfmm_b200_plan *plan, int K, cudaStream_t s, size_t sme
 
 // Upward pass for K states whose sorted, scaled moments are in plan->mom:
 // P2M and M2M, leaving the multipoles in plan->M.  Returns the launch count.
-static int enqueue_upward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing) {
+// With `ntc` (the tensor-core near field's moment blocks, packed for these
+// K states) the leaf multipoles run on the tensor cores where they can.
+static int enqueue_upward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool timing,
+                          const NearTcLaunch *ntc = nullptr) {
   const int n = plan->n;
   int launches = 0;
-  launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
-             plan->p2m_chunk, s, plan->cuboid_p2m ? plan->src_size : nullptr, plan->size_step);
+  if (ntc != nullptr && plan->p2m_tc_ok && !plan->cuboid_p2m && p2m_tc_supported(n, K))
+    launch_p2m_tc(*ntc, plan->basis, plan->M, n, plan->p, K, plan->depth, s);
+  else
+    launch_p2m(plan->src_rel, plan->mom, plan->src_off, plan->basis, plan->M, n, plan->p, K, plan->depth,
+               plan->p2m_chunk, s, plan->cuboid_p2m ? plan->src_size : nullptr, plan->size_step);
   ++launches;
   if (timing) check(cudaEventRecord(plan->ev_t[2], s), "event");
   for (int level = plan->depth - 1; level >= 0; --level) {
@@ -1363,6 +1371,17 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
     launches += enqueue_upward(plan, K, s, false);
     launches += prepare_m2l(plan, K, s);
   }
+  // Tensor-core near field: its moment blocks are packed once, before the
+  // streams fork, for the near field and the tensor-core P2M (on the far
+  // stream) alike; with stage timing the pack counts as near-field time.
+  const bool near_tc = near_on_tensor_cores(plan, K);
+  if (near_tc) ensure_near_tc(plan);
+  NearTcLaunch near_tc_args = near_tc_launch(plan);
+  near_tc_args.packed = near_tc;
+  if (near_tc && !timing) {
+    launch_near_tc_pack(near_tc_args, plan->mom, K, s);
+    ++launches;
+  }
   if (!timing) {
     check(cudaEventRecord(plan->ev_fork, s), "event");
     check(cudaStreamWaitEvent(ns, plan->ev_fork, 0), "wait");
@@ -1370,14 +1389,15 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
   }
   if (timing) check(cudaEventRecord(plan->ev_t[8], ns), "event");
   if (trace) check(cudaEventRecord(plan->ev_t[kTraceP2pBegin], ns), "event");
+  if (near_tc && timing) {
+    launch_near_tc_pack(near_tc_args, plan->mom, K, ns);
+    ++launches;
+  }
   // Inside a batch graph the K = 1 near field takes the uncapped units
   // (same results bit for bit: a K = 1 target's sum does not depend on how
   // its leaf is cut into units).
   const bool wide = plan->in_batch && K == 1;
   const CorunLaunch corun_launch{2 * plan->sm_count, plan->p2p_next_unit};
-  const bool near_tc = near_on_tensor_cores(plan, K);
-  if (near_tc) ensure_near_tc(plan);
-  const NearTcLaunch near_tc_args = near_tc_launch(plan);
   launch_p2p(plan->src_rel, plan->mom, plan->src_off, plan->tgt_rel, wide ? plan->p2p_work_wide : plan->p2p_work,
              wide ? plan->n_p2p_work_wide : plan->n_p2p_work, plan->has_self ? plan->self_idx : nullptr,
              plan->leaf_self, close_geometry(plan), plan->depth, K, want_phi, plan->near, ns, 0, -1, 0, 1.0F,
@@ -1395,7 +1415,7 @@ static int enqueue_evaluation(cdfmm_b200_plan *plan, const void *moments, int dt
     launches += enqueue_downward(plan, K, fs, false, true);
   } else {
     if (trace) check(cudaEventRecord(plan->ev_t[kTraceFarBegin], fs), "event");
-    launches += enqueue_upward(plan, K, fs, timing);
+    launches += enqueue_upward(plan, K, fs, timing, near_tc ? &near_tc_args : nullptr);
     if (trace) check(cudaEventRecord(plan->ev_t[kTraceM2lBegin], fs), "event");
     launches += enqueue_downward(plan, K, fs, timing);
   }

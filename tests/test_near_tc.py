@@ -221,3 +221,30 @@ def test_tensor_core_forms_across_state_counts_and_point_sets():
         assert oracle.rel_l2(b[1], a[1]) < 2e-6, K
         assert oracle.rel_l2(b[2], a[2]) < 2e-6, K
     plan.close()
+
+
+@pytest.mark.parametrize("order,K", [(4, 8), (6, 16), (7, 64)])
+def test_tensor_core_p2m_matches_fp32_p2m(order, K):
+    """With the near field on the tensor cores its packed moment blocks also
+    feed the leaf multipoles (tensor-core P2M, orders <= 7): every node's
+    multipoles (leaves and, through M2M, every level above) agree with the
+    FP32 P2M's to TF32 hi/lo rounding, relative to the node's largest
+    coefficient, for the first and last state; the two are not bit-identical
+    (the tensor-core form ran)."""
+    rng = np.random.default_rng(200 + K)
+    n = 30000
+    x = rng.uniform(0, 1, (n, 3))
+    plan = cdfmm_b200.DevicePlan.from_points(x, order, 3, max_states=K)
+    m = torch.from_numpy(rng.normal(size=(K, n, 3)).astype(np.float32)).cuda()
+    _, _, used32 = _evaluate(plan, m, cdfmm_b200.NEAR_FP32)
+    M32 = [plan.read_expansions("multipole", k).astype(np.float64) for k in (0, K - 1)]
+    _, _, usedtc = _evaluate(plan, m, cdfmm_b200.NEAR_AUTO)
+    Mtc = [plan.read_expansions("multipole", k).astype(np.float64) for k in (0, K - 1)]
+    plan.close()
+    assert (used32, usedtc) == (0, 1)
+    for a, b in zip(M32, Mtc):
+        assert np.all(np.isfinite(b))
+        scale = np.abs(a).max(axis=1)
+        err = np.abs(a - b).max(axis=1)
+        assert np.all(err <= 1e-5 * scale + 1e-30), float((err / np.maximum(scale, 1e-30)).max())
+        assert not np.array_equal(a, b)
