@@ -47,6 +47,7 @@ constexpr uint32_t kPtACol = 64;
 constexpr int kPtSub = 8;            // sources per sub-chunk (2 blocks, 3 k-steps)
 constexpr int kPtMaxMono = 120;      // monomials of degree <= 6 (p <= 7)
 constexpr uint32_t kPtMiscBytes = 128; // barriers and flags ahead of the ring
+constexpr int kPtPosCap = 64;          // leaves of <= 64 blocks: positions staged by one bulk copy
 
 struct PtArgs {
   const float4 *blk_pos; // [(n_blocks + 1) * 4] leaf-relative positions, .w: sorted index (-1: empty)
@@ -59,11 +60,10 @@ struct PtArgs {
   uint32_t wait_limit;
 };
 
-// Bounded wait that suspends the thread until the phase completes (or about
-// 1 us passes); the iteration budget is scaled so the bound stays near the
-// polled one, and limit 0 still expires at once.
+// Bounded, polled wait (the phases a CTA waits for complete within a few
+// microseconds).
 __device__ __forceinline__ bool pt_wait(uint64_t *bar, uint32_t parity, uint32_t limit) {
-  return mbar_wait_suspend(bar, parity, limit > 32u ? limit >> 5 : limit, 1000u);
+  return mbar_wait(bar, parity, limit);
 }
 
 __global__ void __launch_bounds__(kPtThreads, 4) p2m_tc_kernel(const PtArgs a) {
@@ -81,14 +81,17 @@ __global__ void __launch_bounds__(kPtThreads, 4) p2m_tc_kernel(const PtArgs a) {
   uint32_t *tmem_slot = reinterpret_cast<uint32_t *>(mdone + 2);
   int *abort_flag = reinterpret_cast<int *>(tmem_slot + 1);
   int *last_copy = abort_flag + 1; // [2] last sub-chunk whose copies went into each slot
+  uint64_t *pfull = reinterpret_cast<uint64_t *>(smem + 48);
   uint8_t *ring = smem + kPtMiscBytes;
   float *mono = reinterpret_cast<float *>(ring + 2 * slot_bytes); // [8][kPtMaxMono]
+  float4 *spos = reinterpret_cast<float4 *>(mono + kPtSub * kPtMaxMono); // [kPtPosCap * 4] the leaf's positions
 
   const int leaf = blockIdx.x;
   const int b0 = a.blk_off[leaf];
   const int nb = a.blk_off[leaf + 1] - b0;
   const int subs = (nb + 1) / 2;
   const int q1 = a.p - 1; // monomial degree
+  const bool staged = nb > 0 && nb <= kPtPosCap;
 
   // row alpha = tid: the monomial ranks it reads per component and its sign
   int ix[3] = {-1, -1, -1};
@@ -119,9 +122,15 @@ __global__ void __launch_bounds__(kPtThreads, 4) p2m_tc_kernel(const PtArgs a) {
       mbar_init(&bfull[s], 1);
       mbar_init(&mdone[s], 1);
     }
+    mbar_init(pfull, 1);
     *abort_flag = 0;
     last_copy[0] = last_copy[1] = -1;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    if (staged) {
+      // the leaf's block positions (contiguous, 64 bytes per block)
+      mbar_expect_tx(pfull, static_cast<uint32_t>(nb) * 64u);
+      bulk_g2s(spos, a.blk_pos + 4LL * b0, static_cast<uint32_t>(nb) * 64u, pfull);
+    }
     if (subs > 0) issue_copies(0);
   }
   if (warp == 0) tmem_alloc(tmem_slot, kPtTmemCols);
@@ -143,7 +152,16 @@ __global__ void __launch_bounds__(kPtThreads, 4) p2m_tc_kernel(const PtArgs a) {
       const int q = lane >> 2;
       const int g = 2 * i + (q >> 2);
       float4 x = make_float4(0.0F, 0.0F, 0.0F, __int_as_float(-1));
-      if (g < nb) x = a.blk_pos[4LL * (b0 + g) + (q & 3)];
+      bool ok = true;
+      if (i == 0 && staged) ok = pt_wait(pfull, 0, a.wait_limit);
+      if (!__all_sync(0xffffffffu, ok)) {
+        if (lane == 0) {
+          *abort_flag = 1;
+          atomicExch(a.error_flag, 8);
+        }
+      } else if (g < nb) {
+        x = staged ? spos[4 * g + (q & 3)] : a.blk_pos[4LL * (b0 + g) + (q & 3)];
+      }
       monomials_part(x.x, x.y, x.z, q1, mono + q * kPtMaxMono, 1, lane & 3, __float_as_int(x.w) < 0);
     }
     if (tid == 0) {
@@ -209,6 +227,7 @@ __global__ void __launch_bounds__(kPtThreads, 4) p2m_tc_kernel(const PtArgs a) {
       *abort_flag = 1;
       atomicExch(a.error_flag, 8);
     }
+    if (staged) mbar_wait(pfull, 0, kTcWaitLimit); // the position copy has landed (at once unless aborted)
     if (*abort_flag != 0)
       for (int s = 0; s < 2; ++s)
         if (last_copy[s] >= issued) mbar_wait(&bfull[s], static_cast<uint32_t>(last_copy[s] >> 1) & 1u, kTcWaitLimit);
@@ -245,7 +264,8 @@ __global__ void __launch_bounds__(kPtThreads, 4) p2m_tc_kernel(const PtArgs a) {
 }
 
 size_t p2m_tc_smem(int N) {
-  const size_t pipe = 2u * 2u * 96u * static_cast<size_t>(N) + sizeof(float) * kPtSub * kPtMaxMono;
+  const size_t pipe = 2u * 2u * 96u * static_cast<size_t>(N) + sizeof(float) * kPtSub * kPtMaxMono +
+                      sizeof(float4) * 4u * kPtPosCap;
   const size_t rows = sizeof(float) * static_cast<size_t>(kPtThreads) * static_cast<size_t>(N + 1);
   return kPtMiscBytes + std::max(pipe, rows);
 }
