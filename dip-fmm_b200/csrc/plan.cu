@@ -1229,12 +1229,16 @@ static NearTcLaunch near_tc_launch(const cdfmm_b200_plan *plan) {
 
 // Near/far schedule of one evaluation (cdfmm_b200_set_schedule): the
 // co-resident schedule needs the tensor-core M2L (whose CTA fits beside two
-// co-resident near-field CTAs); other evaluations run SEPARATE.
+// co-resident near-field CTAs) and runs only on request; AUTO and every
+// other evaluation run SEPARATE.  (With the traceless M2L, a third of the
+// full-basis one, overlapping it no longer repays the co-resident near
+// field's smaller CTAs: at N = 1M, p = 6, K = 64 with the FP32 near field,
+// 43.5 ms SEPARATE against 46.7 ms CORUN.)
 static int resolved_schedule(const cdfmm_b200_plan *plan, int K) {
   // cuboid sources and the tensor-core near field: no co-resident form
   if (K <= 1 || !m2l_on_tensor_cores(plan, K) || plan->cuboid || near_on_tensor_cores(plan, K))
     return CDFMM_B200_SCHEDULE_SEPARATE;
-  return plan->schedule == CDFMM_B200_SCHEDULE_AUTO ? CDFMM_B200_SCHEDULE_CORUN : plan->schedule;
+  return plan->schedule == CDFMM_B200_SCHEDULE_CORUN ? CDFMM_B200_SCHEDULE_CORUN : CDFMM_B200_SCHEDULE_SEPARATE;
 }
 
 // Shared memory one tensor-core M2L CTA may use to sit beside two

@@ -65,7 +65,7 @@ extern "C" {
 #define CDFMM_B200_RESULTS_ON_HOST 2u
 
 /* Near/far schedule of an evaluation of K > 1 states (cdfmm_b200_set_schedule). */
-#define CDFMM_B200_SCHEDULE_AUTO 0      /* CORUN where the M2L runs on the tensor cores, else SEPARATE */
+#define CDFMM_B200_SCHEDULE_AUTO 0      /* SEPARATE (CORUN runs only on request) */
 #define CDFMM_B200_SCHEDULE_SEPARATE 1  /* full-size near-field CTAs beside a high-priority far field */
 #define CDFMM_B200_SCHEDULE_CORUN 2     /* upward pass first; then near-field CTAs sized to leave one
                                            tensor-core M2L CTA per SM, the near field at high priority */

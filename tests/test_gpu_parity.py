@@ -533,7 +533,8 @@ def test_near_far_schedules_give_the_same_field(K):
     results agree to FP32 rounding (the co-resident form sums each target's
     state blocks of 32 in another order, and the M2L may take another
     pipeline shape) and meet the FP32 bar against the FP64 oracle FMM.  The
-    concurrent trace reports each stream's interval in order.  The schedules
+    concurrent trace reports each stream's interval in order; AUTO resolves
+    to SEPARATE.  The schedules
     are those of the FP32 near field; with the tensor-core near field every
     schedule runs SEPARATE."""
     torch = pytest.importorskip("torch")
@@ -556,7 +557,7 @@ def test_near_far_schedules_give_the_same_field(K):
         plan.evaluate(m, output="both", field=H, potential=phi, synchronize=True)
         plan.set_timing(0)
         st = plan.stats()
-        expect = cdfmm_b200.SCHEDULE_CORUN if sched == cdfmm_b200.SCHEDULE_AUTO else sched
+        expect = cdfmm_b200.SCHEDULE_SEPARATE if sched == cdfmm_b200.SCHEDULE_AUTO else sched
         assert st["schedule_last"] == expect
         assert 0.0 <= st["trace_p2p_begin"] <= st["trace_p2p_end"] <= st["trace_end"]
         assert st["trace_far_begin"] <= st["trace_m2l_begin"] <= st["trace_far_end"] <= st["trace_end"]
@@ -567,7 +568,7 @@ def test_near_far_schedules_give_the_same_field(K):
     for sched, (h, p) in out.items():
         assert oracle.rel_l2(h, base_h) < 1e-6
         assert oracle.rel_l2(p, base_phi) < 1e-6
-    np.testing.assert_array_equal(out[cdfmm_b200.SCHEDULE_CORUN][0], out[cdfmm_b200.SCHEDULE_AUTO][0])
+    np.testing.assert_array_equal(out[cdfmm_b200.SCHEDULE_SEPARATE][0], out[cdfmm_b200.SCHEDULE_AUTO][0])
     ref = oracle.fmm(x, x, m[K - 1].cpu().numpy().astype(np.float64), 5, 3, identities=np.arange(n))
     h, p = out[cdfmm_b200.SCHEDULE_AUTO]
     assert oracle.rel_l2(h[K - 1], ref["H"]) < FP32_REL_L2
