@@ -7,13 +7,17 @@
 // offsets o of class c (implicit list2, see m2l_simt.cu):
 //
 //   D[(t, k), beta] += sum_alpha A_o[(t, k), alpha] * B_o[beta, alpha]
-//   A_o[(t, k), alpha] = 2^(l|alpha|) M_alpha(t - o, state k)   (exact scaling)
+//   A_o[(t, k), alpha] = 2^(l|alpha|) M'_alpha(t - o, state k)   (exact scaling)
 //   B_o[beta, alpha]   = T^(o)[beta][alpha] = D^{alpha+beta} G(o)
 //
-// with each operand split x = hi + lo in BF16 and three products
+// on the traceless-reduced operator (M2lTraceless): alpha runs over the
+// (p+1)^2 - 1 folded moments M' (alpha_z <= 1, the monopole left out) and
+// beta over the (p+1)^2 locals with beta_z <= 1, an exact sub-block of the
+// full matrix; each operand is split x = hi + lo in BF16 with three products
 // A_hi*B_hi + A_hi*B_lo + A_lo*B_hi (the dropped lo*lo term is ~2^-16 of the
-// product), then L = 2^(l(|beta|+1)) D in the epilogue (upstream math:
-// docs/math.md "M2L normalisation and cross-level reuse").
+// product), then the epilogue forms the other locals from the trace
+// relations and stores L = 2^(l(|beta|+1)) D for all n coefficients
+// (upstream math: docs/math.md "M2L normalisation and cross-level reuse").
 //
 // Data movement: a producer warp issues bulk async copies (cp.async.bulk, TMA
 // engine) of each source box's rows (contiguous, already in the canonical
