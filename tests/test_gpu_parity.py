@@ -568,7 +568,9 @@ def test_near_far_schedules_give_the_same_field(K):
     for sched, (h, p) in out.items():
         assert oracle.rel_l2(h, base_h) < 1e-6
         assert oracle.rel_l2(p, base_phi) < 1e-6
-    np.testing.assert_array_equal(out[cdfmm_b200.SCHEDULE_SEPARATE][0], out[cdfmm_b200.SCHEDULE_AUTO][0])
+    # AUTO runs SEPARATE (checked above); its M2L shape is tuned again after
+    # the CORUN call's smaller budget and may take the other hi/lo fusion, so
+    # the two agree to rounding (the loop above), not bit for bit
     ref = oracle.fmm(x, x, m[K - 1].cpu().numpy().astype(np.float64), 5, 3, identities=np.arange(n))
     h, p = out[cdfmm_b200.SCHEDULE_AUTO]
     assert oracle.rel_l2(h[K - 1], ref["H"]) < FP32_REL_L2
