@@ -53,9 +53,14 @@ void launch_unsort(const float4 *res, const int *tgt_inv, int nt, int K, unsigne
                    float *potential, cudaStream_t s, int k_begin, int k_end);
 void configure_far_kernels(size_t max_smem);
 
-// M2L, FP32 SIMT, all levels 2..depth in one launch (overwrites L there).
-void launch_m2l_simt(const float *M, float *L, const float *T, const float *scale_m,
-                     const float *scale_l, const int4 *tiles, int n_tiles, int n, int ld, int K,
+// M2L, FP32 SIMT, all levels 2..depth in one launch (overwrites L there),
+// on the traceless-reduced operator: T = [343][n_in][ld] FP32 sub-blocks
+// (rows the folded moments, columns the n_out reduced locals), fold and
+// expansion tables as built by m2l_traceless(); Mf is scratch for the
+// folded moments of levels 2..depth ([boxes][n_in][K] floats).
+void launch_m2l_simt(const float *M, float *Mf, float *L, const float *T, const float *scale_m,
+                     const float *scale_l, const int4 *tiles, int n_tiles, int n, int ld, int K, int depth,
+                     const int *fold_off, const int *fold, const int *expand, int n_in, int n_out, int n_derived,
                      cudaStream_t s);
 void configure_m2l_simt(size_t max_smem);
 int m2l_simt_beta_per_thread(int n);

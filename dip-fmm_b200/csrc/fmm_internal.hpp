@@ -207,7 +207,9 @@ struct cdfmm_b200_plan {
   int *m2m_off = nullptr, *m2m_pair = nullptr; // pair = g | (in << 16)
   int *l2l_off = nullptr, *l2l_pair = nullptr;
   float *m2m_coef = nullptr, *l2l_coef = nullptr;
-  float *m2l_T = nullptr;
+  float *m2l_T = nullptr;            // traceless FP32 sub-blocks [343][tc_n_in][m2l_ld_red] (SIMT M2L)
+  int m2l_ld_red = 0;
+  float *m2l_fold_buf = nullptr;     // [levels 2..depth boxes][tc_n_in][max_states] folded moments (SIMT M2L)
   float *scale_m = nullptr;    // [depth+1][n] 2^(level*|alpha|)   (exact)
   float *scale_l = nullptr;    // [depth+1][n] 2^(level*(|beta|+1)) (exact)
   int4 *m2l_tiles = nullptr;   // SIMT M2L work tiles (level, class, packed parent origin)

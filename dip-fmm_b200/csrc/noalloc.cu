@@ -136,7 +136,9 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   const size_t near_bytes = align256(sizeof(float4) * static_cast<size_t>(plan->nt) * K);
   const size_t pack_bytes = use_tc ? align256(static_cast<size_t>(boxes + 1) * Kp * plan->tc_Kpad * 2) : 0;
   const size_t tile_bytes = align256(sizeof(int4) * static_cast<size_t>(n_tiles));
-  const size_t need = mom_bytes + 2 * exp_bytes + near_bytes + 2 * pack_bytes + tile_bytes;
+  const size_t fold_bytes =
+      (!use_tc && plan->depth >= 2) ? align256(sizeof(float) * static_cast<size_t>(boxes) * plan->tc_n_in * K) : 0;
+  const size_t need = mom_bytes + 2 * exp_bytes + near_bytes + 2 * pack_bytes + tile_bytes + fold_bytes;
   if (need > kNoAllocScratchBytes)
     return noalloc_fail(plan, CDFMM_B200_ERR_INVALID_ARGUMENT,
                         "evaluate_noalloc needs " + std::to_string(need) + " bytes of scratch for this plan and n_states; "
@@ -162,6 +164,7 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
   void *a_hi = take(pack_bytes);
   void *a_lo = take(pack_bytes);
   int4 *dtiles = reinterpret_cast<int4 *>(take(tile_bytes));
+  float *Mf = reinterpret_cast<float *>(take(fold_bytes));
 
   cudaStream_t s = static_cast<cudaStream_t>(a->stream);
   const unsigned long long call = ++plan->call_seq;
@@ -213,8 +216,9 @@ extern "C" int cdfmm_b200_evaluate_noalloc(cdfmm_b200_plan *plan, const cdfmm_b2
     ta.wait_limit = plan->tc_wait_limit;
     launch_m2l_tc(ta, n_tiles, s);
   } else if (plan->depth >= 2) {
-    launch_m2l_simt(M, L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles, plan->n_tiles, n,
-                    plan->ops.m2l_ld, K, s);
+    launch_m2l_simt(M, Mf, L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles, plan->n_tiles, n,
+                    plan->m2l_ld_red, K, plan->depth, plan->tc_fold_off, plan->tc_fold, plan->tc_expand,
+                    plan->tc_n_in, plan->tc_n_out, plan->tc_n_derived, s);
   }
   for (int level = 3; level <= plan->depth; ++level)
     launch_l2l(L, plan->l2l_off, plan->l2l_pair, plan->l2l_coef, n, K, level, static_cast<int>(plan->ops.l2l_pair_g.size()), s);

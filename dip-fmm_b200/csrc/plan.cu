@@ -120,7 +120,7 @@ void free_plan(cdfmm_b200_plan *p) {
                   p->self_idx, p->leaf_self, p->p2p_work, p->m2m_off, p->m2m_pair, p->l2l_off, p->l2l_pair, p->m2m_coef,
                   p->l2l_coef, p->m2l_T, p->basis, p->mom, p->M, p->L, p->near, p->stage_in,
                   p->stage_out, p->scale_m, p->scale_l, p->m2l_tiles, p->tc_a_hi, p->tc_a_lo,
-                  p->tc_b, p->tc_fold_off, p->tc_fold, p->tc_expand, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
+                  p->tc_b, p->m2l_fold_buf, p->tc_fold_off, p->tc_fold, p->tc_expand, p->tc_tiles, p->error_flag, p->wbuf, p->gpart, p->stage_grad, p->p2p_next_unit,
                   p->close_targets, p->close_r_fp32, p->close_r_exact, p->src_pos64, p->tgt_pos64,
                   p->src_size, p->src_size64, p->cuboid_T, p->cuboid_base, p->ntc_blk_off, p->ntc_blk_src,
                   p->ntc_blk_pos, p->ntc_work, p->ntc_b, p->ngt_blk_off, p->ngt_blk_src, p->ngt_blk_pos,
@@ -495,9 +495,30 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
   upload(plan->scale_l, sl.data(), sl.size(), h2d);
   upload(plan->m2l_tiles, tiles.data(), tiles.size(), h2d);
   if (plan->depth >= 2) {
-    plan->m2l_T = dalloc<float>(ops.m2l_T->size(), bytes);
-    upload(plan->m2l_T, ops.m2l_T->data(), ops.m2l_T->size(), h2d);
-    plan->stats.m2l_matrix_bytes = ops.m2l_T->size() * sizeof(float);
+    // the traceless reduction (both M2L paths): fold and expansion tables,
+    // and the FP32 sub-blocks [343][n_in][ld] the SIMT M2L applies
+    const M2lTraceless red = m2l_traceless(plan->p);
+    plan->tc_n_in = static_cast<int>(red.in_set.size());
+    plan->tc_n_out = static_cast<int>(red.out_set.size());
+    plan->tc_n_derived = red.n_derived;
+    plan->tc_fold_off = dalloc<int>(red.fold_off.size(), bytes);
+    upload(plan->tc_fold_off, red.fold_off.data(), red.fold_off.size(), h2d);
+    plan->tc_fold = dalloc<int>(std::max<size_t>(red.fold.size(), 1), bytes);
+    upload(plan->tc_fold, red.fold.data(), red.fold.size(), h2d);
+    plan->tc_expand = dalloc<int>(red.expand.size(), bytes);
+    upload(plan->tc_expand, red.expand.data(), red.expand.size(), h2d);
+    plan->m2l_ld_red = 16 * m2l_simt_beta_per_thread(plan->tc_n_out);
+    const std::vector<double> &T64 = *ops.m2l_T64;
+    std::vector<float> Tr(static_cast<size_t>(343) * std::max(plan->tc_n_in, 1) * plan->m2l_ld_red, 0.0F);
+    for (size_t slot = 0; slot < 343; ++slot)
+      for (int j = 0; j < plan->tc_n_in; ++j)
+        for (int i = 0; i < plan->tc_n_out; ++i)
+          Tr[(slot * plan->tc_n_in + static_cast<size_t>(j)) * plan->m2l_ld_red + static_cast<size_t>(i)] =
+              static_cast<float>(T64[(slot * n + static_cast<size_t>(red.in_set[static_cast<size_t>(j)])) * n +
+                                     static_cast<size_t>(red.out_set[static_cast<size_t>(i)])]);
+    plan->m2l_T = dalloc<float>(Tr.size(), bytes);
+    upload(plan->m2l_T, Tr.data(), Tr.size(), h2d);
+    plan->stats.m2l_matrix_bytes = Tr.size() * sizeof(float);
   }
 
   lap(plan->stats.setup_ms_operators);
@@ -663,20 +684,16 @@ static void finish_plan(cdfmm_b200_plan *plan, int m2l_mode) {
       const std::shared_ptr<const std::vector<uint16_t>> bt = packed_b_tiles(plan->p, ops, red, Npad, Kpad);
       plan->tc_b = dalloc<uint16_t>(bt->size(), bytes);
       upload(static_cast<uint16_t *>(plan->tc_b), bt->data(), bt->size(), h2d);
-      plan->tc_n_in = static_cast<int>(red.in_set.size());
-      plan->tc_n_out = static_cast<int>(red.out_set.size());
-      plan->tc_n_derived = red.n_derived;
-      plan->tc_fold_off = dalloc<int>(red.fold_off.size(), bytes);
-      upload(plan->tc_fold_off, red.fold_off.data(), red.fold_off.size(), h2d);
-      plan->tc_fold = dalloc<int>(std::max<size_t>(red.fold.size(), 1), bytes);
-      upload(plan->tc_fold, red.fold.data(), red.fold.size(), h2d);
-      plan->tc_expand = dalloc<int>(red.expand.size(), bytes);
-      upload(plan->tc_expand, red.expand.data(), red.expand.size(), h2d);
     } else if (m2l_mode == CDFMM_B200_M2L_BF16X3) {
       throw AbiError(CDFMM_B200_ERR_RUNTIME,
                      "split-BF16 tensor-core M2L needs an sm_100 device and depth >= 2");
     }
     // tensor-core near field: sm_100 devices (layout and buffers on first use)
+    // folded moments of the SIMT M2L, for plans that can take that path
+    if (plan->depth >= 2 && (!plan->tc_supported || plan->max_states > 128))
+      plan->m2l_fold_buf = dalloc<float>(static_cast<size_t>(plan->n_nodes - level_offset(2)) *
+                                             static_cast<size_t>(std::max(plan->tc_n_in, 1)) * plan->max_states,
+                                         bytes);
     plan->ntc_supported = major == 10 && configure_near_tc(smem);
     plan->ngt_supported = plan->ntc_supported && configure_near_grad_tc(smem);
     plan->p2m_tc_ok = plan->ntc_supported && configure_p2m_tc(smem);
@@ -1317,8 +1334,9 @@ static int enqueue_downward(cdfmm_b200_plan *plan, int K, cudaStream_t s, bool t
       plan->stats.m2l_tc_stages = plan->tc_stages;
       plan->stats.m2l_tc_fused = plan->tc_fuse;
     } else if (plan->depth >= 2) {
-      launch_m2l_simt(plan->M, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l, plan->m2l_tiles,
-                      plan->n_tiles, n, plan->ops.m2l_ld, K, s);
+      launch_m2l_simt(plan->M, plan->m2l_fold_buf, plan->L, plan->m2l_T, plan->scale_m, plan->scale_l,
+                      plan->m2l_tiles, plan->n_tiles, n, plan->m2l_ld_red, K, plan->depth, plan->tc_fold_off,
+                      plan->tc_fold, plan->tc_expand, plan->tc_n_in, plan->tc_n_out, plan->tc_n_derived, s);
       ++launches;
     }
     plan->last_m2l_tc = use_tc;
