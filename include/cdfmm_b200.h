@@ -50,7 +50,9 @@ extern "C" {
 
 /* M2L arithmetic. */
 #define CDFMM_B200_M2L_AUTO 0        /* split-BF16 tensor cores on sm_100, depth >= 2, order <= 9 (any K), else FP32 */
-#define CDFMM_B200_M2L_FP32 1        /* FP32 SIMT (the plain per-state path) */
+#define CDFMM_B200_M2L_FP32 1        /* FP32 SIMT (the plain per-state path), on the same traceless-reduced
+                                        operator; plans that can take this path keep a folded-moment buffer
+                                        of (levels 2..depth boxes) x (p+1)^2 x max_states floats */
 #define CDFMM_B200_M2L_BF16X3 2      /* tcgen05, BF16 hi/lo with three products, FP32 accumulate; applies the
                                         traceless-reduced operator ((p+1)^2 - 1 folded moments in, (p+1)^2
                                         locals out, the rest from the trace relations); any order */
