@@ -2252,6 +2252,40 @@ int cdfmm_b200_m2l_stencil(int32_t order, double *out, size_t out_count, int32_t
   }
 }
 
+int cdfmm_b200_m2l_traceless(int32_t order, int32_t *counts, int32_t *in_ranks, int32_t *out_ranks,
+                             int32_t *fold_offsets, int32_t *fold_ranks, int32_t *fold_coefficients,
+                             int32_t *derived) {
+  try {
+    require(order >= 0 && order <= kMaxOrder, "order must be in [0, 10]");
+    require(counts != nullptr, "counts is NULL");
+    const M2lTraceless t = m2l_traceless(order);
+    const int n_out = static_cast<int>(t.out_set.size());
+    counts[0] = static_cast<int32_t>(t.in_set.size());
+    counts[1] = n_out;
+    counts[2] = static_cast<int32_t>(t.fold.size());
+    counts[3] = t.n_derived;
+    if (in_ranks != nullptr) std::copy(t.in_set.begin(), t.in_set.end(), in_ranks);
+    if (out_ranks != nullptr) std::copy(t.out_set.begin(), t.out_set.end(), out_ranks);
+    if (fold_offsets != nullptr) std::copy(t.fold_off.begin(), t.fold_off.end(), fold_offsets);
+    for (size_t f = 0; f < t.fold.size(); ++f) {
+      if (fold_ranks != nullptr) fold_ranks[f] = t.fold[f] & 0xffff;
+      if (fold_coefficients != nullptr) fold_coefficients[f] = (t.fold[f] >> 16) - 64;
+    }
+    if (derived != nullptr)
+      for (int i = 0; i < t.n_derived; ++i) {
+        const int e = t.expand[static_cast<size_t>(n_out + i)];
+        derived[3 * i] = e & 1023;
+        derived[3 * i + 1] = (e >> 10) & 1023;
+        derived[3 * i + 2] = e >> 20;
+      }
+    return CDFMM_B200_OK;
+  } catch (const AbiError &e) {
+    return fail(nullptr, e.code, e.what());
+  } catch (const std::exception &e) {
+    return fail(nullptr, CDFMM_B200_ERR_RUNTIME, e.what());
+  }
+}
+
 const char *cdfmm_b200_last_error(const cdfmm_b200_plan *plan) {
   if (plan != nullptr) return plan->last_error.c_str();
   return g_last_error.c_str();

@@ -47,7 +47,7 @@ EXPORTED = (
     "cdfmm_b200_selftest_bounded_wait", "cdfmm_b200_m2l_shapes", "cdfmm_b200_set_m2l_shape",
     "cdfmm_b200_poll_status", "cdfmm_b200_set_wait_limit", "cdfmm_b200_set_schedule", "cdfmm_b200_batch_groups",
     "cdfmm_b200_plan_create_from_points", "cdfmm_b200_plan_tree", "cdfmm_b200_m2l_stencil",
-    "cdfmm_b200_set_source_cuboids", "cdfmm_b200_set_near_mode",
+    "cdfmm_b200_set_source_cuboids", "cdfmm_b200_set_near_mode", "cdfmm_b200_m2l_traceless",
 )
 
 ROOT_CENTRE, ROOT_HALF_WIDTH = 1, 2
@@ -151,6 +151,7 @@ def library() -> ctypes.CDLL:
     lib.cdfmm_b200_plan_create_from_points.argtypes = [ctypes.POINTER(PointsDesc), ctypes.POINTER(vp)]
     lib.cdfmm_b200_plan_tree.argtypes = [vp, vp, vp, vp, vp, vp, vp, vp]
     lib.cdfmm_b200_m2l_stencil.argtypes = [i32, vp, u64, ctypes.POINTER(i32)]
+    lib.cdfmm_b200_m2l_traceless.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp]
     lib.cdfmm_b200_set_source_cuboids.argtypes = [vp, vp, i32, i32]
     lib.cdfmm_b200_plan_destroy.argtypes = [vp]
     lib.cdfmm_b200_plan_destroy.restype = None
@@ -225,6 +226,27 @@ def m2l_stencil(order: int):
     src = ctypes.c_int32(-1)
     _check(library().cdfmm_b200_m2l_stencil(order, _ptr(out), out.size, ctypes.byref(src)))
     return out, src.value
+
+
+def m2l_traceless(order: int) -> dict:
+    """The traceless reduction the M2L applies at `order`
+    (cdfmm_b200_m2l_traceless): full ranks of the folded moments ("in") and
+    of the computed locals ("out"), the fold as CSR ("fold_offsets",
+    "fold_ranks", "fold_coefficients") and the derived locals as rows
+    (d, s1, s2) with L_d = -(L_s1 + L_s2), in evaluation order."""
+    counts = np.zeros(4, dtype=np.int32)
+    _check(library().cdfmm_b200_m2l_traceless(order, _ptr(counts), None, None, None, None, None, None))
+    n_in, n_out, nnz, nd = (int(c) for c in counts)
+    out = {"in": np.zeros(n_in, np.int32), "out": np.zeros(n_out, np.int32),
+           "fold_offsets": np.zeros(n_in + 1, np.int32), "fold_ranks": np.zeros(max(nnz, 1), np.int32),
+           "fold_coefficients": np.zeros(max(nnz, 1), np.int32), "derived": np.zeros((max(nd, 1), 3), np.int32)}
+    _check(library().cdfmm_b200_m2l_traceless(order, _ptr(counts), _ptr(out["in"]), _ptr(out["out"]),
+                                              _ptr(out["fold_offsets"]), _ptr(out["fold_ranks"]),
+                                              _ptr(out["fold_coefficients"]), _ptr(out["derived"])))
+    out["fold_ranks"] = out["fold_ranks"][:nnz]
+    out["fold_coefficients"] = out["fold_coefficients"][:nnz]
+    out["derived"] = out["derived"][:nd]
+    return out
 
 
 def direct_fp64(sources, moments, targets, self_indices=None, device=0):

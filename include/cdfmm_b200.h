@@ -457,6 +457,19 @@ int cdfmm_b200_m2l_matrix(int32_t order, const double *R, double *out, size_t ou
  * cache, 2 read from the directory.  Host only. */
 int cdfmm_b200_m2l_stencil(int32_t order, double *out, size_t out_count, int32_t *source);
 
+/* The traceless reduction both M2L paths apply at `order` (no counterpart in
+ * the reference, which applies the full basis): counts[4] = {n_in, n_out,
+ * fold entries, derived locals}; with non-NULL arrays (sized from a first
+ * call with NULLs) also in_ranks[n_in] (full ranks of the folded moments),
+ * out_ranks[n_out] (of the computed locals), fold_offsets[n_in + 1],
+ * fold_ranks / fold_coefficients[fold entries] (folded moment j =
+ * sum over its entries of coefficient x M[rank]) and derived[3 x derived
+ * locals] (rank d, s1, s2: L_d = -(L_s1 + L_s2), in evaluation order).
+ * Host only. */
+int cdfmm_b200_m2l_traceless(int32_t order, int32_t *counts, int32_t *in_ranks, int32_t *out_ranks,
+                             int32_t *fold_offsets, int32_t *fold_ranks, int32_t *fold_coefficients,
+                             int32_t *derived);
+
 /* Message of the last failure on this plan (or of the last failure of a call
  * without a plan, on this thread, when plan is NULL).  Never NULL. */
 const char *cdfmm_b200_last_error(const cdfmm_b200_plan *plan);

@@ -86,3 +86,49 @@ def test_derivative_tensors_are_traceless():
             if a + b + c + 2 <= p:
                 s = row[rank(a + 2, b, c)] + row[rank(a, b + 2, c)] + row[rank(a, b, c + 2)]
                 assert abs(s) <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("p", [0, 1, 3, 6, 8, 10])
+def test_library_tables_match_the_restatement(p):
+    """The tables the device kernels use (cdfmm_b200_m2l_traceless) against
+    this file's restatement: the same input and output sets, each folded
+    moment the same signed sum (its own rank first, coefficient 1), and the
+    derived locals in an order where both sources come first; applied to
+    the library's FP64 operators they reproduce the full product."""
+    t = cdfmm_b200.m2l_traceless(p)
+    B = basis(p)
+    n = len(B)
+    ins = [i for i, e in enumerate(B) if e[2] <= 1 and i > 0]
+    outs = [i for i, e in enumerate(B) if e[2] <= 1]
+    assert list(t["in"]) == ins and list(t["out"]) == outs
+    # fold: column j of the CSR equals the restated fold of every moment
+    F = np.zeros((len(ins), n))
+    for j in range(len(ins)):
+        lo, hi = t["fold_offsets"][j], t["fold_offsets"][j + 1]
+        assert t["fold_ranks"][lo] == ins[j] and t["fold_coefficients"][lo] == 1
+        for r, c in zip(t["fold_ranks"][lo:hi], t["fold_coefficients"][lo:hi]):
+            F[j, r] += c
+    for a in range(1, n):
+        e = np.zeros(n)
+        e[a] = 1.0
+        np.testing.assert_array_equal(F[:, a], fold(e, B, p)[ins])
+    # derived locals: sources computed before use, z lowered by two
+    known = set(outs)
+    for d, s1, s2 in t["derived"]:
+        assert s1 in known and s2 in known and d not in known
+        a, b, c = B[d]
+        assert (s1, s2) == (rank(a + 2, b, c - 2), rank(a, b + 2, c - 2))
+        known.add(int(d))
+    assert known == set(range(n))
+    if p >= 2:
+        T, _ = cdfmm_b200.m2l_stencil(p)
+        rng = np.random.default_rng(10 + p)
+        slot = 1 * 49 + 5 * 7 + 3
+        M = rng.normal(size=n)
+        M[0] = 0.0
+        L = np.zeros(n)
+        L[outs] = T[slot][np.ix_(ins, outs)].T @ (F @ M)
+        for d, s1, s2 in t["derived"]:
+            L[d] = -(L[s1] + L[s2])
+        full = T[slot].T @ M
+        assert np.abs(L - full).max() <= 1e-12 * np.abs(full).max()
