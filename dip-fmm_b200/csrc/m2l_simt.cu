@@ -107,10 +107,10 @@ __global__ void __launch_bounds__(128) m2l_simt_kernel(const float *__restrict__
           __syncthreads();
           // matrix rows a0 .. a0+an-1, betas 0 .. BW-1 (ld >= BW, 16-byte rows)
           for (int q = threadIdx.x; q < an * (BW / 4); q += blockDim.x) {
-            const int r = q / (BW / 4);
-            const int c4 = q - r * (BW / 4);
-            reinterpret_cast<float4 *>(sT + r * BW)[c4] =
-                reinterpret_cast<const float4 *>(Ts + static_cast<long long>(a0 + r) * ld)[c4];
+            const int row = q / (BW / 4);
+            const int c4 = q - row * (BW / 4);
+            reinterpret_cast<float4 *>(sT + row * BW)[c4] =
+                reinterpret_cast<const float4 *>(Ts + static_cast<long long>(a0 + row) * ld)[c4];
           }
           for (int q = threadIdx.x; q < kTileTargets * kAlphaChunk; q += blockDim.x) {
             const int u = q / kAlphaChunk;
@@ -190,12 +190,12 @@ __global__ void __launch_bounds__(128) fold_moments_kernel(const float *__restri
 }
 
 template <int J>
-void launch_j(const float *M, float *L, const float *T, const float *sm, const float *sl,
+void launch_j(const float *Mf, float *L, const float *T, const float *sm, const float *sl,
               const int4 *tiles, int n_tiles, int n, int ld, int K, const SimtReduction &r, cudaStream_t s) {
   const size_t smem = sizeof(float) * std::max<size_t>(kAlphaChunk * 16 * J + kTileTargets * (kAlphaChunk + 1),
                                                        static_cast<size_t>(kTileTargets) * (n + 1));
   dim3 grid(n_tiles, K);
-  m2l_simt_kernel<J><<<grid, 128, smem, s>>>(M, L, T, sm, sl, tiles, n, ld, K, level_offset_d(2), r);
+  m2l_simt_kernel<J><<<grid, 128, smem, s>>>(Mf, L, T, sm, sl, tiles, n, ld, K, level_offset_d(2), r);
 }
 
 } // namespace
@@ -221,18 +221,18 @@ void launch_m2l_simt(const float *M, float *Mf, float *L, const float *T, const 
   const int node_base = level_offset_d(2);
   fold_moments_kernel<<<level_offset_d(depth + 1) - node_base, 128, 0, s>>>(M, scale_m, fold_off, fold, n, n_in, K,
                                                                            depth, node_base, Mf);
-  M = Mf; // the main kernel reads the folded moments
+  // the main kernel reads the folded moments
   const SimtReduction r{fold_off, fold, expand, n_in, n_out, n_derived};
   switch (m2l_simt_beta_per_thread(n_out)) {
-  case 1: launch_j<1>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  case 2: launch_j<2>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  case 3: launch_j<3>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  case 4: launch_j<4>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  case 6: launch_j<6>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  case 8: launch_j<8>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  case 11: launch_j<11>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  case 14: launch_j<14>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
-  default: launch_j<18>(M, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 1: launch_j<1>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 2: launch_j<2>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 3: launch_j<3>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 4: launch_j<4>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 6: launch_j<6>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 8: launch_j<8>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 11: launch_j<11>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  case 14: launch_j<14>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
+  default: launch_j<18>(Mf, L, T, scale_m, scale_l, tiles, n_tiles, n, ld, K, r, s); break;
   }
 }
 
